@@ -1,0 +1,255 @@
+/*
+ * skm_gpu.h -- C-ABI of the B200-native evaluation path of Sparse Kernel Machine
+ * (SKM) image registration.
+ *
+ * The entry points replace the member functions of the reference's
+ * `class GpuKernelEvaluator` (include/cuda/GpuEvaluator.h:69-179) one for one, plus
+ * the host-side code that sits directly on top of it in the ITK glue
+ * (regularizers L1/L2/L2,1 and the sign flip of
+ * include/itkRegularizedImageToImageMetricv4.hxx:431-538, and the adaptive-step
+ * optimizer of include/itkAdaptiveStepGradientDescentOptimizerv4.hxx:53-128).
+ *
+ * Conventions shared by every call
+ *  - Plain pointers and sizes; no C++ or torch types cross this boundary.
+ *  - Host buffers are borrowed for the duration of the call only (as in the
+ *    reference, which copies them with cudaMemcpy on every call).
+ *  - ScalarType is double (the reference default, SinglePrecisionType=0,
+ *    include/CommonConfig.h:21-27).  Vector-valued images (control points,
+ *    displacement fields) are arrays of structures: D doubles per texel.
+ *  - Linear texel index is x-fastest: x + X*(y + Y*z) (include/cuda/ImageBase.h:40-49).
+ *  - Parameters/derivatives are planar: value of axis d of control point i is at
+ *    [d*C + i] (include/itkTransformAdapter.hxx:202-236).
+ *  - Every call returns SKM_OK (0) or an error code; skm_last_error() returns the
+ *    message of the last failure on the calling thread.  The reference instead
+ *    prints and calls std::exit(-1) on CUDA errors (include/cuda/CudaUtils.h:25-31)
+ *    and validates arguments in the ITK glue with itkExceptionMacro; both become
+ *    return codes here.
+ *  - All work runs on one CUDA stream owned by the evaluator, on the device that
+ *    was current when the evaluator was created.  Calls return after the device
+ *    work finished (the reference is synchronous too).
+ *  - There is no CPU fallback: without a usable CUDA device every call that needs
+ *    one fails with SKM_ERR_CUDA.
+ */
+#ifndef SKM_GPU_H
+#define SKM_GPU_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SKM_ABI_VERSION 1
+
+/* Status codes. */
+#define SKM_OK              0
+#define SKM_ERR_INVALID     1   /* argument rejected (reference: itkExceptionMacro) */
+#define SKM_ERR_CUDA        2   /* CUDA runtime failure (reference: cudaCheck -> exit) */
+#define SKM_ERR_UNSUPPORTED 3
+#define SKM_ERR_NOMEM       4
+#define SKM_ERR_STATE       5   /* call out of order (e.g. no evaluator) */
+#define SKM_ERR_TIMEOUT     6   /* a bounded device-side wait gave up */
+
+/* GpuKernelEvaluator::MEASURE (include/cuda/GpuEvaluator.h:160). */
+#define SKM_MSE 0
+#define SKM_NCC 1
+#define SKM_LCC 2
+
+/* ImageBase geometry (include/cuda/ImageBase.h:40-49): physical point of index i is
+ * origin + spacing*i, no direction matrix.  For 2-D images entries [2] are ignored. */
+typedef struct skm_geometry {
+    double  origin[3];
+    double  spacing[3];
+    int32_t size[3];
+} skm_geometry;
+
+/* ImageNearest<VecF,D> used as the displacement field of earlier scale levels
+ * (include/cuda/ImageNearest.h, GpuEvaluator.cu:120-126).  data == NULL means
+ * "no field".  The device copy is cached by host pointer identity, exactly like
+ * the reference (GpuEvaluator.cu:120-126): pass a different pointer to refresh it. */
+typedef struct skm_field {
+    const double *data;        /* D doubles per texel, AoS */
+    skm_geometry  geometry;
+} skm_field;
+
+/* Constructor arguments of GpuKernelEvaluator (GpuEvaluator.h:147-154) together
+ * with those of the kernel GKernel<float> (include/cuda/Kernel.h:134-146). */
+typedef struct skm_evaluator_desc {
+    int32_t dimensions;              /* 2 or 3 (reference: SpaceDimensions macro) */
+    int32_t num_parameters;          /* C*D, C = number of control points */
+    int32_t subsample;               /* fixed-grid subsampling rate, 1..100 */
+    int32_t subsample_neighborhood;  /* LCC neighbourhood stride, 1..100 */
+
+    /* kernel (Kernel.h:134-146) */
+    double  sigma_c0;
+    double  sigma_c4;
+    int32_t use_weight_image;        /* non-stationary kernel from a sigma image */
+    double  maximum_weight;          /* largest value of the weight image (or tilt) */
+    const double *weight_image;      /* 1 double per texel, or NULL */
+    skm_geometry  weight_image_geometry;
+    int32_t use_weight_tensor;       /* anisotropic kernel from a covariance image */
+    double  maximum_eigenvalue_covariance[9];  /* row-major DxD */
+    const double *weight_tensor;     /* D*D doubles per texel, row-major, or NULL */
+    skm_geometry  weight_tensor_geometry;
+
+    /* moving image: cubic B-spline interpolation coefficients as produced by
+     * BsplineImage::computeCoeffs (BsplineImage.h:209-221): (size+3) texels per
+     * axis with a one-texel mirror offset.  moving_geometry.size is the size of
+     * the image itself (the BsplineImage constructor adds the 3). */
+    const double *moving_coefficients;
+    skm_geometry  moving_geometry;
+
+    /* fixed image, 1 double per texel */
+    const double *fixed_image;
+    skm_geometry  fixed_geometry;
+
+    /* control-point grid and control-point weight grid (geometry only) */
+    skm_geometry  cp_geometry;
+    skm_geometry  cpw_geometry;
+} skm_evaluator_desc;
+
+/* GpuKernelEvaluator::EvaluationResult (GpuEvaluator.h:138-145).  Regularizer
+ * values are unweighted, as in the reference. */
+typedef struct skm_result {
+    double   measure;
+    double   reg_value_rkhs;
+    double   reg_value_rd;
+    double   reg_value_pg;
+    uint32_t num_pixels_counted;
+} skm_result;
+
+typedef struct skm_evaluator skm_evaluator;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *skm_last_error(void);
+int32_t     skm_abi_version(void);
+
+/* GpuKernelEvaluator::GpuKernelEvaluator (GpuEvaluator.h:147-154, GpuEvaluator.cu:30-91).
+ * Copies the images to device memory; all host pointers in desc are borrowed. */
+int skm_evaluator_create(const skm_evaluator_desc *desc, skm_evaluator **out);
+int skm_evaluator_destroy(skm_evaluator *ev);
+
+/* GpuKernelEvaluator::SetRegularizerRKHS/RD/PG (GpuEvaluator.h:156-158,
+ * GpuEvaluator.cu:786-831).  weight <= 0 switches the term off. */
+int skm_set_regularizer_rkhs(skm_evaluator *ev, double weight);
+int skm_set_regularizer_rd  (skm_evaluator *ev, double weight, double scaling);
+int skm_set_regularizer_pg  (skm_evaluator *ev, double weight, double scaling);
+
+/* GpuKernelEvaluator::getValue (GpuEvaluator.h:162-166, GpuEvaluator.cu:94-357).
+ * cp: C*D doubles (AoS), cpw: C doubles, df: previous-level field or NULL. */
+int skm_get_value(skm_evaluator *ev, int32_t metric,
+                  const double *cp, const double *cpw, const skm_field *df,
+                  int32_t do_resampling, skm_result *out);
+
+/* GpuKernelEvaluator::getValueAndDerivative (GpuEvaluator.h:168-173,
+ * GpuEvaluator.cu:361-714).  derivatives: caller-allocated, C*D doubles, planar;
+ * on return it holds the metric derivative plus the weighted RKHS/RD/PG
+ * gradients, exactly what the reference writes there. */
+int skm_get_value_and_derivative(skm_evaluator *ev, int32_t metric,
+                                 const double *cp, const double *cpw, const skm_field *df,
+                                 double *derivatives, int32_t do_resampling,
+                                 skm_result *out);
+
+/* GpuKernelEvaluator::evaluateDisplacementField (GpuEvaluator.h:175-178,
+ * GpuEvaluator.cu:716-784): dst gets D doubles per fixed-image texel. */
+int skm_evaluate_displacement_field(skm_evaluator *ev,
+                                    const double *cp, const double *cpw, const skm_field *df,
+                                    double *dst);
+
+/* ------------------------------------------------------------------------- */
+/* Metric level: RegularizedImageToImageMetricv4::GetValue/GetValueAndDerivative
+ * (include/itkRegularizedImageToImageMetricv4.hxx:148-213, 316-573).  Adds the
+ * L1, L2,1 and L2 terms (hxx:431-526), the sign flip (hxx:528-529) and the
+ * weighted sum of all terms (hxx:531-538) on the device. */
+typedef struct skm_metric_desc {
+    int32_t metric;            /* SKM_MSE / SKM_NCC / SKM_LCC */
+    double  reg_l1;
+    double  reg_l21;
+    double  reg_l2;
+    double  reg_rkhs;
+    double  reg_rd;
+    double  reg_rd_scaling;
+    double  reg_pg;
+    double  reg_pg_scaling;
+    int32_t use_negative_gradient;   /* reference default: on (hxx:47) */
+    int32_t do_resampling;           /* reference default: on (hxx:46) */
+} skm_metric_desc;
+
+/* The callback tuple of the reference metric (hxx:558-569) plus the total. */
+typedef struct skm_metric_values {
+    double   value;        /* measure + weighted sum of all regularizers */
+    double   measure;
+    double   reg_value;    /* weighted sum of all regularizers */
+    double   reg_l1;
+    double   reg_l21;
+    double   reg_l2;
+    double   reg_rkhs;
+    double   reg_rd;
+    double   reg_pg;
+    uint32_t num_pixels_counted;
+} skm_metric_values;
+
+/* parameters/derivative: planar C*D doubles.  derivative may be NULL (value only). */
+int skm_metric_evaluate(skm_evaluator *ev, const skm_metric_desc *metric,
+                        const double *parameters, const double *cpw, const skm_field *df,
+                        double *derivative, skm_metric_values *out);
+
+/* ------------------------------------------------------------------------- */
+/* Device-resident optimizer: AdaptiveStepGradientDescentOptimizerv4 over
+ * StandardGradientDescentOptimizerv4 (include/itkAdaptiveStepGradientDescentOptimizerv4.hxx:53-128,
+ * include/itkStandardGradientDescentOptimizerv4.hxx:83-166) driven by the ITK v4
+ * gradient-descent loop (previous position, evaluate, step, keep best).  Parameters,
+ * gradients and optimizer state stay in device memory; one iteration is one
+ * metric evaluation plus one update, replayed from a CUDA graph. */
+typedef struct skm_optimizer_desc {
+    double  a;                  /* initial step size */
+    double  A;                  /* reference: 20 (SKMReg.cxx:400) */
+    double  alpha;              /* reference: 1 */
+    double  f_max;              /* reference: 1e7 */
+    double  f_min;              /* reference: -1e6 */
+    double  omega;              /* reference: 1 */
+    int32_t orthant_projection;
+    int32_t number_of_iterations;
+    int32_t return_best_parameters_and_value;
+} skm_optimizer_desc;
+
+typedef struct skm_optimizer_state {
+    int32_t  iteration;        /* iterations done */
+    double   current_time;     /* adaptive time t */
+    double   learning_rate;    /* last step size */
+    double   value;            /* metric value of the last evaluation */
+    double   best_value;
+    double   scalar_product;   /* <g, g_prev> of the last step */
+    uint32_t num_pixels_counted;
+} skm_optimizer_state;
+
+typedef struct skm_optimizer skm_optimizer;
+
+int skm_optimizer_create(skm_evaluator *ev, const skm_optimizer_desc *opt,
+                         const skm_metric_desc *metric,
+                         const double *initial_parameters, const double *cpw,
+                         const skm_field *df, skm_optimizer **out);
+/* Runs up to `iterations` more iterations (never past number_of_iterations). */
+int skm_optimizer_run(skm_optimizer *o, int32_t iterations);
+/* Enqueue up to `iterations` more iterations on the evaluator's stream without waiting;
+ * if stream_out is not NULL it receives that cudaStream_t (for event timing). */
+int skm_optimizer_enqueue(skm_optimizer *o, int32_t iterations, void *stream_out);
+/* Current position, or the best one if best != 0 (ReturnBestParametersAndValue). */
+int skm_optimizer_get_parameters(skm_optimizer *o, int32_t best, double *parameters);
+int skm_optimizer_get_state(skm_optimizer *o, skm_optimizer_state *out);
+int skm_optimizer_destroy(skm_optimizer *o);
+
+/* ------------------------------------------------------------------------- */
+/* BsplineImage::computeCoeffs (include/cuda/BsplineImage.h:37-108,174-221) on
+ * the GPU: cubic B-spline prefilter (pole sqrt(3)-2, mirror boundaries) followed
+ * by the one-texel mirror padding.  image: prod(size) doubles; coefficients:
+ * prod(size+3) doubles. */
+int skm_bspline_coefficients(int32_t dimensions, const int32_t *size,
+                             const double *image, double *coefficients);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SKM_GPU_H */

@@ -1,0 +1,747 @@
+// skm_capi.cu -- the evaluator object behind the C-ABI of include/skm_gpu.h.
+//
+// One evaluator owns every device buffer it needs (allocated once at creation, like
+// GpuKernelEvaluator's constructor, GpuEvaluator.cu:30-91), one CUDA stream and pinned
+// host staging buffers.  A call uploads the parameters, runs the launch sequence
+//   [pack] -> [grid shifts] -> value pass -> statistics -> derivative+regularizers -> result
+// on the stream and copies the scalars and the derivative back.  Every reduction is
+// done on the device in a fixed order; no host loops over per-voxel arrays remain.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/skm_gpu.h"
+#include "skm_device.cuh"
+#include "skm_kernels.cuh"
+#include "skm_prefilter.cuh"
+#include "skm_table.cuh"
+
+using namespace skm;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define SKM_CUDA(call)                                                                                 \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return fail(SKM_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,    \
+                                           cudaGetErrorString(e_));                                    \
+    } while (0)
+
+#define SKM_CHECK_LAUNCH() SKM_CUDA(cudaPeekAtLastError())
+
+template <typename T>
+int dalloc(T **p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) n = 1;
+    SKM_CUDA(cudaMalloc((void **)p, n * sizeof(T)));
+    return SKM_OK;
+}
+
+Geo make_geo(const skm_geometry &g, int D, int pad)
+{
+    Geo r;
+    for (int d = 0; d < 3; ++d) {
+        if (d < D) {
+            r.o[d] = g.origin[d];
+            r.s[d] = g.spacing[d];
+            r.inv[d] = 1.0 / g.spacing[d];
+            r.n[d] = g.size[d] + pad;
+        } else {
+            r.o[d] = 0.0; r.s[d] = 1.0; r.inv[d] = 1.0; r.n[d] = 1;
+        }
+    }
+    r.st[0] = 1;
+    r.st[1] = r.n[0];
+    r.st[2] = (long long)r.n[0] * r.n[1];
+    return r;
+}
+
+long long texels(const skm_geometry &g, int D)
+{
+    long long n = 1;
+    for (int d = 0; d < D; ++d) n *= g.size[d];
+    return n;
+}
+
+bool geometry_ok(const skm_geometry &g, int D)
+{
+    for (int d = 0; d < D; ++d)
+        if (g.size[d] < 1 || !(g.spacing[d] > 0.0)) return false;
+    return true;
+}
+
+void rng_jump_table(RngJump &J)
+{
+    unsigned long long m = 6364136223846793005ULL, a = 1ULL;   // PCG32 multiplier, increment (seq|1)
+    for (int i = 0; i < 64; ++i) {
+        J.mul[i] = m;
+        J.add[i] = a;
+        a = a * (m + 1ULL);
+        m = m * m;
+    }
+}
+
+unsigned long long rng_advance_host(unsigned long long s, unsigned long long steps, const RngJump &J)
+{
+    int i = 0;
+    while (steps) {
+        if (steps & 1ULL) s = s * J.mul[i] + J.add[i];
+        steps >>= 1;
+        ++i;
+    }
+    return s;
+}
+
+constexpr int kValueThreads = 256;
+constexpr int kDerivThreads = 256;     // 8 warps = 8 control points per block
+
+}  // namespace
+
+struct skm_evaluator {
+    int device = 0;
+    int D = 3;
+    cudaStream_t stream = nullptr;
+    EvalParams P{};
+    skm_geometry fixed_geo{}, cp_geo{};
+    int nparams = 0;
+    long long N = 0, Ns = 0, C = 0;
+    int value_blocks = 0, deriv_blocks = 0, dense_blocks = 0;
+
+    // device memory
+    float *d_fixed = nullptr, *d_coeffs = nullptr, *d_wimg = nullptr, *d_wten = nullptr;
+    float4 *d_cpd = nullptr, *d_df = nullptr, *d_samp = nullptr, *d_dense = nullptr, *d_dense_sw = nullptr;
+    unsigned char *d_dense_in = nullptr, *d_dense_sw_in = nullptr;
+    uint32_t *d_shifts = nullptr;
+    double *d_in = nullptr;          // uploaded parameters (AoS or planar) followed by weights
+    double *d_part = nullptr, *d_stats = nullptr, *d_deriv = nullptr, *d_rpart = nullptr, *d_out = nullptr;
+    long long df_texels = 0;
+
+    // pinned host staging
+    double *h_in = nullptr, *h_out = nullptr;
+
+    // phase-table fast path (stationary kernel, integral spacing ratio)
+    TablePlan table{};
+
+    // state of GpuKernelEvaluator
+    double reg_rkhs = 0, reg_rd = 0, rd_scaling = 1, reg_pg = 0, pg_scaling = 1;
+    unsigned long long rng_state = 0xBA5EBA11DEADBEEFULL;
+    bool evaluated_once = false;
+    const double *df_key = nullptr;
+    RngJump jump{};
+    bool use_table = true;
+
+    ~skm_evaluator()
+    {
+        if (device >= 0) cudaSetDevice(device);
+        void *bufs[] = {d_fixed, d_coeffs, d_wimg, d_wten, d_cpd, d_df, d_samp, d_dense, d_dense_sw, d_dense_in,
+                        d_dense_sw_in, d_shifts, d_in, d_part, d_stats, d_deriv, d_rpart, d_out};
+        for (void *b : bufs)
+            if (b) cudaFree(b);
+        table_free(table);
+        if (h_in) cudaFreeHost(h_in);
+        if (h_out) cudaFreeHost(h_out);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+// ------------------------------------------------------------------------------------------------
+// dispatch over dimension and kernel kind
+template <template <int, int> class F, typename... A>
+static int dispatch(int D, int kind, A &&...a)
+{
+    if (D == 3) {
+        if (kind == kStationary) return F<3, kStationary>::run(a...);
+        if (kind == kWeightImage) return F<3, kWeightImage>::run(a...);
+        return F<3, kWeightTensor>::run(a...);
+    }
+    if (kind == kStationary) return F<2, kStationary>::run(a...);
+    if (kind == kWeightImage) return F<2, kWeightImage>::run(a...);
+    return F<2, kWeightTensor>::run(a...);
+}
+
+template <int D, int KIND>
+struct LaunchValue {
+    static int run(skm_evaluator *e)
+    {
+        value_kernel<D, KIND><<<e->value_blocks, kValueThreads, 0, e->stream>>>(e->P, e->d_samp, e->d_part);
+        SKM_CHECK_LAUNCH();
+        return SKM_OK;
+    }
+};
+
+template <int D, int KIND>
+struct LaunchLccValue {
+    static int run(skm_evaluator *e)
+    {
+        dense_kernel<D, KIND, false><<<e->dense_blocks, 256, 0, e->stream>>>(e->P, e->d_dense, e->d_dense_in);
+        SKM_CHECK_LAUNCH();
+        if (D == 3 && KIND != kStationary) {
+            dense_kernel<D, KIND, true><<<e->dense_blocks, 256, 0, e->stream>>>(e->P, e->d_dense_sw, e->d_dense_sw_in);
+            SKM_CHECK_LAUNCH();
+        }
+        lcc_value_kernel<D, KIND><<<e->value_blocks, kValueThreads, 0, e->stream>>>(e->P, e->d_dense, e->d_dense_in,
+                                                                                      e->d_part);
+        SKM_CHECK_LAUNCH();
+        return SKM_OK;
+    }
+};
+
+template <int D, int KIND>
+struct LaunchDeriv {
+    static int run(skm_evaluator *e, DerivParams Q)
+    {
+        derivative_kernel<D, KIND><<<e->deriv_blocks, kDerivThreads, 0, e->stream>>>(e->P, Q);
+        SKM_CHECK_LAUNCH();
+        return SKM_OK;
+    }
+};
+
+template <int D, int KIND>
+struct LaunchRegValue {
+    static int run(skm_evaluator *e, DerivParams Q)
+    {
+        regvalue_kernel<D, KIND><<<e->deriv_blocks, kDerivThreads, 0, e->stream>>>(e->P, Q);
+        SKM_CHECK_LAUNCH();
+        return SKM_OK;
+    }
+};
+
+template <int D, int KIND>
+struct LaunchDisp {
+    static int run(skm_evaluator *e, double *out)
+    {
+        displacement_kernel<D, KIND><<<e->dense_blocks, 256, 0, e->stream>>>(e->P, out);
+        SKM_CHECK_LAUNCH();
+        return SKM_OK;
+    }
+};
+
+// ------------------------------------------------------------------------------------------------
+extern "C" const char *skm_last_error(void) { return g_last_error.c_str(); }
+extern "C" int32_t skm_abi_version(void) { return SKM_ABI_VERSION; }
+
+static int validate_desc(const skm_evaluator_desc *d)
+{
+    if (!d) return fail(SKM_ERR_INVALID, "descriptor is NULL");
+    int D = d->dimensions;
+    if (D != 2 && D != 3) return fail(SKM_ERR_INVALID, "dimensions must be 2 or 3 (got %d)", D);
+    if (d->subsample < 1 || d->subsample > 100)          // metric hxx:87-89
+        return fail(SKM_ERR_INVALID, "subsample must be in [1,100] (got %d)", d->subsample);
+    if (d->subsample_neighborhood < 1 || d->subsample_neighborhood > 100)   // hxx:91-93
+        return fail(SKM_ERR_INVALID, "subsample_neighborhood must be in [1,100] (got %d)",
+                    d->subsample_neighborhood);
+    if (!(d->sigma_c0 > 0.0) || !(d->sigma_c4 > 0.0))    // itkTransformAdapter.hxx:412-414
+        return fail(SKM_ERR_INVALID, "kernel parameters have to be positive");
+    if (!d->fixed_image || !d->moving_coefficients) return fail(SKM_ERR_INVALID, "image data is NULL");
+    if (!geometry_ok(d->fixed_geometry, D) || !geometry_ok(d->moving_geometry, D) ||
+        !geometry_ok(d->cp_geometry, D) || !geometry_ok(d->cpw_geometry, D))
+        return fail(SKM_ERR_INVALID, "invalid geometry (size < 1 or spacing <= 0)");
+    for (int k = 0; k < D; ++k) {
+        if (d->moving_geometry.size[k] < 2)   // the prefilter's anti-causal start reads c[len-2]
+            return fail(SKM_ERR_INVALID, "moving image must have at least 2 texels per axis");
+        if (d->cpw_geometry.size[k] != d->cp_geometry.size[k])
+            return fail(SKM_ERR_INVALID, "control-point weight grid must match the control-point grid");
+        if (d->fixed_geometry.size[k] / d->subsample < 1)
+            return fail(SKM_ERR_INVALID, "subsample larger than the fixed image");
+    }
+    long long C = texels(d->cp_geometry, D);
+    if ((long long)d->num_parameters != C * D)
+        return fail(SKM_ERR_INVALID, "num_parameters (%d) != control points (%lld) * D", d->num_parameters, C);
+    if (d->use_weight_image && d->use_weight_tensor)
+        return fail(SKM_ERR_INVALID, "weight image and weight tensor are exclusive");
+    if (d->use_weight_image) {
+        if (!d->weight_image || !geometry_ok(d->weight_image_geometry, D))
+            return fail(SKM_ERR_INVALID, "weight image missing");
+        long long n = texels(d->weight_image_geometry, D);
+        for (long long i = 0; i < n; ++i)
+            if (!(d->weight_image[i] > 1e-8))          // itkTransformAdapter.hxx:325-327
+                return fail(SKM_ERR_INVALID, "weighting image has to be strictly positive everywhere");
+    }
+    if (d->use_weight_tensor) {
+        if (!d->weight_tensor || !geometry_ok(d->weight_tensor_geometry, D))
+            return fail(SKM_ERR_INVALID, "weight tensor missing");
+        long long n = texels(d->weight_tensor_geometry, D);
+        for (long long i = 0; i < n; ++i) {            // itkTransformAdapter.hxx:346-350
+            const double *m = d->weight_tensor + i * D * D;
+            double det = D == 2 ? m[0] * m[3] - m[1] * m[2]
+                                : m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+                                      m[2] * (m[3] * m[7] - m[4] * m[6]);
+            if (!(det > 0.0)) return fail(SKM_ERR_INVALID, "weighting tensors must be positive definite");
+        }
+    }
+    return SKM_OK;
+}
+
+extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator **out)
+{
+    if (!out) return fail(SKM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int rc = validate_desc(d);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SKM_ERR_CUDA, "no CUDA device available (this library has no CPU fallback)");
+    }
+    skm_evaluator *e = new skm_evaluator();
+    int D = d->dimensions;
+    e->D = D;
+    if (cudaGetDevice(&e->device) != cudaSuccess) {
+        delete e;
+        return fail(SKM_ERR_CUDA, "cudaGetDevice failed");
+    }
+    rc = [&]() -> int {
+        SKM_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+        e->fixed_geo = d->fixed_geometry;
+        e->cp_geo = d->cp_geometry;
+        e->nparams = d->num_parameters;
+        e->N = texels(d->fixed_geometry, D);
+        e->C = texels(d->cp_geometry, D);
+        EvalParams &P = e->P;
+        P.sub = d->subsample;
+        P.nbh = d->subsample_neighborhood;
+        P.fixed = make_geo(d->fixed_geometry, D, 0);
+        P.mov = make_geo(d->moving_geometry, D, 3);
+        P.cp = make_geo(d->cp_geometry, D, 0);
+        P.df = make_geo(d->fixed_geometry, D, 0);
+        P.has_df = 0;
+        long long ns = 1;
+        for (int k = 0; k < 3; ++k) {
+            P.ss[k] = k < D ? d->fixed_geometry.size[k] / d->subsample : 1;
+            ns *= P.ss[k];
+        }
+        P.Ns = e->Ns = ns;
+        P.C = e->C;
+        e->value_blocks = (int)((ns + kValueThreads - 1) / kValueThreads);
+        e->deriv_blocks = (int)((e->C + (kDerivThreads / 32) - 1) / (kDerivThreads / 32));
+        e->dense_blocks = (int)((e->N + 255) / 256);
+
+        // kernel parameters: GKernel<float> members are floats (Kernel.h:216-221)
+        KernelParams &K = P.K;
+        K.kind = d->use_weight_image ? kWeightImage : (d->use_weight_tensor ? kWeightTensor : kStationary);
+        K.sc0 = (float)d->sigma_c0;
+        K.sc4 = (float)d->sigma_c4;
+        K.inv_sc0 = 1.0f / K.sc0;
+        K.inv_sc4 = 1.0f / K.sc4;
+        K.support_min = K.sc4 < K.sc0 ? K.sc4 : K.sc0;
+        K.maxw = (float)d->maximum_weight;
+        for (int i = 0; i < 9; ++i) K.maxcov[i] = (float)d->maximum_eigenvalue_covariance[i];
+        K.wimg = nullptr;
+        K.wten = nullptr;
+        K.gw = make_geo(d->weight_image_geometry, D, 0);
+        K.gt = make_geo(d->weight_tensor_geometry, D, 0);
+
+        // images: converted to float on the host once, then uploaded
+        long long ncoef = 1;
+        for (int k = 0; k < D; ++k) ncoef *= (d->moving_geometry.size[k] + 3);
+        std::vector<float> tmp((size_t)std::max(e->N, ncoef));
+        for (long long i = 0; i < e->N; ++i) tmp[i] = (float)d->fixed_image[i];
+        if (dalloc(&e->d_fixed, e->N)) return SKM_ERR_CUDA;
+        SKM_CUDA(cudaMemcpy(e->d_fixed, tmp.data(), e->N * sizeof(float), cudaMemcpyHostToDevice));
+        for (long long i = 0; i < ncoef; ++i) tmp[i] = (float)d->moving_coefficients[i];
+        if (dalloc(&e->d_coeffs, ncoef)) return SKM_ERR_CUDA;
+        SKM_CUDA(cudaMemcpy(e->d_coeffs, tmp.data(), ncoef * sizeof(float), cudaMemcpyHostToDevice));
+        if (d->use_weight_image) {
+            long long n = texels(d->weight_image_geometry, D);
+            std::vector<float> w((size_t)n);
+            for (long long i = 0; i < n; ++i) w[i] = (float)d->weight_image[i];
+            if (dalloc(&e->d_wimg, n)) return SKM_ERR_CUDA;
+            SKM_CUDA(cudaMemcpy(e->d_wimg, w.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+            K.wimg = e->d_wimg;
+        }
+        if (d->use_weight_tensor) {
+            long long n = texels(d->weight_tensor_geometry, D) * D * D;
+            std::vector<float> w((size_t)n);
+            for (long long i = 0; i < n; ++i) w[i] = (float)d->weight_tensor[i];
+            if (dalloc(&e->d_wten, n)) return SKM_ERR_CUDA;
+            SKM_CUDA(cudaMemcpy(e->d_wten, w.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+            K.wten = e->d_wten;
+        }
+        P.fixed_data = e->d_fixed;
+        P.coeffs = e->d_coeffs;
+
+        if (dalloc(&e->d_cpd, e->C)) return SKM_ERR_CUDA;
+        P.cpd = e->d_cpd;
+        if (P.sub > 1) {
+            if (dalloc(&e->d_shifts, e->Ns)) return SKM_ERR_CUDA;
+        }
+        P.shifts = e->d_shifts;
+        if (dalloc(&e->d_samp, e->Ns)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_in, e->C * (D + 1))) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_part, (size_t)NQ * e->value_blocks)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_stats, NS)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_deriv, e->nparams)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_rpart, (size_t)NR * e->deriv_blocks)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_out, NO)) return SKM_ERR_CUDA;
+        SKM_CUDA(cudaMallocHost((void **)&e->h_in, sizeof(double) * e->C * (D + 1)));
+        SKM_CUDA(cudaMallocHost((void **)&e->h_out, sizeof(double) * (e->nparams + NO)));
+        rng_jump_table(e->jump);
+        int trc = table_plan(e->table, e->P, D, e->stream);
+        if (trc) return trc;
+        return SKM_OK;
+    }();
+    if (rc) {
+        delete e;
+        return rc;
+    }
+    *out = e;
+    return SKM_OK;
+}
+
+extern "C" int skm_evaluator_destroy(skm_evaluator *e)
+{
+    delete e;
+    return SKM_OK;
+}
+
+extern "C" int skm_set_regularizer_rkhs(skm_evaluator *e, double w)
+{
+    if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
+    e->reg_rkhs = w;
+    return SKM_OK;
+}
+
+extern "C" int skm_set_regularizer_rd(skm_evaluator *e, double w, double scaling)
+{
+    if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
+    e->reg_rd = w;
+    e->rd_scaling = scaling;
+    return SKM_OK;
+}
+
+extern "C" int skm_set_regularizer_pg(skm_evaluator *e, double w, double scaling)
+{
+    if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
+    e->reg_pg = w;
+    e->pg_scaling = scaling;
+    return SKM_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+static int upload_field(skm_evaluator *e, const skm_field *df)
+{
+    const double *key = (df && df->data) ? df->data : nullptr;
+    if (key == e->df_key) return SKM_OK;           // cached by host pointer (GpuEvaluator.cu:120-126)
+    e->df_key = key;
+    e->P.has_df = 0;
+    if (!key) return SKM_OK;
+    int D = e->D;
+    if (!geometry_ok(df->geometry, D)) return fail(SKM_ERR_INVALID, "invalid displacement-field geometry");
+    long long n = texels(df->geometry, D);
+    if (n > e->df_texels) {
+        if (e->d_df) cudaFree(e->d_df);
+        e->d_df = nullptr;
+        if (dalloc(&e->d_df, n)) return SKM_ERR_CUDA;
+        e->df_texels = n;
+    }
+    std::vector<float4> tmp((size_t)n);
+    for (long long i = 0; i < n; ++i)
+        tmp[i] = make_float4((float)key[i * D], (float)key[i * D + 1], D > 2 ? (float)key[i * D + 2] : 0.f, 0.f);
+    SKM_CUDA(cudaMemcpyAsync(e->d_df, tmp.data(), n * sizeof(float4), cudaMemcpyHostToDevice, e->stream));
+    SKM_CUDA(cudaStreamSynchronize(e->stream));
+    e->P.df = make_geo(df->geometry, D, 0);
+    e->P.dfd = e->d_df;
+    e->P.has_df = 1;
+    return SKM_OK;
+}
+
+// H2D of the parameters (AoS control points or planar parameters) and the weights.
+static int upload_params(skm_evaluator *e, const double *cp, const double *cpw, bool planar)
+{
+    if (!cp || !cpw) return fail(SKM_ERR_INVALID, "control points / weights are NULL");
+    const long long C = e->C, n = C * e->D;
+    std::memcpy(e->h_in, cp, sizeof(double) * n);
+    std::memcpy(e->h_in + n, cpw, sizeof(double) * C);
+    SKM_CUDA(cudaMemcpyAsync(e->d_in, e->h_in, sizeof(double) * (n + C), cudaMemcpyHostToDevice, e->stream));
+    int blocks = (int)((C + 255) / 256);
+    if (planar)
+        pack_cp_planar<<<blocks, 256, 0, e->stream>>>(e->d_in, e->d_in + n, C, e->D, e->d_cpd);
+    else
+        pack_cp_aos<<<blocks, 256, 0, e->stream>>>(e->d_in, e->d_in + n, C, e->D, e->d_cpd);
+    SKM_CHECK_LAUNCH();
+    return SKM_OK;
+}
+
+static int draw_shifts(skm_evaluator *e, int do_resampling)
+{
+    if (e->P.sub <= 1) return SKM_OK;
+    if (e->evaluated_once && !do_resampling) return SKM_OK;    // GpuEvaluator.cu:107-115
+    int blocks = (int)((e->Ns + 255) / 256);
+    shifts_kernel<<<blocks, 256, 0, e->stream>>>(e->rng_state, e->jump, e->Ns, e->D, e->P.sub, e->d_shifts);
+    SKM_CHECK_LAUNCH();
+    e->rng_state = rng_advance_host(e->rng_state, (unsigned long long)e->Ns * e->D, e->jump);
+    e->evaluated_once = true;
+    return SKM_OK;
+}
+
+static int ensure_dense(skm_evaluator *e)
+{
+    if (!e->d_dense) {
+        if (dalloc(&e->d_dense, e->N)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_dense_in, e->N)) return SKM_ERR_CUDA;
+    }
+    if (e->D == 3 && e->P.K.kind != kStationary && !e->d_dense_sw) {
+        if (dalloc(&e->d_dense_sw, e->N)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_dense_sw_in, e->N)) return SKM_ERR_CUDA;
+    }
+    return SKM_OK;
+}
+
+struct RegWeights {
+    double rkhs, rd, rd_scaling, pg, pg_scaling, l1, l21, l2;
+    int with_metric, negate;
+};
+
+// The full device sequence of one evaluation (everything after the parameter upload).
+static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const RegWeights &w, const double *params)
+{
+    int rc = SKM_OK;
+    const int D = e->D, kind = e->P.K.kind;
+    if (metric == SKM_LCC) {
+        if ((rc = ensure_dense(e))) return rc;
+        if ((rc = dispatch<LaunchLccValue>(D, kind, e))) return rc;
+    } else {
+        bool tab = e->use_table && e->table.enabled;
+        if (tab) rc = table_value(e->table, e->P, e->d_samp, e->d_part, e->value_blocks, e->stream);
+        else rc = dispatch<LaunchValue>(D, kind, e);
+        if (rc) return rc;
+    }
+    stats_kernel<<<1, 1024, 0, e->stream>>>(e->d_part, e->value_blocks, metric, e->d_stats);
+    SKM_CHECK_LAUNCH();
+    DerivParams Q{};
+    Q.metric = metric;
+    Q.with_metric = w.with_metric;
+    Q.reg_rkhs = w.rkhs;
+    Q.reg_rd = w.rd;
+    Q.rd_scaling = w.rd_scaling;
+    Q.reg_pg = w.pg;
+    Q.pg_scaling = w.pg_scaling;
+    Q.reg_l1 = w.l1;
+    Q.reg_l21 = w.l21;
+    Q.reg_l2 = w.l2;
+    Q.negate = w.negate;
+    Q.stats = e->d_stats;
+    Q.params = params;
+    Q.samp = e->d_samp;
+    Q.dense = e->d_dense;
+    Q.dense_in = e->d_dense_in;
+    Q.dense_sw = e->d_dense_sw;
+    Q.dense_sw_in = e->d_dense_sw_in;
+    Q.deriv = e->d_deriv;
+    Q.rpart = e->d_rpart;
+    bool any_reg = w.rkhs > 0 || w.rd > 0 || w.pg > 0 || w.with_metric;
+    if (derivative) {
+        bool tab = e->use_table && e->table.enabled && metric != SKM_LCC;
+        if (tab) rc = table_derivative(e->table, e->P, Q, e->deriv_blocks, e->stream);
+        else rc = dispatch<LaunchDeriv>(D, kind, e, Q);
+        if (rc) return rc;
+    } else if (any_reg) {
+        if ((rc = dispatch<LaunchRegValue>(D, kind, e, Q))) return rc;
+    }
+    result_kernel<<<1, 256, 0, e->stream>>>(e->d_stats, (derivative || any_reg) ? e->d_rpart : nullptr,
+                                           e->deriv_blocks, w.rkhs, w.rd, w.pg, w.l1, w.l21, w.l2, e->d_out);
+    SKM_CHECK_LAUNCH();
+    return SKM_OK;
+}
+
+static int fetch(skm_evaluator *e, double *derivative)
+{
+    SKM_CUDA(cudaMemcpyAsync(e->h_out, e->d_out, sizeof(double) * NO, cudaMemcpyDeviceToHost, e->stream));
+    if (derivative)
+        SKM_CUDA(cudaMemcpyAsync(e->h_out + NO, e->d_deriv, sizeof(double) * e->nparams, cudaMemcpyDeviceToHost,
+                                 e->stream));
+    SKM_CUDA(cudaStreamSynchronize(e->stream));
+    if (derivative) std::memcpy(derivative, e->h_out + NO, sizeof(double) * e->nparams);
+    return SKM_OK;
+}
+
+static int check_metric(int metric)
+{
+    if (metric != SKM_MSE && metric != SKM_NCC && metric != SKM_LCC)
+        return fail(SKM_ERR_INVALID, "unknown metric %d", metric);
+    return SKM_OK;
+}
+
+static int evaluate_common(skm_evaluator *e, int32_t metric, const double *cp, const double *cpw,
+                           const skm_field *df, double *derivatives, int32_t do_resampling, skm_result *out)
+{
+    if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
+    int rc;
+    if ((rc = check_metric(metric))) return rc;
+    SKM_CUDA(cudaSetDevice(e->device));
+    if ((rc = upload_field(e, df))) return rc;
+    if ((rc = upload_params(e, cp, cpw, false))) return rc;
+    if ((rc = draw_shifts(e, do_resampling))) return rc;
+    RegWeights w{};
+    w.rkhs = e->reg_rkhs > 0 ? e->reg_rkhs : 0.0;
+    w.rd = e->reg_rd > 0 ? e->reg_rd : 0.0;
+    w.rd_scaling = e->rd_scaling;
+    w.pg = e->reg_pg > 0 ? e->reg_pg : 0.0;
+    w.pg_scaling = e->pg_scaling;
+    if ((rc = run_evaluation(e, metric, derivatives != nullptr, w, nullptr))) return rc;
+    if ((rc = fetch(e, derivatives))) return rc;
+    if (out) {
+        out->measure = e->h_out[O_MEASURE];
+        out->reg_value_rkhs = e->h_out[O_RKHS];
+        out->reg_value_rd = e->h_out[O_RD];
+        out->reg_value_pg = e->h_out[O_PG];
+        out->num_pixels_counted = (uint32_t)e->h_out[O_COUNT];
+    }
+    return SKM_OK;
+}
+
+extern "C" int skm_get_value(skm_evaluator *e, int32_t metric, const double *cp, const double *cpw,
+                             const skm_field *df, int32_t do_resampling, skm_result *out)
+{
+    return evaluate_common(e, metric, cp, cpw, df, nullptr, do_resampling, out);
+}
+
+extern "C" int skm_get_value_and_derivative(skm_evaluator *e, int32_t metric, const double *cp, const double *cpw,
+                                            const skm_field *df, double *derivatives, int32_t do_resampling,
+                                            skm_result *out)
+{
+    if (!derivatives) return fail(SKM_ERR_INVALID, "derivatives is NULL");
+    return evaluate_common(e, metric, cp, cpw, df, derivatives, do_resampling, out);
+}
+
+static int validate_metric(const skm_metric_desc *m)
+{
+    if (!m) return fail(SKM_ERR_INVALID, "metric descriptor is NULL");
+    int rc = check_metric(m->metric);
+    if (rc) return rc;
+    if (m->reg_l1 < 0 || m->reg_l21 < 0 || m->reg_l2 < 0 || m->reg_rkhs < 0 || m->reg_rd < 0 || m->reg_pg < 0)
+        return fail(SKM_ERR_INVALID, "Regularization weights must be positive.");          // hxx:79-84
+    if (!(m->reg_rd_scaling > 0) || !(m->reg_pg_scaling > 0))
+        return fail(SKM_ERR_INVALID, "Robust regularization scales must be strictly positive.");   // hxx:86-88
+    return SKM_OK;
+}
+
+// Device part of one metric evaluation on already-uploaded planar parameters (e->d_in).
+int skm_metric_device(skm_evaluator *e, const skm_metric_desc *m, bool derivative)
+{
+    RegWeights w{};
+    w.rkhs = m->reg_rkhs;
+    w.rd = m->reg_rd;
+    w.rd_scaling = m->reg_rd_scaling;
+    w.pg = m->reg_pg;
+    w.pg_scaling = m->reg_pg_scaling;
+    w.l1 = m->reg_l1;
+    w.l21 = m->reg_l21;
+    w.l2 = m->reg_l2;
+    w.with_metric = 1;
+    w.negate = m->use_negative_gradient;
+    return run_evaluation(e, m->metric, derivative, w, e->d_in);
+}
+
+extern "C" int skm_metric_evaluate(skm_evaluator *e, const skm_metric_desc *m, const double *parameters,
+                                   const double *cpw, const skm_field *df, double *derivative,
+                                   skm_metric_values *out)
+{
+    if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
+    int rc;
+    if ((rc = validate_metric(m))) return rc;
+    SKM_CUDA(cudaSetDevice(e->device));
+    if ((rc = upload_field(e, df))) return rc;
+    if ((rc = upload_params(e, parameters, cpw, true))) return rc;
+    if ((rc = draw_shifts(e, m->do_resampling))) return rc;
+    if ((rc = skm_metric_device(e, m, derivative != nullptr))) return rc;
+    if ((rc = fetch(e, derivative))) return rc;
+    if (out) {
+        const double *o = e->h_out;
+        out->value = o[O_VALUE];
+        out->measure = o[O_MEASURE];
+        out->reg_value = o[O_REG];
+        out->reg_l1 = o[O_L1];
+        out->reg_l21 = o[O_L21];
+        out->reg_l2 = o[O_L2];
+        out->reg_rkhs = o[O_RKHS];
+        out->reg_rd = o[O_RD];
+        out->reg_pg = o[O_PG];
+        out->num_pixels_counted = (uint32_t)o[O_COUNT];
+    }
+    return SKM_OK;
+}
+
+extern "C" int skm_evaluate_displacement_field(skm_evaluator *e, const double *cp, const double *cpw,
+                                               const skm_field *df, double *dst)
+{
+    if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
+    if (!dst) return fail(SKM_ERR_INVALID, "dst is NULL");
+    int rc;
+    SKM_CUDA(cudaSetDevice(e->device));
+    if ((rc = upload_field(e, df))) return rc;
+    if ((rc = upload_params(e, cp, cpw, false))) return rc;
+    double *d_out = nullptr;
+    if (dalloc(&d_out, (size_t)e->N * e->D)) return SKM_ERR_CUDA;
+    rc = dispatch<LaunchDisp>(e->D, e->P.K.kind, e, d_out);
+    if (!rc) {
+        cudaError_t c1 = cudaMemcpyAsync(dst, d_out, sizeof(double) * e->N * e->D, cudaMemcpyDeviceToHost, e->stream);
+        cudaError_t c2 = cudaStreamSynchronize(e->stream);
+        if (c1 != cudaSuccess || c2 != cudaSuccess)
+            rc = fail(SKM_ERR_CUDA, "displacement field copy failed: %s",
+                      cudaGetErrorString(c1 != cudaSuccess ? c1 : c2));
+    }
+    cudaFree(d_out);
+    return rc;
+}
+
+// ------------------------------------------------------------------------------------------------
+extern "C" int skm_bspline_coefficients(int32_t D, const int32_t *size, const double *image, double *coeffs)
+{
+    if (D != 2 && D != 3) return fail(SKM_ERR_INVALID, "dimensions must be 2 or 3");
+    if (!size || !image || !coeffs) return fail(SKM_ERR_INVALID, "NULL argument");
+    int X = size[0], Y = size[1], Z = D == 3 ? size[2] : 1;
+    if (X < 2 || Y < 2 || (D == 3 && Z < 2)) return fail(SKM_ERR_INVALID, "need at least 2 texels per axis");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SKM_ERR_CUDA, "no CUDA device available (this library has no CPU fallback)");
+    }
+    long long n = (long long)X * Y * Z;
+    long long pn = (long long)(X + 3) * (Y + 3) * (D == 3 ? Z + 3 : 1);
+    double *d_img = nullptr, *d_out = nullptr;
+    cudaStream_t s = nullptr;
+    int rc = [&]() -> int {
+        SKM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        if (dalloc(&d_img, n)) return SKM_ERR_CUDA;
+        if (dalloc(&d_out, pn)) return SKM_ERR_CUDA;
+        SKM_CUDA(cudaMemcpyAsync(d_img, image, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        const double pole = sqrt(3.0) - 2.0;
+        if (D == 3) {                                  // z, then y, then x (BsplineImage.h:182-195)
+            bs_prefilter_axis<<<(int)(((long long)X * Y + 127) / 128), 128, 0, s>>>(d_img, X, Y, Z, 2, pole);
+            bs_prefilter_axis<<<(int)(((long long)X * Z + 127) / 128), 128, 0, s>>>(d_img, X, Y, Z, 1, pole);
+            bs_prefilter_axis<<<(int)(((long long)Y * Z + 127) / 128), 128, 0, s>>>(d_img, X, Y, Z, 0, pole);
+        } else {                                       // x, then y (BsplineImage.h:174-180)
+            bs_prefilter_axis<<<(Y + 127) / 128, 128, 0, s>>>(d_img, X, Y, 1, 0, pole);
+            bs_prefilter_axis<<<(X + 127) / 128, 128, 0, s>>>(d_img, X, Y, 1, 1, pole);
+        }
+        SKM_CHECK_LAUNCH();
+        bs_mirror_pad<<<(int)((pn + 255) / 256), 256, 0, s>>>(d_img, X, Y, Z, D, d_out);
+        SKM_CHECK_LAUNCH();
+        SKM_CUDA(cudaMemcpyAsync(coeffs, d_out, pn * sizeof(double), cudaMemcpyDeviceToHost, s));
+        SKM_CUDA(cudaStreamSynchronize(s));
+        return SKM_OK;
+    }();
+    if (d_img) cudaFree(d_img);
+    if (d_out) cudaFree(d_out);
+    if (s) cudaStreamDestroy(s);
+    return rc;
+}
+
+#include "skm_optimizer.cuh"

@@ -1,0 +1,369 @@
+// skm_device.cuh -- device-side building blocks of the SKM evaluation path on sm_100a.
+//
+// Geometry, the Wendland kernel family, the cubic B-spline sampler, the PCG32 grid
+// shifts and deterministic block reductions.  Every formula restates a reference
+// function (ChristophJud/SKMImageRegistration, include/cuda/...) cited at its
+// definition; the arithmetic split is: positions and index boxes in double (they
+// decide which control points / samples contribute, so they follow the reference's
+// double arithmetic exactly), kernel values and sums over taps in float, global sums
+// in double.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace skm {
+
+constexpr int kMaxDim = 3;
+
+// ImageBase (include/cuda/ImageBase.h:40-100): physical = o + s*idx, local = inv*(p - o).
+struct Geo {
+    double o[3];
+    double s[3];
+    double inv[3];
+    int n[3];
+    long long st[3];
+};
+
+enum KernelKind : int { kStationary = 0, kWeightImage = 1, kWeightTensor = 2 };
+
+// GKernel<float> (include/cuda/Kernel.h:134-209).
+struct KernelParams {
+    int kind;
+    float sc0, sc4;          // sigma C0 / C4
+    float inv_sc0, inv_sc4;
+    float support_min;       // min(sigmaC4, sigmaC0) (float members, Kernel.h:158-161)
+    float maxw;              // maximum weight (float member)
+    float maxcov[9];         // maximum-eigenvalue covariance (MatF, float)
+    const float *wimg;       // weight image (sigma per texel)
+    Geo gw;
+    const float *wten;       // covariance tensors, D*D floats per texel
+    Geo gt;
+};
+
+template <int D>
+__device__ __forceinline__ void to_global(const Geo &g, const double *idx, double *p)
+{
+#pragma unroll
+    for (int d = 0; d < D; ++d) p[d] = g.o[d] + g.s[d] * idx[d];
+}
+
+template <int D>
+__device__ __forceinline__ void to_local(const Geo &g, const double *p, double *l)
+{
+#pragma unroll
+    for (int d = 0; d < D; ++d) l[d] = g.inv[d] * (p[d] - g.o[d]);
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// ImageNearest::atGlobal index (ImageNearest.h:69-84): int(local + 0.5), truncating.
+template <int D>
+__device__ __forceinline__ long long nearest_index(const Geo &g, const double *p)
+{
+    double l[3];
+    to_local<D>(g, p, l);
+    long long lin = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        int i = (int)(l[d] + 0.5);
+        if (i < 0 || i >= g.n[d]) return -1;
+        lin += g.st[d] * i;
+    }
+    return lin;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Wendland kernel family (Kernel.h:48-131), float like GKernel<float>.
+
+__device__ __forceinline__ float wendland_c4(float r)
+{
+    float f = fmaxf(0.0f, 1.0f - r);
+    float f2 = f * f;
+    return f2 * f2 * f2 * (3.0f + 18.0f * r + 35.0f * r * r) * (1.0f / 3.0f);
+}
+
+__device__ __forceinline__ float wendland_c0(float r)
+{
+    float f = fmaxf(0.0f, 1.0f - r);
+    return f * f;
+}
+
+// stationary C4*C0 product (Kernel.h:96-103); the C0 factor is always active (USE_WENDLAND_C0
+// is tested with #ifdef and defined either way).
+__device__ __forceinline__ float k_stationary(const KernelParams &K, float r)
+{
+    return wendland_c4(r * K.inv_sc4) * wendland_c0(r * K.inv_sc0);
+}
+
+template <int D>
+__device__ __forceinline__ float det_m(const float *m)
+{
+    if (D == 2) return m[0] * m[3] - m[2] * m[1];
+    return m[0] * m[4] * m[8] + m[3] * m[7] * m[2] + m[6] * m[1] * m[5] - m[0] * m[7] * m[5] -
+           m[6] * m[4] * m[2] - m[3] * m[1] * m[8];
+}
+
+// v^T inv(M) v with the adjugate/determinant inverse of Mat.h:238-257.
+template <int D>
+__device__ __forceinline__ float quad_inv(const float *m, const float *v)
+{
+    float dt = det_m<D>(m);
+    if (D == 2) {
+        float a00 = m[3] / dt, a01 = -m[1] / dt, a10 = -m[2] / dt, a11 = m[0] / dt;
+        float r0 = v[0] * a00 + v[1] * a10, r1 = v[0] * a01 + v[1] * a11;   // (v*inv)_i = sum_k v_k inv[k][i]
+        return r0 * v[0] + r1 * v[1];
+    }
+#define M_(i, j) m[(i) * 3 + (j)]
+    float a[9] = {M_(1, 1) * M_(2, 2) - M_(1, 2) * M_(2, 1), M_(0, 2) * M_(2, 1) - M_(0, 1) * M_(2, 2),
+                  M_(0, 1) * M_(1, 2) - M_(0, 2) * M_(1, 1), M_(1, 2) * M_(2, 0) - M_(1, 0) * M_(2, 2),
+                  M_(0, 0) * M_(2, 2) - M_(0, 2) * M_(2, 0), M_(0, 2) * M_(1, 0) - M_(0, 0) * M_(1, 2),
+                  M_(1, 0) * M_(2, 1) - M_(1, 1) * M_(2, 0), M_(0, 1) * M_(2, 0) - M_(0, 0) * M_(2, 1),
+                  M_(0, 0) * M_(1, 1) - M_(0, 1) * M_(1, 0)};
+#undef M_
+    float q = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float r = v[0] * (a[0 * 3 + i] / dt) + v[1] * (a[1 * 3 + i] / dt) + v[2] * (a[2 * 3 + i] / dt);
+        q += r * v[i];
+    }
+    return q;
+}
+
+// maxEigenValue (Mat.h:259-281) in double (support radius only).
+template <int D>
+__device__ __forceinline__ double max_eig(const double *m)
+{
+    if (D == 2) {
+        double tr = m[0] + m[3];
+        double dt = m[0] * m[3] - m[2] * m[1];
+        double disc = tr * tr - 4.0 * dt;
+        return 0.5 * (tr + sqrt(disc > 0.0 ? disc : 0.0));
+    }
+    double triSq = m[1] * m[1] + m[2] * m[2] + m[5] * m[5];
+    if (triSq == 0.0) return fmax(m[0], fmax(m[4], m[8]));
+    double q = (1.0 / 3.0) * (m[0] + m[4] + m[8]);
+    double pSq = 2.0 * triSq + (m[0] - q) * (m[0] - q) + (m[4] - q) * (m[4] - q) + (m[8] - q) * (m[8] - q);
+    double p = sqrt(pSq * (1.0 / 6.0));
+    double b0 = m[0] - q, b4 = m[4] - q, b8 = m[8] - q;
+    double dt = b0 * b4 * b8 + m[3] * m[7] * m[2] + m[6] * m[1] * m[5] - b0 * m[7] * m[5] - m[6] * b4 * m[2] -
+                m[3] * m[1] * b8;
+    double r = dt * (0.5 / (p * p * p));
+    r = fmin(1.0, fmax(-1.0, r));
+    double phi = (1.0 / 3.0) * acos(r);
+    return q + 2.0 * p * cos(phi);
+}
+
+// Per-point information of GKernel::evaluate(p, q, [sigmaP | covP]) and its support radius.
+struct PInfo {
+    double support;
+    float sigma;
+    float cov[9];
+};
+
+template <int D>
+__device__ __forceinline__ float sigma_at(const KernelParams &K, const double *p)
+{
+    long long i = nearest_index<D>(K.gw, p);
+    return i >= 0 ? K.wimg[i] : 0.0f;     // ImageNearest default 0 (ImageNearest.h:41-45)
+}
+
+template <int D>
+__device__ __forceinline__ void cov_at(const KernelParams &K, const double *p, float *c)
+{
+    long long i = nearest_index<D>(K.gt, p);
+    if (i >= 0) {
+#pragma unroll
+        for (int e = 0; e < D * D; ++e) c[e] = K.wten[i * D * D + e];
+    } else {                               // identity default (ImageNearest.h:47-51)
+#pragma unroll
+        for (int e = 0; e < D * D; ++e) c[e] = (e % (D + 1) == 0) ? 1.0f : 0.0f;
+    }
+}
+
+// getRegionSupport overloads (Kernel.h:158-171).
+template <int KIND, int D>
+__device__ __forceinline__ void pinfo_at(const KernelParams &K, const double *p, PInfo &pi)
+{
+    double smin = (double)K.support_min;
+    if (KIND == kWeightImage) {
+        pi.sigma = sigma_at<D>(K, p);
+        pi.support = smin / sqrt(2.0 / ((double)K.maxw + (double)pi.sigma));
+    } else if (KIND == kWeightTensor) {
+        cov_at<D>(K, p, pi.cov);
+        double s[9];
+#pragma unroll
+        for (int e = 0; e < D * D; ++e) s[e] = (double)K.maxcov[e] + (double)pi.cov[e];
+        pi.support = smin / sqrt(2.0 / max_eig<D>(s));
+    } else {
+        pi.support = smin;
+    }
+}
+
+// GKernel::evaluate(p, q, p-side info) with v = p - q given in float and q's global
+// position (needed for the sigma / covariance lookup at q).
+template <int KIND, int D>
+__device__ __forceinline__ float k_eval(const KernelParams &K, const float *v, const double *q, const PInfo &pi)
+{
+    if (KIND == kStationary) {
+        float r2 = 0.0f;
+#pragma unroll
+        for (int d = 0; d < D; ++d) r2 = fmaf(v[d], v[d], r2);
+        return k_stationary(K, sqrtf(r2));
+    } else if (KIND == kWeightImage) {
+        // evaluateNonStationary (Kernel.h:105-117): F^2 * C4(sqrtQ) * C0(sqrtQ)
+        float sp = pi.sigma, sq = sigma_at<D>(K, q);
+        float F = powf(fabsf(sp), 0.25f) * powf(fabsf(sq), 0.25f) * powf(fabsf((sp + sq) * 0.5f), -0.5f);
+        float r2 = 0.0f;
+#pragma unroll
+        for (int d = 0; d < D; ++d) r2 = fmaf(v[d], v[d], r2);
+        float sqrtQ = sqrtf(2.0f / (sp + sq)) * sqrtf(r2);
+        return F * wendland_c4(sqrtQ * K.inv_sc4) * F * wendland_c0(sqrtQ * K.inv_sc0);
+    } else {
+        // evaluateAnisotropic (Kernel.h:119-131)
+        float cq[9], ms[9];
+        cov_at<D>(K, q, cq);
+#pragma unroll
+        for (int e = 0; e < D * D; ++e) ms[e] = (pi.cov[e] + cq[e]) * 0.5f;
+        float sqrtQ = sqrtf(quad_inv<D>(ms, v));
+        float F = powf(det_m<D>(pi.cov), 0.25f) * powf(det_m<D>(cq), 0.25f) * powf(det_m<D>(ms), -0.5f);
+        return F * wendland_c4(sqrtQ * K.inv_sc4) * F * wendland_c0(sqrtQ * K.inv_sc0);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// cubic B-spline image (BsplineImage.h:110-144, 247-265, 285-296).  `mg` is the padded
+// coefficient geometry (size+3 per axis), `l` the moving-image local coordinate in double.
+template <int D>
+__device__ __forceinline__ bool bspline_inside(const Geo &mg, const double *l)
+{
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+        if (l[d] < -0.5 || l[d] + 3.5 >= (double)mg.n[d]) return false;
+    return true;
+}
+
+template <int D>
+__device__ __forceinline__ void bspline_derivs(const float *__restrict__ c, const Geo &mg, const double *l,
+                                               float &val, float *grad)
+{
+    int ii[3] = {0, 0, 0};
+    float W[4][3], dW[4][3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        ii[d] = (int)l[d];                       // VecI(idx): truncation toward zero
+        float w = (float)(l[d] - (double)ii[d]);
+        float w3 = (1.0f / 6.0f) * w * w * w;
+        float w0 = (1.0f / 6.0f) + 0.5f * w * (w - 1.0f) - w3;
+        float w2 = w + w0 - 2.0f * w3;
+        W[3][d] = w3; W[0][d] = w0; W[2][d] = w2; W[1][d] = 1.0f - w0 - w2 - w3;
+        float d3 = 0.5f * w * w;
+        float d0 = w - 0.5f - d3;
+        float d2 = 1.0f + d0 - 2.0f * d3;
+        dW[3][d] = d3; dW[0][d] = d0; dW[2][d] = d2; dW[1][d] = -d0 - d2 - d3;
+    }
+    if (D == 3) {
+        float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+        const long long sy = mg.st[1], sz = mg.st[2];
+        const float *base = c + ii[0] + ii[1] * sy + ii[2] * sz;
+#pragma unroll
+        for (int z = 0; z < 4; ++z) {
+            float z0 = 0.f, z1 = 0.f, z3 = 0.f;
+#pragma unroll
+            for (int y = 0; y < 4; ++y) {
+                const float *row = base + y * sy + z * sz;
+                float a = __ldg(row), b = __ldg(row + 1), e = __ldg(row + 2), f = __ldg(row + 3);
+                float dx = dW[0][0] * a + dW[1][0] * b + dW[2][0] * e + dW[3][0] * f;
+                float vx = W[0][0] * a + W[1][0] * b + W[2][0] * e + W[3][0] * f;
+                z0 += W[y][1] * dx;
+                z1 += dW[y][1] * vx;
+                z3 += W[y][1] * vx;
+            }
+            c0 += W[z][2] * z0;
+            c1 += W[z][2] * z1;
+            c2 += dW[z][2] * z3;
+            c3 += W[z][2] * z3;
+        }
+        val = c3;
+        grad[0] = c0 * (float)mg.inv[0];
+        grad[1] = c1 * (float)mg.inv[1];
+        grad[2] = c2 * (float)mg.inv[2];
+    } else {
+        float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+        const long long sy = mg.st[1];
+        const float *base = c + ii[0] + ii[1] * sy;
+#pragma unroll
+        for (int y = 0; y < 4; ++y) {
+            const float *row = base + y * sy;
+            float a = __ldg(row), b = __ldg(row + 1), e = __ldg(row + 2), f = __ldg(row + 3);
+            float dx = dW[0][0] * a + dW[1][0] * b + dW[2][0] * e + dW[3][0] * f;
+            float vx = W[0][0] * a + W[1][0] * b + W[2][0] * e + W[3][0] * f;
+            c0 += W[y][1] * dx;
+            c1 += dW[y][1] * vx;
+            c2 += W[y][1] * vx;
+        }
+        val = c2;
+        grad[0] = c0 * (float)mg.inv[0];
+        grad[1] = c1 * (float)mg.inv[1];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// PCG32 stream of UniformRng (UniformRng.h:28-46) with LCG jump-ahead so that every sample
+// draws its own D values of the sequential stream in parallel.
+struct RngJump {
+    unsigned long long mul[64];   // a^(2^i)
+    unsigned long long add[64];   // c*(a^(2^i)-1)/(a-1)
+};
+
+__device__ __forceinline__ unsigned long long lcg_advance(unsigned long long state, unsigned long long steps,
+                                                          const RngJump &J)
+{
+    int i = 0;
+    while (steps) {
+        if (steps & 1ull) state = state * J.mul[i] + J.add[i];
+        steps >>= 1;
+        ++i;
+    }
+    return state;
+}
+
+__device__ __forceinline__ unsigned pcg32_output(unsigned long long old)
+{
+    unsigned xorshifted = (unsigned)(((old >> 18u) ^ old) >> 27u);
+    unsigned rot = (unsigned)(old >> 59u);
+    return (xorshifted >> rot) | (xorshifted << ((unsigned)(-(int)rot) & 31));
+}
+
+// ---------------------------------------------------------------------------------------------
+// deterministic reductions (fixed shuffle tree, fixed block order)
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum NV values over the block; result valid in thread 0.  `sh` holds NV*32 doubles.
+template <int NV>
+__device__ __forceinline__ void block_sum(double *v, double *sh)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k * 32 + warp] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double x = lane < nw ? sh[k * 32 + lane] : 0.0;
+            v[k] = warp_sum(x);
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace skm

@@ -1,0 +1,919 @@
+// skm_kernels.cuh -- the evaluation kernels (any kernel kind, 2-D/3-D, any subsampling).
+//
+// Work decomposition (B200): the value pass is one thread per sample that fuses the
+// kernel-machine transform, the B-spline warp and the metric statistics and writes a
+// per-sample (grad M, m) record plus per-block FP64 partial sums; the derivative is a
+// control-point-owned gather with one warp per control point, lanes striding the
+// control point's sample box and a fixed shuffle tree reducing the lanes -- no atomics,
+// so results are bitwise reproducible.  The regularizers of the same control point run
+// in the same warp and are added in the reference's order.
+#pragma once
+
+#include "skm_device.cuh"
+
+namespace skm {
+
+// per-block partial quantities of the value pass (laid out [quantity][block])
+enum { Q_COUNT = 0, Q_D2, Q_SF, Q_SM, Q_SFF, Q_SMM, Q_SFM, Q_CC, NQ };
+// per-block partial quantities of the derivative pass
+enum { R_RKHS = 0, R_RD, R_PG, R_L1, R_L21, R_L2, NR };
+// global statistics written by stats_kernel and read by the derivative pass
+enum {
+    S_COUNT = 0, S_MEASURE, S_COEF_F, S_COEF_M, S_COEF_C, S_MEAN_F, S_MEAN_M, S_DENOM, S_SFM, S_SMM,
+    S_VALID, NS
+};
+// result vector written by result_kernel
+enum {
+    O_MEASURE = 0, O_RKHS, O_RD, O_PG, O_L1, O_L21, O_L2, O_REG, O_VALUE, O_COUNT, NO
+};
+
+struct EvalParams {
+    int sub, nbh;
+    Geo fixed;         // fixed image
+    Geo mov;           // B-spline coefficients (size+3 per axis), moving image origin/spacing
+    Geo cp;            // control-point grid
+    Geo df;            // previous-level displacement field
+    int has_df;
+    int ss[3];         // subsampled grid = size/subsample (GpuEvaluator.cu:44)
+    long long Ns;      // number of samples
+    long long C;       // control points
+    const float *__restrict__ fixed_data;
+    const float *__restrict__ coeffs;
+    const float4 *__restrict__ cpd;     // (alpha_x, alpha_y, alpha_z, w) per control point
+    const float4 *__restrict__ dfd;     // displacement field, 4 floats per texel
+    const uint32_t *__restrict__ shifts; // packed per-sample shift (8 bits per axis)
+    KernelParams K;
+};
+
+struct DerivParams {
+    int metric;                 // 0 MSE, 1 NCC, 2 LCC
+    int with_metric;            // 1: metric-level call (host regularizers + sign)
+    double reg_rkhs, reg_rd, rd_scaling, reg_pg, pg_scaling;
+    double reg_l1, reg_l21, reg_l2;
+    int negate;
+    const double *__restrict__ stats;
+    const double *__restrict__ params;   // planar parameters (metric level), else null
+    const float4 *__restrict__ samp;     // (grad M, m) per sample
+    const float4 *__restrict__ dense;    // LCC: (grad M, m) per fixed texel
+    const unsigned char *__restrict__ dense_in;
+    const float4 *__restrict__ dense_sw; // LCC 3-D swapped-kernel field (non-stationary kinds)
+    const unsigned char *__restrict__ dense_sw_in;
+    double *__restrict__ deriv;          // planar output
+    double *__restrict__ rpart;          // [NR][blocks]
+};
+
+// ---- sample positions ------------------------------------------------------------------------
+template <int D>
+__device__ __forceinline__ void cell_of(const int *n, long long t, int *c)
+{
+    c[0] = (int)(t % n[0]);
+    c[1] = D > 1 ? (int)((t / n[0]) % n[1]) : 0;
+    c[2] = D > 2 ? (int)(t / ((long long)n[0] * n[1])) : 0;
+}
+
+// samplePos = cell*subsample + shift (MSE.cu:171-174).  A shift equal to the subsample
+// rate (a draw of exactly UINT_MAX) can place the last cell's sample outside the image,
+// where the reference reads out of bounds; such a sample is treated as outside here.
+template <int D>
+__device__ __forceinline__ bool sample_pos(const EvalParams &P, long long t, int *sp)
+{
+    int c[3];
+    cell_of<D>(P.ss, t, c);
+    sp[0] = c[0]; sp[1] = c[1]; sp[2] = c[2];
+    if (P.sub != 1) {
+        uint32_t s = P.shifts[t];
+#pragma unroll
+        for (int d = 0; d < D; ++d) sp[d] = c[d] * P.sub + (int)((s >> (8 * d)) & 0xffu);
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+            if (sp[d] >= P.fixed.n[d]) return false;
+    }
+    return true;
+}
+
+template <int D>
+__device__ __forceinline__ long long lin_of(const Geo &g, const int *i)
+{
+    long long r = i[0];
+    if (D > 1) r += g.st[1] * i[1];
+    if (D > 2) r += g.st[2] * i[2];
+    return r;
+}
+
+// ---- forward transform -----------------------------------------------------------------------
+// u += sum over the control-point box of w_i k(p, c_i) alpha_i (DisplacementField.cu:53-72).
+// SWAP evaluates k(c_i, p) with p's kernel information (3-D LCC derivative, LCC.cu:429-442).
+template <int D, int KIND, bool SWAP>
+__device__ __forceinline__ void transform_add(const EvalParams &P, const double *p, const PInfo &pi, float *u)
+{
+    double ip[3];
+    to_local<D>(P.cp, p, ip);
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    float base[3], hs[3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        double sh = pi.support / P.cp.s[d];
+        lo[d] = clampi((int)(ip[d] - sh + 1.0), 0, P.cp.n[d] - 1);
+        hi[d] = clampi((int)(ip[d] + sh), 0, P.cp.n[d] - 1);
+        base[d] = (float)(p[d] - (P.cp.o[d] + P.cp.s[d] * (double)lo[d]));
+        hs[d] = (float)P.cp.s[d];
+    }
+    float ux = 0.f, uy = 0.f, uz = 0.f;
+    for (int z = lo[2]; z <= hi[2]; ++z) {
+        for (int y = lo[1]; y <= hi[1]; ++y) {
+            long long row = (long long)z * P.cp.st[2] + (long long)y * P.cp.st[1];
+            for (int x = lo[0]; x <= hi[0]; ++x) {
+                float v[3];
+                v[0] = base[0] - hs[0] * (float)(x - lo[0]);
+                if (D > 1) v[1] = base[1] - hs[1] * (float)(y - lo[1]);
+                if (D > 2) v[2] = base[2] - hs[2] * (float)(z - lo[2]);
+                float k;
+                if (KIND == kStationary) {
+                    k = k_eval<KIND, D>(P.K, v, nullptr, pi);
+                } else {
+                    double q[3], qi[3] = {(double)x, (double)y, (double)z};
+                    to_global<D>(P.cp, qi, q);
+                    if (SWAP) {
+                        // k(c_i, p) with sigma/cov taken at p for both ends
+                        float vn[3];
+#pragma unroll
+                        for (int d = 0; d < D; ++d) vn[d] = -v[d];
+                        k = k_eval<KIND, D>(P.K, vn, p, pi);
+                    } else {
+                        k = k_eval<KIND, D>(P.K, v, q, pi);
+                    }
+                }
+                float4 c = __ldg(P.cpd + row + x);
+                float wk = c.w * k;
+                ux = fmaf(wk, c.x, ux);
+                uy = fmaf(wk, c.y, uy);
+                if (D > 2) uz = fmaf(wk, c.z, uz);
+            }
+        }
+    }
+    u[0] += ux;
+    u[1] += uy;
+    if (D > 2) u[2] += uz;
+}
+
+// moving-image point of fixed point p: p + DF(p) + u(p), returned in moving local coordinates.
+template <int D, int KIND, bool SWAP>
+__device__ __forceinline__ void moving_local(const EvalParams &P, const double *p, double *ml)
+{
+    double mp[3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) mp[d] = p[d];
+    if (P.has_df) {
+        long long i = nearest_index<D>(P.df, p);
+        if (i >= 0) {
+            float4 v = P.dfd[i];
+            mp[0] += v.x;
+            if (D > 1) mp[1] += v.y;
+            if (D > 2) mp[2] += v.z;
+        }
+    }
+    PInfo pi;
+    pinfo_at<KIND, D>(P.K, p, pi);
+    float u[3] = {0.f, 0.f, 0.f};
+    transform_add<D, KIND, SWAP>(P, p, pi, u);
+#pragma unroll
+    for (int d = 0; d < D; ++d) mp[d] += (double)u[d];
+    to_local<D>(P.mov, mp, ml);
+}
+
+// ---- value pass ------------------------------------------------------------------------------
+template <int D, int KIND>
+__global__ void __launch_bounds__(256) value_kernel(EvalParams P, float4 *__restrict__ samp,
+                                                    double *__restrict__ part)
+{
+    __shared__ double sh[NQ * 32];
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) v[k] = 0.0;
+    if (t < P.Ns) {
+        int sp[3];
+        float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (sample_pos<D>(P, t, sp)) {
+            double fi[3] = {(double)sp[0], (double)sp[1], (double)sp[2]}, p[3], ml[3];
+            to_global<D>(P.fixed, fi, p);
+            moving_local<D, KIND, false>(P, p, ml);
+            if (bspline_inside<D>(P.mov, ml)) {
+                float m, g[3] = {0.f, 0.f, 0.f};
+                bspline_derivs<D>(P.coeffs, P.mov, ml, m, g);
+                double f = (double)P.fixed_data[lin_of<D>(P.fixed, sp)];
+                double md = (double)m;
+                v[Q_COUNT] = 1.0;
+                v[Q_D2] = (md - f) * (md - f);
+                v[Q_SF] = f;
+                v[Q_SM] = md;
+                v[Q_SFF] = f * f;
+                v[Q_SMM] = md * md;
+                v[Q_SFM] = f * md;
+                rec = make_float4(g[0], g[1], D > 2 ? g[2] : 0.f, m);
+            }
+        }
+        samp[t] = rec;
+    }
+    block_sum<NQ>(v, sh);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) part[(long long)k * gridDim.x + blockIdx.x] = v[k];
+}
+
+// ---- statistics (GpuEvaluator.cu:449-571 host loops, on the device, FP64, fixed order) ------
+__global__ void __launch_bounds__(1024) stats_kernel(const double *__restrict__ part, int nblocks, int metric,
+                                                     double *__restrict__ stats)
+{
+    __shared__ double sh[NQ * 32];
+    double v[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += part[(long long)k * nblocks + b];
+        v[k] = s;
+    }
+    block_sum<NQ>(v, sh);
+    if (threadIdx.x == 0) {
+        double n = v[Q_COUNT];
+        double st[NS];
+        for (int k = 0; k < NS; ++k) st[k] = 0.0;
+        st[S_COUNT] = n;
+        if (metric == 0) {
+            st[S_MEASURE] = v[Q_D2] / n;                       // cu:462-470
+            st[S_COEF_F] = -2.0 / n;                           // 2*(m-f)/n  (MSE.cu:291, cu:599-603)
+            st[S_COEF_M] = 2.0 / n;
+            st[S_COEF_C] = 0.0;
+        } else if (metric == 1) {
+            double sf = v[Q_SF], sm = v[Q_SM];
+            double sff = v[Q_SFF] - sf * sf / n;               // cu:519-524
+            double smm = v[Q_SMM] - sm * sm / n;
+            double sfm = v[Q_SFM] - sf * sm / n;
+            double denom = -1.0 * sqrt(sff * smm);
+            st[S_MEASURE] = denom != 0.0 ? sfm / denom : 0.0;
+            st[S_MEAN_F] = sf / n;
+            st[S_MEAN_M] = sm / n;
+            st[S_DENOM] = denom;
+            st[S_SFM] = sfm;
+            st[S_SMM] = smm;
+            // (dF - (sfm/smm) dM)/denom with dF = sum (f - mf) w k gradM, dM = sum (m - mm) w k gradM
+            // (NCC.cu:177-179, cu:624-633) == w sum k gradM (a f + b m + c)
+            if (denom != 0.0) {
+                double rho = sfm / smm;
+                st[S_COEF_F] = 1.0 / denom;
+                st[S_COEF_M] = -rho / denom;
+                st[S_COEF_C] = (-st[S_MEAN_F] + rho * st[S_MEAN_M]) / denom;
+            }
+        } else {
+            st[S_MEASURE] = v[Q_CC] / n;                       // cu:556-570
+            st[S_COEF_C] = 1.0 / n;                            // derivatives /= pixelsCounted (cu:642-646)
+        }
+        st[S_VALID] = 1.0;
+        for (int k = 0; k < NS; ++k) stats[k] = st[k];
+    }
+}
+
+// ---- derivative pass: warp per control point ------------------------------------------------
+// Sample box of a control point (MSE.cu:255-263 / NCC.cu:138-146 for 3-D MSE/NCC;
+// MSE.cu:273-280 and LCC.cu:236-244 / 722-729 for 2-D and LCC): truncation toward zero,
+// clamped to the (subsampled) grid.
+template <int D>
+__device__ __forceinline__ void derivative_box(const EvalParams &P, bool wide, const double *ip, double support,
+                                               int *lo, int *hi)
+{
+    lo[1] = hi[1] = lo[2] = hi[2] = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        double sh = support / P.fixed.s[d];
+        if (P.sub != 1) {
+            double fs = (double)(float)P.sub;
+            if (wide) {
+                lo[d] = (int)((ip[d] - sh) / fs);
+                hi[d] = (int)((ip[d] + sh) / fs + 1.0);
+            } else {
+                lo[d] = (int)((ip[d] - sh) / fs + 1.0);
+                hi[d] = (int)((ip[d] + sh) / fs);
+            }
+            lo[d] = clampi(lo[d], 0, P.ss[d] - 1);
+            hi[d] = clampi(hi[d], 0, P.ss[d] - 1);
+        } else {
+            if (wide) {
+                lo[d] = (int)(ip[d] - sh);
+                hi[d] = (int)(ip[d] + sh + 1.0);
+            } else {
+                lo[d] = (int)(ip[d] - sh + 1.0);
+                hi[d] = (int)(ip[d] + sh);
+            }
+            lo[d] = clampi(lo[d], 0, P.fixed.n[d] - 1);
+            hi[d] = clampi(hi[d], 0, P.fixed.n[d] - 1);
+        }
+    }
+}
+
+// Regularizers of control point j over its control-point box (GpuEvaluatorRegularizers.cu),
+// lanes striding the box.  Values accumulate in double, gradients in float.
+template <int D, int KIND>
+__device__ __forceinline__ void regularizers_of(const EvalParams &P, const DerivParams &Q, const int *j,
+                                                long long jl, const double *gp, const PInfo &pj, float4 cj, int lane,
+                                                double *val, float *der_rkhs, float *der_rd, float *der_pg)
+{
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        double sh = pj.support / P.cp.s[d];
+        lo[d] = clampi((int)((double)j[d] - sh + 1.0), 0, P.cp.n[d] - 1);
+        hi[d] = clampi((int)((double)j[d] + sh), 0, P.cp.n[d] - 1);
+    }
+    const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+    const int total = nx * ny * nz;
+    const float wj = cj.w;
+    const float cjv[3] = {cj.x, cj.y, cj.z};
+    const bool rkhs = Q.reg_rkhs > 0.0, rd = Q.reg_rd > 0.0, pg = Q.reg_pg > 0.0;
+    const float pgs = (float)Q.pg_scaling;
+    for (int t = lane; t < total; t += 32) {
+        int x = lo[0] + t % nx;
+        int y = lo[1] + (t / nx) % ny;
+        int z = lo[2] + t / (nx * ny);
+        int ii[3] = {x, y, z};
+        float v[3];
+#pragma unroll
+        for (int d = 0; d < D; ++d) v[d] = -(float)P.cp.s[d] * (float)(ii[d] - j[d]);
+        float k;
+        if (KIND == kStationary) {
+            k = k_eval<KIND, D>(P.K, v, nullptr, pj);
+        } else {
+            double qi[3] = {(double)x, (double)y, (double)z}, q[3];
+            to_global<D>(P.cp, qi, q);
+            k = k_eval<KIND, D>(P.K, v, q, pj);
+        }
+        if (k == 0.0f) continue;
+        float4 ci4 = __ldg(P.cpd + lin_of<D>(P.cp, ii));
+        float ci[3] = {ci4.x, ci4.y, ci4.z};
+        float kw = k * wj;
+        if (rkhs) {                                            // Regularizers.cu:68-73
+            double dot = 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) dot += (double)cjv[d] * (double)ci[d];
+            val[R_RKHS] += (double)kw * dot;
+#pragma unroll
+            for (int d = 0; d < D; ++d) der_rkhs[d] = fmaf(2.0f * kw, ci[d], der_rkhs[d]);
+        }
+        if (rd) {                                              // Regularizers.cu:141-144
+            double l2 = 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                double e = (double)cjv[d] - (double)ci[d];
+                l2 += e * e;
+            }
+            val[R_RD] += l2 * (double)kw;
+#pragma unroll
+            for (int d = 0; d < D; ++d) der_rd[d] = fmaf(4.0f * kw, cjv[d] - ci[d], der_rd[d]);
+        }
+        if (pg) {
+            if (D == 3) {                                      // Regularizers.cu:218-237
+                float cr0 = ci[1] * cjv[2] - ci[2] * cjv[1];
+                float cr1 = ci[2] * cjv[0] - ci[0] * cjv[2];
+                float cr2 = ci[0] * cjv[1] - ci[1] * cjv[0];
+                double n2 = (double)cr0 * cr0 + (double)cr1 * cr1 + (double)cr2 * cr2;
+                double s = (double)pgs;
+                val[R_PG] += (double)kw * s * s / 2.0 * log(1.0 + n2 / s);
+                float den = 2.0f * ((float)n2 / pgs + 1.0f);
+                float dp0 = 2.0f * ci[2] * (ci[2] * cjv[0] - ci[0] * cjv[2]) - 2.0f * ci[1] * (ci[0] * cjv[1] - ci[1] * cjv[0]);
+                float dp1 = 2.0f * ci[0] * (ci[0] * cjv[1] - ci[1] * cjv[0]) - 2.0f * ci[2] * (ci[1] * cjv[2] - ci[2] * cjv[1]);
+                float dp2 = 2.0f * ci[1] * (ci[1] * cjv[2] - ci[2] * cjv[1]) - 2.0f * ci[0] * (ci[2] * cjv[0] - ci[0] * cjv[2]);
+                der_pg[0] = fmaf(2.0f * kw, pgs * dp0 / den, der_pg[0]);
+                der_pg[1] = fmaf(2.0f * kw, pgs * dp1 / den, der_pg[1]);
+                der_pg[2] = fmaf(2.0f * kw, pgs * dp2 / den, der_pg[2]);
+            } else {                                           // Regularizers.cu:447-459
+                float val2d = ci[0] * cjv[1] - ci[1] * cjv[0];
+                double v2 = (double)val2d * val2d;
+                double s = (double)pgs;
+                val[R_PG] += (double)kw * s * s / 2.0 * log(1.0 + v2 / s);
+                float factor = (float)v2 / pgs + 1.0f;
+                der_pg[0] = fmaf(2.0f * kw, -pgs * ci[1] * val2d / factor, der_pg[0]);
+                der_pg[1] = fmaf(2.0f * kw, pgs * ci[0] * val2d / factor, der_pg[1]);
+            }
+        }
+    }
+}
+
+// LCC window statistics and derivative accumulators of one sample (LCC.cu:296-530).
+template <int D, int KIND>
+__device__ __forceinline__ void lcc_sample_derivative(const EvalParams &P, const DerivParams &Q, const double *gp,
+                                                      const double *pt, float *der)
+{
+    PInfo ps;
+    pinfo_at<KIND, D>(P.K, pt, ps);
+    double fl[3];
+    to_local<D>(P.fixed, pt, fl);
+    int flo[3] = {0, 0, 0}, fhi[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        double sh = ps.support / P.fixed.s[d];
+        flo[d] = clampi((int)(fl[d] - sh + 1.0), 0, P.fixed.n[d] - 1);
+        fhi[d] = clampi((int)(fl[d] + sh), 0, P.fixed.n[d] - 1);
+    }
+    const bool swapped = (D == 3 && KIND != kStationary);
+    const float4 *dense = swapped ? Q.dense_sw : Q.dense;
+    const unsigned char *dense_in = swapped ? Q.dense_sw_in : Q.dense_in;
+    double sf = 0, sm = 0, sff = 0, smm = 0, sfm = 0;
+    double mkcka[3] = {0, 0, 0}, mkcmkcka[3] = {0, 0, 0}, fkcmka[3] = {0, 0, 0};
+    int n = 0;
+    for (int z = flo[2]; z <= fhi[2]; z += P.nbh)
+        for (int y = flo[1]; y <= fhi[1]; y += P.nbh)
+            for (int x = flo[0]; x <= fhi[0]; x += P.nbh) {
+                int ni[3] = {x, y, z};
+                double nf[3] = {(double)x, (double)y, (double)z}, q[3];
+                to_global<D>(P.fixed, nf, q);
+                PInfo pn;
+                pinfo_at<KIND, D>(P.K, q, pn);
+                // neighborhoodWeight with the neighbour's support passed as float (LCC.cu:28-35)
+                double sup = (double)(float)pn.support;
+                double r2 = 0.0;
+#pragma unroll
+                for (int d = 0; d < D; ++d) r2 += (pt[d] - q[d]) * (pt[d] - q[d]);
+                double t = r2 / (sup * sup);
+                double t2 = t * t;
+                double rr = t2 * t2 * t;                       // (r/support)^10
+                double kwf = 1.0 - rr;
+                if (kwf <= 0.0) continue;
+                double kw = kwf * kwf;
+                long long nl = lin_of<D>(P.fixed, ni);
+                if (!dense_in[nl]) continue;
+                // ka = k(cp, n) with the neighbour's kernel information (LCC.cu:449-461)
+                float v[3];
+#pragma unroll
+                for (int d = 0; d < D; ++d) v[d] = (float)(gp[d] - q[d]);
+                float ka = k_eval<KIND, D>(P.K, v, q, pn);
+                float4 rec = dense[nl];
+                double mv = (double)rec.w * kw;
+                double fv = kw * (double)P.fixed_data[nl];
+                sf += fv; sm += mv; sff += fv * fv; smm += mv * mv; sfm += fv * mv;
+                double g[3] = {rec.x, rec.y, rec.z};
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    double gk = g[d] * kw * (double)ka;
+                    mkcmkcka[d] += mv * gk;
+                    mkcka[d] += gk;
+                    fkcmka[d] += fv * gk;
+                }
+                ++n;
+            }
+    if (n > 0) {
+        double msf = sf / n, msm = sm / n;
+        double d1 = sff - 2.0 * msf * sf + n * msf * msf;
+        double u = d1 * (smm - 2.0 * msm * sm + n * msm * msm);
+        double vv = sfm - msm * sf - msf * sm + n * msf * msm;
+        if (fabs(u) > 1e-16) {
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                double vd = 2.0 * vv * (fkcmka[d] - msf * mkcka[d]);
+                double ud = 2.0 * d1 * (mkcmkcka[d] - msm * mkcka[d]);
+                der[d] += (float)(-(vd * u - ud * (vv * vv)) / (u * u));
+            }
+        }
+    }
+}
+
+template <int D, int KIND>
+__global__ void __launch_bounds__(256) derivative_kernel(EvalParams P, DerivParams Q)
+{
+    __shared__ double shv[NR][8];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long j_lin = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    double val[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) val[k] = 0.0;
+    if (j_lin < P.C) {
+        int j[3];
+        cell_of<D>(P.cp.n, j_lin, j);
+        double jf[3] = {(double)j[0], (double)j[1], (double)j[2]}, gp[3], ip[3];
+        to_global<D>(P.cp, jf, gp);
+        const float4 cj = __ldg(P.cpd + j_lin);
+        PInfo pj;
+        pinfo_at<KIND, D>(P.K, gp, pj);
+        float acc[3] = {0.f, 0.f, 0.f};
+        const double *st = Q.stats;
+        if (Q.metric != 2) {
+            const bool wide = (D == 3);
+            to_local<D>(P.fixed, gp, ip);
+            int lo[3], hi[3];
+            derivative_box<D>(P, wide, ip, pj.support, lo, hi);
+            const float cf = (float)st[S_COEF_F], cm = (float)st[S_COEF_M], cc = (float)st[S_COEF_C];
+            const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+            const int per_plane = nx * ny;
+            const int sub = P.sub;
+            // offsets relative to the first sample cell of the box
+            int base_pos[3] = {lo[0] * sub, lo[1] * sub, lo[2] * sub};
+            float base[3], hs[3];
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                base[d] = (float)(gp[d] - (P.fixed.o[d] + P.fixed.s[d] * (double)base_pos[d]));
+                hs[d] = (float)P.fixed.s[d];
+            }
+            for (int zz = 0; zz < nz; ++zz) {
+                const int z = lo[2] + zz;
+                int x = lane % nx, y = lane / nx;              // lane position in the (y,x) plane
+                for (int t = lane; t < per_plane; t += 32) {
+                    const int cx = lo[0] + x, cy = lo[1] + y;
+                    long long idx;
+                    int pos[3] = {cx, cy, z};
+                    if (sub != 1) {
+                        idx = cx + (long long)P.ss[0] * (cy + (long long)P.ss[1] * z);
+                        uint32_t s = __ldg(P.shifts + idx);
+#pragma unroll
+                        for (int d = 0; d < D; ++d) pos[d] = pos[d] * sub + (int)((s >> (8 * d)) & 0xffu);
+                    } else {
+                        idx = lin_of<D>(P.fixed, pos);
+                    }
+                    float4 rec = __ldg(Q.samp + idx);
+                    if (rec.x != 0.f || rec.y != 0.f || rec.z != 0.f) {
+                        float v[3];
+                        v[0] = base[0] - hs[0] * (float)(pos[0] - base_pos[0]);
+                        if (D > 1) v[1] = base[1] - hs[1] * (float)(pos[1] - base_pos[1]);
+                        if (D > 2) v[2] = base[2] - hs[2] * (float)(pos[2] - base_pos[2]);
+                        float k;
+                        if (KIND == kStationary) {
+                            k = k_eval<KIND, D>(P.K, v, nullptr, pj);
+                        } else {
+                            double pf[3] = {(double)pos[0], (double)pos[1], (double)pos[2]}, q[3];
+                            to_global<D>(P.fixed, pf, q);
+                            k = k_eval<KIND, D>(P.K, v, q, pj);
+                        }
+                        if (k != 0.0f) {
+                            float f = __ldg(P.fixed_data + lin_of<D>(P.fixed, pos));
+                            float coef = fmaf(cf, f, fmaf(cm, rec.w, cc)) * k;
+                            acc[0] = fmaf(coef, rec.x, acc[0]);
+                            acc[1] = fmaf(coef, rec.y, acc[1]);
+                            if (D > 2) acc[2] = fmaf(coef, rec.z, acc[2]);
+                        }
+                    }
+                    x += 32;
+                    while (x >= nx) { x -= nx; ++y; }
+                }
+            }
+        } else {
+            // LCC: lanes over the samples of the box, each lane walks its sample's window
+            to_local<D>(P.fixed, gp, ip);
+            int lo[3], hi[3];
+            derivative_box<D>(P, false, ip, pj.support, lo, hi);
+            const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+            const int total = nx * ny * nz;
+            for (int t = lane; t < total; t += 32) {
+                int cell[3] = {lo[0] + t % nx, lo[1] + (t / nx) % ny, lo[2] + t / (nx * ny)};
+                int pos[3] = {cell[0], cell[1], cell[2]};
+                if (P.sub != 1) {
+                    long long idx = cell[0] + (long long)P.ss[0] * (cell[1] + (long long)P.ss[1] * cell[2]);
+                    uint32_t s = __ldg(P.shifts + idx);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) pos[d] = cell[d] * P.sub + (int)((s >> (8 * d)) & 0xffu);
+                }
+                double pf[3] = {(double)pos[0], (double)pos[1], (double)pos[2]}, pt[3];
+                to_global<D>(P.fixed, pf, pt);
+                lcc_sample_derivative<D, KIND>(P, Q, gp, pt, acc);
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) acc[d] = warp_sum(acc[d]);
+
+        float drk[3] = {0.f, 0.f, 0.f}, drd[3] = {0.f, 0.f, 0.f}, dpg[3] = {0.f, 0.f, 0.f};
+        if (Q.reg_rkhs > 0.0 || Q.reg_rd > 0.0 || Q.reg_pg > 0.0) {
+            regularizers_of<D, KIND>(P, Q, j, j_lin, gp, pj, cj, lane, val, drk, drd, dpg);
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                drk[d] = warp_sum(drk[d]);
+                drd[d] = warp_sum(drd[d]);
+                dpg[d] = warp_sum(dpg[d]);
+            }
+#pragma unroll
+            for (int k = R_RKHS; k <= R_PG; ++k) val[k] = warp_sum(val[k]);
+        }
+        if (lane == 0) {
+            const double n = st[S_COUNT];
+            double pc[3] = {0, 0, 0}, pn2 = 0.0;
+            if (Q.with_metric) {
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    pc[d] = Q.params[j_lin + d * P.C];
+                    pn2 += pc[d] * pc[d];
+                }
+            }
+            const double pnorm = sqrt(pn2);
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                double g;
+                if (Q.metric == 1)
+                    g = st[S_DENOM] != 0.0 ? (double)cj.w * (double)acc[d] : 0.0;
+                else if (Q.metric == 0)
+                    g = (double)cj.w * (double)acc[d];
+                else
+                    g = (double)acc[d] / n;                    // LCC derivative omits w_i (LCC.cu:518)
+                if (Q.reg_rkhs > 0.0) g += (double)drk[d] * Q.reg_rkhs;
+                if (Q.reg_rd > 0.0) g += (double)drd[d] * Q.reg_rd;
+                if (Q.reg_pg > 0.0) g += (double)dpg[d] * Q.reg_pg;
+                if (Q.with_metric) {
+                    const double par = pc[d];
+                    if (Q.reg_l1 > 0.0) {                      // metric hxx:447-466
+                        const double w = Q.reg_l1;
+                        if (fabs(par) > 0.0) g += w * (par < 0.0 ? -1.0 : 1.0);
+                        else if (g < -w) g += w;
+                        else if (g > w) g -= w;
+                        else g = 0.0;
+                    }
+                    if (Q.reg_l2 > 0.0) g += Q.reg_l2 * 2.0 * par;   // hxx:482-485
+                    if (Q.reg_l21 > 0.0) {                     // hxx:504-521
+                        const double w = Q.reg_l21;
+                        if (pnorm > 0.0) g += w * par / pnorm;
+                        else if (g < -w) g += w;
+                        else if (g > w) g -= w;
+                        else g = 0.0;
+                    }
+                    if (Q.negate) g = -g;
+                }
+                Q.deriv[j_lin + d * P.C] = g;
+            }
+            if (Q.with_metric) {
+                double l1 = 0.0;
+#pragma unroll
+                for (int d = 0; d < D; ++d) l1 += fabs(pc[d]);
+                val[R_L1] = l1;
+                val[R_L2] = pn2;
+                val[R_L21] = pnorm;
+            }
+        }
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NR; ++k) shv[k][wib] = val[k];
+    __syncthreads();
+    if (threadIdx.x < NR) {
+        double s = 0.0;
+        const int nw = blockDim.x >> 5;
+        for (int w = 0; w < nw; ++w) s += shv[threadIdx.x][w];
+        Q.rpart[(long long)threadIdx.x * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// Regularizer values only (getValue, GpuEvaluator.cu:300-353) over the control-point grid.
+template <int D, int KIND>
+__global__ void __launch_bounds__(256) regvalue_kernel(EvalParams P, DerivParams Q)
+{
+    __shared__ double shv[NR][8];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long j_lin = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    double val[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) val[k] = 0.0;
+    if (j_lin < P.C) {
+        int j[3];
+        cell_of<D>(P.cp.n, j_lin, j);
+        double jf[3] = {(double)j[0], (double)j[1], (double)j[2]}, gp[3];
+        to_global<D>(P.cp, jf, gp);
+        const float4 cj = __ldg(P.cpd + j_lin);
+        PInfo pj;
+        pinfo_at<KIND, D>(P.K, gp, pj);
+        float drk[3] = {0.f, 0.f, 0.f}, drd[3] = {0.f, 0.f, 0.f}, dpg[3] = {0.f, 0.f, 0.f};
+        regularizers_of<D, KIND>(P, Q, j, j_lin, gp, pj, cj, lane, val, drk, drd, dpg);
+#pragma unroll
+        for (int k = R_RKHS; k <= R_PG; ++k) val[k] = warp_sum(val[k]);
+        if (lane == 0 && Q.with_metric) {
+            double l1 = 0.0, n2 = 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                double par = Q.params[j_lin + d * P.C];
+                l1 += fabs(par);
+                n2 += par * par;
+            }
+            val[R_L1] = l1;
+            val[R_L2] = n2;
+            val[R_L21] = sqrt(n2);
+        }
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NR; ++k) shv[k][wib] = val[k];
+    __syncthreads();
+    if (threadIdx.x < NR) {
+        double s = 0.0;
+        const int nw = blockDim.x >> 5;
+        for (int w = 0; w < nw; ++w) s += shv[threadIdx.x][w];
+        Q.rpart[(long long)threadIdx.x * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// final scalars: measure, regularizer values, weighted sum (metric hxx:531-538, 572)
+__global__ void __launch_bounds__(256) result_kernel(const double *__restrict__ stats, const double *__restrict__ rpart,
+                                                     int nblocks, double w_rkhs, double w_rd, double w_pg, double w_l1,
+                                                     double w_l21, double w_l2, double *__restrict__ out)
+{
+    __shared__ double sh[NR * 32];
+    double v[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+        double s = 0.0;
+        if (rpart)
+            for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += rpart[(long long)k * nblocks + b];
+        v[k] = s;
+    }
+    block_sum<NR>(v, sh);
+    if (threadIdx.x == 0) {
+        double reg = 0.0;
+        if (w_l1 > 0) reg += w_l1 * v[R_L1];
+        if (w_l21 > 0) reg += w_l21 * v[R_L21];
+        if (w_l2 > 0) reg += w_l2 * v[R_L2];
+        if (w_rkhs > 0) reg += w_rkhs * v[R_RKHS];
+        if (w_rd > 0) reg += w_rd * v[R_RD];
+        if (w_pg > 0) reg += w_pg * v[R_PG];
+        out[O_MEASURE] = stats[S_MEASURE];
+        out[O_RKHS] = v[R_RKHS];
+        out[O_RD] = v[R_RD];
+        out[O_PG] = v[R_PG];
+        out[O_L1] = v[R_L1];
+        out[O_L21] = v[R_L21];
+        out[O_L2] = v[R_L2];
+        out[O_REG] = reg;
+        out[O_VALUE] = stats[S_MEASURE] + reg;
+        out[O_COUNT] = stats[S_COUNT];
+    }
+}
+
+// ---- LCC: dense fields and per-sample values --------------------------------------------------
+// (grad M, m) and the inside flag at every fixed texel: the neighbour transforms of the
+// reference's LCC windows (LCC.cu:112-176) evaluated once per texel instead of per window.
+template <int D, int KIND, bool SWAP>
+__global__ void __launch_bounds__(256) dense_kernel(EvalParams P, float4 *__restrict__ dense,
+                                                    unsigned char *__restrict__ dense_in)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long N = (long long)P.fixed.n[0] * P.fixed.n[1] * P.fixed.n[2];
+    if (t >= N) return;
+    int c[3];
+    cell_of<D>(P.fixed.n, t, c);
+    double fi[3] = {(double)c[0], (double)c[1], (double)c[2]}, p[3], ml[3];
+    to_global<D>(P.fixed, fi, p);
+    moving_local<D, KIND, SWAP>(P, p, ml);
+    float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
+    unsigned char in = 0;
+    if (bspline_inside<D>(P.mov, ml)) {
+        float m, g[3] = {0.f, 0.f, 0.f};
+        bspline_derivs<D>(P.coeffs, P.mov, ml, m, g);
+        rec = make_float4(g[0], g[1], D > 2 ? g[2] : 0.f, m);
+        in = 1;
+    }
+    dense[t] = rec;
+    dense_in[t] = in;
+}
+
+// LCC value per sample (LCC.cu:38-204) from the dense fields.
+template <int D, int KIND>
+__global__ void __launch_bounds__(256) lcc_value_kernel(EvalParams P, const float4 *__restrict__ dense,
+                                                        const unsigned char *__restrict__ dense_in,
+                                                        double *__restrict__ part)
+{
+    __shared__ double sh[NQ * 32];
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) v[k] = 0.0;
+    if (t < P.Ns) {
+        int sp[3];
+        if (sample_pos<D>(P, t, sp)) {
+            double fi[3] = {(double)sp[0], (double)sp[1], (double)sp[2]}, p[3];
+            to_global<D>(P.fixed, fi, p);
+            long long pl = lin_of<D>(P.fixed, sp);
+            v[Q_COUNT] = dense_in[pl] ? 1.0 : 0.0;
+            PInfo pi;
+            pinfo_at<KIND, D>(P.K, p, pi);
+            double fl[3];
+            to_local<D>(P.fixed, p, fl);
+            int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                double shf = pi.support / P.fixed.s[d];
+                lo[d] = clampi((int)(fl[d] - shf + 1.0), 0, P.fixed.n[d] - 1);
+                hi[d] = clampi((int)(fl[d] + shf), 0, P.fixed.n[d] - 1);
+            }
+            double sf = 0, sm = 0, sff = 0, smm = 0, sfm = 0;
+            int n = 0;
+            for (int z = lo[2]; z <= hi[2]; z += P.nbh)
+                for (int y = lo[1]; y <= hi[1]; y += P.nbh)
+                    for (int x = lo[0]; x <= hi[0]; x += P.nbh) {
+                        int ni[3] = {x, y, z};
+                        double nf[3] = {(double)x, (double)y, (double)z}, q[3];
+                        to_global<D>(P.fixed, nf, q);
+                        double sup;
+                        if (KIND == kStationary) {
+                            sup = (double)P.K.support_min;
+                        } else {
+                            PInfo pn;
+                            pinfo_at<KIND, D>(P.K, q, pn);
+                            sup = (double)(float)pn.support;
+                        }
+                        double r2 = 0.0;
+#pragma unroll
+                        for (int d = 0; d < D; ++d) r2 += (p[d] - q[d]) * (p[d] - q[d]);
+                        double tt = r2 / (sup * sup);
+                        double t2 = tt * tt;
+                        double kwf = 1.0 - t2 * t2 * tt;
+                        if (kwf <= 0.0) continue;
+                        double kw = kwf * kwf;
+                        long long nl = lin_of<D>(P.fixed, ni);
+                        if (!dense_in[nl]) continue;
+                        double mv = (double)dense[nl].w * kw;
+                        double fv = kw * (double)P.fixed_data[nl];
+                        sf += fv; sm += mv; sff += fv * fv; smm += mv * mv; sfm += fv * mv;
+                        ++n;
+                    }
+            if (n > 0) {
+                double msf = sf / n, msm = sm / n;
+                double d1 = sff - 2.0 * msf * sf + n * msf * msf;
+                double d2 = smm - 2.0 * msm * sm + n * msm * msm;
+                if (d1 > 0 && d2 > 0) {
+                    double cc = sfm - msm * sf - msf * sm + n * msf * msm;
+                    v[Q_CC] = -cc * cc / (d1 * d2);
+                }
+            }
+        }
+    }
+    block_sum<NQ>(v, sh);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) part[(long long)k * gridDim.x + blockIdx.x] = v[k];
+}
+
+// ---- displacement field (DisplacementField.cu:24-127) -----------------------------------------
+template <int D, int KIND>
+__global__ void __launch_bounds__(256) displacement_kernel(EvalParams P, double *__restrict__ out)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long N = (long long)P.fixed.n[0] * P.fixed.n[1] * P.fixed.n[2];
+    if (t >= N) return;
+    int c[3];
+    cell_of<D>(P.fixed.n, t, c);
+    double fi[3] = {(double)c[0], (double)c[1], (double)c[2]}, p[3];
+    to_global<D>(P.fixed, fi, p);
+    double u[3] = {0.0, 0.0, 0.0};
+    if (P.has_df) {
+        long long i = nearest_index<D>(P.df, p);
+        if (i >= 0) {
+            float4 v = P.dfd[i];
+            u[0] = v.x; u[1] = v.y; u[2] = v.z;
+        }
+    }
+    PInfo pi;
+    pinfo_at<KIND, D>(P.K, p, pi);
+    float uf[3] = {0.f, 0.f, 0.f};
+    transform_add<D, KIND, false>(P, p, pi, uf);
+#pragma unroll
+    for (int d = 0; d < D; ++d) out[t * D + d] = u[d] + (double)uf[d];
+}
+
+// ---- small helpers ----------------------------------------------------------------------------
+// pack AoS doubles (alpha) + weights into float4 records
+__global__ void pack_cp_aos(const double *__restrict__ cp, const double *__restrict__ cpw, long long C, int D,
+                            float4 *__restrict__ out)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) return;
+    float4 r;
+    r.x = (float)cp[i * D];
+    r.y = (float)cp[i * D + 1];
+    r.z = D > 2 ? (float)cp[i * D + 2] : 0.f;
+    r.w = (float)cpw[i];
+    out[i] = r;
+}
+
+// pack planar parameters (metric level, itkTransformAdapter.hxx:202-236) + weights
+__global__ void pack_cp_planar(const double *__restrict__ params, const double *__restrict__ cpw, long long C, int D,
+                               float4 *__restrict__ out)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) return;
+    float4 r;
+    r.x = (float)params[i];
+    r.y = (float)params[i + C];
+    r.z = D > 2 ? (float)params[i + 2 * C] : 0.f;
+    r.w = (float)cpw[i];
+    out[i] = r;
+}
+
+// grid shifts of the PCG32 stream (GpuEvaluator.cu:107-118): texel t takes draws D*t..D*t+D-1
+// counted from `state`; shift = int(nextI/double(UINT_MAX) * subsample).
+__global__ void shifts_kernel(unsigned long long state, RngJump J, long long Ns, int D, int sub,
+                              uint32_t *__restrict__ shifts)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= Ns) return;
+    unsigned long long s = lcg_advance(state, (unsigned long long)t * D, J);
+    uint32_t packed = 0;
+    for (int d = 0; d < D; ++d) {
+        unsigned out = pcg32_output(s);
+        s = s * 6364136223846793005ULL + 1ULL;
+        double f = (double)out / 4294967295.0;
+        int sh = (int)(f * (double)sub);
+        packed |= (uint32_t)sh << (8 * d);
+    }
+    shifts[t] = packed;
+}
+
+}  // namespace skm

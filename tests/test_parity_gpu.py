@@ -1,0 +1,156 @@
+"""CUDA evaluation path (through the C-ABI) against the FP64 oracle.
+
+Tolerances (stated against the FP64 oracle, FP32 arithmetic on the device):
+  * transform / displacement field: max |u - u_ref| <= 1e-5 * max |u_ref|
+  * metric values and regularizer values: relative error <= 1e-5
+  * derivatives: max |g - g_ref| <= 1e-4 * max |g_ref|
+  * pixel counts: exact
+"""
+import numpy as np
+import pytest
+
+from helpers import make_problem, max_rel, rel_err
+from oracle import oracle as O
+from skmimageregistration_b200 import abi
+from skmimageregistration_b200.abi import MetricDesc, OptimizerDesc
+from skmimageregistration_b200.evaluator import GpuKernelEvaluator, Optimizer, bspline_coefficients
+
+pytestmark = pytest.mark.gpu
+
+TOL_FIELD = 1e-5
+TOL_VALUE = 1e-5
+TOL_DERIV = 1e-4
+
+KINDS = ["stationary", "weight_image", "weight_tensor"]
+
+
+def _df_for(pb, seed=3):
+    rng = np.random.default_rng(seed)
+    return rng.normal(0, 0.7, (pb.n_texels, pb.D))
+
+
+@pytest.mark.parametrize("D", [2, 3])
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("with_df", [False, True])
+def test_displacement_field(D, kind, with_df):
+    pb, cp, cpw = make_problem(D, kind, seed=11)
+    df = _df_for(pb) if with_df else None
+    ev = GpuKernelEvaluator(pb)
+    got = ev.evaluateDisplacementField(cp, cpw, df)
+    ref = O.Oracle(pb).displacement_field(cp, cpw, df)
+    assert max_rel(got, ref) <= TOL_FIELD
+
+
+@pytest.mark.parametrize("D", [2, 3])
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("metric", [abi.MSE, abi.NCC])
+@pytest.mark.parametrize("sub", [1, 3])
+def test_value_and_derivative(D, kind, metric, sub):
+    pb, cp, cpw = make_problem(D, kind, subsample=sub, seed=5 + sub)
+    ev = GpuKernelEvaluator(pb)
+    orc = O.Oracle(pb)
+    df = _df_for(pb, 7)
+    for call in range(2):            # second call redraws the sample shifts
+        r, g = ev.getValueAndDerivative(metric, cp, cpw, df)
+        ro, go = orc.evaluate(metric, cp, cpw, df)
+        assert r["num_pixels_counted"] == ro["num_pixels_counted"]
+        assert rel_err(r["measure"], ro["measure"]) <= TOL_VALUE, (r, ro)
+        assert max_rel(g, go) <= TOL_DERIV
+
+
+@pytest.mark.parametrize("D", [2, 3])
+@pytest.mark.parametrize("metric", [abi.MSE, abi.NCC])
+def test_get_value_matches_value_and_derivative(D, metric):
+    """GetValue == GetValueAndDerivative value (itkFiniteDifferenceTest.cpp:188-217)."""
+    pb, cp, cpw = make_problem(D, seed=21)
+    ev = GpuKernelEvaluator(pb)
+    ev.SetRegularizerRD(1e-2)
+    v = ev.getValue(metric, cp, cpw)
+    r, _ = ev.getValueAndDerivative(metric, cp, cpw)
+    assert v["measure"] == r["measure"]
+    assert v["reg_value_rd"] == pytest.approx(r["reg_value_rd"], rel=1e-12)
+
+
+@pytest.mark.parametrize("D", [2, 3])
+@pytest.mark.parametrize("kind", KINDS)
+def test_regularizers(D, kind):
+    pb, cp, cpw = make_problem(D, kind, seed=31)
+    ev = GpuKernelEvaluator(pb)
+    orc = O.Oracle(pb)
+    ev.SetRegularizerRKHS(0.3)
+    ev.SetRegularizerRD(0.2, 1.0)
+    ev.SetRegularizerPG(0.1, 0.7)
+    orc.set_regularizers(0.3, 0.2, 1.0, 0.1, 0.7)
+    r, g = ev.getValueAndDerivative(abi.NCC, cp, cpw)
+    ro, go = orc.evaluate(abi.NCC, cp, cpw)
+    for k in ("measure", "reg_value_rkhs", "reg_value_rd", "reg_value_pg"):
+        assert rel_err(r[k], ro[k]) <= TOL_VALUE, k
+    assert max_rel(g, go) <= TOL_DERIV
+
+
+@pytest.mark.parametrize("D", [2, 3])
+@pytest.mark.parametrize("kind", ["stationary", "weight_image"])
+def test_lcc(D, kind):
+    shape = (10, 11, 12) if D == 3 else (24, 26)
+    pb, cp, cpw = make_problem(D, kind, subsample=2, nbh=2, shape=shape, seed=41, sigma_c4=3.0, sigma_c0=6.0,
+                               cp_spacing=1.5)
+    ev = GpuKernelEvaluator(pb)
+    orc = O.Oracle(pb)
+    r, g = ev.getValueAndDerivative(abi.LCC, cp, cpw)
+    ro, go = orc.evaluate(abi.LCC, cp, cpw)
+    assert r["num_pixels_counted"] == ro["num_pixels_counted"]
+    assert rel_err(r["measure"], ro["measure"]) <= TOL_VALUE
+    assert max_rel(g, go) <= TOL_DERIV
+
+
+@pytest.mark.parametrize("D", [2, 3])
+def test_metric_level(D):
+    pb, cp, cpw = make_problem(D, seed=51)
+    params = np.ascontiguousarray(cp.T.reshape(-1))
+    params[::7] = 0.0                                   # exercise the zero-parameter subgradient branches
+    ev = GpuKernelEvaluator(pb)
+    orc = O.Oracle(pb)
+    for m in (MetricDesc.make("ncc", l1=1e-3, l21=2e-3, l2=1e-3, rd=1e-2),
+              MetricDesc.make("mse", l1=5e-4, rkhs=1e-2, pg=1e-3, pg_scaling=0.5)):
+        v, g = ev.metric(m, params, cpw)
+        vo, go = orc.metric(m, params, cpw)
+        for k in ("value", "measure", "reg_value", "reg_l1", "reg_l21", "reg_l2"):
+            assert rel_err(v[k], vo[k]) <= TOL_VALUE, k
+        assert max_rel(g, go) <= TOL_DERIV
+
+
+def test_bspline_prefilter_gpu():
+    rng = np.random.default_rng(3)
+    for shape in [(9, 10, 11), (13, 17)]:
+        img = rng.uniform(0, 1, shape)
+        np.testing.assert_allclose(bspline_coefficients(img), O.bspline_coefficients(img), rtol=0, atol=1e-12)
+
+
+def test_deterministic():
+    pb, cp, cpw = make_problem(3, seed=61)
+    ev = GpuKernelEvaluator(pb)
+    ev.SetRegularizerRD(1e-2)
+    r1, g1 = ev.getValueAndDerivative(abi.NCC, cp, cpw)
+    r2, g2 = ev.getValueAndDerivative(abi.NCC, cp, cpw)
+    assert r1 == r2
+    assert np.array_equal(g1, g2)
+
+
+@pytest.mark.parametrize("D", [2, 3])
+def test_optimizer_matches_oracle(D):
+    pb, _, cpw = make_problem(D, seed=71, weights=False)
+    P = pb.num_parameters
+    m = MetricDesc.make("ncc", rd=1e-3)
+    o = OptimizerDesc.make(a=2.0, number_of_iterations=6)
+    ev = GpuKernelEvaluator(pb)
+    opt = Optimizer(ev, o, m, np.zeros(P), cpw)
+    oo = O.OracleOptimizer(O.Oracle(pb), o, m, np.zeros(P), cpw)
+    for it in range(3):
+        opt.run(2)
+        vals = oo.run(2)
+        st = opt.state()
+        assert st["iteration"] == oo.state.iteration
+        assert rel_err(st["value"], vals[-1]) <= 1e-4
+        assert rel_err(st["current_time"], oo.state.current_time) <= 1e-3 or abs(oo.state.current_time) < 1e-9
+        assert max_rel(opt.parameters(), oo.position) <= 1e-3
+    assert max_rel(opt.parameters(best=True), oo.best) <= 1e-3
