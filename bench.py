@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Benchmark: SKM optimizer iterations per second on one or more B200s.
+
+One step = one iteration of the adaptive-step gradient-descent optimizer on the
+``ncc128`` workload (128x128x96 pair, 24,576 control points, kernel support 12
+voxels, NCC + RD regularizer 1e-3, every voxel sampled): transform + B-spline warp +
+NCC statistics + control-point derivative + regularizer + parameter update.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+* ``value``: device-resident loop (parameters and optimizer state stay in HBM, one CUDA
+  graph per iteration); each timed iteration is bracketed by CUDA events on the
+  evaluator's stream, with an L2 flush (256 MB write) before every iteration outside
+  the events.  N > 1: one independent pair per GPU (weak scaling), value = all
+  iterations / slowest rank's time.
+* ``e2e``: the reference-facing C-ABI call with host buffers, the way the ITK glue
+  drives it: per step the planar parameters and weights go host->device, value and
+  derivative come back device->host, and the optimizer update runs on the host.
+* ``cpu_baseline`` / ``--impl reference``: the FP64 CPU restatement of the same
+  evaluation (oracle/, OpenMP over all host cores); the reference itself has no CPU
+  implementation of this path.  The reference arm additionally times the reference's
+  own CUDA evaluator (built from its sources for sm_100a) when it is available.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ncc128")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps (capped at 300)")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def measured_peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def fp32_peak_tflops(torch):
+    """CUDA-core FP32 peak measured live: cuBLAS SGEMM 8192^3 with TF32 off, best of 5."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.backends.cudnn.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    b = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    best = None
+    for _ in range(6):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        ms = s.elapsed_time(e)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def pair_count(pb):
+    """(fixed texel, control point) pairs inside the forward box (separable per axis)."""
+    tot = 1
+    support = min(pb.sigma_c4, pb.sigma_c0)
+    for d in range(pb.D):
+        n = pb.size[d]
+        idx = np.arange(n)
+        p = pb.origin[d] + pb.spacing[d] * idx
+        ip = (p - pb.cp_origin[d]) / pb.cp_sp[d]
+        sh = support / pb.cp_sp[d]
+        lo = np.clip(np.trunc(ip - sh + 1.0), 0, pb.cp_size[d] - 1)
+        hi = np.clip(np.trunc(ip + sh), 0, pb.cp_size[d] - 1)
+        tot *= int((hi - lo + 1).sum())
+    return tot
+
+
+# ------------------------------------------------------------------------------------------------
+def cpu_port_rate(pb, mdesc, budget_s=20.0, max_steps=5, min_steps=1, threads=None):
+    """FP64 CPU restatement: full-size metric evaluations + host update, steps/s."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count()
+    O.set_num_threads(threads)
+    orc = O.Oracle(pb)
+    P = pb.num_parameters
+    params = np.zeros(P)
+    cpw = np.ones(pb.C)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        _, g = orc.metric(mdesc, params, cpw)
+        params = params + 1e-3 * g
+        steps += 1
+        el = time.perf_counter() - t0
+        if steps >= max_steps or (steps >= min_steps and el >= budget_s):
+            break
+    return steps / el, steps, el, threads
+
+
+def reference_cuda_rate(pb, mdesc, budget_s=20.0, max_steps=50):
+    """The reference's own GpuKernelEvaluator (oracle/_ref, double build), driven like its ITK glue."""
+    from oracle import oracle as O
+    path = O.ref_gpu_path(pb.D, True)
+    if not os.path.exists(path):
+        return None
+    ref = O.RefGpu(pb, double=True)
+    ref.set_regularizers(mdesc.reg_rkhs, mdesc.reg_rd, mdesc.reg_rd_scaling, mdesc.reg_pg, mdesc.reg_pg_scaling)
+    P = pb.num_parameters
+    cp = np.zeros((pb.C, pb.D))
+    cpw = np.ones(pb.C)
+    ref.evaluate(mdesc.metric, cp, cpw)                     # warm-up
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        _, g = ref.evaluate(mdesc.metric, cp, cpw)
+        cp = cp - 1e-3 * g.reshape(pb.D, -1).T                # negated gradient step (metric hxx:528)
+        steps += 1
+        el = time.perf_counter() - t0
+        if steps >= max_steps or el >= budget_s:
+            break
+    ref.close()
+    return steps / el, steps, el
+
+
+# ------------------------------------------------------------------------------------------------
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    from skmimageregistration_b200 import workloads
+    from oracle import oracle as O
+    pb, m, o, info = workloads.make(args.workload, seed=0, coefficients=O.bspline_coefficients)
+    # each step is one full-size FP64 evaluation + update; bounded to ~2 minutes in total
+    warm = min(args.warmup, 1)
+    if warm:
+        cpu_port_rate(pb, m, budget_s=0.0, max_steps=warm)
+    rate, steps, el, threads = cpu_port_rate(pb, m, budget_s=90.0, max_steps=max(1, min(args.steps, 40)),
+                                             min_steps=1)
+    line = {
+        "metric": "optimizer_iterations_per_s", "value": rate, "unit": "iter/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1e3 / rate,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(info, timing="CPU wall clock per full-size evaluation + update"),
+        "cpu_baseline": {"value": rate, "unit": "iter/s", "cores": threads, "kind": "port",
+                         "sample": "%d full-size 128x128x96 NCC+RD evaluations (FP64 restatement, OpenMP)" % steps},
+        "e2e": {"value": rate, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    try:
+        import torch
+        if torch.cuda.is_available():
+            r = reference_cuda_rate(pb, m)
+            if r is not None:
+                line["reference_cuda_evaluator"] = {
+                    "value": r[0], "unit": "iter/s", "steps": r[1],
+                    "note": "reference GpuKernelEvaluator (double build, -use_fast_math, sm_100a) driven like "
+                            "its ITK glue; host loop, wall clock"}
+    except Exception as exc:                                 # reported, not fatal
+        line["reference_cuda_evaluator"] = {"unavailable": str(exc)[:200]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from skmimageregistration_b200 import workloads
+    from skmimageregistration_b200.evaluator import GpuKernelEvaluator, Optimizer
+
+    torch.cuda.set_device(local_rank)
+    pb, mdesc, odesc, info = workloads.make(args.workload, seed=rank)
+    P = pb.num_parameters
+    cpw = np.ones(pb.C)
+    ev = GpuKernelEvaluator(pb)
+    opt = Optimizer(ev, odesc, mdesc, np.zeros(P), cpw)
+    stream = torch.cuda.ExternalStream(opt.enqueue(0))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # warm-up
+    opt.enqueue(args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    time.sleep(0.25)
+    with torch.cuda.stream(stream):
+        for i in range(args.steps):
+            flush.fill_(float(i))                   # evict L2 (256 MB > 126 MB) outside the events
+            starts[i].record(stream)
+            opt.enqueue(1)
+            ends[i].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * args.steps / (ms * 1e-3)
+    kernels_per_iter = opt.graph_kernel_count()
+
+    # per-phase timing (CUDA events on the evaluator's stream, same iteration un-graphed)
+    prof_iters = min(max(args.steps, 20), 200)
+    phases = opt.profile(prof_iters)
+    state = opt.state()
+
+    # e2e: reference-facing C-ABI call with host buffers + host-side optimizer update
+    e2e_steps = args.e2e_steps or min(args.steps, 300)
+    ev2 = GpuKernelEvaluator(pb)
+    params = np.zeros(P)
+    base = np.zeros(P)
+    prev = np.zeros(P)
+    t_sim = 0.0
+    ev2.metric(mdesc, params, cpw)                  # warm-up
+    e2e_s = 0.0
+    for i in range(e2e_steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(i))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        v, g = ev2.metric(mdesc, params, cpw)
+        # AdaptiveStepGradientDescentOptimizerv4 update on the host (ITK glue path)
+        lr = odesc.a / (odesc.A + t_sim + 1.0) ** odesc.alpha
+        sp = float(g @ prev)
+        prev = g
+        params = base + g * lr
+        base = params
+        x = -sp
+        t_sim = max(0.0, t_sim + odesc.f_min + (odesc.f_max - odesc.f_min) /
+                    (1.0 - (odesc.f_max / odesc.f_min) * math.exp(-x / odesc.omega)))
+        e2e_s += time.perf_counter() - t0
+    e2e_rate = e2e_steps / e2e_s
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_rate = world * e2e_steps / float(t.item())
+    h2d = (P + pb.C) * 8
+    d2h = P * 8 + 10 * 8
+
+    line = None
+    if rank == 0:
+        hbm_peak, hbm_src = measured_peaks()
+        fp32_peak = fp32_peak_tflops(torch)
+        pairs = pair_count(pb)
+        dom = max(("value", "derivative"), key=lambda k: phases[k])
+        Fk = 22.0
+        flops = {"value": pairs * (Fk + 7.0) + pb.n_texels * 2 * 64 * 4,
+                 "derivative": pairs * (Fk + 6.0 * 2 + 1.0)}
+        bytes_alg = {"value": pb.n_texels * 4 + pb.moving_coefficients.size * 4 + pb.C * 16 + pb.n_texels * 16,
+                     "derivative": pb.n_texels * (16 + 4) + pb.C * 16 + P * 8}
+        dom_ms = phases[dom]
+        achieved = flops[dom] / (dom_ms * 1e-3) / 1e12
+        hbm_ach = bytes_alg[dom] / (dom_ms * 1e-3) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic_%s.json" % args.workload)
+        if os.path.exists(tpath):
+            try:
+                traffic = json.load(open(tpath)).get(dom)
+            except Exception:
+                traffic = None
+        line = {
+            "metric": "optimizer_iterations_per_s", "value": value, "unit": "iter/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded %s pair per GPU)" % args.workload,
+            "config": dict(info, parallelism="pair-parallel x%d (independent replicas, no collective)" % world,
+                           l2="flushed before every timed iteration (256 MB write outside the events)",
+                           timing="CUDA events on the evaluator stream around each graph-replayed iteration",
+                           arithmetic="FP32 kernel sums, FP64 global sums"),
+            "clocks": clocks,
+            "gpu_launches": kernels_per_iter * args.steps,
+            "kernels_per_iteration": kernels_per_iter,
+            "phases_ms": phases,
+            "final_state": state,
+            "roofline": {
+                "kernel": "derivative_kernel" if dom == "derivative" else "value_kernel",
+                "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": traffic,
+                "peak_source": "cuBLAS SGEMM 8192^3, TF32 off, measured live in this run",
+                "algorithmic_flops_per_launch": flops[dom], "pairs_per_launch": pairs,
+                "hbm": {"achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_ach / hbm_peak,
+                        "algorithmic_bytes_per_launch": bytes_alg[dom], "peak_source": hbm_src},
+            },
+            "e2e": {"value": e2e_rate, "unit": "iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps},
+        }
+    opt.close()
+    ev.close()
+    ev2.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O  # noqa: F401  (CPU baseline leg only)
+        rate, steps, el, threads = cpu_port_rate(pb, mdesc, budget_s=15.0, max_steps=5)
+        line["cpu_baseline"] = {"value": rate, "unit": "iter/s", "cores": threads, "kind": "port",
+                                "sample": "%d full-size evaluations + update, FP64 restatement, %.1f s" % (steps, el)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

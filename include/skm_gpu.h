@@ -235,6 +235,12 @@ int skm_optimizer_run(skm_optimizer *o, int32_t iterations);
 /* Enqueue up to `iterations` more iterations on the evaluator's stream without waiting;
  * if stream_out is not NULL it receives that cudaStream_t (for event timing). */
 int skm_optimizer_enqueue(skm_optimizer *o, int32_t iterations, void *stream_out);
+/* Runs up to `iterations` iterations outside the graph with CUDA events between the
+ * phases; phase_ms[0..6] receives the mean milliseconds of: parameter packing, grid
+ * shifts, value pass, statistics, derivative + regularizers, result, optimizer update. */
+int skm_optimizer_profile(skm_optimizer *o, int32_t iterations, double *phase_ms, int32_t nphase);
+/* Number of kernel launches in one captured iteration. */
+int skm_optimizer_graph_kernel_count(skm_optimizer *o, int32_t *count);
 /* Current position, or the best one if best != 0 (ReturnBestParametersAndValue). */
 int skm_optimizer_get_parameters(skm_optimizer *o, int32_t best, double *parameters);
 int skm_optimizer_get_state(skm_optimizer *o, skm_optimizer_state *out);

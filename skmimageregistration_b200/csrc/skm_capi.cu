@@ -509,7 +509,10 @@ struct RegWeights {
 };
 
 // The full device sequence of one evaluation (everything after the parameter upload).
-static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const RegWeights &w, const double *params)
+// ev (optional, 4 events): recorded after the value pass, the statistics, the derivative pass and
+// the result kernel, for per-phase timing.
+static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const RegWeights &w, const double *params,
+                          cudaEvent_t *ev = nullptr)
 {
     int rc = SKM_OK;
     const int D = e->D, kind = e->P.K.kind;
@@ -522,8 +525,10 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
         else rc = dispatch<LaunchValue>(D, kind, e);
         if (rc) return rc;
     }
+    if (ev) SKM_CUDA(cudaEventRecord(ev[0], e->stream));
     stats_kernel<<<1, 1024, 0, e->stream>>>(e->d_part, e->value_blocks, metric, e->d_stats);
     SKM_CHECK_LAUNCH();
+    if (ev) SKM_CUDA(cudaEventRecord(ev[1], e->stream));
     DerivParams Q{};
     Q.metric = metric;
     Q.with_metric = w.with_metric;
@@ -554,9 +559,11 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     } else if (any_reg) {
         if ((rc = dispatch<LaunchRegValue>(D, kind, e, Q))) return rc;
     }
+    if (ev) SKM_CUDA(cudaEventRecord(ev[2], e->stream));
     result_kernel<<<1, 256, 0, e->stream>>>(e->d_stats, (derivative || any_reg) ? e->d_rpart : nullptr,
                                            e->deriv_blocks, w.rkhs, w.rd, w.pg, w.l1, w.l21, w.l2, e->d_out);
     SKM_CHECK_LAUNCH();
+    if (ev) SKM_CUDA(cudaEventRecord(ev[3], e->stream));
     return SKM_OK;
 }
 

@@ -636,9 +636,10 @@ __global__ void __launch_bounds__(256) derivative_kernel(EvalParams P, DerivPara
                 double l1 = 0.0;
 #pragma unroll
                 for (int d = 0; d < D; ++d) l1 += fabs(pc[d]);
-                val[R_L1] = l1;
-                val[R_L2] = pn2;
-                val[R_L21] = pnorm;
+                // each term is computed only when its weight is positive (metric hxx:431,469,491)
+                val[R_L1] = Q.reg_l1 > 0.0 ? l1 : 0.0;
+                val[R_L2] = Q.reg_l2 > 0.0 ? pn2 : 0.0;
+                val[R_L21] = Q.reg_l21 > 0.0 ? pnorm : 0.0;
             }
         }
     }
@@ -684,9 +685,9 @@ __global__ void __launch_bounds__(256) regvalue_kernel(EvalParams P, DerivParams
                 l1 += fabs(par);
                 n2 += par * par;
             }
-            val[R_L1] = l1;
-            val[R_L2] = n2;
-            val[R_L21] = sqrt(n2);
+            val[R_L1] = Q.reg_l1 > 0.0 ? l1 : 0.0;
+            val[R_L2] = Q.reg_l2 > 0.0 ? n2 : 0.0;
+            val[R_L21] = Q.reg_l21 > 0.0 ? sqrt(n2) : 0.0;
         }
     }
     if (lane == 0)

@@ -111,13 +111,17 @@ struct skm_optimizer {
     }
 };
 
-// launches of one optimizer iteration (captured into the graph)
-static int optimizer_iteration(skm_optimizer *o)
+// launches of one optimizer iteration (captured into the graph).  ev (optional, 8 events):
+// start, after pack, after shifts, after value, after statistics, after derivative, after result,
+// after the update -- used by skm_optimizer_profile.
+static int optimizer_iteration(skm_optimizer *o, cudaEvent_t *ev = nullptr)
 {
     skm_evaluator *e = o->e;
     const long long C = e->C;
+    if (ev) SKM_CUDA(cudaEventRecord(ev[0], e->stream));
     pack_cp_planar<<<(int)((C + 255) / 256), 256, 0, e->stream>>>(o->d_pos, o->d_cpw, C, e->D, e->d_cpd);
     SKM_CHECK_LAUNCH();
+    if (ev) SKM_CUDA(cudaEventRecord(ev[1], e->stream));
     if (e->P.sub > 1 && o->md.do_resampling) {
         shifts_dev_kernel<<<(int)((e->Ns + 255) / 256), 256, 0, e->stream>>>(o->d_rng, e->jump, e->Ns, e->D, e->P.sub,
                                                                             e->d_shifts);
@@ -136,7 +140,8 @@ static int optimizer_iteration(skm_optimizer *o)
     w.l2 = o->md.reg_l2;
     w.with_metric = 1;
     w.negate = o->md.use_negative_gradient;
-    int rc = run_evaluation(e, o->md.metric, true, w, o->d_pos);
+    if (ev) SKM_CUDA(cudaEventRecord(ev[2], e->stream));
+    int rc = run_evaluation(e, o->md.metric, true, w, o->d_pos, ev ? ev + 3 : nullptr);
     if (rc) return rc;
     opt_step_kernel<<<o->step_blocks, 256, 0, e->stream>>>(e->d_deriv, o->d_tmp, o->d_base, o->d_pos, o->d_best,
                                                           o->d_scal, e->d_out, o->P, o->od.orthant_projection, o->od.a,
@@ -145,6 +150,7 @@ static int optimizer_iteration(skm_optimizer *o)
     opt_finish_kernel<<<1, 32, 0, e->stream>>>(o->d_sp, o->step_blocks, o->d_scal, e->d_out, o->od.a, o->od.A,
                                               o->od.alpha, o->od.f_max, o->od.f_min, o->od.omega);
     SKM_CHECK_LAUNCH();
+    if (ev) SKM_CUDA(cudaEventRecord(ev[7], e->stream));
     return SKM_OK;
 }
 
@@ -274,5 +280,59 @@ extern "C" int skm_optimizer_destroy(skm_optimizer *o)
 {
     if (o && o->e) cudaSetDevice(o->e->device);
     delete o;
+    return SKM_OK;
+}
+
+// Runs up to `iterations` iterations un-graphed with CUDA events between the phases and
+// returns the mean time per phase in milliseconds: [pack, shifts, value pass, statistics,
+// derivative+regularizers, result, update].  The iterations advance the optimizer like
+// skm_optimizer_run.
+extern "C" int skm_optimizer_profile(skm_optimizer *o, int32_t iterations, double *phase_ms, int32_t nphase)
+{
+    if (!o) return fail(SKM_ERR_STATE, "optimizer is NULL");
+    if (!phase_ms || nphase < 7) return fail(SKM_ERR_INVALID, "phase_ms needs 7 entries");
+    skm_evaluator *e = o->e;
+    SKM_CUDA(cudaSetDevice(e->device));
+    int n = std::min<int>(iterations, o->od.number_of_iterations - o->iteration);
+    cudaEvent_t ev[8];
+    for (int i = 0; i < 8; ++i) SKM_CUDA(cudaEventCreate(&ev[i]));
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    int rc = SKM_OK;
+    for (int it = 0; it < n && !rc; ++it) {
+        rc = optimizer_iteration(o, ev);
+        if (rc) break;
+        cudaError_t ce = cudaEventSynchronize(ev[7]);
+        if (ce != cudaSuccess) {
+            rc = fail(SKM_ERR_CUDA, "profile: %s", cudaGetErrorString(ce));
+            break;
+        }
+        // ev: 0 start, 1 pack, 2 shifts, 3 value, 4 stats, 5 derivative, 6 result, 7 update
+        for (int p = 0; p < 7; ++p) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[p], ev[p + 1]);
+            acc[p] += ms;
+        }
+        o->iteration++;
+    }
+    for (int i = 0; i < 8; ++i) cudaEventDestroy(ev[i]);
+    for (int p = 0; p < 7; ++p) phase_ms[p] = n > 0 ? acc[p] / n : 0.0;
+    return rc;
+}
+
+// Number of kernel launches in one captured optimizer iteration.
+extern "C" int skm_optimizer_graph_kernel_count(skm_optimizer *o, int32_t *count)
+{
+    if (!o || !o->graph) return fail(SKM_ERR_STATE, "optimizer has no graph");
+    size_t n = 0;
+    SKM_CUDA(cudaGraphGetNodes(o->graph, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    SKM_CUDA(cudaGraphGetNodes(o->graph, nodes.data(), &n));
+    int k = 0;
+    for (size_t i = 0; i < n; ++i) {
+        cudaGraphNodeType t;
+        SKM_CUDA(cudaGraphNodeGetType(nodes[i], &t));
+        if (t == cudaGraphNodeTypeKernel) ++k;
+    }
+    *count = k;
     return SKM_OK;
 }

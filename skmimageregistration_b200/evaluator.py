@@ -60,6 +60,8 @@ def lib():
                                            C.POINTER(Field), C.POINTER(C.c_void_p)]
         L.skm_optimizer_run.argtypes = [C.c_void_p, C.c_int32]
         L.skm_optimizer_enqueue.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.skm_optimizer_profile.argtypes = [C.c_void_p, C.c_int32, _dp, C.c_int32]
+        L.skm_optimizer_graph_kernel_count.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
         L.skm_optimizer_get_parameters.argtypes = [C.c_void_p, C.c_int32, _dp]
         L.skm_optimizer_get_state.argtypes = [C.c_void_p, C.POINTER(OptimizerState)]
         L.skm_optimizer_destroy.argtypes = [C.c_void_p]
@@ -195,6 +197,19 @@ class Optimizer:
         s = C.c_void_p()
         check(lib().skm_optimizer_enqueue(self.h, int(iterations), C.byref(s)))
         return s.value
+
+    PHASES = ("pack", "shifts", "value", "stats", "derivative", "result", "update")
+
+    def profile(self, iterations):
+        """Mean milliseconds per phase over `iterations` un-graphed iterations."""
+        out = np.zeros(7)
+        check(lib().skm_optimizer_profile(self.h, int(iterations), dptr(out), 7))
+        return dict(zip(self.PHASES, out.tolist()))
+
+    def graph_kernel_count(self):
+        n = C.c_int32()
+        check(lib().skm_optimizer_graph_kernel_count(self.h, C.byref(n)))
+        return n.value
 
     def parameters(self, best=False):
         out = np.zeros(self.ev.problem.num_parameters)
