@@ -254,6 +254,35 @@ int skm_optimizer_destroy(skm_optimizer *o);
 int skm_bspline_coefficients(int32_t dimensions, const int32_t *size,
                              const double *image, double *coefficients);
 
+/* ------------------------------------------------------------------------- */
+/* Metric value without any device allocation.  No counterpart in the reference.
+ *
+ * For callers that must not allocate device memory at evaluation time: frameworks that
+ * own the whole device memory budget, real-time loops that cannot afford the implicit
+ * device synchronisation of cudaMalloc/cudaFree, or code that plans every buffer up
+ * front.  The caller passes device buffers for the inputs and for the result; the call
+ * allocates nothing (no cudaMalloc, no allocating library routine) and only launches
+ * kernels on `stream` (a cudaStream_t, NULL = default stream), returning without
+ * waiting.  Intermediate partial sums live in one fixed array inside the library
+ * (458,752 bytes, held by every device that loads the library until the process exits).
+ *
+ *   fixed_image          device, float, prod(fixed size) texels
+ *   moving_coefficients  device, float, prod(moving size + 3) B-spline coefficients
+ *   control_points       device, 4 floats per control point: alpha x, y, z (0 in 2-D), weight
+ *   result               device, 2 doubles: measure, number of pixels counted
+ *
+ * Same value as skm_get_value for a stationary kernel, subsample 1, no displacement
+ * field, MSE or NCC.  Limit: at most 2,097,152 fixed-image texels; larger images are
+ * rejected with SKM_ERR_INVALID.  Every call on a device shares the array and leaves its
+ * contents behind (each call overwrites what it reads), so calls that overlap on the GPU
+ * race.  The first call on each device looks up the array's device address; make that
+ * first call before any stream capture.  Errors are reported through skm_last_error(). */
+int skm_value_noalloc(int32_t dimensions, int32_t metric,
+                      const skm_geometry *fixed_geometry, const float *fixed_image,
+                      const skm_geometry *moving_geometry, const float *moving_coefficients,
+                      const skm_geometry *cp_geometry, const float *control_points,
+                      double sigma_c0, double sigma_c4, double *result, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

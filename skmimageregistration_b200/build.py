@@ -13,8 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libskm_b200.so")
-SOURCES = ["csrc/skm_capi.cu"]
-DEPS = ["csrc/skm_capi.cu", "csrc/skm_device.cuh", "csrc/skm_kernels.cuh", "csrc/skm_prefilter.cuh",
+SOURCES = ["csrc/skm_capi.cu", "csrc/skm_noalloc.cu"]
+DEPS = ["csrc/skm_capi.cu", "csrc/skm_noalloc.cu", "csrc/skm_device.cuh", "csrc/skm_kernels.cuh", "csrc/skm_prefilter.cuh",
         "csrc/skm_table.cuh", "csrc/skm_optimizer.cuh", "../include/skm_gpu.h"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",

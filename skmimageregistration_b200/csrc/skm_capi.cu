@@ -234,6 +234,9 @@ struct LaunchDisp {
 
 // ------------------------------------------------------------------------------------------------
 extern "C" const char *skm_last_error(void) { return g_last_error.c_str(); }
+
+// lets other translation units of the library report through skm_last_error()
+void skm_internal_set_error(const char *msg) { g_last_error = msg; }
 extern "C" int32_t skm_abi_version(void) { return SKM_ABI_VERSION; }
 
 static int validate_desc(const skm_evaluator_desc *d)

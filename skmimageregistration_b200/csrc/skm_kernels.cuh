@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(256) value_kernel(EvalParams P, float4 *__rest
 }
 
 // ---- statistics (GpuEvaluator.cu:449-571 host loops, on the device, FP64, fixed order) ------
-__global__ void __launch_bounds__(1024) stats_kernel(const double *__restrict__ part, int nblocks, int metric,
+static __global__ void __launch_bounds__(1024) stats_kernel(const double *__restrict__ part, int nblocks, int metric,
                                                      double *__restrict__ stats)
 {
     __shared__ double sh[NQ * 32];
@@ -703,7 +703,7 @@ __global__ void __launch_bounds__(256) regvalue_kernel(EvalParams P, DerivParams
 }
 
 // final scalars: measure, regularizer values, weighted sum (metric hxx:531-538, 572)
-__global__ void __launch_bounds__(256) result_kernel(const double *__restrict__ stats, const double *__restrict__ rpart,
+static __global__ void __launch_bounds__(256) result_kernel(const double *__restrict__ stats, const double *__restrict__ rpart,
                                                      int nblocks, double w_rkhs, double w_rd, double w_pg, double w_l1,
                                                      double w_l21, double w_l2, double *__restrict__ out)
 {
@@ -871,7 +871,7 @@ __global__ void __launch_bounds__(256) displacement_kernel(EvalParams P, double 
 
 // ---- small helpers ----------------------------------------------------------------------------
 // pack AoS doubles (alpha) + weights into float4 records
-__global__ void pack_cp_aos(const double *__restrict__ cp, const double *__restrict__ cpw, long long C, int D,
+static __global__ void pack_cp_aos(const double *__restrict__ cp, const double *__restrict__ cpw, long long C, int D,
                             float4 *__restrict__ out)
 {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -885,7 +885,7 @@ __global__ void pack_cp_aos(const double *__restrict__ cp, const double *__restr
 }
 
 // pack planar parameters (metric level, itkTransformAdapter.hxx:202-236) + weights
-__global__ void pack_cp_planar(const double *__restrict__ params, const double *__restrict__ cpw, long long C, int D,
+static __global__ void pack_cp_planar(const double *__restrict__ params, const double *__restrict__ cpw, long long C, int D,
                                float4 *__restrict__ out)
 {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -900,7 +900,7 @@ __global__ void pack_cp_planar(const double *__restrict__ params, const double *
 
 // grid shifts of the PCG32 stream (GpuEvaluator.cu:107-118): texel t takes draws D*t..D*t+D-1
 // counted from `state`; shift = int(nextI/double(UINT_MAX) * subsample).
-__global__ void shifts_kernel(unsigned long long state, RngJump J, long long Ns, int D, int sub,
+static __global__ void shifts_kernel(unsigned long long state, RngJump J, long long Ns, int D, int sub,
                               uint32_t *__restrict__ shifts)
 {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
