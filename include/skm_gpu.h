@@ -130,6 +130,13 @@ int32_t     skm_abi_version(void);
 int skm_evaluator_create(const skm_evaluator_desc *desc, skm_evaluator **out);
 int skm_evaluator_destroy(skm_evaluator *ev);
 
+/* Kernel path selection (no counterpart in the reference, which has one path).
+ * request: -1 query only, 0 automatic (phase-table path where it applies), 1 generic
+ * kernels only.  *active (may be NULL) receives the path MSE/NCC calls take:
+ * 1 generic, 2 phase table (stationary kernel, control spacing an integer multiple of
+ * the fixed spacing, subsample 1).  Both paths compute the same sums. */
+int skm_evaluator_path(skm_evaluator *ev, int32_t request, int32_t *active);
+
 /* GpuKernelEvaluator::SetRegularizerRKHS/RD/PG (GpuEvaluator.h:156-158,
  * GpuEvaluator.cu:786-831).  weight <= 0 switches the term off. */
 int skm_set_regularizer_rkhs(skm_evaluator *ev, double weight);

@@ -121,7 +121,7 @@ struct skm_evaluator {
     skm_geometry fixed_geo{}, cp_geo{};
     int nparams = 0;
     long long N = 0, Ns = 0, C = 0;
-    int value_blocks = 0, deriv_blocks = 0, dense_blocks = 0;
+    int value_blocks = 0, deriv_blocks = 0, dense_blocks = 0, gather_blocks = 0;
 
     // device memory
     float *d_fixed = nullptr, *d_coeffs = nullptr, *d_wimg = nullptr, *d_wten = nullptr;
@@ -334,6 +334,7 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         e->value_blocks = (int)((ns + kValueThreads - 1) / kValueThreads);
         e->deriv_blocks = (int)((e->C + (kDerivThreads / 32) - 1) / (kDerivThreads / 32));
         e->dense_blocks = (int)((e->N + 255) / 256);
+        e->gather_blocks = (int)((e->C + 255) / 256);
 
         // kernel parameters: GKernel<float> members are floats (Kernel.h:216-221)
         KernelParams &K = P.K;
@@ -390,13 +391,15 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         if (dalloc(&e->d_part, (size_t)NQ * e->value_blocks)) return SKM_ERR_CUDA;
         if (dalloc(&e->d_stats, NS)) return SKM_ERR_CUDA;
         if (dalloc(&e->d_deriv, e->nparams)) return SKM_ERR_CUDA;
-        if (dalloc(&e->d_rpart, (size_t)NR * e->deriv_blocks)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_rpart, (size_t)NR * std::max(e->deriv_blocks, e->gather_blocks))) return SKM_ERR_CUDA;
         if (dalloc(&e->d_out, NO)) return SKM_ERR_CUDA;
         SKM_CUDA(cudaMallocHost((void **)&e->h_in, sizeof(double) * e->C * (D + 1)));
         SKM_CUDA(cudaMallocHost((void **)&e->h_out, sizeof(double) * (e->nparams + NO)));
         rng_jump_table(e->jump);
         int trc = table_plan(e->table, e->P, D, e->stream);
-        if (trc) return trc;
+        if (trc) return fail(SKM_ERR_CUDA, "table plan failed: %s", cudaGetErrorString(cudaGetLastError()));
+        if (e->table.enabled && table_set_attributes(e->table))
+            return fail(SKM_ERR_CUDA, "table kernel attributes: %s", cudaGetErrorString(cudaGetLastError()));
         return SKM_OK;
     }();
     if (rc) {
@@ -410,6 +413,16 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
 extern "C" int skm_evaluator_destroy(skm_evaluator *e)
 {
     delete e;
+    return SKM_OK;
+}
+
+extern "C" int skm_evaluator_path(skm_evaluator *e, int32_t request, int32_t *active)
+{
+    if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
+    if (request == 1) e->use_table = false;
+    else if (request == 0) e->use_table = true;
+    else if (request != -1) return fail(SKM_ERR_INVALID, "path request must be -1, 0 or 1");
+    if (active) *active = (e->use_table && e->table.enabled) ? 2 : 1;
     return SKM_OK;
 }
 
@@ -522,14 +535,21 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     if (metric == SKM_LCC) {
         if ((rc = ensure_dense(e))) return rc;
         if ((rc = dispatch<LaunchLccValue>(D, kind, e))) return rc;
-    } else {
-        bool tab = e->use_table && e->table.enabled;
-        if (tab) rc = table_value(e->table, e->P, e->d_samp, e->d_part, e->value_blocks, e->stream);
-        else rc = dispatch<LaunchValue>(D, kind, e);
-        if (rc) return rc;
+    }
+    const bool tab = e->use_table && e->table.enabled && metric != SKM_LCC;
+    if (metric != SKM_LCC) {
+        if (tab) {
+            if (table_value(e->table, e->P, D, e->stream))
+                return fail(SKM_ERR_CUDA, "table value pass: %s", cudaGetErrorString(cudaGetLastError()));
+        } else if ((rc = dispatch<LaunchValue>(D, kind, e))) {
+            return rc;
+        }
     }
     if (ev) SKM_CUDA(cudaEventRecord(ev[0], e->stream));
-    stats_kernel<<<1, 1024, 0, e->stream>>>(e->d_part, e->value_blocks, metric, e->d_stats);
+    if (tab)
+        stats_kernel<<<1, 1024, 0, e->stream>>>(e->table.d_part, e->table.dev.value_blocks, metric, e->d_stats);
+    else
+        stats_kernel<<<1, 1024, 0, e->stream>>>(e->d_part, e->value_blocks, metric, e->d_stats);
     SKM_CHECK_LAUNCH();
     if (ev) SKM_CUDA(cudaEventRecord(ev[1], e->stream));
     DerivParams Q{};
@@ -555,16 +575,19 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     Q.rpart = e->d_rpart;
     bool any_reg = w.rkhs > 0 || w.rd > 0 || w.pg > 0 || w.with_metric;
     if (derivative) {
-        bool tab = e->use_table && e->table.enabled && metric != SKM_LCC;
-        if (tab) rc = table_derivative(e->table, e->P, Q, e->deriv_blocks, e->stream);
-        else rc = dispatch<LaunchDeriv>(D, kind, e, Q);
-        if (rc) return rc;
+        if (tab) {
+            if (table_derivative(e->table, e->P, Q, D, e->gather_blocks, e->stream))
+                return fail(SKM_ERR_CUDA, "table derivative: %s", cudaGetErrorString(cudaGetLastError()));
+        } else if ((rc = dispatch<LaunchDeriv>(D, kind, e, Q))) {
+            return rc;
+        }
     } else if (any_reg) {
         if ((rc = dispatch<LaunchRegValue>(D, kind, e, Q))) return rc;
     }
     if (ev) SKM_CUDA(cudaEventRecord(ev[2], e->stream));
-    result_kernel<<<1, 256, 0, e->stream>>>(e->d_stats, (derivative || any_reg) ? e->d_rpart : nullptr,
-                                           e->deriv_blocks, w.rkhs, w.rd, w.pg, w.l1, w.l21, w.l2, e->d_out);
+    const int rblocks = (derivative && tab) ? e->gather_blocks : e->deriv_blocks;
+    result_kernel<<<1, 256, 0, e->stream>>>(e->d_stats, (derivative || any_reg) ? e->d_rpart : nullptr, rblocks,
+                                           w.rkhs, w.rd, w.pg, w.l1, w.l21, w.l2, e->d_out);
     SKM_CHECK_LAUNCH();
     if (ev) SKM_CUDA(cudaEventRecord(ev[3], e->stream));
     return SKM_OK;

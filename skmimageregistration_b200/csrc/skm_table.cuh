@@ -1,23 +1,727 @@
-// skm_table.cuh -- phase-table fast path (stationary kernel on commensurate grids).
-// Not planned for this evaluator: every call takes the generic kernels.
+// skm_table.cuh -- phase-table fast path: stationary kernel on commensurate grids.
+//
+// When the control-point spacing is an integer multiple h_d of the fixed-image spacing and
+// every texel is sampled, a texel x = h*a + p (phase p in [0,h)^D) lies at cp-index
+// coordinate  q + phi(p)  with an integer cell q and a fractional offset phi that depends on
+// the phase only.  The kernel value between texel (q, p) and control point q + t is then a
+// table entry T[p][t] (stationary kernel, Kernel.h:96-103), and
+//   forward:     u(q, p)   = sum_t T[p][t] * (w alpha)[q + t]          (a 3-D transposed convolution)
+//   derivative:  d[j]      = w_j * sum_t sum_p T[p][t] * g(j - t, p)  (its adjoint)
+// with g = (metric coefficient) * grad M per texel.  The sums run over exactly the control
+// points inside the kernel support -- the same set the reference's truncated boxes visit for a
+// stationary kernel (every point they add outside the support has k = 0).
+//
+// Kernels (one launch each):
+//   table_value_kernel      T x A register-blocked transform for 4 z-phases per thread, then
+//                           B-spline warp + metric statistics per texel; records (grad M, m) in
+//                           cell-phase layout and per-block FP64 partials.
+//   table_contrib_kernel    Contrib[t][cell] = sum_p T[p][t] g(cell, p): a register-blocked GEMM
+//                           (taps x phases x cells) with T and the cells' g tile in shared memory.
+//   table_gather_kernel     control-point-owned gather d[j] = w_j sum_t Contrib[t][j - t] (fixed
+//                           order, no atomics) fused with RKHS/RD/PG (cp-offset kernel table),
+//                           L1/L2/L2,1 and the sign flip; per-block FP64 partials of the values.
 #pragma once
+
+#include <cmath>
+#include <vector>
 
 #include "skm_kernels.cuh"
 
 namespace skm {
 
-struct TablePlan {
-    bool enabled = false;
+constexpr int kTabMaxPhase = 8;      // phases per axis
+constexpr int kTabMaxTap = 10;       // taps per axis
+constexpr int kTabContribThreads = 288;   // 9 warps
+constexpr int kTabCells = 32;        // cells per contrib block
+constexpr int kTabTapChunk = 12;     // taps per thread in the contrib GEMM
+
+struct TableDev {
+    int D;
+    int h[3];            // phases per axis
+    int nph;             // h0*h1*h2
+    int tlo[3], nt[3];   // tap offsets t in [tlo, tlo + nt) per axis
+    int ntap, ntap_pad;  // nt0*nt1*nt2, rounded up to kTabTapChunk
+    int qmin[3], nq[3];  // cells covering the fixed image
+    long long ncell;
+    int qoff[3][kTabMaxPhase];   // cell of texel h*a + p is a + qoff[p]
+    int clo[3], nc[3];           // control-point offsets of the regularizer box
+    const float *tfwd;   // [tap][(px,py)][pz]
+    const float *tgemm;  // [phase][ntap_pad]
+    const float *kcp;    // [nc0*nc1*nc2] kernel between control points at an offset
+    float4 *rec;         // [cell][phase]: grad M, m
+    const float *fixcp;  // [cell][phase]: fixed image value (0 outside)
+    float *contrib;      // [3][ntap][ncell]
+    double *part;        // [NQ][value blocks]
+    int value_blocks, tile_x, tile_y, tiles_x, tiles_y, tiles_z;
 };
 
-inline int table_plan(TablePlan &t, const EvalParams &, int, cudaStream_t)
+struct TablePlan {
+    bool enabled = false;
+    TableDev dev{};
+    float *d_tfwd = nullptr, *d_tgemm = nullptr, *d_kcp = nullptr, *d_fixcp = nullptr, *d_contrib = nullptr;
+    float4 *d_rec = nullptr;
+    double *d_part = nullptr;
+    int hl = 1;          // phases per thread in the value kernel (template argument)
+};
+
+// ------------------------------------------------------------------------------------------------
+// value pass
+template <int D, int HL>
+__global__ void __launch_bounds__(256) table_value_kernel(EvalParams P, TableDev T)
 {
-    t.enabled = false;
+    extern __shared__ float4 smem4[];
+    __shared__ double sh[NQ * 32];
+    const int nphxy = T.h[0] * T.h[1];
+    const int ncell_blk = blockDim.x / nphxy;
+    // A tile: (tile_x + nt0 - 1) x (tile_y + nt1 - 1) x nt2 control points (w*alpha)
+    const int ax = T.tile_x + T.nt[0] - 1, ay = T.tile_y + T.nt[1] - 1, az = T.nt[2];
+    float4 *A = smem4;
+    float *tf = reinterpret_cast<float *>(smem4 + ax * ay * az);
+    const int tile = blockIdx.x;
+    const int tx0 = (tile % T.tiles_x) * T.tile_x;
+    const int ty0 = ((tile / T.tiles_x) % T.tiles_y) * T.tile_y;
+    const int tz0 = tile / (T.tiles_x * T.tiles_y);
+    // cell origin of the tile (cell coordinates relative to qmin)
+    const int q0[3] = {T.qmin[0] + tx0, T.qmin[1] + ty0, T.qmin[2] + tz0};
+    for (int i = threadIdx.x; i < ax * ay * az; i += blockDim.x) {
+        int x = i % ax, y = (i / ax) % ay, z = i / (ax * ay);
+        int j[3] = {q0[0] + T.tlo[0] + x, q0[1] + T.tlo[1] + y, q0[2] + T.tlo[2] + z};
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool in = j[0] >= 0 && j[0] < P.cp.n[0] && j[1] >= 0 && j[1] < P.cp.n[1] && j[2] >= 0 && j[2] < P.cp.n[2];
+        if (in) {
+            float4 c = P.cpd[j[0] + P.cp.st[1] * j[1] + P.cp.st[2] * j[2]];
+            a = make_float4(c.w * c.x, c.w * c.y, c.w * c.z, 0.f);
+        }
+        A[i] = a;
+    }
+    const int tf_n = T.ntap * nphxy * HL;
+    for (int i = threadIdx.x; i < tf_n; i += blockDim.x) tf[i] = T.tfwd[i];
+    __syncthreads();
+
+    const int pxy = threadIdx.x % nphxy;
+    const int cl = threadIdx.x / nphxy;            // cell within the block
+    const int px = pxy % T.h[0], py = pxy / T.h[0];
+    const int cx = cl % T.tile_x, cy = cl / T.tile_x;
+    double v[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) v[k] = 0.0;
+    const bool cell_ok = cl < ncell_blk && tx0 + cx < T.nq[0] && ty0 + cy < T.nq[1];
+    if (cell_ok) {
+        float acc[HL][3];
+#pragma unroll
+        for (int k = 0; k < HL; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.f;
+        int tap = 0;
+        for (int tz = 0; tz < T.nt[2]; ++tz)
+            for (int ty = 0; ty < T.nt[1]; ++ty) {
+                const float4 *arow = A + (cx + ax * ((cy + ty) + ay * tz));
+                for (int tx = 0; tx < T.nt[0]; ++tx, ++tap) {
+                    const float4 a = arow[tx];
+                    const float *t = tf + (tap * nphxy + pxy) * HL;
+                    if (HL == 4) {
+                        const float4 t4 = *reinterpret_cast<const float4 *>(t);
+                        const float tv[4] = {t4.x, t4.y, t4.z, t4.w};
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            acc[k][0] = fmaf(tv[k], a.x, acc[k][0]);
+                            acc[k][1] = fmaf(tv[k], a.y, acc[k][1]);
+                            acc[k][2] = fmaf(tv[k], a.z, acc[k][2]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < HL; ++k) {
+                            const float tv = t[k];
+                            acc[k][0] = fmaf(tv, a.x, acc[k][0]);
+                            acc[k][1] = fmaf(tv, a.y, acc[k][1]);
+                            acc[k][2] = fmaf(tv, a.z, acc[k][2]);
+                        }
+                    }
+                }
+            }
+        const int q[3] = {q0[0] + cx, q0[1] + cy, q0[2]};
+        const long long cell_lin = (long long)(tx0 + cx) + (long long)T.nq[0] * ((ty0 + cy) + (long long)T.nq[1] * tz0);
+#pragma unroll
+        for (int k = 0; k < HL; ++k) {
+            const int pz = k;
+            const int ph[3] = {px, py, pz};
+            int x[3] = {0, 0, 0};
+            bool ok = true;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                x[d] = T.h[d] * (q[d] - T.qoff[d][ph[d]]) + ph[d];
+                if (x[d] < 0 || x[d] >= P.fixed.n[d]) ok = false;
+            }
+            const int p_lin = px + T.h[0] * (py + T.h[1] * pz);
+            float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (ok) {
+                double fi[3] = {(double)x[0], (double)x[1], (double)x[2]}, p[3], mp[3], ml[3];
+                to_global<D>(P.fixed, fi, p);
+#pragma unroll
+                for (int d = 0; d < D; ++d) mp[d] = p[d];
+                if (P.has_df) {
+                    long long i = nearest_index<D>(P.df, p);
+                    if (i >= 0) {
+                        float4 dv = P.dfd[i];
+                        mp[0] += dv.x;
+                        if (D > 1) mp[1] += dv.y;
+                        if (D > 2) mp[2] += dv.z;
+                    }
+                }
+#pragma unroll
+                for (int d = 0; d < D; ++d) mp[d] += (double)acc[k][d];
+                to_local<D>(P.mov, mp, ml);
+                if (bspline_inside<D>(P.mov, ml)) {
+                    float m, g[3] = {0.f, 0.f, 0.f};
+                    bspline_derivs<D>(P.coeffs, P.mov, ml, m, g);
+                    double f = (double)T.fixcp[cell_lin * T.nph + p_lin];
+                    double md = (double)m;
+                    v[Q_COUNT] += 1.0;
+                    v[Q_D2] += (md - f) * (md - f);
+                    v[Q_SF] += f;
+                    v[Q_SM] += md;
+                    v[Q_SFF] += f * f;
+                    v[Q_SMM] += md * md;
+                    v[Q_SFM] += f * md;
+                    rec = make_float4(g[0], g[1], D > 2 ? g[2] : 0.f, m);
+                }
+            }
+            T.rec[cell_lin * T.nph + p_lin] = rec;
+        }
+    }
+    block_sum<NQ>(v, sh);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) T.part[(long long)k * gridDim.x + blockIdx.x] = v[k];
+}
+
+// ------------------------------------------------------------------------------------------------
+// Contrib[t][cell] = sum_p T[p][t] * g(cell, p),  g = (a f + b m + c) grad M
+__global__ void __launch_bounds__(kTabContribThreads) table_contrib_kernel(TableDev T, const double *__restrict__ stats)
+{
+    extern __shared__ float4 smem4[];
+    const int nph = T.nph, ntp = T.ntap_pad;
+    const int gst = nph + 1;                                  // padded row: lanes hit distinct banks
+    float4 *G = smem4;                                        // [kTabCells][nph + 1]
+    float *tg = reinterpret_cast<float *>(smem4 + kTabCells * gst);   // [nph][ntp]
+    const long long c0 = (long long)blockIdx.x * kTabCells;
+    const float cf = (float)stats[S_COEF_F], cm = (float)stats[S_COEF_M], cc = (float)stats[S_COEF_C];
+    for (int i = threadIdx.x; i < kTabCells * nph; i += blockDim.x) {
+        const int c = i / nph, p = i % nph;
+        float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (c0 + c < T.ncell) {
+            const long long idx = (c0 + c) * nph + p;
+            const float4 r = T.rec[idx];
+            const float coef = fmaf(cf, T.fixcp[idx], fmaf(cm, r.w, cc));
+            g = make_float4(coef * r.x, coef * r.y, coef * r.z, 0.f);
+        }
+        G[c * gst + p] = g;         // row = cell
+    }
+    for (int i = threadIdx.x; i < nph * ntp; i += blockDim.x) tg[i] = T.tgemm[i];
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int nchunk = ntp / kTabTapChunk;
+    const long long cell = c0 + lane;
+    for (int ch = warp; ch < nchunk; ch += nwarps) {
+        float acc[kTabTapChunk][3];
+#pragma unroll
+        for (int k = 0; k < kTabTapChunk; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.f;
+        const float *trow = tg + ch * kTabTapChunk;
+        const float4 *grow = G + lane * gst;
+        for (int p = 0; p < nph; ++p) {
+            const float4 g = grow[p];
+            const float4 ta = *reinterpret_cast<const float4 *>(trow + p * ntp);
+            const float4 tb = *reinterpret_cast<const float4 *>(trow + p * ntp + 4);
+            const float4 tc = *reinterpret_cast<const float4 *>(trow + p * ntp + 8);
+            const float tv[12] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w, tc.x, tc.y, tc.z, tc.w};
+#pragma unroll
+            for (int k = 0; k < kTabTapChunk; ++k) {
+                acc[k][0] = fmaf(tv[k], g.x, acc[k][0]);
+                acc[k][1] = fmaf(tv[k], g.y, acc[k][1]);
+                acc[k][2] = fmaf(tv[k], g.z, acc[k][2]);
+            }
+        }
+        if (cell < T.ncell) {
+#pragma unroll
+            for (int k = 0; k < kTabTapChunk; ++k) {
+                const int tap = ch * kTabTapChunk + k;
+                if (tap < T.ntap) {
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        T.contrib[((long long)d * T.ntap + tap) * T.ncell + cell] = acc[k][d];
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// d[j] = w_j sum_t Contrib[t][j - t]  + regularizers + metric-level terms; thread per control point.
+template <int D>
+__global__ void __launch_bounds__(256) table_gather_kernel(EvalParams P, TableDev T, DerivParams Q)
+{
+    __shared__ double shv[NR][32];
+    __shared__ float kcp_s[1024];
+    const int nkcp = T.nc[0] * T.nc[1] * T.nc[2];
+    for (int i = threadIdx.x; i < nkcp; i += blockDim.x) kcp_s[i] = T.kcp[i];
+    __syncthreads();
+    const long long j_lin = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double val[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) val[k] = 0.0;
+    if (j_lin < P.C) {
+        int j[3];
+        cell_of<D>(P.cp.n, j_lin, j);
+        const float4 cj = P.cpd[j_lin];
+        const double *st = Q.stats;
+        float acc[3] = {0.f, 0.f, 0.f};
+        const int ntap = T.ntap;
+        const long long ncell = T.ncell;
+        int tap = 0;
+        for (int tz = 0; tz < T.nt[2]; ++tz) {
+            const int qz = j[2] - (T.tlo[2] + tz) - T.qmin[2];
+            for (int ty = 0; ty < T.nt[1]; ++ty) {
+                const int qy = j[1] - (T.tlo[1] + ty) - T.qmin[1];
+                const bool rowok = qz >= 0 && qz < T.nq[2] && qy >= 0 && qy < T.nq[1];
+                const long long rowbase = ((long long)qz * T.nq[1] + qy) * T.nq[0];
+#pragma unroll 2
+                for (int tx = 0; tx < T.nt[0]; ++tx, ++tap) {
+                    const int qx = j[0] - (T.tlo[0] + tx) - T.qmin[0];
+                    if (rowok && qx >= 0 && qx < T.nq[0]) {
+                        const long long c = rowbase + qx;
+                        acc[0] += __ldg(T.contrib + (long long)tap * ncell + c);
+                        acc[1] += __ldg(T.contrib + ((long long)ntap + tap) * ncell + c);
+                        if (D > 2) acc[2] += __ldg(T.contrib + ((long long)2 * ntap + tap) * ncell + c);
+                    }
+                }
+            }
+        }
+        // regularizers over the control-point box (GpuEvaluatorRegularizers.cu), kernel from the table
+        float drk[3] = {0.f, 0.f, 0.f}, drd[3] = {0.f, 0.f, 0.f}, dpg[3] = {0.f, 0.f, 0.f};
+        const bool rkhs = Q.reg_rkhs > 0.0, rd = Q.reg_rd > 0.0, pg = Q.reg_pg > 0.0;
+        if (rkhs || rd || pg) {
+            const float wj = cj.w;
+            const float cjv[3] = {cj.x, cj.y, cj.z};
+            const float pgs = (float)Q.pg_scaling;
+            int o = 0;
+            for (int oz = 0; oz < T.nc[2]; ++oz)
+                for (int oy = 0; oy < T.nc[1]; ++oy)
+                    for (int ox = 0; ox < T.nc[0]; ++ox, ++o) {
+                        const int ii[3] = {j[0] + T.clo[0] + ox, j[1] + T.clo[1] + oy, j[2] + T.clo[2] + oz};
+                        if (ii[0] < 0 || ii[0] >= P.cp.n[0] || ii[1] < 0 || ii[1] >= P.cp.n[1] || ii[2] < 0 ||
+                            ii[2] >= P.cp.n[2])
+                            continue;
+                        const float k = kcp_s[o];
+                        if (k == 0.0f) continue;
+                        const float4 ci4 = __ldg(P.cpd + lin_of<D>(P.cp, ii));
+                        const float ci[3] = {ci4.x, ci4.y, ci4.z};
+                        const float kw = k * wj;
+                        if (rkhs) {
+                            double dot = 0.0;
+#pragma unroll
+                            for (int d = 0; d < D; ++d) dot += (double)cjv[d] * (double)ci[d];
+                            val[R_RKHS] += (double)kw * dot;
+#pragma unroll
+                            for (int d = 0; d < D; ++d) drk[d] = fmaf(2.0f * kw, ci[d], drk[d]);
+                        }
+                        if (rd) {
+                            double l2 = 0.0;
+#pragma unroll
+                            for (int d = 0; d < D; ++d) {
+                                double e = (double)cjv[d] - (double)ci[d];
+                                l2 += e * e;
+                            }
+                            val[R_RD] += l2 * (double)kw;
+#pragma unroll
+                            for (int d = 0; d < D; ++d) drd[d] = fmaf(4.0f * kw, cjv[d] - ci[d], drd[d]);
+                        }
+                        if (pg) {
+                            if (D == 3) {
+                                float cr0 = ci[1] * cjv[2] - ci[2] * cjv[1];
+                                float cr1 = ci[2] * cjv[0] - ci[0] * cjv[2];
+                                float cr2 = ci[0] * cjv[1] - ci[1] * cjv[0];
+                                double n2 = (double)cr0 * cr0 + (double)cr1 * cr1 + (double)cr2 * cr2;
+                                double s = (double)pgs;
+                                val[R_PG] += (double)kw * s * s / 2.0 * log(1.0 + n2 / s);
+                                float den = 2.0f * ((float)n2 / pgs + 1.0f);
+                                float dp0 = 2.0f * ci[2] * (ci[2] * cjv[0] - ci[0] * cjv[2]) - 2.0f * ci[1] * (ci[0] * cjv[1] - ci[1] * cjv[0]);
+                                float dp1 = 2.0f * ci[0] * (ci[0] * cjv[1] - ci[1] * cjv[0]) - 2.0f * ci[2] * (ci[1] * cjv[2] - ci[2] * cjv[1]);
+                                float dp2 = 2.0f * ci[1] * (ci[1] * cjv[2] - ci[2] * cjv[1]) - 2.0f * ci[0] * (ci[2] * cjv[0] - ci[0] * cjv[2]);
+                                dpg[0] = fmaf(2.0f * kw, pgs * dp0 / den, dpg[0]);
+                                dpg[1] = fmaf(2.0f * kw, pgs * dp1 / den, dpg[1]);
+                                dpg[2] = fmaf(2.0f * kw, pgs * dp2 / den, dpg[2]);
+                            } else {
+                                float v2d = ci[0] * cjv[1] - ci[1] * cjv[0];
+                                double v2 = (double)v2d * v2d;
+                                double s = (double)pgs;
+                                val[R_PG] += (double)kw * s * s / 2.0 * log(1.0 + v2 / s);
+                                float factor = (float)v2 / pgs + 1.0f;
+                                dpg[0] = fmaf(2.0f * kw, -pgs * ci[1] * v2d / factor, dpg[0]);
+                                dpg[1] = fmaf(2.0f * kw, pgs * ci[0] * v2d / factor, dpg[1]);
+                            }
+                        }
+                    }
+        }
+        double pc[3] = {0, 0, 0}, pn2 = 0.0;
+        if (Q.with_metric) {
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                pc[d] = Q.params[j_lin + d * P.C];
+                pn2 += pc[d] * pc[d];
+            }
+        }
+        const double pnorm = sqrt(pn2);
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            double g;
+            if (Q.metric == 1)
+                g = st[S_DENOM] != 0.0 ? (double)cj.w * (double)acc[d] : 0.0;
+            else
+                g = (double)cj.w * (double)acc[d];
+            if (rkhs) g += (double)drk[d] * Q.reg_rkhs;
+            if (rd) g += (double)drd[d] * Q.reg_rd;
+            if (pg) g += (double)dpg[d] * Q.reg_pg;
+            if (Q.with_metric) {
+                const double par = pc[d];
+                if (Q.reg_l1 > 0.0) {
+                    const double w = Q.reg_l1;
+                    if (fabs(par) > 0.0) g += w * (par < 0.0 ? -1.0 : 1.0);
+                    else if (g < -w) g += w;
+                    else if (g > w) g -= w;
+                    else g = 0.0;
+                }
+                if (Q.reg_l2 > 0.0) g += Q.reg_l2 * 2.0 * par;
+                if (Q.reg_l21 > 0.0) {
+                    const double w = Q.reg_l21;
+                    if (pnorm > 0.0) g += w * par / pnorm;
+                    else if (g < -w) g += w;
+                    else if (g > w) g -= w;
+                    else g = 0.0;
+                }
+                if (Q.negate) g = -g;
+            }
+            Q.deriv[j_lin + d * P.C] = g;
+        }
+        if (Q.with_metric) {
+            double l1 = 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) l1 += fabs(pc[d]);
+            val[R_L1] = Q.reg_l1 > 0.0 ? l1 : 0.0;
+            val[R_L2] = Q.reg_l2 > 0.0 ? pn2 : 0.0;
+            val[R_L21] = Q.reg_l21 > 0.0 ? pnorm : 0.0;
+        }
+    }
+    // fixed-order block reduction of the per-control-point values
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+        double s = warp_sum(val[k]);
+        if (lane == 0) shv[k][warp] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < NR) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += shv[threadIdx.x][w];
+        Q.rpart[(long long)threadIdx.x * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side
+
+inline float wendland_host(double r, double sc4, double sc0)
+{
+    // the same float profile the device evaluates (k_stationary) on a double distance
+    float rf = (float)r;
+    float t4 = rf * (1.0f / (float)sc4), t0 = rf * (1.0f / (float)sc0);
+    float f4 = fmaxf(0.0f, 1.0f - t4), f0 = fmaxf(0.0f, 1.0f - t0);
+    float f2 = f4 * f4;
+    return f2 * f2 * f2 * (3.0f + 18.0f * t4 + 35.0f * t4 * t4) * (1.0f / 3.0f) * (f0 * f0);
+}
+
+// Decides whether the table path applies and builds its tables.  Returns 0 (also when the
+// path does not apply; plan.enabled says which) or a CUDA error code.
+inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t stream)
+{
+    pl.enabled = false;
+    if (P.K.kind != kStationary || P.sub != 1) return 0;
+    TableDev &T = pl.dev;
+    T = TableDev{};
+    T.D = D;
+    const double S = (double)P.K.support_min;
+    double phi[3][kTabMaxPhase];
+    for (int d = 0; d < 3; ++d) {
+        if (d >= D) {
+            T.h[d] = 1;
+            T.qoff[d][0] = 0;
+            phi[d][0] = 0.0;
+            continue;
+        }
+        const double ratio = P.cp.s[d] / P.fixed.s[d];
+        const int h = (int)llround(ratio);
+        if (h < 1 || h > kTabMaxPhase || fabs(ratio - h) > 1e-9 * ratio) return 0;
+        T.h[d] = h;
+        // cell and fractional offset of every texel exactly as the device computes them
+        int qo[kTabMaxPhase];
+        bool seen[kTabMaxPhase] = {false};
+        for (int x = 0; x < P.fixed.n[d]; ++x) {
+            const double p = P.fixed.o[d] + P.fixed.s[d] * (double)x;
+            const double ip = P.cp.inv[d] * (p - P.cp.o[d]);
+            const double q = floor(ip);
+            const int ph = x % h, a = x / h;
+            const int off = (int)q - a;
+            const double fr = ip - q;
+            if (!seen[ph]) {
+                seen[ph] = true;
+                qo[ph] = off;
+                phi[d][ph] = fr;
+            } else if (qo[ph] != off || fabs(phi[d][ph] - fr) > 1e-9) {
+                return 0;                        // phases do not repeat exactly
+            }
+        }
+        for (int ph = 0; ph < h; ++ph) {
+            if (!seen[ph]) {                    // image shorter than one cell: derive from phase 0 rule
+                const double p = P.fixed.o[d] + P.fixed.s[d] * (double)ph;
+                const double ip = P.cp.inv[d] * (p - P.cp.o[d]);
+                qo[ph] = (int)floor(ip);
+                phi[d][ph] = ip - floor(ip);
+            }
+            T.qoff[d][ph] = qo[ph];
+        }
+    }
+    T.nph = T.h[0] * T.h[1] * T.h[2];
+    if (T.nph * 16 > 4096 || (T.h[0] * T.h[1]) > 256) return 0;
+    // tap range per axis: every t with |phi - t| * spacing < S for some phase
+    for (int d = 0; d < 3; ++d) {
+        if (d >= D) {
+            T.tlo[d] = 0;
+            T.nt[d] = 1;
+            continue;
+        }
+        const double R = S / P.cp.s[d];
+        int lo = 1 << 30, hi = -(1 << 30);
+        for (int t = -(int)ceil(R) - 1; t <= (int)ceil(R) + 1; ++t)
+            for (int ph = 0; ph < T.h[d]; ++ph)
+                if (fabs(phi[d][ph] - t) < R) {
+                    lo = std::min(lo, t);
+                    hi = std::max(hi, t);
+                }
+        if (hi < lo) return 0;
+        T.tlo[d] = lo;
+        T.nt[d] = hi - lo + 1;
+        if (T.nt[d] > kTabMaxTap) return 0;
+    }
+    T.ntap = T.nt[0] * T.nt[1] * T.nt[2];
+    T.ntap_pad = ((T.ntap + kTabTapChunk - 1) / kTabTapChunk) * kTabTapChunk;
+    // cells covering the fixed image
+    long long ncell = 1;
+    for (int d = 0; d < 3; ++d) {
+        if (d >= D) {
+            T.qmin[d] = 0;
+            T.nq[d] = 1;
+            continue;
+        }
+        int qmn = 1 << 30, qmx = -(1 << 30);
+        for (int ph = 0; ph < T.h[d]; ++ph) {
+            for (int x = ph; x < P.fixed.n[d]; x += T.h[d]) {
+                const int q = x / T.h[d] + T.qoff[d][ph];
+                qmn = std::min(qmn, q);
+                qmx = std::max(qmx, q);
+            }
+        }
+        T.qmin[d] = qmn;
+        T.nq[d] = qmx - qmn + 1;
+        ncell *= T.nq[d];
+    }
+    T.ncell = ncell;
+    // regularizer box offsets: trunc(j - R + 1) .. trunc(j + R) for interior j (Regularizers.cu:52-53)
+    for (int d = 0; d < 3; ++d) {
+        if (d >= D) {
+            T.clo[d] = 0;
+            T.nc[d] = 1;
+            continue;
+        }
+        // offsets of an interior control point j, evaluated with the reference's double
+        // arithmetic trunc(j - R + 1) .. trunc(j + R) at a large j
+        const double R = S / P.cp.s[d];
+        const double jb = 4096.0;
+        const int lo = (int)(jb - R + 1.0) - 4096;
+        const int hi = (int)(jb + R) - 4096;
+        T.clo[d] = lo;
+        T.nc[d] = hi - lo + 1;
+    }
+    if (T.nc[0] * T.nc[1] * T.nc[2] > 1024) return 0;
+    // value-kernel tiling: threads = (px,py) phases x cells; HL = z phases per thread
+    const int nphxy = T.h[0] * T.h[1];
+    const int hl = T.h[2];
+    if (!(hl == 1 || hl == 2 || hl == 4 || hl == 8)) return 0;
+    if (256 % nphxy != 0) return 0;
+    const int cells = 256 / nphxy;
+    int tx = 1;
+    while (tx * tx < cells) tx *= 2;
+    T.tile_x = std::min(tx, cells);
+    T.tile_y = cells / T.tile_x;
+    T.tiles_x = (T.nq[0] + T.tile_x - 1) / T.tile_x;
+    T.tiles_y = (T.nq[1] + T.tile_y - 1) / T.tile_y;
+    T.tiles_z = T.nq[2];
+    T.value_blocks = T.tiles_x * T.tiles_y * T.tiles_z;
+    pl.hl = hl;
+
+    // tables (kernel evaluated on the exact double offset, float profile)
+    std::vector<float> tfwd((size_t)T.ntap * nphxy * hl), tgemm((size_t)T.nph * T.ntap_pad, 0.f);
+    std::vector<float> kcp((size_t)T.nc[0] * T.nc[1] * T.nc[2]);
+    int tap = 0;
+    for (int tz = 0; tz < T.nt[2]; ++tz)
+        for (int ty = 0; ty < T.nt[1]; ++ty)
+            for (int tx2 = 0; tx2 < T.nt[0]; ++tx2, ++tap) {
+                const int t[3] = {T.tlo[0] + tx2, T.tlo[1] + ty, T.tlo[2] + tz};
+                for (int pz = 0; pz < T.h[2]; ++pz)
+                    for (int py = 0; py < T.h[1]; ++py)
+                        for (int px = 0; px < T.h[0]; ++px) {
+                            const int ph[3] = {px, py, pz};
+                            double r2 = 0.0;
+                            for (int d = 0; d < D; ++d) {
+                                const double e = (phi[d][ph[d]] - (double)t[d]) * P.cp.s[d];
+                                r2 += e * e;
+                            }
+                            const float k = wendland_host(sqrt(r2), P.K.sc4, P.K.sc0);
+                            tfwd[((size_t)tap * nphxy + px + T.h[0] * py) * hl + pz] = k;
+                            tgemm[(size_t)(px + T.h[0] * (py + T.h[1] * pz)) * T.ntap_pad + tap] = k;
+                        }
+            }
+    int o = 0;
+    for (int oz = 0; oz < T.nc[2]; ++oz)
+        for (int oy = 0; oy < T.nc[1]; ++oy)
+            for (int ox = 0; ox < T.nc[0]; ++ox, ++o) {
+                const int off[3] = {T.clo[0] + ox, T.clo[1] + oy, T.clo[2] + oz};
+                double r2 = 0.0;
+                for (int d = 0; d < D; ++d) {
+                    const double e = (double)off[d] * P.cp.s[d];
+                    r2 += e * e;
+                }
+                kcp[o] = wendland_host(sqrt(r2), P.K.sc4, P.K.sc0);
+            }
+    // fixed image in cell-phase layout
+    std::vector<float> fix((size_t)T.ncell * T.nph, 0.f);
+    std::vector<float> fixed_host((size_t)P.fixed.n[0] * P.fixed.n[1] * P.fixed.n[2]);
+    if (cudaMemcpy(fixed_host.data(), P.fixed_data, fixed_host.size() * sizeof(float), cudaMemcpyDeviceToHost) !=
+        cudaSuccess)
+        return 2;
+    for (int z = 0; z < P.fixed.n[2]; ++z)
+        for (int y = 0; y < P.fixed.n[1]; ++y)
+            for (int x = 0; x < P.fixed.n[0]; ++x) {
+                const int c[3] = {x, y, z};
+                long long cell = 0, mul = 1;
+                int ph = 0, phmul = 1;
+                for (int d = 0; d < 3; ++d) {
+                    const int p = c[d] % T.h[d];
+                    const int q = c[d] / T.h[d] + T.qoff[d][p] - T.qmin[d];
+                    cell += mul * q;
+                    mul *= T.nq[d];
+                    ph += phmul * p;
+                    phmul *= T.h[d];
+                }
+                fix[cell * T.nph + ph] = fixed_host[x + (size_t)P.fixed.n[0] * (y + (size_t)P.fixed.n[1] * z)];
+            }
+    auto up = [&](float **dst, const std::vector<float> &src) -> bool {
+        if (cudaMalloc((void **)dst, std::max<size_t>(1, src.size()) * sizeof(float)) != cudaSuccess) return false;
+        return cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(float), cudaMemcpyHostToDevice, stream) ==
+               cudaSuccess;
+    };
+    if (!up(&pl.d_tfwd, tfwd) || !up(&pl.d_tgemm, tgemm) || !up(&pl.d_kcp, kcp) || !up(&pl.d_fixcp, fix)) return 2;
+    if (cudaMalloc((void **)&pl.d_rec, (size_t)T.ncell * T.nph * sizeof(float4)) != cudaSuccess) return 2;
+    if (cudaMalloc((void **)&pl.d_contrib, (size_t)3 * T.ntap * T.ncell * sizeof(float)) != cudaSuccess) return 2;
+    if (cudaMalloc((void **)&pl.d_part, (size_t)NQ * T.value_blocks * sizeof(double)) != cudaSuccess) return 2;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return 2;
+    T.tfwd = pl.d_tfwd;
+    T.tgemm = pl.d_tgemm;
+    T.kcp = pl.d_kcp;
+    T.fixcp = pl.d_fixcp;
+    T.rec = pl.d_rec;
+    T.contrib = pl.d_contrib;
+    T.part = pl.d_part;
+    // shared memory of the launches
+    const size_t smem_value = (size_t)(T.tile_x + T.nt[0] - 1) * (T.tile_y + T.nt[1] - 1) * T.nt[2] * sizeof(float4) +
+                              (size_t)T.ntap * nphxy * hl * sizeof(float);
+    const size_t smem_contrib =
+        (size_t)kTabCells * (T.nph + 1) * sizeof(float4) + (size_t)T.nph * T.ntap_pad * sizeof(float);
+    if (smem_value > 200 * 1024 || smem_contrib > 200 * 1024) return 0;
+    pl.enabled = true;
     return 0;
 }
 
-inline int table_value(TablePlan &, const EvalParams &, float4 *, double *, int, cudaStream_t) { return 3; }
-inline int table_derivative(TablePlan &, const EvalParams &, const DerivParams &, int, cudaStream_t) { return 3; }
-inline void table_free(TablePlan &) {}
+inline size_t table_value_smem(const TableDev &T)
+{
+    return (size_t)(T.tile_x + T.nt[0] - 1) * (T.tile_y + T.nt[1] - 1) * T.nt[2] * sizeof(float4) +
+           (size_t)T.ntap * T.h[0] * T.h[1] * T.h[2] * sizeof(float);
+}
+
+inline size_t table_contrib_smem(const TableDev &T)
+{
+    return (size_t)kTabCells * (T.nph + 1) * sizeof(float4) + (size_t)T.nph * T.ntap_pad * sizeof(float);
+}
+
+// dynamic shared memory limits of the table kernels (set once, outside any stream capture)
+inline int table_set_attributes(const TablePlan &pl)
+{
+    const int sv = (int)table_value_smem(pl.dev), sc = (int)table_contrib_smem(pl.dev);
+    cudaError_t e = cudaSuccess;
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (pl.dev.D == 3) {
+        if (pl.hl == 1) e = cudaFuncSetAttribute(table_value_kernel<3, 1>, a, sv);
+        else if (pl.hl == 2) e = cudaFuncSetAttribute(table_value_kernel<3, 2>, a, sv);
+        else if (pl.hl == 4) e = cudaFuncSetAttribute(table_value_kernel<3, 4>, a, sv);
+        else e = cudaFuncSetAttribute(table_value_kernel<3, 8>, a, sv);
+    } else {
+        e = cudaFuncSetAttribute(table_value_kernel<2, 1>, a, sv);
+    }
+    if (e != cudaSuccess) return 2;
+    return cudaFuncSetAttribute(table_contrib_kernel, a, sc) == cudaSuccess ? 0 : 2;
+}
+
+template <int D, int HL>
+inline int table_value_launch(TablePlan &pl, const EvalParams &P, cudaStream_t s)
+{
+    const size_t smem = table_value_smem(pl.dev);
+    table_value_kernel<D, HL><<<pl.dev.value_blocks, 256, smem, s>>>(P, pl.dev);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
+}
+
+// value pass of the table path; writes its own partials (pl.d_part, pl.dev.value_blocks blocks)
+inline int table_value(TablePlan &pl, const EvalParams &P, int D, cudaStream_t s)
+{
+    if (D == 3) {
+        switch (pl.hl) {
+        case 1: return table_value_launch<3, 1>(pl, P, s);
+        case 2: return table_value_launch<3, 2>(pl, P, s);
+        case 4: return table_value_launch<3, 4>(pl, P, s);
+        default: return table_value_launch<3, 8>(pl, P, s);
+        }
+    }
+    return table_value_launch<2, 1>(pl, P, s);
+}
+
+inline int table_derivative(TablePlan &pl, const EvalParams &P, const DerivParams &Q, int D, int gather_blocks,
+                            cudaStream_t s)
+{
+    const size_t smem = table_contrib_smem(pl.dev);
+    const int blocks = (int)((pl.dev.ncell + kTabCells - 1) / kTabCells);
+    table_contrib_kernel<<<blocks, kTabContribThreads, smem, s>>>(pl.dev, Q.stats);
+    if (cudaPeekAtLastError() != cudaSuccess) return 2;
+    if (D == 3)
+        table_gather_kernel<3><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+    else
+        table_gather_kernel<2><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
+}
+
+inline void table_free(TablePlan &pl)
+{
+    float *f[] = {pl.d_tfwd, pl.d_tgemm, pl.d_kcp, pl.d_fixcp, pl.d_contrib};
+    for (float *p : f)
+        if (p) cudaFree(p);
+    if (pl.d_rec) cudaFree(pl.d_rec);
+    if (pl.d_part) cudaFree(pl.d_part);
+    pl = TablePlan{};
+}
 
 }  // namespace skm

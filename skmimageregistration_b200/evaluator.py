@@ -47,6 +47,7 @@ def lib():
         L.skm_abi_version.restype = C.c_int32
         L.skm_evaluator_create.argtypes = [C.POINTER(EvaluatorDesc), C.POINTER(C.c_void_p)]
         L.skm_evaluator_destroy.argtypes = [C.c_void_p]
+        L.skm_evaluator_path.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
         L.skm_set_regularizer_rkhs.argtypes = [C.c_void_p, C.c_double]
         L.skm_set_regularizer_rd.argtypes = [C.c_void_p, C.c_double, C.c_double]
         L.skm_set_regularizer_pg.argtypes = [C.c_void_p, C.c_double, C.c_double]
@@ -114,6 +115,14 @@ class GpuKernelEvaluator:
             self.close()
         except Exception:
             pass
+
+    GENERIC, TABLE = 1, 2
+
+    def path(self, request=-1):
+        """Select (0 auto, 1 generic) and/or query the kernel path: returns 1 generic, 2 table."""
+        a = C.c_int32()
+        check(lib().skm_evaluator_path(self.h, int(request), C.byref(a)))
+        return a.value
 
     # --- GpuEvaluator.h:156-158
     def SetRegularizerRKHS(self, weight):

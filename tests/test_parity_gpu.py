@@ -154,3 +154,68 @@ def test_optimizer_matches_oracle(D):
         assert rel_err(st["current_time"], oo.state.current_time) <= 1e-3 or abs(oo.state.current_time) < 1e-9
         assert max_rel(opt.parameters(), oo.position) <= 1e-3
     assert max_rel(opt.parameters(best=True), oo.best) <= 1e-3
+
+
+# ---- phase-table path (stationary kernel, control spacing = h * fixed spacing, subsample 1) ----
+TABLE_CASES = [
+    # D, h, shape, sigma_c4, sigma_c0
+    (3, 2, (14, 16, 18), 4.5, 9.0),
+    (3, 4, (20, 22, 26), 9.0, 18.0),
+    (2, 4, (40, 44), 9.0, 18.0),
+    (2, 8, (48, 56), 16.0, 32.0),
+]
+
+
+def _table_problem(D, h, shape, s4, s0, seed, **kw):
+    return make_problem(D, "stationary", shape=shape, seed=seed, sigma_c4=s4, sigma_c0=s0, cp_spacing=float(h),
+                        spacing=(1.0,) * D, origin=tuple([0.5, -1.0, 2.0][:D]), **kw)
+
+
+@pytest.mark.parametrize("case", TABLE_CASES)
+@pytest.mark.parametrize("metric", [abi.MSE, abi.NCC])
+@pytest.mark.parametrize("with_df", [False, True])
+def test_table_path_matches_oracle_and_generic(case, metric, with_df):
+    D, h, shape, s4, s0 = case
+    pb, cp, cpw = _table_problem(D, h, shape, s4, s0, seed=91)
+    df = _df_for(pb, 9) if with_df else None
+    ev = GpuKernelEvaluator(pb)
+    assert ev.path() == GpuKernelEvaluator.TABLE
+    ev.SetRegularizerRD(0.05)
+    ev.SetRegularizerRKHS(0.02)
+    r, g = ev.getValueAndDerivative(metric, cp, cpw, df)
+    orc = O.Oracle(pb)
+    orc.set_regularizers(rkhs=0.02, rd=0.05)
+    ro, go = orc.evaluate(metric, cp, cpw, df)
+    assert r["num_pixels_counted"] == ro["num_pixels_counted"]
+    for k in ("measure", "reg_value_rd", "reg_value_rkhs"):
+        assert rel_err(r[k], ro[k]) <= TOL_VALUE, k
+    assert max_rel(g, go) <= TOL_DERIV
+    assert ev.path(1) == GpuKernelEvaluator.GENERIC
+    r2, g2 = ev.getValueAndDerivative(metric, cp, cpw, df)
+    assert r2["num_pixels_counted"] == r["num_pixels_counted"]
+    assert rel_err(r["measure"], r2["measure"]) <= TOL_VALUE
+    assert max_rel(g, g2) <= TOL_DERIV
+
+
+@pytest.mark.parametrize("case", TABLE_CASES[:3])
+def test_table_path_metric_level_and_optimizer(case):
+    D, h, shape, s4, s0 = case
+    pb, cp, cpw = _table_problem(D, h, shape, s4, s0, seed=93, weights=False)
+    params = np.ascontiguousarray(cp.T.reshape(-1))
+    params[::5] = 0.0
+    ev = GpuKernelEvaluator(pb)
+    assert ev.path() == GpuKernelEvaluator.TABLE
+    orc = O.Oracle(pb)
+    m = MetricDesc.make("ncc", l1=1e-3, l21=1e-3, l2=1e-3, rd=1e-2, pg=1e-3)
+    v, g = ev.metric(m, params, cpw)
+    vo, go = orc.metric(m, params, cpw)
+    for k in ("value", "measure", "reg_value"):
+        assert rel_err(v[k], vo[k]) <= TOL_VALUE, k
+    assert max_rel(g, go) <= TOL_DERIV
+    o = OptimizerDesc.make(a=2.0, number_of_iterations=4)
+    opt = Optimizer(ev, o, MetricDesc.make("ncc", rd=1e-3), np.zeros(pb.num_parameters), cpw)
+    oo = O.OracleOptimizer(orc, o, MetricDesc.make("ncc", rd=1e-3), np.zeros(pb.num_parameters), cpw)
+    opt.run(4)
+    vals = oo.run(4)
+    assert rel_err(opt.state()["value"], vals[-1]) <= 1e-4
+    assert max_rel(opt.parameters(), oo.position) <= 1e-3
