@@ -125,10 +125,12 @@ struct skm_evaluator {
 
     // device memory
     float *d_fixed = nullptr, *d_coeffs = nullptr, *d_wimg = nullptr, *d_wten = nullptr;
+    float4 *d_coeffs4 = nullptr;
     float4 *d_cpd = nullptr, *d_df = nullptr, *d_samp = nullptr, *d_dense = nullptr, *d_dense_sw = nullptr;
     unsigned char *d_dense_in = nullptr, *d_dense_sw_in = nullptr;
     uint32_t *d_shifts = nullptr;
     double *d_in = nullptr;          // uploaded parameters (AoS or planar) followed by weights
+    unsigned *d_counters = nullptr;   // ticket counters of the fused last-block finalizations
     double *d_part = nullptr, *d_stats = nullptr, *d_deriv = nullptr, *d_rpart = nullptr, *d_out = nullptr;
     long long df_texels = 0;
 
@@ -149,8 +151,8 @@ struct skm_evaluator {
     ~skm_evaluator()
     {
         if (device >= 0) cudaSetDevice(device);
-        void *bufs[] = {d_fixed, d_coeffs, d_wimg, d_wten, d_cpd, d_df, d_samp, d_dense, d_dense_sw, d_dense_in,
-                        d_dense_sw_in, d_shifts, d_in, d_part, d_stats, d_deriv, d_rpart, d_out};
+        void *bufs[] = {d_fixed, d_coeffs, d_coeffs4, d_wimg, d_wten, d_cpd, d_df, d_samp, d_dense, d_dense_sw, d_dense_in,
+                        d_dense_sw_in, d_shifts, d_in, d_counters, d_part, d_stats, d_deriv, d_rpart, d_out};
         for (void *b : bufs)
             if (b) cudaFree(b);
         table_free(table);
@@ -334,7 +336,7 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         e->value_blocks = (int)((ns + kValueThreads - 1) / kValueThreads);
         e->deriv_blocks = (int)((e->C + (kDerivThreads / 32) - 1) / (kDerivThreads / 32));
         e->dense_blocks = (int)((e->N + 255) / 256);
-        e->gather_blocks = (int)((e->C + 255) / 256);
+        e->gather_blocks = (int)((e->C + 31) / 32);
 
         // kernel parameters: GKernel<float> members are floats (Kernel.h:216-221)
         KernelParams &K = P.K;
@@ -361,6 +363,14 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         for (long long i = 0; i < ncoef; ++i) tmp[i] = (float)d->moving_coefficients[i];
         if (dalloc(&e->d_coeffs, ncoef)) return SKM_ERR_CUDA;
         SKM_CUDA(cudaMemcpy(e->d_coeffs, tmp.data(), ncoef * sizeof(float), cudaMemcpyHostToDevice));
+        {   // row-expanded copy: one aligned 16-byte load per B-spline stencil row
+            std::vector<float4> c4((size_t)ncoef);
+            for (long long i = 0; i < ncoef; ++i)
+                c4[i] = make_float4(tmp[i], i + 1 < ncoef ? tmp[i + 1] : 0.f, i + 2 < ncoef ? tmp[i + 2] : 0.f,
+                                    i + 3 < ncoef ? tmp[i + 3] : 0.f);
+            if (dalloc(&e->d_coeffs4, ncoef)) return SKM_ERR_CUDA;
+            SKM_CUDA(cudaMemcpy(e->d_coeffs4, c4.data(), ncoef * sizeof(float4), cudaMemcpyHostToDevice));
+        }
         if (d->use_weight_image) {
             long long n = texels(d->weight_image_geometry, D);
             std::vector<float> w((size_t)n);
@@ -379,6 +389,7 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         }
         P.fixed_data = e->d_fixed;
         P.coeffs = e->d_coeffs;
+        P.coeffs4 = e->d_coeffs4;
 
         if (dalloc(&e->d_cpd, e->C)) return SKM_ERR_CUDA;
         P.cpd = e->d_cpd;
@@ -390,6 +401,8 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         if (dalloc(&e->d_in, e->C * (D + 1))) return SKM_ERR_CUDA;
         if (dalloc(&e->d_part, (size_t)NQ * e->value_blocks)) return SKM_ERR_CUDA;
         if (dalloc(&e->d_stats, NS)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_counters, 4)) return SKM_ERR_CUDA;
+        SKM_CUDA(cudaMemset(e->d_counters, 0, 4 * sizeof(unsigned)));
         if (dalloc(&e->d_deriv, e->nparams)) return SKM_ERR_CUDA;
         if (dalloc(&e->d_rpart, (size_t)NR * std::max(e->deriv_blocks, e->gather_blocks))) return SKM_ERR_CUDA;
         if (dalloc(&e->d_out, NO)) return SKM_ERR_CUDA;
@@ -398,7 +411,7 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         rng_jump_table(e->jump);
         int trc = table_plan(e->table, e->P, D, e->stream);
         if (trc) return fail(SKM_ERR_CUDA, "table plan failed: %s", cudaGetErrorString(cudaGetLastError()));
-        if (e->table.enabled && table_set_attributes(e->table))
+        if (e->table.enabled && (table_set_attributes(e->table) || table_size_grids(e->table)))
             return fail(SKM_ERR_CUDA, "table kernel attributes: %s", cudaGetErrorString(cudaGetLastError()));
         return SKM_OK;
     }();
@@ -539,18 +552,17 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     const bool tab = e->use_table && e->table.enabled && metric != SKM_LCC;
     if (metric != SKM_LCC) {
         if (tab) {
-            if (table_value(e->table, e->P, D, e->stream))
+            if (table_value(e->table, e->P, D, metric, e->d_stats, e->d_counters, e->stream))
                 return fail(SKM_ERR_CUDA, "table value pass: %s", cudaGetErrorString(cudaGetLastError()));
         } else if ((rc = dispatch<LaunchValue>(D, kind, e))) {
             return rc;
         }
     }
     if (ev) SKM_CUDA(cudaEventRecord(ev[0], e->stream));
-    if (tab)
-        stats_kernel<<<1, 1024, 0, e->stream>>>(e->table.d_part, e->table.dev.value_blocks, metric, e->d_stats);
-    else
+    if (!tab) {                                  // the table path computes the statistics in its warp kernel
         stats_kernel<<<1, 1024, 0, e->stream>>>(e->d_part, e->value_blocks, metric, e->d_stats);
-    SKM_CHECK_LAUNCH();
+        SKM_CHECK_LAUNCH();
+    }
     if (ev) SKM_CUDA(cudaEventRecord(ev[1], e->stream));
     DerivParams Q{};
     Q.metric = metric;
@@ -573,6 +585,8 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     Q.dense_sw_in = e->d_dense_sw_in;
     Q.deriv = e->d_deriv;
     Q.rpart = e->d_rpart;
+    Q.out = e->d_out;
+    Q.counter = e->d_counters + 1;
     bool any_reg = w.rkhs > 0 || w.rd > 0 || w.pg > 0 || w.with_metric;
     if (derivative) {
         if (tab) {
@@ -585,10 +599,11 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
         if ((rc = dispatch<LaunchRegValue>(D, kind, e, Q))) return rc;
     }
     if (ev) SKM_CUDA(cudaEventRecord(ev[2], e->stream));
-    const int rblocks = (derivative && tab) ? e->gather_blocks : e->deriv_blocks;
-    result_kernel<<<1, 256, 0, e->stream>>>(e->d_stats, (derivative || any_reg) ? e->d_rpart : nullptr, rblocks,
-                                           w.rkhs, w.rd, w.pg, w.l1, w.l21, w.l2, e->d_out);
-    SKM_CHECK_LAUNCH();
+    if (!(derivative && tab)) {                 // the table gather computes the result itself
+        result_kernel<<<1, 256, 0, e->stream>>>(e->d_stats, (derivative || any_reg) ? e->d_rpart : nullptr,
+                                               e->deriv_blocks, w.rkhs, w.rd, w.pg, w.l1, w.l21, w.l2, e->d_out);
+        SKM_CHECK_LAUNCH();
+    }
     if (ev) SKM_CUDA(cudaEventRecord(ev[3], e->stream));
     return SKM_OK;
 }

@@ -308,6 +308,71 @@ __device__ __forceinline__ void bspline_derivs(const float *__restrict__ c, cons
     }
 }
 
+// Same as bspline_derivs, reading the coefficients from the row-expanded copy
+// c4[i] = (c[i], c[i+1], c[i+2], c[i+3]): one aligned 16-byte load per stencil row.
+template <int D>
+__device__ __forceinline__ void bspline_derivs4(const float4 *__restrict__ c4, const Geo &mg, const double *l,
+                                                float &val, float *grad)
+{
+    int ii[3] = {0, 0, 0};
+    float W[4][3], dW[4][3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        ii[d] = (int)l[d];
+        float w = (float)(l[d] - (double)ii[d]);
+        float w3 = (1.0f / 6.0f) * w * w * w;
+        float w0 = (1.0f / 6.0f) + 0.5f * w * (w - 1.0f) - w3;
+        float w2 = w + w0 - 2.0f * w3;
+        W[3][d] = w3; W[0][d] = w0; W[2][d] = w2; W[1][d] = 1.0f - w0 - w2 - w3;
+        float d3 = 0.5f * w * w;
+        float d0 = w - 0.5f - d3;
+        float d2 = 1.0f + d0 - 2.0f * d3;
+        dW[3][d] = d3; dW[0][d] = d0; dW[2][d] = d2; dW[1][d] = -d0 - d2 - d3;
+    }
+    if (D == 3) {
+        float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+        const long long sy = mg.st[1], sz = mg.st[2];
+        const float4 *base = c4 + ii[0] + ii[1] * sy + ii[2] * sz;
+#pragma unroll
+        for (int z = 0; z < 4; ++z) {
+            float z0 = 0.f, z1 = 0.f, z3 = 0.f;
+#pragma unroll
+            for (int y = 0; y < 4; ++y) {
+                const float4 r = __ldg(base + y * sy + z * sz);
+                float dx = dW[0][0] * r.x + dW[1][0] * r.y + dW[2][0] * r.z + dW[3][0] * r.w;
+                float vx = W[0][0] * r.x + W[1][0] * r.y + W[2][0] * r.z + W[3][0] * r.w;
+                z0 += W[y][1] * dx;
+                z1 += dW[y][1] * vx;
+                z3 += W[y][1] * vx;
+            }
+            c0 += W[z][2] * z0;
+            c1 += W[z][2] * z1;
+            c2 += dW[z][2] * z3;
+            c3 += W[z][2] * z3;
+        }
+        val = c3;
+        grad[0] = c0 * (float)mg.inv[0];
+        grad[1] = c1 * (float)mg.inv[1];
+        grad[2] = c2 * (float)mg.inv[2];
+    } else {
+        float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+        const long long sy = mg.st[1];
+        const float4 *base = c4 + ii[0] + ii[1] * sy;
+#pragma unroll
+        for (int y = 0; y < 4; ++y) {
+            const float4 r = __ldg(base + y * sy);
+            float dx = dW[0][0] * r.x + dW[1][0] * r.y + dW[2][0] * r.z + dW[3][0] * r.w;
+            float vx = W[0][0] * r.x + W[1][0] * r.y + W[2][0] * r.z + W[3][0] * r.w;
+            c0 += W[y][1] * dx;
+            c1 += dW[y][1] * vx;
+            c2 += W[y][1] * vx;
+        }
+        val = c2;
+        grad[0] = c0 * (float)mg.inv[0];
+        grad[1] = c1 * (float)mg.inv[1];
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // PCG32 stream of UniformRng (UniformRng.h:28-46) with LCG jump-ahead so that every sample
 // draws its own D values of the sequential stream in parallel.

@@ -39,6 +39,7 @@ struct EvalParams {
     long long C;       // control points
     const float *__restrict__ fixed_data;
     const float *__restrict__ coeffs;
+    const float4 *__restrict__ coeffs4;  // row-expanded coefficients (c[i], c[i+1], c[i+2], c[i+3])
     const float4 *__restrict__ cpd;     // (alpha_x, alpha_y, alpha_z, w) per control point
     const float4 *__restrict__ dfd;     // displacement field, 4 floats per texel
     const uint32_t *__restrict__ shifts; // packed per-sample shift (8 bits per axis)
@@ -60,6 +61,8 @@ struct DerivParams {
     const unsigned char *__restrict__ dense_sw_in;
     double *__restrict__ deriv;          // planar output
     double *__restrict__ rpart;          // [NR][blocks]
+    double *__restrict__ out;            // result vector (fused finalization)
+    unsigned *counter;                   // ticket counter of the fused finalization
 };
 
 // ---- sample positions ------------------------------------------------------------------------
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(256) value_kernel(EvalParams P, float4 *__rest
             moving_local<D, KIND, false>(P, p, ml);
             if (bspline_inside<D>(P.mov, ml)) {
                 float m, g[3] = {0.f, 0.f, 0.f};
-                bspline_derivs<D>(P.coeffs, P.mov, ml, m, g);
+                bspline_derivs4<D>(P.coeffs4, P.mov, ml, m, g);
                 double f = (double)P.fixed_data[lin_of<D>(P.fixed, sp)];
                 double md = (double)m;
                 v[Q_COUNT] = 1.0;
@@ -222,55 +225,85 @@ __global__ void __launch_bounds__(256) value_kernel(EvalParams P, float4 *__rest
 }
 
 // ---- statistics (GpuEvaluator.cu:449-571 host loops, on the device, FP64, fixed order) ------
+// global statistics from the summed quantities (the host loops of GpuEvaluator.cu:449-571)
+__device__ inline void stats_finalize(const double *v, int metric, double *__restrict__ stats)
+{
+    double n = v[Q_COUNT];
+    double st[NS];
+    for (int k = 0; k < NS; ++k) st[k] = 0.0;
+    st[S_COUNT] = n;
+    if (metric == 0) {
+        st[S_MEASURE] = v[Q_D2] / n;                       // cu:462-470
+        st[S_COEF_F] = -2.0 / n;                           // 2*(m-f)/n  (MSE.cu:291, cu:599-603)
+        st[S_COEF_M] = 2.0 / n;
+        st[S_COEF_C] = 0.0;
+    } else if (metric == 1) {
+        double sf = v[Q_SF], sm = v[Q_SM];
+        double sff = v[Q_SFF] - sf * sf / n;               // cu:519-524
+        double smm = v[Q_SMM] - sm * sm / n;
+        double sfm = v[Q_SFM] - sf * sm / n;
+        double denom = -1.0 * sqrt(sff * smm);
+        st[S_MEASURE] = denom != 0.0 ? sfm / denom : 0.0;
+        st[S_MEAN_F] = sf / n;
+        st[S_MEAN_M] = sm / n;
+        st[S_DENOM] = denom;
+        st[S_SFM] = sfm;
+        st[S_SMM] = smm;
+        // (dF - (sfm/smm) dM)/denom with dF = sum (f - mf) w k gradM, dM = sum (m - mm) w k gradM
+        // (NCC.cu:177-179, cu:624-633) == w sum k gradM (a f + b m + c)
+        if (denom != 0.0) {
+            double rho = sfm / smm;
+            st[S_COEF_F] = 1.0 / denom;
+            st[S_COEF_M] = -rho / denom;
+            st[S_COEF_C] = (-st[S_MEAN_F] + rho * st[S_MEAN_M]) / denom;
+        }
+    } else {
+        st[S_MEASURE] = v[Q_CC] / n;                       // cu:556-570
+        st[S_COEF_C] = 1.0 / n;                            // derivatives /= pixelsCounted (cu:642-646)
+    }
+    st[S_VALID] = 1.0;
+    for (int k = 0; k < NS; ++k) stats[k] = st[k];
+}
+
+// Sums the NV per-block partials [k][nblocks] with the whole block in a fixed order (L2 reads,
+// bypassing L1 so that partials written by other blocks of the same launch are seen).
+template <int NV>
+__device__ __forceinline__ void sum_partials(const double *part, int nblocks, double *v, double *sh)
+{
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += __ldcg(part + (long long)k * nblocks + b);
+        v[k] = s;
+    }
+    block_sum<NV>(v, sh);
+}
+
+// "Last block finalizes": every block has written its partials; the block that arrives last
+// (atomic ticket) returns true, after which it may read all partials.  The ticket counter is
+// reset by that block, so the pattern can repeat in the next launch (and in graph replays).
+__device__ __forceinline__ bool last_block_arrived(unsigned *counter)
+{
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned ticket = atomicAdd(counter, 1u);
+        last = (ticket == gridDim.x - 1);
+        if (last) *counter = 0u;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
 static __global__ void __launch_bounds__(1024) stats_kernel(const double *__restrict__ part, int nblocks, int metric,
                                                      double *__restrict__ stats)
 {
     __shared__ double sh[NQ * 32];
     double v[NQ];
-#pragma unroll
-    for (int k = 0; k < NQ; ++k) {
-        double s = 0.0;
-        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += part[(long long)k * nblocks + b];
-        v[k] = s;
-    }
-    block_sum<NQ>(v, sh);
-    if (threadIdx.x == 0) {
-        double n = v[Q_COUNT];
-        double st[NS];
-        for (int k = 0; k < NS; ++k) st[k] = 0.0;
-        st[S_COUNT] = n;
-        if (metric == 0) {
-            st[S_MEASURE] = v[Q_D2] / n;                       // cu:462-470
-            st[S_COEF_F] = -2.0 / n;                           // 2*(m-f)/n  (MSE.cu:291, cu:599-603)
-            st[S_COEF_M] = 2.0 / n;
-            st[S_COEF_C] = 0.0;
-        } else if (metric == 1) {
-            double sf = v[Q_SF], sm = v[Q_SM];
-            double sff = v[Q_SFF] - sf * sf / n;               // cu:519-524
-            double smm = v[Q_SMM] - sm * sm / n;
-            double sfm = v[Q_SFM] - sf * sm / n;
-            double denom = -1.0 * sqrt(sff * smm);
-            st[S_MEASURE] = denom != 0.0 ? sfm / denom : 0.0;
-            st[S_MEAN_F] = sf / n;
-            st[S_MEAN_M] = sm / n;
-            st[S_DENOM] = denom;
-            st[S_SFM] = sfm;
-            st[S_SMM] = smm;
-            // (dF - (sfm/smm) dM)/denom with dF = sum (f - mf) w k gradM, dM = sum (m - mm) w k gradM
-            // (NCC.cu:177-179, cu:624-633) == w sum k gradM (a f + b m + c)
-            if (denom != 0.0) {
-                double rho = sfm / smm;
-                st[S_COEF_F] = 1.0 / denom;
-                st[S_COEF_M] = -rho / denom;
-                st[S_COEF_C] = (-st[S_MEAN_F] + rho * st[S_MEAN_M]) / denom;
-            }
-        } else {
-            st[S_MEASURE] = v[Q_CC] / n;                       // cu:556-570
-            st[S_COEF_C] = 1.0 / n;                            // derivatives /= pixelsCounted (cu:642-646)
-        }
-        st[S_VALID] = 1.0;
-        for (int k = 0; k < NS; ++k) stats[k] = st[k];
-    }
+    sum_partials<NQ>(part, nblocks, v, sh);
+    if (threadIdx.x == 0) stats_finalize(v, metric, stats);
 }
 
 // ---- derivative pass: warp per control point ------------------------------------------------
@@ -703,39 +736,41 @@ __global__ void __launch_bounds__(256) regvalue_kernel(EvalParams P, DerivParams
 }
 
 // final scalars: measure, regularizer values, weighted sum (metric hxx:531-538, 572)
+__device__ inline void result_finalize(const double *stats, const double *v, double w_rkhs, double w_rd,
+                                       double w_pg, double w_l1, double w_l21, double w_l2, double *__restrict__ out)
+{
+    double reg = 0.0;
+    if (w_l1 > 0) reg += w_l1 * v[R_L1];
+    if (w_l21 > 0) reg += w_l21 * v[R_L21];
+    if (w_l2 > 0) reg += w_l2 * v[R_L2];
+    if (w_rkhs > 0) reg += w_rkhs * v[R_RKHS];
+    if (w_rd > 0) reg += w_rd * v[R_RD];
+    if (w_pg > 0) reg += w_pg * v[R_PG];
+    out[O_MEASURE] = stats[S_MEASURE];
+    out[O_RKHS] = v[R_RKHS];
+    out[O_RD] = v[R_RD];
+    out[O_PG] = v[R_PG];
+    out[O_L1] = v[R_L1];
+    out[O_L21] = v[R_L21];
+    out[O_L2] = v[R_L2];
+    out[O_REG] = reg;
+    out[O_VALUE] = stats[S_MEASURE] + reg;
+    out[O_COUNT] = stats[S_COUNT];
+}
+
 static __global__ void __launch_bounds__(256) result_kernel(const double *__restrict__ stats, const double *__restrict__ rpart,
                                                      int nblocks, double w_rkhs, double w_rd, double w_pg, double w_l1,
                                                      double w_l21, double w_l2, double *__restrict__ out)
 {
     __shared__ double sh[NR * 32];
     double v[NR];
+    if (rpart) {
+        sum_partials<NR>(rpart, nblocks, v, sh);
+    } else {
 #pragma unroll
-    for (int k = 0; k < NR; ++k) {
-        double s = 0.0;
-        if (rpart)
-            for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += rpart[(long long)k * nblocks + b];
-        v[k] = s;
+        for (int k = 0; k < NR; ++k) v[k] = 0.0;
     }
-    block_sum<NR>(v, sh);
-    if (threadIdx.x == 0) {
-        double reg = 0.0;
-        if (w_l1 > 0) reg += w_l1 * v[R_L1];
-        if (w_l21 > 0) reg += w_l21 * v[R_L21];
-        if (w_l2 > 0) reg += w_l2 * v[R_L2];
-        if (w_rkhs > 0) reg += w_rkhs * v[R_RKHS];
-        if (w_rd > 0) reg += w_rd * v[R_RD];
-        if (w_pg > 0) reg += w_pg * v[R_PG];
-        out[O_MEASURE] = stats[S_MEASURE];
-        out[O_RKHS] = v[R_RKHS];
-        out[O_RD] = v[R_RD];
-        out[O_PG] = v[R_PG];
-        out[O_L1] = v[R_L1];
-        out[O_L21] = v[R_L21];
-        out[O_L2] = v[R_L2];
-        out[O_REG] = reg;
-        out[O_VALUE] = stats[S_MEASURE] + reg;
-        out[O_COUNT] = stats[S_COUNT];
-    }
+    if (threadIdx.x == 0) result_finalize(stats, v, w_rkhs, w_rd, w_pg, w_l1, w_l21, w_l2, out);
 }
 
 // ---- LCC: dense fields and per-sample values --------------------------------------------------
@@ -757,7 +792,7 @@ __global__ void __launch_bounds__(256) dense_kernel(EvalParams P, float4 *__rest
     unsigned char in = 0;
     if (bspline_inside<D>(P.mov, ml)) {
         float m, g[3] = {0.f, 0.f, 0.f};
-        bspline_derivs<D>(P.coeffs, P.mov, ml, m, g);
+        bspline_derivs4<D>(P.coeffs4, P.mov, ml, m, g);
         rec = make_float4(g[0], g[1], D > 2 ? g[2] : 0.f, m);
         in = 1;
     }

@@ -40,14 +40,18 @@ __global__ void rng_advance_kernel(unsigned long long *state, RngJump J, unsigne
     if (threadIdx.x == 0 && blockIdx.x == 0) *state = lcg_advance(*state, steps, J);
 }
 
+// One optimizer step over all parameters; the last block (fixed-order sum of the per-block
+// <g, g_prev> partials) then updates the adaptive time, the best value and the counters.
 __global__ void __launch_bounds__(256) opt_step_kernel(const double *__restrict__ g, double *__restrict__ tmp,
                                                        double *__restrict__ base, double *__restrict__ pos,
-                                                       double *__restrict__ best, const double *__restrict__ scal,
+                                                       double *__restrict__ best, double *__restrict__ scal,
                                                        const double *__restrict__ out, long long P, int orthant,
-                                                       double a, double A, double alpha, double *__restrict__ sp_part)
+                                                       double a, double A, double alpha, double f_max, double f_min,
+                                                       double omega, double *__restrict__ sp_part, unsigned *counter)
 {
     __shared__ double sh[32];
-    const double lr = a / pow(A + scal[T_TIME] + 1.0, alpha);
+    const double t = scal[T_TIME];
+    const double lr = a / pow(A + t + 1.0, alpha);
     const bool improving = out[O_VALUE] < scal[T_BEST];
     double sp = 0.0;
     for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < P; j += (long long)gridDim.x * blockDim.x) {
@@ -64,26 +68,21 @@ __global__ void __launch_bounds__(256) opt_step_kernel(const double *__restrict_
     double v[1] = {sp};
     block_sum<1>(v, sh);
     if (threadIdx.x == 0) sp_part[blockIdx.x] = v[0];
-}
-
-__global__ void opt_finish_kernel(const double *__restrict__ sp_part, int nblocks, double *__restrict__ scal,
-                                  const double *__restrict__ out, double a, double A, double alpha, double f_max,
-                                  double f_min, double omega)
-{
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double sp = 0.0;
-    for (int b = 0; b < nblocks; ++b) sp += sp_part[b];
-    const double t = scal[T_TIME];
-    const double lr = a / pow(A + t + 1.0, alpha);
-    const double x = -sp;
-    const double f = f_min + (f_max - f_min) / (1.0 - (f_max / f_min) * exp(-x / omega));
-    scal[T_TIME] = fmax(0.0, t + f);
-    if (out[O_VALUE] < scal[T_BEST]) scal[T_BEST] = out[O_VALUE];
-    scal[T_LR] = lr;
-    scal[T_SP] = sp;
-    scal[T_VALUE] = out[O_VALUE];
-    scal[T_ITER] += 1.0;
-    scal[T_COUNT] = out[O_COUNT];
+    if (last_block_arrived(counter)) {
+        double w[1];
+        sum_partials<1>(sp_part, gridDim.x, w, sh);
+        if (threadIdx.x == 0) {
+            const double x = -w[0];
+            const double f = f_min + (f_max - f_min) / (1.0 - (f_max / f_min) * exp(-x / omega));
+            scal[T_TIME] = fmax(0.0, t + f);
+            if (out[O_VALUE] < scal[T_BEST]) scal[T_BEST] = out[O_VALUE];
+            scal[T_LR] = lr;
+            scal[T_SP] = w[0];
+            scal[T_VALUE] = out[O_VALUE];
+            scal[T_ITER] += 1.0;
+            scal[T_COUNT] = out[O_COUNT];
+        }
+    }
 }
 
 }  // namespace
@@ -145,10 +144,8 @@ static int optimizer_iteration(skm_optimizer *o, cudaEvent_t *ev = nullptr)
     if (rc) return rc;
     opt_step_kernel<<<o->step_blocks, 256, 0, e->stream>>>(e->d_deriv, o->d_tmp, o->d_base, o->d_pos, o->d_best,
                                                           o->d_scal, e->d_out, o->P, o->od.orthant_projection, o->od.a,
-                                                          o->od.A, o->od.alpha, o->d_sp);
-    SKM_CHECK_LAUNCH();
-    opt_finish_kernel<<<1, 32, 0, e->stream>>>(o->d_sp, o->step_blocks, o->d_scal, e->d_out, o->od.a, o->od.A,
-                                              o->od.alpha, o->od.f_max, o->od.f_min, o->od.omega);
+                                                          o->od.A, o->od.alpha, o->od.f_max, o->od.f_min, o->od.omega,
+                                                          o->d_sp, e->d_counters + 2);
     SKM_CHECK_LAUNCH();
     if (ev) SKM_CUDA(cudaEventRecord(ev[7], e->stream));
     return SKM_OK;

@@ -12,8 +12,9 @@
 // stationary kernel (every point they add outside the support has k = 0).
 //
 // Kernels (one launch each):
-//   table_value_kernel      T x A register-blocked transform for 4 z-phases per thread, then
-//                           B-spline warp + metric statistics per texel; records (grad M, m) in
+//   table_transform_kernel  T x A register-blocked transform (4 z-phases of 2 cells per thread),
+//                           u in cell-phase layout.
+//   table_warp_kernel       per texel: B-spline warp + metric statistics; records (grad M, m) in
 //                           cell-phase layout and per-block FP64 partials.
 //   table_contrib_kernel    Contrib[t][cell] = sum_p T[p][t] g(cell, p): a register-blocked GEMM
 //                           (taps x phases x cells) with T and the cells' g tile in shared memory.
@@ -49,6 +50,7 @@ struct TableDev {
     const float *tgemm;  // [phase][ntap_pad]
     const float *kcp;    // [nc0*nc1*nc2] kernel between control points at an offset
     float4 *rec;         // [cell][phase]: grad M, m
+    float4 *ucp;         // [cell][phase]: u = sum_t T w alpha
     const float *fixcp;  // [cell][phase]: fixed image value (0 outside)
     float *contrib;      // [3][ntap][ncell]
     double *part;        // [NQ][value blocks]
@@ -59,138 +61,175 @@ struct TablePlan {
     bool enabled = false;
     TableDev dev{};
     float *d_tfwd = nullptr, *d_tgemm = nullptr, *d_kcp = nullptr, *d_fixcp = nullptr, *d_contrib = nullptr;
-    float4 *d_rec = nullptr;
+    float4 *d_rec = nullptr, *d_ucp = nullptr;
     double *d_part = nullptr;
-    int hl = 1;          // phases per thread in the value kernel (template argument)
+    int hl = 1;          // z phases per thread in the transform kernel (template argument)
+    int ncz = 1;         // cells per thread along z in the transform kernel
+    int transform_blocks = 0, contrib_blocks = 0;
 };
 
 // ------------------------------------------------------------------------------------------------
-// value pass
-template <int D, int HL>
-__global__ void __launch_bounds__(256) table_value_kernel(EvalParams P, TableDev T)
+// value pass, part 1: u(q, p) = sum_t T[p][t] (w alpha)[q + t] for HL z-phases of NCZ cells
+// (stacked along z) per thread.  Threads of a warp share the control-point values (2 cells) and
+// read 16 different table rows, so every tap costs 3 shared-memory wavefronts per 12*NCZ FMAs.
+template <int HL, int NCZ>
+__global__ void __launch_bounds__(256) table_transform_kernel(EvalParams P, TableDev T)
 {
     extern __shared__ float4 smem4[];
-    __shared__ double sh[NQ * 32];
     const int nphxy = T.h[0] * T.h[1];
     const int ncell_blk = blockDim.x / nphxy;
-    // A tile: (tile_x + nt0 - 1) x (tile_y + nt1 - 1) x nt2 control points (w*alpha)
-    const int ax = T.tile_x + T.nt[0] - 1, ay = T.tile_y + T.nt[1] - 1, az = T.nt[2];
+    const int ax = T.tile_x + T.nt[0] - 1, ay = T.tile_y + T.nt[1] - 1, az = NCZ + T.nt[2] - 1;
     float4 *A = smem4;
     float *tf = reinterpret_cast<float *>(smem4 + ax * ay * az);
-    const int tile = blockIdx.x;
-    const int tx0 = (tile % T.tiles_x) * T.tile_x;
-    const int ty0 = ((tile / T.tiles_x) % T.tiles_y) * T.tile_y;
-    const int tz0 = tile / (T.tiles_x * T.tiles_y);
-    // cell origin of the tile (cell coordinates relative to qmin)
-    const int q0[3] = {T.qmin[0] + tx0, T.qmin[1] + ty0, T.qmin[2] + tz0};
-    for (int i = threadIdx.x; i < ax * ay * az; i += blockDim.x) {
-        int x = i % ax, y = (i / ax) % ay, z = i / (ax * ay);
-        int j[3] = {q0[0] + T.tlo[0] + x, q0[1] + T.tlo[1] + y, q0[2] + T.tlo[2] + z};
-        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
-        bool in = j[0] >= 0 && j[0] < P.cp.n[0] && j[1] >= 0 && j[1] < P.cp.n[1] && j[2] >= 0 && j[2] < P.cp.n[2];
-        if (in) {
-            float4 c = P.cpd[j[0] + P.cp.st[1] * j[1] + P.cp.st[2] * j[2]];
-            a = make_float4(c.w * c.x, c.w * c.y, c.w * c.z, 0.f);
-        }
-        A[i] = a;
-    }
-    const int tf_n = T.ntap * nphxy * HL;
-    for (int i = threadIdx.x; i < tf_n; i += blockDim.x) tf[i] = T.tfwd[i];
-    __syncthreads();
-
+    // the table once per block (16-byte loads), then the block walks its tiles
+    const int tf_n4 = T.ntap * nphxy * HL / 4;
+    for (int i = threadIdx.x; i < tf_n4; i += blockDim.x)
+        reinterpret_cast<float4 *>(tf)[i] = __ldg(reinterpret_cast<const float4 *>(T.tfwd) + i);
+    for (int i = tf_n4 * 4 + threadIdx.x; i < T.ntap * nphxy * HL; i += blockDim.x) tf[i] = T.tfwd[i];
     const int pxy = threadIdx.x % nphxy;
-    const int cl = threadIdx.x / nphxy;            // cell within the block
+    const int cl = threadIdx.x / nphxy;
     const int px = pxy % T.h[0], py = pxy / T.h[0];
     const int cx = cl % T.tile_x, cy = cl / T.tile_x;
-    double v[NQ];
+    const int ntiles = T.tiles_x * T.tiles_y * T.tiles_z;
+    const int nt0 = T.nt[0];
+    const int plane = ax * ay;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int tx0 = (tile % T.tiles_x) * T.tile_x;
+        const int ty0 = ((tile / T.tiles_x) % T.tiles_y) * T.tile_y;
+        const int tz0 = (tile / (T.tiles_x * T.tiles_y)) * NCZ;
+        const int q0[3] = {T.qmin[0] + tx0, T.qmin[1] + ty0, T.qmin[2] + tz0};
+        __syncthreads();                                   // previous tile done with A
+        for (int i = threadIdx.x; i < ax * ay * az; i += blockDim.x) {
+            const int x = i % ax, y = (i / ax) % ay, z = i / (ax * ay);
+            const int j[3] = {q0[0] + T.tlo[0] + x, q0[1] + T.tlo[1] + y, q0[2] + T.tlo[2] + z};
+            float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (j[0] >= 0 && j[0] < P.cp.n[0] && j[1] >= 0 && j[1] < P.cp.n[1] && j[2] >= 0 && j[2] < P.cp.n[2]) {
+                const float4 c = __ldg(P.cpd + j[0] + P.cp.st[1] * j[1] + P.cp.st[2] * j[2]);
+                a = make_float4(c.w * c.x, c.w * c.y, c.w * c.z, 0.f);
+            }
+            A[i] = a;
+        }
+        __syncthreads();
+        if (cl >= ncell_blk || tx0 + cx >= T.nq[0] || ty0 + cy >= T.nq[1]) continue;
+        float acc[NCZ][HL][3];
 #pragma unroll
-    for (int k = 0; k < NQ; ++k) v[k] = 0.0;
-    const bool cell_ok = cl < ncell_blk && tx0 + cx < T.nq[0] && ty0 + cy < T.nq[1];
-    if (cell_ok) {
-        float acc[HL][3];
+        for (int c = 0; c < NCZ; ++c)
 #pragma unroll
-        for (int k = 0; k < HL; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.f;
+            for (int k = 0; k < HL; ++k) acc[c][k][0] = acc[c][k][1] = acc[c][k][2] = 0.f;
         int tap = 0;
         for (int tz = 0; tz < T.nt[2]; ++tz)
             for (int ty = 0; ty < T.nt[1]; ++ty) {
-                const float4 *arow = A + (cx + ax * ((cy + ty) + ay * tz));
-                for (int tx = 0; tx < T.nt[0]; ++tx, ++tap) {
-                    const float4 a = arow[tx];
-                    const float *t = tf + (tap * nphxy + pxy) * HL;
+                const float4 *arow = A + (cx + ax * (cy + ty) + plane * tz);
+                const float *trow = tf + (tap * nphxy + pxy) * HL;
+#pragma unroll 3
+                for (int tx = 0; tx < nt0; ++tx) {
+                    float tv[HL];
                     if (HL == 4) {
-                        const float4 t4 = *reinterpret_cast<const float4 *>(t);
-                        const float tv[4] = {t4.x, t4.y, t4.z, t4.w};
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            acc[k][0] = fmaf(tv[k], a.x, acc[k][0]);
-                            acc[k][1] = fmaf(tv[k], a.y, acc[k][1]);
-                            acc[k][2] = fmaf(tv[k], a.z, acc[k][2]);
-                        }
+                        const float4 t4 = *reinterpret_cast<const float4 *>(trow + tx * nphxy * HL);
+                        tv[0] = t4.x; tv[1] = t4.y; tv[2] = t4.z; tv[3] = t4.w;
                     } else {
 #pragma unroll
+                        for (int k = 0; k < HL; ++k) tv[k] = trow[tx * nphxy * HL + k];
+                    }
+#pragma unroll
+                    for (int c = 0; c < NCZ; ++c) {
+                        const float4 a = arow[tx + plane * c];
+#pragma unroll
                         for (int k = 0; k < HL; ++k) {
-                            const float tv = t[k];
-                            acc[k][0] = fmaf(tv, a.x, acc[k][0]);
-                            acc[k][1] = fmaf(tv, a.y, acc[k][1]);
-                            acc[k][2] = fmaf(tv, a.z, acc[k][2]);
+                            acc[c][k][0] = fmaf(tv[k], a.x, acc[c][k][0]);
+                            acc[c][k][1] = fmaf(tv[k], a.y, acc[c][k][1]);
+                            acc[c][k][2] = fmaf(tv[k], a.z, acc[c][k][2]);
                         }
                     }
                 }
+                tap += nt0;
             }
-        const int q[3] = {q0[0] + cx, q0[1] + cy, q0[2]};
-        const long long cell_lin = (long long)(tx0 + cx) + (long long)T.nq[0] * ((ty0 + cy) + (long long)T.nq[1] * tz0);
 #pragma unroll
-        for (int k = 0; k < HL; ++k) {
-            const int pz = k;
-            const int ph[3] = {px, py, pz};
-            int x[3] = {0, 0, 0};
-            bool ok = true;
+        for (int c = 0; c < NCZ; ++c) {
+            if (tz0 + c >= T.nq[2]) break;
+            const long long cell =
+                (long long)(tx0 + cx) + (long long)T.nq[0] * ((ty0 + cy) + (long long)T.nq[1] * (tz0 + c));
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                x[d] = T.h[d] * (q[d] - T.qoff[d][ph[d]]) + ph[d];
-                if (x[d] < 0 || x[d] >= P.fixed.n[d]) ok = false;
+            for (int k = 0; k < HL; ++k) {
+                const int p_lin = px + T.h[0] * (py + T.h[1] * k);
+                T.ucp[cell * T.nph + p_lin] = make_float4(acc[c][k][0], acc[c][k][1], acc[c][k][2], 0.f);
             }
-            const int p_lin = px + T.h[0] * (py + T.h[1] * pz);
-            float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (ok) {
-                double fi[3] = {(double)x[0], (double)x[1], (double)x[2]}, p[3], mp[3], ml[3];
-                to_global<D>(P.fixed, fi, p);
-#pragma unroll
-                for (int d = 0; d < D; ++d) mp[d] = p[d];
-                if (P.has_df) {
-                    long long i = nearest_index<D>(P.df, p);
-                    if (i >= 0) {
-                        float4 dv = P.dfd[i];
-                        mp[0] += dv.x;
-                        if (D > 1) mp[1] += dv.y;
-                        if (D > 2) mp[2] += dv.z;
-                    }
-                }
-#pragma unroll
-                for (int d = 0; d < D; ++d) mp[d] += (double)acc[k][d];
-                to_local<D>(P.mov, mp, ml);
-                if (bspline_inside<D>(P.mov, ml)) {
-                    float m, g[3] = {0.f, 0.f, 0.f};
-                    bspline_derivs<D>(P.coeffs, P.mov, ml, m, g);
-                    double f = (double)T.fixcp[cell_lin * T.nph + p_lin];
-                    double md = (double)m;
-                    v[Q_COUNT] += 1.0;
-                    v[Q_D2] += (md - f) * (md - f);
-                    v[Q_SF] += f;
-                    v[Q_SM] += md;
-                    v[Q_SFF] += f * f;
-                    v[Q_SMM] += md * md;
-                    v[Q_SFM] += f * md;
-                    rec = make_float4(g[0], g[1], D > 2 ? g[2] : 0.f, m);
-                }
-            }
-            T.rec[cell_lin * T.nph + p_lin] = rec;
         }
+    }
+}
+
+// value pass, part 2: one thread per (cell, phase) texel -- displacement field, B-spline warp,
+// metric statistics (FP64 block partials) and the (grad M, m) record, all in cell-phase order
+// so that a warp covers a compact brick of texels.
+template <int D>
+__global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev T, int metric, double *stats,
+                                                         unsigned *counter)
+{
+    __shared__ double sh[NQ * 32];
+    double v[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) v[k] = 0.0;
+    const long long total = T.ncell * T.nph;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long cell = i / T.nph;
+        const int p_lin = (int)(i - cell * T.nph);
+        const int cc[3] = {(int)(cell % T.nq[0]), (int)((cell / T.nq[0]) % T.nq[1]),
+                           (int)(cell / ((long long)T.nq[0] * T.nq[1]))};
+        const int ph[3] = {p_lin % T.h[0], (p_lin / T.h[0]) % T.h[1], p_lin / (T.h[0] * T.h[1])};
+        int x[3];
+        bool ok = true;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            x[d] = T.h[d] * (T.qmin[d] + cc[d] - T.qoff[d][ph[d]]) + ph[d];
+            if (x[d] < 0 || x[d] >= P.fixed.n[d]) ok = false;
+        }
+        float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ok) {
+            const float4 u = T.ucp[i];
+            double fi[3] = {(double)x[0], (double)x[1], (double)x[2]}, p[3], mp[3], ml[3];
+            to_global<D>(P.fixed, fi, p);
+#pragma unroll
+            for (int d = 0; d < D; ++d) mp[d] = p[d];
+            if (P.has_df) {
+                const long long di = nearest_index<D>(P.df, p);
+                if (di >= 0) {
+                    const float4 dv = P.dfd[di];
+                    mp[0] += dv.x;
+                    if (D > 1) mp[1] += dv.y;
+                    if (D > 2) mp[2] += dv.z;
+                }
+            }
+            mp[0] += (double)u.x;
+            if (D > 1) mp[1] += (double)u.y;
+            if (D > 2) mp[2] += (double)u.z;
+            to_local<D>(P.mov, mp, ml);
+            if (bspline_inside<D>(P.mov, ml)) {
+                float m, g[3] = {0.f, 0.f, 0.f};
+                bspline_derivs4<D>(P.coeffs4, P.mov, ml, m, g);
+                const double f = (double)T.fixcp[i];
+                const double md = (double)m;
+                v[Q_COUNT] += 1.0;
+                v[Q_D2] += (md - f) * (md - f);
+                v[Q_SF] += f;
+                v[Q_SM] += md;
+                v[Q_SFF] += f * f;
+                v[Q_SMM] += md * md;
+                v[Q_SFM] += f * md;
+                rec = make_float4(g[0], g[1], D > 2 ? g[2] : 0.f, m);
+            }
+        }
+        T.rec[i] = rec;
     }
     block_sum<NQ>(v, sh);
     if (threadIdx.x == 0)
 #pragma unroll
         for (int k = 0; k < NQ; ++k) T.part[(long long)k * gridDim.x + blockIdx.x] = v[k];
+    if (last_block_arrived(counter)) {                     // fused statistics, fixed order
+        double w[NQ];
+        sum_partials<NQ>(T.part, gridDim.x, w, sh);
+        if (threadIdx.x == 0) stats_finalize(w, metric, stats);
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -202,52 +241,57 @@ __global__ void __launch_bounds__(kTabContribThreads) table_contrib_kernel(Table
     const int gst = nph + 1;                                  // padded row: lanes hit distinct banks
     float4 *G = smem4;                                        // [kTabCells][nph + 1]
     float *tg = reinterpret_cast<float *>(smem4 + kTabCells * gst);   // [nph][ntp]
-    const long long c0 = (long long)blockIdx.x * kTabCells;
     const float cf = (float)stats[S_COEF_F], cm = (float)stats[S_COEF_M], cc = (float)stats[S_COEF_C];
-    for (int i = threadIdx.x; i < kTabCells * nph; i += blockDim.x) {
-        const int c = i / nph, p = i % nph;
-        float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (c0 + c < T.ncell) {
-            const long long idx = (c0 + c) * nph + p;
-            const float4 r = T.rec[idx];
-            const float coef = fmaf(cf, T.fixcp[idx], fmaf(cm, r.w, cc));
-            g = make_float4(coef * r.x, coef * r.y, coef * r.z, 0.f);
-        }
-        G[c * gst + p] = g;         // row = cell
-    }
-    for (int i = threadIdx.x; i < nph * ntp; i += blockDim.x) tg[i] = T.tgemm[i];
-    __syncthreads();
-
+    for (int i = threadIdx.x; i < nph * ntp / 4; i += blockDim.x)
+        reinterpret_cast<float4 *>(tg)[i] = __ldg(reinterpret_cast<const float4 *>(T.tgemm) + i);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int nchunk = ntp / kTabTapChunk;
-    const long long cell = c0 + lane;
-    for (int ch = warp; ch < nchunk; ch += nwarps) {
-        float acc[kTabTapChunk][3];
-#pragma unroll
-        for (int k = 0; k < kTabTapChunk; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.f;
-        const float *trow = tg + ch * kTabTapChunk;
-        const float4 *grow = G + lane * gst;
-        for (int p = 0; p < nph; ++p) {
-            const float4 g = grow[p];
-            const float4 ta = *reinterpret_cast<const float4 *>(trow + p * ntp);
-            const float4 tb = *reinterpret_cast<const float4 *>(trow + p * ntp + 4);
-            const float4 tc = *reinterpret_cast<const float4 *>(trow + p * ntp + 8);
-            const float tv[12] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w, tc.x, tc.y, tc.z, tc.w};
-#pragma unroll
-            for (int k = 0; k < kTabTapChunk; ++k) {
-                acc[k][0] = fmaf(tv[k], g.x, acc[k][0]);
-                acc[k][1] = fmaf(tv[k], g.y, acc[k][1]);
-                acc[k][2] = fmaf(tv[k], g.z, acc[k][2]);
+    const long long ntiles = (T.ncell + kTabCells - 1) / kTabCells;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long c0 = tile * kTabCells;
+        __syncthreads();                                      // previous tile done with G
+        for (int i = threadIdx.x; i < kTabCells * nph; i += blockDim.x) {
+            const int c = i / nph, p = i % nph;
+            float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (c0 + c < T.ncell) {
+                const long long idx = (c0 + c) * nph + p;
+                const float4 r = T.rec[idx];
+                const float coef = fmaf(cf, T.fixcp[idx], fmaf(cm, r.w, cc));
+                g = make_float4(coef * r.x, coef * r.y, coef * r.z, 0.f);
             }
+            G[c * gst + p] = g;
         }
-        if (cell < T.ncell) {
+        __syncthreads();
+        const long long cell = c0 + lane;
+        for (int ch = warp; ch < nchunk; ch += nwarps) {
+            float acc[kTabTapChunk][3];
 #pragma unroll
-            for (int k = 0; k < kTabTapChunk; ++k) {
-                const int tap = ch * kTabTapChunk + k;
-                if (tap < T.ntap) {
+            for (int k = 0; k < kTabTapChunk; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.f;
+            const float *trow = tg + ch * kTabTapChunk;
+            const float4 *grow = G + lane * gst;
+#pragma unroll 4
+            for (int p = 0; p < nph; ++p) {
+                const float4 g = grow[p];
+                const float4 ta = *reinterpret_cast<const float4 *>(trow + p * ntp);
+                const float4 tb = *reinterpret_cast<const float4 *>(trow + p * ntp + 4);
+                const float4 tc = *reinterpret_cast<const float4 *>(trow + p * ntp + 8);
+                const float tv[12] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w, tc.x, tc.y, tc.z, tc.w};
 #pragma unroll
-                    for (int d = 0; d < 3; ++d)
-                        T.contrib[((long long)d * T.ntap + tap) * T.ncell + cell] = acc[k][d];
+                for (int k = 0; k < kTabTapChunk; ++k) {
+                    acc[k][0] = fmaf(tv[k], g.x, acc[k][0]);
+                    acc[k][1] = fmaf(tv[k], g.y, acc[k][1]);
+                    acc[k][2] = fmaf(tv[k], g.z, acc[k][2]);
+                }
+            }
+            if (cell < T.ncell) {
+#pragma unroll
+                for (int k = 0; k < kTabTapChunk; ++k) {
+                    const int tap = ch * kTabTapChunk + k;
+                    if (tap < T.ntap) {
+#pragma unroll
+                        for (int d = 0; d < 3; ++d)
+                            T.contrib[((long long)d * T.ntap + tap) * T.ncell + cell] = acc[k][d];
+                    }
                 }
             }
         }
@@ -255,112 +299,140 @@ __global__ void __launch_bounds__(kTabContribThreads) table_contrib_kernel(Table
 }
 
 // ------------------------------------------------------------------------------------------------
-// d[j] = w_j sum_t Contrib[t][j - t]  + regularizers + metric-level terms; thread per control point.
+// d[j] = w_j sum_t Contrib[t][j - t] + regularizers + metric-level terms.  A block owns 32
+// consecutive control points; its 8 warps split the taps (and the regularizer offsets) so that
+// every warp load reads 32 consecutive cells of one Contrib row; warp 0 then combines the 8
+// partial sums in a fixed order -- deterministic, no atomics.
+constexpr int kGatherGroups = 8;
+
 template <int D>
 __global__ void __launch_bounds__(256) table_gather_kernel(EvalParams P, TableDev T, DerivParams Q)
 {
-    __shared__ double shv[NR][32];
+    __shared__ float sacc[kGatherGroups][3][32];
+    __shared__ float sreg[kGatherGroups][9][32];
+    __shared__ double sval[kGatherGroups][3][32];
     __shared__ float kcp_s[1024];
     const int nkcp = T.nc[0] * T.nc[1] * T.nc[2];
     for (int i = threadIdx.x; i < nkcp; i += blockDim.x) kcp_s[i] = T.kcp[i];
     __syncthreads();
-    const long long j_lin = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double val[NR];
-#pragma unroll
-    for (int k = 0; k < NR; ++k) val[k] = 0.0;
-    if (j_lin < P.C) {
-        int j[3];
-        cell_of<D>(P.cp.n, j_lin, j);
-        const float4 cj = P.cpd[j_lin];
-        const double *st = Q.stats;
-        float acc[3] = {0.f, 0.f, 0.f};
-        const int ntap = T.ntap;
+    const int lane = threadIdx.x & 31, grp = threadIdx.x >> 5;
+    const long long j_lin = (long long)blockIdx.x * 32 + lane;
+    const bool active = j_lin < P.C;
+    int j[3] = {0, 0, 0};
+    if (active) cell_of<D>(P.cp.n, j_lin, j);
+    const float4 cj = active ? P.cpd[j_lin] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float acc[3] = {0.f, 0.f, 0.f};
+    if (active) {
+        const int ntap = T.ntap, nt0 = T.nt[0], nt01 = T.nt[0] * T.nt[1];
         const long long ncell = T.ncell;
-        int tap = 0;
-        for (int tz = 0; tz < T.nt[2]; ++tz) {
+#pragma unroll 4
+        for (int tap = grp; tap < ntap; tap += kGatherGroups) {
+            const int tx = tap % nt0, ty = (tap / nt0) % T.nt[1], tz = tap / nt01;
+            const int qx = j[0] - (T.tlo[0] + tx) - T.qmin[0];
+            const int qy = j[1] - (T.tlo[1] + ty) - T.qmin[1];
             const int qz = j[2] - (T.tlo[2] + tz) - T.qmin[2];
-            for (int ty = 0; ty < T.nt[1]; ++ty) {
-                const int qy = j[1] - (T.tlo[1] + ty) - T.qmin[1];
-                const bool rowok = qz >= 0 && qz < T.nq[2] && qy >= 0 && qy < T.nq[1];
-                const long long rowbase = ((long long)qz * T.nq[1] + qy) * T.nq[0];
-#pragma unroll 2
-                for (int tx = 0; tx < T.nt[0]; ++tx, ++tap) {
-                    const int qx = j[0] - (T.tlo[0] + tx) - T.qmin[0];
-                    if (rowok && qx >= 0 && qx < T.nq[0]) {
-                        const long long c = rowbase + qx;
-                        acc[0] += __ldg(T.contrib + (long long)tap * ncell + c);
-                        acc[1] += __ldg(T.contrib + ((long long)ntap + tap) * ncell + c);
-                        if (D > 2) acc[2] += __ldg(T.contrib + ((long long)2 * ntap + tap) * ncell + c);
-                    }
+            if (qx >= 0 && qx < T.nq[0] && qy >= 0 && qy < T.nq[1] && qz >= 0 && qz < T.nq[2]) {
+                const long long c = ((long long)qz * T.nq[1] + qy) * T.nq[0] + qx;
+                acc[0] += __ldg(T.contrib + (long long)tap * ncell + c);
+                acc[1] += __ldg(T.contrib + ((long long)ntap + tap) * ncell + c);
+                if (D > 2) acc[2] += __ldg(T.contrib + ((long long)2 * ntap + tap) * ncell + c);
+            }
+        }
+    }
+    // regularizer parts over this group's share of the control-point offsets
+    float drk[3] = {0.f, 0.f, 0.f}, drd[3] = {0.f, 0.f, 0.f}, dpg[3] = {0.f, 0.f, 0.f};
+    double vr = 0.0, vd = 0.0, vp = 0.0;
+    const bool rkhs = Q.reg_rkhs > 0.0, rd = Q.reg_rd > 0.0, pg = Q.reg_pg > 0.0;
+    if (active && (rkhs || rd || pg)) {
+        const float wj = cj.w;
+        const float cjv[3] = {cj.x, cj.y, cj.z};
+        const float pgs = (float)Q.pg_scaling;
+        const int nc0 = T.nc[0], nc01 = T.nc[0] * T.nc[1];
+        for (int o = grp; o < nkcp; o += kGatherGroups) {
+            const float k = kcp_s[o];
+            if (k == 0.0f) continue;
+            const int ii[3] = {j[0] + T.clo[0] + o % nc0, j[1] + T.clo[1] + (o / nc0) % T.nc[1],
+                               j[2] + T.clo[2] + o / nc01};
+            if (ii[0] < 0 || ii[0] >= P.cp.n[0] || ii[1] < 0 || ii[1] >= P.cp.n[1] || ii[2] < 0 || ii[2] >= P.cp.n[2])
+                continue;
+            const float4 ci4 = __ldg(P.cpd + lin_of<D>(P.cp, ii));
+            const float ci[3] = {ci4.x, ci4.y, ci4.z};
+            const float kw = k * wj;
+            if (rkhs) {                                        // Regularizers.cu:68-73
+                double dot = 0.0;
+#pragma unroll
+                for (int d = 0; d < D; ++d) dot += (double)cjv[d] * (double)ci[d];
+                vr += (double)kw * dot;
+#pragma unroll
+                for (int d = 0; d < D; ++d) drk[d] = fmaf(2.0f * kw, ci[d], drk[d]);
+            }
+            if (rd) {                                          // Regularizers.cu:141-144
+                double l2 = 0.0;
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    const double e = (double)cjv[d] - (double)ci[d];
+                    l2 += e * e;
+                }
+                vd += l2 * (double)kw;
+#pragma unroll
+                for (int d = 0; d < D; ++d) drd[d] = fmaf(4.0f * kw, cjv[d] - ci[d], drd[d]);
+            }
+            if (pg) {
+                if (D == 3) {                                  // Regularizers.cu:218-237
+                    const float cr0 = ci[1] * cjv[2] - ci[2] * cjv[1];
+                    const float cr1 = ci[2] * cjv[0] - ci[0] * cjv[2];
+                    const float cr2 = ci[0] * cjv[1] - ci[1] * cjv[0];
+                    const double n2 = (double)cr0 * cr0 + (double)cr1 * cr1 + (double)cr2 * cr2;
+                    const double sc = (double)pgs;
+                    vp += (double)kw * sc * sc / 2.0 * log(1.0 + n2 / sc);
+                    const float den = 2.0f * ((float)n2 / pgs + 1.0f);
+                    const float dp0 = 2.0f * ci[2] * (ci[2] * cjv[0] - ci[0] * cjv[2]) - 2.0f * ci[1] * (ci[0] * cjv[1] - ci[1] * cjv[0]);
+                    const float dp1 = 2.0f * ci[0] * (ci[0] * cjv[1] - ci[1] * cjv[0]) - 2.0f * ci[2] * (ci[1] * cjv[2] - ci[2] * cjv[1]);
+                    const float dp2 = 2.0f * ci[1] * (ci[1] * cjv[2] - ci[2] * cjv[1]) - 2.0f * ci[0] * (ci[2] * cjv[0] - ci[0] * cjv[2]);
+                    dpg[0] = fmaf(2.0f * kw, pgs * dp0 / den, dpg[0]);
+                    dpg[1] = fmaf(2.0f * kw, pgs * dp1 / den, dpg[1]);
+                    dpg[2] = fmaf(2.0f * kw, pgs * dp2 / den, dpg[2]);
+                } else {                                       // Regularizers.cu:447-459
+                    const float v2d = ci[0] * cjv[1] - ci[1] * cjv[0];
+                    const double v2 = (double)v2d * v2d;
+                    const double sc = (double)pgs;
+                    vp += (double)kw * sc * sc / 2.0 * log(1.0 + v2 / sc);
+                    const float factor = (float)v2 / pgs + 1.0f;
+                    dpg[0] = fmaf(2.0f * kw, -pgs * ci[1] * v2d / factor, dpg[0]);
+                    dpg[1] = fmaf(2.0f * kw, pgs * ci[0] * v2d / factor, dpg[1]);
                 }
             }
         }
-        // regularizers over the control-point box (GpuEvaluatorRegularizers.cu), kernel from the table
-        float drk[3] = {0.f, 0.f, 0.f}, drd[3] = {0.f, 0.f, 0.f}, dpg[3] = {0.f, 0.f, 0.f};
-        const bool rkhs = Q.reg_rkhs > 0.0, rd = Q.reg_rd > 0.0, pg = Q.reg_pg > 0.0;
-        if (rkhs || rd || pg) {
-            const float wj = cj.w;
-            const float cjv[3] = {cj.x, cj.y, cj.z};
-            const float pgs = (float)Q.pg_scaling;
-            int o = 0;
-            for (int oz = 0; oz < T.nc[2]; ++oz)
-                for (int oy = 0; oy < T.nc[1]; ++oy)
-                    for (int ox = 0; ox < T.nc[0]; ++ox, ++o) {
-                        const int ii[3] = {j[0] + T.clo[0] + ox, j[1] + T.clo[1] + oy, j[2] + T.clo[2] + oz};
-                        if (ii[0] < 0 || ii[0] >= P.cp.n[0] || ii[1] < 0 || ii[1] >= P.cp.n[1] || ii[2] < 0 ||
-                            ii[2] >= P.cp.n[2])
-                            continue;
-                        const float k = kcp_s[o];
-                        if (k == 0.0f) continue;
-                        const float4 ci4 = __ldg(P.cpd + lin_of<D>(P.cp, ii));
-                        const float ci[3] = {ci4.x, ci4.y, ci4.z};
-                        const float kw = k * wj;
-                        if (rkhs) {
-                            double dot = 0.0;
+    }
 #pragma unroll
-                            for (int d = 0; d < D; ++d) dot += (double)cjv[d] * (double)ci[d];
-                            val[R_RKHS] += (double)kw * dot;
+    for (int d = 0; d < 3; ++d) {
+        sacc[grp][d][lane] = acc[d];
+        sreg[grp][d][lane] = drk[d];
+        sreg[grp][3 + d][lane] = drd[d];
+        sreg[grp][6 + d][lane] = dpg[d];
+    }
+    sval[grp][0][lane] = vr;
+    sval[grp][1][lane] = vd;
+    sval[grp][2][lane] = vp;
+    __syncthreads();
+    double val[NR];
 #pragma unroll
-                            for (int d = 0; d < D; ++d) drk[d] = fmaf(2.0f * kw, ci[d], drk[d]);
-                        }
-                        if (rd) {
-                            double l2 = 0.0;
+    for (int k = 0; k < NR; ++k) val[k] = 0.0;
+    if (grp == 0 && active) {
+        float a[3] = {0.f, 0.f, 0.f}, rk[3] = {0.f, 0.f, 0.f}, rdd[3] = {0.f, 0.f, 0.f}, rp[3] = {0.f, 0.f, 0.f};
+        for (int g = 0; g < kGatherGroups; ++g) {           // fixed combination order
 #pragma unroll
-                            for (int d = 0; d < D; ++d) {
-                                double e = (double)cjv[d] - (double)ci[d];
-                                l2 += e * e;
-                            }
-                            val[R_RD] += l2 * (double)kw;
-#pragma unroll
-                            for (int d = 0; d < D; ++d) drd[d] = fmaf(4.0f * kw, cjv[d] - ci[d], drd[d]);
-                        }
-                        if (pg) {
-                            if (D == 3) {
-                                float cr0 = ci[1] * cjv[2] - ci[2] * cjv[1];
-                                float cr1 = ci[2] * cjv[0] - ci[0] * cjv[2];
-                                float cr2 = ci[0] * cjv[1] - ci[1] * cjv[0];
-                                double n2 = (double)cr0 * cr0 + (double)cr1 * cr1 + (double)cr2 * cr2;
-                                double s = (double)pgs;
-                                val[R_PG] += (double)kw * s * s / 2.0 * log(1.0 + n2 / s);
-                                float den = 2.0f * ((float)n2 / pgs + 1.0f);
-                                float dp0 = 2.0f * ci[2] * (ci[2] * cjv[0] - ci[0] * cjv[2]) - 2.0f * ci[1] * (ci[0] * cjv[1] - ci[1] * cjv[0]);
-                                float dp1 = 2.0f * ci[0] * (ci[0] * cjv[1] - ci[1] * cjv[0]) - 2.0f * ci[2] * (ci[1] * cjv[2] - ci[2] * cjv[1]);
-                                float dp2 = 2.0f * ci[1] * (ci[1] * cjv[2] - ci[2] * cjv[1]) - 2.0f * ci[0] * (ci[2] * cjv[0] - ci[0] * cjv[2]);
-                                dpg[0] = fmaf(2.0f * kw, pgs * dp0 / den, dpg[0]);
-                                dpg[1] = fmaf(2.0f * kw, pgs * dp1 / den, dpg[1]);
-                                dpg[2] = fmaf(2.0f * kw, pgs * dp2 / den, dpg[2]);
-                            } else {
-                                float v2d = ci[0] * cjv[1] - ci[1] * cjv[0];
-                                double v2 = (double)v2d * v2d;
-                                double s = (double)pgs;
-                                val[R_PG] += (double)kw * s * s / 2.0 * log(1.0 + v2 / s);
-                                float factor = (float)v2 / pgs + 1.0f;
-                                dpg[0] = fmaf(2.0f * kw, -pgs * ci[1] * v2d / factor, dpg[0]);
-                                dpg[1] = fmaf(2.0f * kw, pgs * ci[0] * v2d / factor, dpg[1]);
-                            }
-                        }
-                    }
+            for (int d = 0; d < 3; ++d) {
+                a[d] += sacc[g][d][lane];
+                rk[d] += sreg[g][d][lane];
+                rdd[d] += sreg[g][3 + d][lane];
+                rp[d] += sreg[g][6 + d][lane];
+            }
+            val[R_RKHS] += sval[g][0][lane];
+            val[R_RD] += sval[g][1][lane];
+            val[R_PG] += sval[g][2][lane];
         }
+        const double *st = Q.stats;
         double pc[3] = {0, 0, 0}, pn2 = 0.0;
         if (Q.with_metric) {
 #pragma unroll
@@ -374,23 +446,23 @@ __global__ void __launch_bounds__(256) table_gather_kernel(EvalParams P, TableDe
         for (int d = 0; d < D; ++d) {
             double g;
             if (Q.metric == 1)
-                g = st[S_DENOM] != 0.0 ? (double)cj.w * (double)acc[d] : 0.0;
+                g = st[S_DENOM] != 0.0 ? (double)cj.w * (double)a[d] : 0.0;
             else
-                g = (double)cj.w * (double)acc[d];
-            if (rkhs) g += (double)drk[d] * Q.reg_rkhs;
-            if (rd) g += (double)drd[d] * Q.reg_rd;
-            if (pg) g += (double)dpg[d] * Q.reg_pg;
+                g = (double)cj.w * (double)a[d];
+            if (rkhs) g += (double)rk[d] * Q.reg_rkhs;
+            if (rd) g += (double)rdd[d] * Q.reg_rd;
+            if (pg) g += (double)rp[d] * Q.reg_pg;
             if (Q.with_metric) {
                 const double par = pc[d];
-                if (Q.reg_l1 > 0.0) {
+                if (Q.reg_l1 > 0.0) {                          // metric hxx:447-466
                     const double w = Q.reg_l1;
                     if (fabs(par) > 0.0) g += w * (par < 0.0 ? -1.0 : 1.0);
                     else if (g < -w) g += w;
                     else if (g > w) g -= w;
                     else g = 0.0;
                 }
-                if (Q.reg_l2 > 0.0) g += Q.reg_l2 * 2.0 * par;
-                if (Q.reg_l21 > 0.0) {
+                if (Q.reg_l2 > 0.0) g += Q.reg_l2 * 2.0 * par;  // hxx:482-485
+                if (Q.reg_l21 > 0.0) {                         // hxx:504-521
                     const double w = Q.reg_l21;
                     if (pnorm > 0.0) g += w * par / pnorm;
                     else if (g < -w) g += w;
@@ -410,20 +482,23 @@ __global__ void __launch_bounds__(256) table_gather_kernel(EvalParams P, TableDe
             val[R_L21] = Q.reg_l21 > 0.0 ? pnorm : 0.0;
         }
     }
-    // fixed-order block reduction of the per-control-point values
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (grp == 0) {
 #pragma unroll
-    for (int k = 0; k < NR; ++k) {
-        double s = warp_sum(val[k]);
-        if (lane == 0) shv[k][warp] = s;
+        for (int k = 0; k < NR; ++k) {
+            const double sum = warp_sum(val[k]);
+            if (lane == 0) Q.rpart[(long long)k * gridDim.x + blockIdx.x] = sum;
+        }
     }
-    __syncthreads();
-    if (threadIdx.x < NR) {
-        double s = 0.0;
-        for (int w = 0; w < nw; ++w) s += shv[threadIdx.x][w];
-        Q.rpart[(long long)threadIdx.x * gridDim.x + blockIdx.x] = s;
+    if (last_block_arrived(Q.counter)) {                   // fused result, fixed order
+        __shared__ double shr[NR * 32];
+        double w[NR];
+        sum_partials<NR>(Q.rpart, gridDim.x, w, shr);
+        if (threadIdx.x == 0)
+            result_finalize(Q.stats, w, Q.reg_rkhs, Q.reg_rd, Q.reg_pg, Q.reg_l1, Q.reg_l21, Q.reg_l2, Q.out);
     }
 }
+
+
 
 // ------------------------------------------------------------------------------------------------
 // host side
@@ -550,11 +625,12 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
         T.nc[d] = hi - lo + 1;
     }
     if (T.nc[0] * T.nc[1] * T.nc[2] > 1024) return 0;
-    // value-kernel tiling: threads = (px,py) phases x cells; HL = z phases per thread
+    // transform tiling: threads = (px,py) phases x cells; each thread HL z-phases of NCZ cells
     const int nphxy = T.h[0] * T.h[1];
     const int hl = T.h[2];
     if (!(hl == 1 || hl == 2 || hl == 4 || hl == 8)) return 0;
     if (256 % nphxy != 0) return 0;
+    const int ncz = D == 3 ? 2 : 1;
     const int cells = 256 / nphxy;
     int tx = 1;
     while (tx * tx < cells) tx *= 2;
@@ -562,9 +638,11 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     T.tile_y = cells / T.tile_x;
     T.tiles_x = (T.nq[0] + T.tile_x - 1) / T.tile_x;
     T.tiles_y = (T.nq[1] + T.tile_y - 1) / T.tile_y;
-    T.tiles_z = T.nq[2];
-    T.value_blocks = T.tiles_x * T.tiles_y * T.tiles_z;
+    T.tiles_z = (T.nq[2] + ncz - 1) / ncz;
+    pl.transform_blocks = T.tiles_x * T.tiles_y * T.tiles_z;
+    T.value_blocks = (int)std::min<long long>((T.ncell * T.nph + 255) / 256, 148LL * 8);
     pl.hl = hl;
+    pl.ncz = ncz;
 
     // tables (kernel evaluated on the exact double offset, float profile)
     std::vector<float> tfwd((size_t)T.ntap * nphxy * hl), tgemm((size_t)T.nph * T.ntap_pad, 0.f);
@@ -629,6 +707,7 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     };
     if (!up(&pl.d_tfwd, tfwd) || !up(&pl.d_tgemm, tgemm) || !up(&pl.d_kcp, kcp) || !up(&pl.d_fixcp, fix)) return 2;
     if (cudaMalloc((void **)&pl.d_rec, (size_t)T.ncell * T.nph * sizeof(float4)) != cudaSuccess) return 2;
+    if (cudaMalloc((void **)&pl.d_ucp, (size_t)T.ncell * T.nph * sizeof(float4)) != cudaSuccess) return 2;
     if (cudaMalloc((void **)&pl.d_contrib, (size_t)3 * T.ntap * T.ncell * sizeof(float)) != cudaSuccess) return 2;
     if (cudaMalloc((void **)&pl.d_part, (size_t)NQ * T.value_blocks * sizeof(double)) != cudaSuccess) return 2;
     if (cudaStreamSynchronize(stream) != cudaSuccess) return 2;
@@ -637,11 +716,12 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     T.kcp = pl.d_kcp;
     T.fixcp = pl.d_fixcp;
     T.rec = pl.d_rec;
+    T.ucp = pl.d_ucp;
     T.contrib = pl.d_contrib;
     T.part = pl.d_part;
     // shared memory of the launches
-    const size_t smem_value = (size_t)(T.tile_x + T.nt[0] - 1) * (T.tile_y + T.nt[1] - 1) * T.nt[2] * sizeof(float4) +
-                              (size_t)T.ntap * nphxy * hl * sizeof(float);
+    const size_t smem_value = (size_t)(T.tile_x + T.nt[0] - 1) * (T.tile_y + T.nt[1] - 1) * (ncz + T.nt[2] - 1) *
+                                  sizeof(float4) + (size_t)T.ntap * nphxy * hl * sizeof(float);
     const size_t smem_contrib =
         (size_t)kTabCells * (T.nph + 1) * sizeof(float4) + (size_t)T.nph * T.ntap_pad * sizeof(float);
     if (smem_value > 200 * 1024 || smem_contrib > 200 * 1024) return 0;
@@ -649,9 +729,10 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     return 0;
 }
 
-inline size_t table_value_smem(const TableDev &T)
+inline size_t table_value_smem(const TablePlan &pl)
 {
-    return (size_t)(T.tile_x + T.nt[0] - 1) * (T.tile_y + T.nt[1] - 1) * T.nt[2] * sizeof(float4) +
+    const TableDev &T = pl.dev;
+    return (size_t)(T.tile_x + T.nt[0] - 1) * (T.tile_y + T.nt[1] - 1) * (pl.ncz + T.nt[2] - 1) * sizeof(float4) +
            (size_t)T.ntap * T.h[0] * T.h[1] * T.h[2] * sizeof(float);
 }
 
@@ -663,49 +744,84 @@ inline size_t table_contrib_smem(const TableDev &T)
 // dynamic shared memory limits of the table kernels (set once, outside any stream capture)
 inline int table_set_attributes(const TablePlan &pl)
 {
-    const int sv = (int)table_value_smem(pl.dev), sc = (int)table_contrib_smem(pl.dev);
+    const int sv = (int)table_value_smem(pl), sc = (int)table_contrib_smem(pl.dev);
     cudaError_t e = cudaSuccess;
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (pl.dev.D == 3) {
-        if (pl.hl == 1) e = cudaFuncSetAttribute(table_value_kernel<3, 1>, a, sv);
-        else if (pl.hl == 2) e = cudaFuncSetAttribute(table_value_kernel<3, 2>, a, sv);
-        else if (pl.hl == 4) e = cudaFuncSetAttribute(table_value_kernel<3, 4>, a, sv);
-        else e = cudaFuncSetAttribute(table_value_kernel<3, 8>, a, sv);
+        if (pl.hl == 1) e = cudaFuncSetAttribute(table_transform_kernel<1, 2>, a, sv);
+        else if (pl.hl == 2) e = cudaFuncSetAttribute(table_transform_kernel<2, 2>, a, sv);
+        else if (pl.hl == 4) e = cudaFuncSetAttribute(table_transform_kernel<4, 2>, a, sv);
+        else e = cudaFuncSetAttribute(table_transform_kernel<8, 2>, a, sv);
     } else {
-        e = cudaFuncSetAttribute(table_value_kernel<2, 1>, a, sv);
+        e = cudaFuncSetAttribute(table_transform_kernel<1, 1>, a, sv);
     }
     if (e != cudaSuccess) return 2;
     return cudaFuncSetAttribute(table_contrib_kernel, a, sc) == cudaSuccess ? 0 : 2;
 }
 
-template <int D, int HL>
-inline int table_value_launch(TablePlan &pl, const EvalParams &P, cudaStream_t s)
+// Persistent grid sizes: resident blocks per SM x SMs, capped by the work.
+inline int table_size_grids(TablePlan &pl)
 {
-    const size_t smem = table_value_smem(pl.dev);
-    table_value_kernel<D, HL><<<pl.dev.value_blocks, 256, smem, s>>>(P, pl.dev);
+    int dev = 0, sms = 0, bt = 0, bc = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 2;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 2;
+    cudaError_t e;
+    const int sv = (int)table_value_smem(pl);
+    if (pl.dev.D == 3) {
+        if (pl.hl == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<1, 2>, 256, sv);
+        else if (pl.hl == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<2, 2>, 256, sv);
+        else if (pl.hl == 4) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<4, 2>, 256, sv);
+        else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<8, 2>, 256, sv);
+    } else {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<1, 1>, 256, sv);
+    }
+    if (e != cudaSuccess) return 2;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bc, table_contrib_kernel, kTabContribThreads,
+                                                      table_contrib_smem(pl.dev)) != cudaSuccess)
+        return 2;
+    const int ntiles = pl.dev.tiles_x * pl.dev.tiles_y * pl.dev.tiles_z;
+    const long long ctiles = (pl.dev.ncell + kTabCells - 1) / kTabCells;
+    pl.transform_blocks = std::max(1, std::min(ntiles, std::max(1, bt) * sms));
+    pl.contrib_blocks = (int)std::max<long long>(1, std::min<long long>(ctiles, (long long)std::max(1, bc) * sms));
+    return 0;
+}
+
+template <int HL, int NCZ>
+inline int table_transform_launch(TablePlan &pl, const EvalParams &P, cudaStream_t s)
+{
+    table_transform_kernel<HL, NCZ><<<pl.transform_blocks, 256, table_value_smem(pl), s>>>(P, pl.dev);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
-// value pass of the table path; writes its own partials (pl.d_part, pl.dev.value_blocks blocks)
-inline int table_value(TablePlan &pl, const EvalParams &P, int D, cudaStream_t s)
+// value pass of the table path: transform, then warp + statistics; writes its own partials
+// (pl.d_part, pl.dev.value_blocks blocks)
+inline int table_value(TablePlan &pl, const EvalParams &P, int D, int metric, double *stats, unsigned *counter,
+                       cudaStream_t s)
 {
+    int rc;
     if (D == 3) {
         switch (pl.hl) {
-        case 1: return table_value_launch<3, 1>(pl, P, s);
-        case 2: return table_value_launch<3, 2>(pl, P, s);
-        case 4: return table_value_launch<3, 4>(pl, P, s);
-        default: return table_value_launch<3, 8>(pl, P, s);
+        case 1: rc = table_transform_launch<1, 2>(pl, P, s); break;
+        case 2: rc = table_transform_launch<2, 2>(pl, P, s); break;
+        case 4: rc = table_transform_launch<4, 2>(pl, P, s); break;
+        default: rc = table_transform_launch<8, 2>(pl, P, s); break;
         }
+    } else {
+        rc = table_transform_launch<1, 1>(pl, P, s);
     }
-    return table_value_launch<2, 1>(pl, P, s);
+    if (rc) return rc;
+    if (D == 3)
+        table_warp_kernel<3><<<pl.dev.value_blocks, 256, 0, s>>>(P, pl.dev, metric, stats, counter);
+    else
+        table_warp_kernel<2><<<pl.dev.value_blocks, 256, 0, s>>>(P, pl.dev, metric, stats, counter);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
 inline int table_derivative(TablePlan &pl, const EvalParams &P, const DerivParams &Q, int D, int gather_blocks,
                             cudaStream_t s)
 {
     const size_t smem = table_contrib_smem(pl.dev);
-    const int blocks = (int)((pl.dev.ncell + kTabCells - 1) / kTabCells);
-    table_contrib_kernel<<<blocks, kTabContribThreads, smem, s>>>(pl.dev, Q.stats);
+    table_contrib_kernel<<<pl.contrib_blocks, kTabContribThreads, smem, s>>>(pl.dev, Q.stats);
     if (cudaPeekAtLastError() != cudaSuccess) return 2;
     if (D == 3)
         table_gather_kernel<3><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
@@ -720,6 +836,7 @@ inline void table_free(TablePlan &pl)
     for (float *p : f)
         if (p) cudaFree(p);
     if (pl.d_rec) cudaFree(pl.d_rec);
+    if (pl.d_ucp) cudaFree(pl.d_ucp);
     if (pl.d_part) cudaFree(pl.d_part);
     pl = TablePlan{};
 }
