@@ -595,11 +595,17 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
         } else if ((rc = dispatch<LaunchDeriv>(D, kind, e, Q))) {
             return rc;
         }
+    } else if (any_reg && tab) {
+        // values only, through the same gather (and the same sums) as the derivative call, so
+        // that GetValue and GetValueAndDerivative return identical values
+        Q.values_only = 1;
+        if (table_derivative_gather_only(e->table, e->P, Q, D, e->gather_blocks, e->stream))
+            return fail(SKM_ERR_CUDA, "table regularizer values: %s", cudaGetErrorString(cudaGetLastError()));
     } else if (any_reg) {
         if ((rc = dispatch<LaunchRegValue>(D, kind, e, Q))) return rc;
     }
     if (ev) SKM_CUDA(cudaEventRecord(ev[2], e->stream));
-    if (!(derivative && tab)) {                 // the table gather computes the result itself
+    if (!((derivative || any_reg) && tab)) {    // the table gather computes the result itself
         result_kernel<<<1, 256, 0, e->stream>>>(e->d_stats, (derivative || any_reg) ? e->d_rpart : nullptr,
                                                e->deriv_blocks, w.rkhs, w.rd, w.pg, w.l1, w.l21, w.l2, e->d_out);
         SKM_CHECK_LAUNCH();

@@ -63,6 +63,7 @@ struct DerivParams {
     double *__restrict__ rpart;          // [NR][blocks]
     double *__restrict__ out;            // result vector (fused finalization)
     unsigned *counter;                   // ticket counter of the fused finalization
+    int values_only;                     // table gather: regularizer values only (getValue)
 };
 
 // ---- sample positions ------------------------------------------------------------------------

@@ -73,7 +73,7 @@ struct TablePlan {
 // (stacked along z) per thread.  Threads of a warp share the control-point values (2 cells) and
 // read 16 different table rows, so every tap costs 3 shared-memory wavefronts per 12*NCZ FMAs.
 template <int HL, int NCZ>
-__global__ void __launch_bounds__(256) table_transform_kernel(EvalParams P, TableDev T)
+__global__ void __launch_bounds__(256, 2) table_transform_kernel(EvalParams P, TableDev T)
 {
     extern __shared__ float4 smem4[];
     const int nphxy = T.h[0] * T.h[1];
@@ -166,9 +166,9 @@ __global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev 
                                                          unsigned *counter)
 {
     __shared__ double sh[NQ * 32];
-    double v[NQ];
+    float vf[NQ];                 // per-thread partials over a few texels; block sums in double
 #pragma unroll
-    for (int k = 0; k < NQ; ++k) v[k] = 0.0;
+    for (int k = 0; k < NQ; ++k) vf[k] = 0.f;
     const long long total = T.ncell * T.nph;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
@@ -207,20 +207,22 @@ __global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev 
             if (bspline_inside<D>(P.mov, ml)) {
                 float m, g[3] = {0.f, 0.f, 0.f};
                 bspline_derivs4<D>(P.coeffs4, P.mov, ml, m, g);
-                const double f = (double)T.fixcp[i];
-                const double md = (double)m;
-                v[Q_COUNT] += 1.0;
-                v[Q_D2] += (md - f) * (md - f);
-                v[Q_SF] += f;
-                v[Q_SM] += md;
-                v[Q_SFF] += f * f;
-                v[Q_SMM] += md * md;
-                v[Q_SFM] += f * md;
+                const float f = T.fixcp[i];
+                vf[Q_COUNT] += 1.f;
+                vf[Q_D2] += (m - f) * (m - f);
+                vf[Q_SF] += f;
+                vf[Q_SM] += m;
+                vf[Q_SFF] += f * f;
+                vf[Q_SMM] += m * m;
+                vf[Q_SFM] += f * m;
                 rec = make_float4(g[0], g[1], D > 2 ? g[2] : 0.f, m);
             }
         }
         T.rec[i] = rec;
     }
+    double v[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) v[k] = (double)vf[k];
     block_sum<NQ>(v, sh);
     if (threadIdx.x == 0)
 #pragma unroll
@@ -312,8 +314,12 @@ __global__ void __launch_bounds__(256) table_gather_kernel(EvalParams P, TableDe
     __shared__ float sreg[kGatherGroups][9][32];
     __shared__ double sval[kGatherGroups][3][32];
     __shared__ float kcp_s[1024];
+    __shared__ int4 tapoff[kTabMaxTap * kTabMaxTap * kTabMaxTap];   // (tx+tlo, ty+tlo, tz+tlo) per tap
     const int nkcp = T.nc[0] * T.nc[1] * T.nc[2];
     for (int i = threadIdx.x; i < nkcp; i += blockDim.x) kcp_s[i] = T.kcp[i];
+    for (int i = threadIdx.x; i < T.ntap; i += blockDim.x)
+        tapoff[i] = make_int4(T.tlo[0] + T.qmin[0] + i % T.nt[0], T.tlo[1] + T.qmin[1] + (i / T.nt[0]) % T.nt[1],
+                              T.tlo[2] + T.qmin[2] + i / (T.nt[0] * T.nt[1]), 0);
     __syncthreads();
     const int lane = threadIdx.x & 31, grp = threadIdx.x >> 5;
     const long long j_lin = (long long)blockIdx.x * 32 + lane;
@@ -322,20 +328,20 @@ __global__ void __launch_bounds__(256) table_gather_kernel(EvalParams P, TableDe
     if (active) cell_of<D>(P.cp.n, j_lin, j);
     const float4 cj = active ? P.cpd[j_lin] : make_float4(0.f, 0.f, 0.f, 0.f);
     float acc[3] = {0.f, 0.f, 0.f};
-    if (active) {
-        const int ntap = T.ntap, nt0 = T.nt[0], nt01 = T.nt[0] * T.nt[1];
+    if (active && !Q.values_only) {
+        const int ntap = T.ntap;
         const long long ncell = T.ncell;
+        const float *c0p = T.contrib, *c1p = T.contrib + (long long)ntap * ncell,
+                    *c2p = T.contrib + 2LL * ntap * ncell;
 #pragma unroll 4
         for (int tap = grp; tap < ntap; tap += kGatherGroups) {
-            const int tx = tap % nt0, ty = (tap / nt0) % T.nt[1], tz = tap / nt01;
-            const int qx = j[0] - (T.tlo[0] + tx) - T.qmin[0];
-            const int qy = j[1] - (T.tlo[1] + ty) - T.qmin[1];
-            const int qz = j[2] - (T.tlo[2] + tz) - T.qmin[2];
-            if (qx >= 0 && qx < T.nq[0] && qy >= 0 && qy < T.nq[1] && qz >= 0 && qz < T.nq[2]) {
-                const long long c = ((long long)qz * T.nq[1] + qy) * T.nq[0] + qx;
-                acc[0] += __ldg(T.contrib + (long long)tap * ncell + c);
-                acc[1] += __ldg(T.contrib + ((long long)ntap + tap) * ncell + c);
-                if (D > 2) acc[2] += __ldg(T.contrib + ((long long)2 * ntap + tap) * ncell + c);
+            const int4 o = tapoff[tap];
+            const int qx = j[0] - o.x, qy = j[1] - o.y, qz = j[2] - o.z;
+            if ((unsigned)qx < (unsigned)T.nq[0] && (unsigned)qy < (unsigned)T.nq[1] && (unsigned)qz < (unsigned)T.nq[2]) {
+                const long long c = (long long)tap * ncell + ((long long)qz * T.nq[1] + qy) * T.nq[0] + qx;
+                acc[0] += __ldg(c0p + c);
+                acc[1] += __ldg(c1p + c);
+                if (D > 2) acc[2] += __ldg(c2p + c);
             }
         }
     }
@@ -630,7 +636,7 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     const int hl = T.h[2];
     if (!(hl == 1 || hl == 2 || hl == 4 || hl == 8)) return 0;
     if (256 % nphxy != 0) return 0;
-    const int ncz = D == 3 ? 2 : 1;
+    const int ncz = D == 3 ? 4 : 1;
     const int cells = 256 / nphxy;
     int tx = 1;
     while (tx * tx < cells) tx *= 2;
@@ -748,10 +754,10 @@ inline int table_set_attributes(const TablePlan &pl)
     cudaError_t e = cudaSuccess;
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (pl.dev.D == 3) {
-        if (pl.hl == 1) e = cudaFuncSetAttribute(table_transform_kernel<1, 2>, a, sv);
-        else if (pl.hl == 2) e = cudaFuncSetAttribute(table_transform_kernel<2, 2>, a, sv);
-        else if (pl.hl == 4) e = cudaFuncSetAttribute(table_transform_kernel<4, 2>, a, sv);
-        else e = cudaFuncSetAttribute(table_transform_kernel<8, 2>, a, sv);
+        if (pl.hl == 1) e = cudaFuncSetAttribute(table_transform_kernel<1, 4>, a, sv);
+        else if (pl.hl == 2) e = cudaFuncSetAttribute(table_transform_kernel<2, 4>, a, sv);
+        else if (pl.hl == 4) e = cudaFuncSetAttribute(table_transform_kernel<4, 4>, a, sv);
+        else e = cudaFuncSetAttribute(table_transform_kernel<8, 4>, a, sv);
     } else {
         e = cudaFuncSetAttribute(table_transform_kernel<1, 1>, a, sv);
     }
@@ -768,10 +774,10 @@ inline int table_size_grids(TablePlan &pl)
     cudaError_t e;
     const int sv = (int)table_value_smem(pl);
     if (pl.dev.D == 3) {
-        if (pl.hl == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<1, 2>, 256, sv);
-        else if (pl.hl == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<2, 2>, 256, sv);
-        else if (pl.hl == 4) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<4, 2>, 256, sv);
-        else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<8, 2>, 256, sv);
+        if (pl.hl == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<1, 4>, 256, sv);
+        else if (pl.hl == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<2, 4>, 256, sv);
+        else if (pl.hl == 4) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<4, 4>, 256, sv);
+        else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<8, 4>, 256, sv);
     } else {
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, table_transform_kernel<1, 1>, 256, sv);
     }
@@ -801,10 +807,10 @@ inline int table_value(TablePlan &pl, const EvalParams &P, int D, int metric, do
     int rc;
     if (D == 3) {
         switch (pl.hl) {
-        case 1: rc = table_transform_launch<1, 2>(pl, P, s); break;
-        case 2: rc = table_transform_launch<2, 2>(pl, P, s); break;
-        case 4: rc = table_transform_launch<4, 2>(pl, P, s); break;
-        default: rc = table_transform_launch<8, 2>(pl, P, s); break;
+        case 1: rc = table_transform_launch<1, 4>(pl, P, s); break;
+        case 2: rc = table_transform_launch<2, 4>(pl, P, s); break;
+        case 4: rc = table_transform_launch<4, 4>(pl, P, s); break;
+        default: rc = table_transform_launch<8, 4>(pl, P, s); break;
         }
     } else {
         rc = table_transform_launch<1, 1>(pl, P, s);
@@ -823,6 +829,16 @@ inline int table_derivative(TablePlan &pl, const EvalParams &P, const DerivParam
     const size_t smem = table_contrib_smem(pl.dev);
     table_contrib_kernel<<<pl.contrib_blocks, kTabContribThreads, smem, s>>>(pl.dev, Q.stats);
     if (cudaPeekAtLastError() != cudaSuccess) return 2;
+    if (D == 3)
+        table_gather_kernel<3><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+    else
+        table_gather_kernel<2><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
+}
+
+inline int table_derivative_gather_only(TablePlan &pl, const EvalParams &P, const DerivParams &Q, int D,
+                                        int gather_blocks, cudaStream_t s)
+{
     if (D == 3)
         table_gather_kernel<3><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
     else
