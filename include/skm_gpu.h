@@ -137,6 +137,22 @@ int skm_evaluator_destroy(skm_evaluator *ev);
  * the fixed spacing, subsample 1).  Both paths compute the same sums. */
 int skm_evaluator_path(skm_evaluator *ev, int32_t request, int32_t *active);
 
+/* Work description of an evaluator (no counterpart in the reference): the kernel path and
+ * the sizes that set the cost of one evaluation. */
+typedef struct skm_evaluator_info {
+    int32_t path;                     /* 1 generic kernels, 2 phase table */
+    int32_t dimensions;
+    int64_t fixed_texels;
+    int64_t samples;                  /* fixed texels / subsample^D */
+    int64_t control_points;
+    int32_t table_phases;             /* texels per control-point cell (table path) */
+    int32_t table_taps;               /* control points per cell in the kernel support */
+    int32_t table_cells_per_axis[3];
+    int64_t table_cells;
+    int32_t table_regularizer_offsets;
+} skm_evaluator_info;
+int skm_evaluator_describe(skm_evaluator *ev, skm_evaluator_info *out);
+
 /* GpuKernelEvaluator::SetRegularizerRKHS/RD/PG (GpuEvaluator.h:156-158,
  * GpuEvaluator.cu:786-831).  weight <= 0 switches the term off. */
 int skm_set_regularizer_rkhs(skm_evaluator *ev, double weight);
@@ -243,8 +259,9 @@ int skm_optimizer_run(skm_optimizer *o, int32_t iterations);
  * if stream_out is not NULL it receives that cudaStream_t (for event timing). */
 int skm_optimizer_enqueue(skm_optimizer *o, int32_t iterations, void *stream_out);
 /* Runs up to `iterations` iterations outside the graph with CUDA events between the
- * phases; phase_ms[0..6] receives the mean milliseconds of: parameter packing, grid
- * shifts, value pass, statistics, derivative + regularizers, result, optimizer update. */
+ * phases; phase_ms[0..8] receives the mean milliseconds of: parameter packing, grid
+ * shifts, transform (generic path: the whole value pass), warp + statistics, statistics,
+ * contrib GEMM (table path), derivative gather + regularizers, result, optimizer update. */
 int skm_optimizer_profile(skm_optimizer *o, int32_t iterations, double *phase_ms, int32_t nphase);
 /* Number of kernel launches in one captured iteration. */
 int skm_optimizer_graph_kernel_count(skm_optimizer *o, int32_t *count);

@@ -90,6 +90,26 @@ class Result(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class EvaluatorInfo(C.Structure):
+    _fields_ = [
+        ("path", C.c_int32),
+        ("dimensions", C.c_int32),
+        ("fixed_texels", C.c_int64),
+        ("samples", C.c_int64),
+        ("control_points", C.c_int64),
+        ("table_phases", C.c_int32),
+        ("table_taps", C.c_int32),
+        ("table_cells_per_axis", C.c_int32 * 3),
+        ("table_cells", C.c_int64),
+        ("table_regularizer_offsets", C.c_int32),
+    ]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["table_cells_per_axis"] = list(self.table_cells_per_axis)
+        return d
+
+
 class MetricDesc(C.Structure):
     _fields_ = [
         ("metric", C.c_int32),

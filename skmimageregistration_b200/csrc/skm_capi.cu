@@ -439,6 +439,28 @@ extern "C" int skm_evaluator_path(skm_evaluator *e, int32_t request, int32_t *ac
     return SKM_OK;
 }
 
+extern "C" int skm_evaluator_describe(skm_evaluator *e, skm_evaluator_info *out)
+{
+    if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
+    if (!out) return fail(SKM_ERR_INVALID, "out is NULL");
+    skm_evaluator_info r{};
+    r.path = (e->use_table && e->table.enabled) ? 2 : 1;
+    r.dimensions = e->D;
+    r.fixed_texels = e->N;
+    r.samples = e->Ns;
+    r.control_points = e->C;
+    if (e->table.enabled) {
+        const TableDev &T = e->table.dev;
+        r.table_phases = T.nph;
+        r.table_taps = T.ntap;
+        for (int d = 0; d < 3; ++d) r.table_cells_per_axis[d] = T.nq[d];
+        r.table_cells = T.ncell;
+        r.table_regularizer_offsets = T.nc[0] * T.nc[1] * T.nc[2];
+    }
+    *out = r;
+    return SKM_OK;
+}
+
 extern "C" int skm_set_regularizer_rkhs(skm_evaluator *e, double w)
 {
     if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
@@ -538,8 +560,9 @@ struct RegWeights {
 };
 
 // The full device sequence of one evaluation (everything after the parameter upload).
-// ev (optional, 4 events): recorded after the value pass, the statistics, the derivative pass and
-// the result kernel, for per-phase timing.
+// ev (optional, 6 events), for per-phase timing: after the transform (table path; the whole value
+// pass on the generic path), after the warp + statistics kernel, after the statistics kernel, after
+// the contrib GEMM (table path), after the derivative gather and after the result kernel.
 static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const RegWeights &w, const double *params,
                           cudaEvent_t *ev = nullptr)
 {
@@ -552,18 +575,19 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     const bool tab = e->use_table && e->table.enabled && metric != SKM_LCC;
     if (metric != SKM_LCC) {
         if (tab) {
-            if (table_value(e->table, e->P, D, metric, e->d_stats, e->d_counters, e->stream))
+            if (table_value(e->table, e->P, D, metric, e->d_stats, e->d_counters, e->stream, ev ? ev[0] : nullptr))
                 return fail(SKM_ERR_CUDA, "table value pass: %s", cudaGetErrorString(cudaGetLastError()));
         } else if ((rc = dispatch<LaunchValue>(D, kind, e))) {
             return rc;
         }
     }
-    if (ev) SKM_CUDA(cudaEventRecord(ev[0], e->stream));
+    if (ev && !tab) SKM_CUDA(cudaEventRecord(ev[0], e->stream));
+    if (ev) SKM_CUDA(cudaEventRecord(ev[1], e->stream));
     if (!tab) {                                  // the table path computes the statistics in its warp kernel
         stats_kernel<<<1, 1024, 0, e->stream>>>(e->d_part, e->value_blocks, metric, e->d_stats);
         SKM_CHECK_LAUNCH();
     }
-    if (ev) SKM_CUDA(cudaEventRecord(ev[1], e->stream));
+    if (ev) SKM_CUDA(cudaEventRecord(ev[2], e->stream));
     DerivParams Q{};
     Q.metric = metric;
     Q.with_metric = w.with_metric;
@@ -590,10 +614,11 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     bool any_reg = w.rkhs > 0 || w.rd > 0 || w.pg > 0 || w.with_metric;
     if (derivative) {
         if (tab) {
-            if (table_derivative(e->table, e->P, Q, D, e->gather_blocks, e->stream))
+            if (table_derivative(e->table, e->P, Q, D, e->gather_blocks, e->stream, ev ? ev[3] : nullptr))
                 return fail(SKM_ERR_CUDA, "table derivative: %s", cudaGetErrorString(cudaGetLastError()));
-        } else if ((rc = dispatch<LaunchDeriv>(D, kind, e, Q))) {
-            return rc;
+        } else {
+            if (ev) SKM_CUDA(cudaEventRecord(ev[3], e->stream));
+            if ((rc = dispatch<LaunchDeriv>(D, kind, e, Q))) return rc;
         }
     } else if (any_reg && tab) {
         // values only, through the same gather (and the same sums) as the derivative call, so
@@ -604,13 +629,14 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     } else if (any_reg) {
         if ((rc = dispatch<LaunchRegValue>(D, kind, e, Q))) return rc;
     }
-    if (ev) SKM_CUDA(cudaEventRecord(ev[2], e->stream));
+    if (ev && !derivative) SKM_CUDA(cudaEventRecord(ev[3], e->stream));
+    if (ev) SKM_CUDA(cudaEventRecord(ev[4], e->stream));
     if (!((derivative || any_reg) && tab)) {    // the table gather computes the result itself
         result_kernel<<<1, 256, 0, e->stream>>>(e->d_stats, (derivative || any_reg) ? e->d_rpart : nullptr,
                                                e->deriv_blocks, w.rkhs, w.rd, w.pg, w.l1, w.l21, w.l2, e->d_out);
         SKM_CHECK_LAUNCH();
     }
-    if (ev) SKM_CUDA(cudaEventRecord(ev[3], e->stream));
+    if (ev) SKM_CUDA(cudaEventRecord(ev[5], e->stream));
     return SKM_OK;
 }
 

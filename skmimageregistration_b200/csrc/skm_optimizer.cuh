@@ -110,9 +110,9 @@ struct skm_optimizer {
     }
 };
 
-// launches of one optimizer iteration (captured into the graph).  ev (optional, 8 events):
-// start, after pack, after shifts, after value, after statistics, after derivative, after result,
-// after the update -- used by skm_optimizer_profile.
+// launches of one optimizer iteration (captured into the graph).  ev (optional, 10 events):
+// start, after pack, after shifts, the six events of run_evaluation, after the update -- used by
+// skm_optimizer_profile.
 static int optimizer_iteration(skm_optimizer *o, cudaEvent_t *ev = nullptr)
 {
     skm_evaluator *e = o->e;
@@ -147,7 +147,7 @@ static int optimizer_iteration(skm_optimizer *o, cudaEvent_t *ev = nullptr)
                                                           o->od.A, o->od.alpha, o->od.f_max, o->od.f_min, o->od.omega,
                                                           o->d_sp, e->d_counters + 2);
     SKM_CHECK_LAUNCH();
-    if (ev) SKM_CUDA(cudaEventRecord(ev[7], e->stream));
+    if (ev) SKM_CUDA(cudaEventRecord(ev[9], e->stream));
     return SKM_OK;
 }
 
@@ -281,38 +281,37 @@ extern "C" int skm_optimizer_destroy(skm_optimizer *o)
 }
 
 // Runs up to `iterations` iterations un-graphed with CUDA events between the phases and
-// returns the mean time per phase in milliseconds: [pack, shifts, value pass, statistics,
-// derivative+regularizers, result, update].  The iterations advance the optimizer like
-// skm_optimizer_run.
+// returns the mean time per phase in milliseconds: [pack, shifts, transform (generic: value pass),
+// warp + statistics, statistics, contrib GEMM, derivative gather (generic: derivative pass),
+// result, update].  The iterations advance the optimizer like skm_optimizer_run.
 extern "C" int skm_optimizer_profile(skm_optimizer *o, int32_t iterations, double *phase_ms, int32_t nphase)
 {
     if (!o) return fail(SKM_ERR_STATE, "optimizer is NULL");
-    if (!phase_ms || nphase < 7) return fail(SKM_ERR_INVALID, "phase_ms needs 7 entries");
+    if (!phase_ms || nphase < 9) return fail(SKM_ERR_INVALID, "phase_ms needs 9 entries");
     skm_evaluator *e = o->e;
     SKM_CUDA(cudaSetDevice(e->device));
     int n = std::min<int>(iterations, o->od.number_of_iterations - o->iteration);
-    cudaEvent_t ev[8];
-    for (int i = 0; i < 8; ++i) SKM_CUDA(cudaEventCreate(&ev[i]));
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    cudaEvent_t ev[10];
+    for (int i = 0; i < 10; ++i) SKM_CUDA(cudaEventCreate(&ev[i]));
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     int rc = SKM_OK;
     for (int it = 0; it < n && !rc; ++it) {
         rc = optimizer_iteration(o, ev);
         if (rc) break;
-        cudaError_t ce = cudaEventSynchronize(ev[7]);
+        cudaError_t ce = cudaEventSynchronize(ev[9]);
         if (ce != cudaSuccess) {
             rc = fail(SKM_ERR_CUDA, "profile: %s", cudaGetErrorString(ce));
             break;
         }
-        // ev: 0 start, 1 pack, 2 shifts, 3 value, 4 stats, 5 derivative, 6 result, 7 update
-        for (int p = 0; p < 7; ++p) {
+        for (int p = 0; p < 9; ++p) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev[p], ev[p + 1]);
             acc[p] += ms;
         }
         o->iteration++;
     }
-    for (int i = 0; i < 8; ++i) cudaEventDestroy(ev[i]);
-    for (int p = 0; p < 7; ++p) phase_ms[p] = n > 0 ? acc[p] / n : 0.0;
+    for (int i = 0; i < 10; ++i) cudaEventDestroy(ev[i]);
+    for (int p = 0; p < 9; ++p) phase_ms[p] = n > 0 ? acc[p] / n : 0.0;
     return rc;
 }
 

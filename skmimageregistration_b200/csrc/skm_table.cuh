@@ -802,7 +802,7 @@ inline int table_transform_launch(TablePlan &pl, const EvalParams &P, cudaStream
 // value pass of the table path: transform, then warp + statistics; writes its own partials
 // (pl.d_part, pl.dev.value_blocks blocks)
 inline int table_value(TablePlan &pl, const EvalParams &P, int D, int metric, double *stats, unsigned *counter,
-                       cudaStream_t s)
+                       cudaStream_t s, cudaEvent_t mid = nullptr)
 {
     int rc;
     if (D == 3) {
@@ -816,6 +816,7 @@ inline int table_value(TablePlan &pl, const EvalParams &P, int D, int metric, do
         rc = table_transform_launch<1, 1>(pl, P, s);
     }
     if (rc) return rc;
+    if (mid && cudaEventRecord(mid, s) != cudaSuccess) return 2;
     if (D == 3)
         table_warp_kernel<3><<<pl.dev.value_blocks, 256, 0, s>>>(P, pl.dev, metric, stats, counter);
     else
@@ -824,11 +825,12 @@ inline int table_value(TablePlan &pl, const EvalParams &P, int D, int metric, do
 }
 
 inline int table_derivative(TablePlan &pl, const EvalParams &P, const DerivParams &Q, int D, int gather_blocks,
-                            cudaStream_t s)
+                            cudaStream_t s, cudaEvent_t mid = nullptr)
 {
     const size_t smem = table_contrib_smem(pl.dev);
     table_contrib_kernel<<<pl.contrib_blocks, kTabContribThreads, smem, s>>>(pl.dev, Q.stats);
     if (cudaPeekAtLastError() != cudaSuccess) return 2;
+    if (mid && cudaEventRecord(mid, s) != cudaSuccess) return 2;
     if (D == 3)
         table_gather_kernel<3><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
     else

@@ -19,7 +19,7 @@ import os
 import numpy as np
 
 from . import abi
-from .abi import (EvaluatorDesc, Field, MetricDesc, MetricValues, OptimizerDesc, OptimizerState, Result,
+from .abi import (EvaluatorDesc, EvaluatorInfo, Field, MetricDesc, MetricValues, OptimizerDesc, OptimizerState, Result,
                   dptr, field)
 from .problem import Problem, aos_to_flat, flat_to_aos
 
@@ -47,6 +47,7 @@ def lib():
         L.skm_abi_version.restype = C.c_int32
         L.skm_evaluator_create.argtypes = [C.POINTER(EvaluatorDesc), C.POINTER(C.c_void_p)]
         L.skm_evaluator_destroy.argtypes = [C.c_void_p]
+        L.skm_evaluator_describe.argtypes = [C.c_void_p, C.POINTER(EvaluatorInfo)]
         L.skm_evaluator_path.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
         L.skm_set_regularizer_rkhs.argtypes = [C.c_void_p, C.c_double]
         L.skm_set_regularizer_rd.argtypes = [C.c_void_p, C.c_double, C.c_double]
@@ -123,6 +124,12 @@ class GpuKernelEvaluator:
         a = C.c_int32()
         check(lib().skm_evaluator_path(self.h, int(request), C.byref(a)))
         return a.value
+
+    def describe(self):
+        """Kernel path and the sizes that set the cost of one evaluation."""
+        info = EvaluatorInfo()
+        check(lib().skm_evaluator_describe(self.h, C.byref(info)))
+        return info.as_dict()
 
     # --- GpuEvaluator.h:156-158
     def SetRegularizerRKHS(self, weight):
@@ -207,12 +214,12 @@ class Optimizer:
         check(lib().skm_optimizer_enqueue(self.h, int(iterations), C.byref(s)))
         return s.value
 
-    PHASES = ("pack", "shifts", "value", "stats", "derivative", "result", "update")
+    PHASES = ("pack", "shifts", "transform", "warp", "stats", "contrib", "gather", "result", "update")
 
     def profile(self, iterations):
         """Mean milliseconds per phase over `iterations` un-graphed iterations."""
-        out = np.zeros(7)
-        check(lib().skm_optimizer_profile(self.h, int(iterations), dptr(out), 7))
+        out = np.zeros(9)
+        check(lib().skm_optimizer_profile(self.h, int(iterations), dptr(out), 9))
         return dict(zip(self.PHASES, out.tolist()))
 
     def graph_kernel_count(self):
