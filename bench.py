@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ncc128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--gemm", default="auto", choices=["auto", "cuda"],
+                    help="table-path GEMMs: auto = tensor cores where they fit, cuda = CUDA-core kernels")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps (capped at 300)")
     return ap.parse_args()
 
@@ -139,6 +141,26 @@ def fp32_peak_tflops(torch):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def tf32_peak_tflops(torch):
+    """Tensor-core TF32 peak measured live: cuBLAS FP32 GEMM 8192^3 with TF32 allowed, best of 5."""
+    torch.backends.cuda.matmul.allow_tf32 = True
+    n = 8192
+    a = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    b = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    best = None
+    for _ in range(6):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        ms = s.elapsed_time(e)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    torch.backends.cuda.matmul.allow_tf32 = False
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
 def pair_count(pb):
     """(fixed texel, control point) pairs inside the forward box (separable per axis)."""
     tot = 1
@@ -158,9 +180,12 @@ def pair_count(pb):
 def kernel_work(pb, info, phases):
     """Per-kernel executed work (FLOPs) and algorithmic bytes of one iteration, with its time.
 
-    Table path: the transform and the contrib GEMM each execute 3 FMAs per (cell, phase, tap)
-    triple; the warp kernel evaluates a 4^D-tap B-spline with gradient per texel; the gather adds
-    3 values per (control point, tap).  Bytes count every input once and every output once.
+    Table path: the transform and the contrib GEMM each need 3 FMAs per (cell, phase, tap)
+    triple (algorithmic FLOPs); on the tensor cores (path 3) they execute, per tile of 128
+    (component, cell) rows, MMAs of N x K with N = 1.5 x tc_transform_n (hi x [hi; lo] and lo x hi)
+    and 3 x tc_contrib_n (hi hi, hi lo, lo hi) -- "tensor_flops".  The warp kernel evaluates a
+    4^D-tap B-spline with gradient per texel; the gather adds 3 values per (control point, tap).
+    Bytes count every input once and every output once.
     Generic path: one kernel evaluation (22 FLOP) per (texel, control point) pair in support.
     """
     D = pb.D
@@ -168,16 +193,26 @@ def kernel_work(pb, info, phases):
     ncoef = pb.moving_coefficients.size
     taps_b = 4 ** D
     bspline_flops = N * (2 * taps_b * 2 + 2 * (taps_b // 4) * 3)
-    if info["path"] == 2:
+    if info["path"] in (2, 3):
         cells, nph, ntap = info["table_cells"], info["table_phases"], info["table_taps"]
-        gemm = 2.0 * 3 * cells * nph * ntap
+        gemm = 2.0 * D * cells * nph * ntap
+        tc = info["path"] == 3
+        tr = {"name": "table_transform_tc_kernel" if tc else "table_transform_kernel",
+              "bound": "tensor" if tc else "fp32", "ms": phases["transform"],
+              "flops": gemm, "bytes": C * 16 + nph * ntap * 4 + cells * nph * 4 * D}
+        co = {"name": "table_contrib_tc_kernel" if tc else "table_contrib_kernel",
+              "bound": "tensor" if tc else "fp32", "ms": phases["contrib"], "flops": gemm,
+              "bytes": cells * nph * (16 + 4) + nph * ntap * 4 + D * ntap * cells * 4}
+        if tc:
+            tr["tensor_flops"] = (2.0 * 128 * 1.5 * info["tc_transform_n"] * info["tc_transform_k"]
+                                  * info["tc_transform_tiles"])
+            co["tensor_flops"] = (2.0 * 128 * 3 * info["tc_contrib_n"] * info["tc_contrib_k"]
+                                  * info["tc_contrib_tiles"])
         return {
-            "transform": {"name": "table_transform_kernel", "bound": "fp32", "ms": phases["transform"],
-                          "flops": gemm, "bytes": C * 16 + nph * ntap * 4 + cells * nph * 16},
+            "transform": tr,
             "warp": {"name": "table_warp_kernel", "bound": "hbm", "ms": phases["warp"], "flops": bspline_flops,
-                     "bytes": cells * nph * (16 + 4 + 16) + ncoef * 4},
-            "contrib": {"name": "table_contrib_kernel", "bound": "fp32", "ms": phases["contrib"], "flops": gemm,
-                        "bytes": cells * nph * (16 + 4) + nph * ntap * 4 + 3 * ntap * cells * 4},
+                     "bytes": cells * nph * (4 * D + 4 + 16) + ncoef * 4},
+            "contrib": co,
             "gather": {"name": "table_gather_kernel", "bound": "hbm", "ms": phases["gather"],
                        "flops": 3.0 * C * ntap + 20.0 * C * info["table_regularizer_offsets"],
                        "bytes": 3 * ntap * cells * 4 + C * 16 + C * D * 8},
@@ -286,6 +321,8 @@ def run_ours(args, rank, world, local_rank):
     P = pb.num_parameters
     cpw = np.ones(pb.C)
     ev = GpuKernelEvaluator(pb)
+    gemm_request = GpuKernelEvaluator.AUTO if args.gemm == "auto" else GpuKernelEvaluator.REQ_TABLE_CUDA_CORES
+    ev.path(gemm_request)
     opt = Optimizer(ev, odesc, mdesc, np.zeros(P), cpw)
     stream = torch.cuda.ExternalStream(opt.enqueue(0))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -327,6 +364,7 @@ def run_ours(args, rank, world, local_rank):
     # e2e: reference-facing C-ABI call with host buffers + host-side optimizer update
     e2e_steps = args.e2e_steps or min(args.steps, 300)
     ev2 = GpuKernelEvaluator(pb)
+    ev2.path(gemm_request)
     params = np.zeros(P)
     base = np.zeros(P)
     prev = np.zeros(P)
@@ -361,6 +399,7 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0:
         hbm_peak, hbm_src = measured_peaks()
         fp32_peak = fp32_peak_tflops(torch)
+        tf32_peak = tf32_peak_tflops(torch)
         info = ev.describe()
         kernels = kernel_work(pb, info, phases)
         dom = max(kernels, key=lambda k: kernels[k]["ms"])
@@ -377,7 +416,18 @@ def run_ours(args, rank, world, local_rank):
             v["gbs"] = v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] > 0 else None
             v["fp32_frac"] = v["tflops"] / fp32_peak if v["tflops"] is not None else None
             v["hbm_frac"] = v["gbs"] / hbm_peak if v["gbs"] is not None else None
-        if kd["bound"] == "fp32":
+            if "tensor_flops" in v:
+                v["tensor_tflops"] = v["tensor_flops"] / (v["ms"] * 1e-3) / 1e12 if v["ms"] > 0 else None
+                v["tensor_frac"] = v["tensor_tflops"] / tf32_peak if v["tensor_tflops"] is not None else None
+        if kd["bound"] == "tensor":
+            roof = {"kernel": kd["name"], "bound": "tensor", "achieved": kd["tensor_tflops"], "peak": tf32_peak,
+                    "unit": "TFLOP/s", "frac": kd["tensor_frac"], "traffic": traffic,
+                    "peak_source": "cuBLAS FP32 GEMM 8192^3 with TF32 tensor cores, measured live in this run",
+                    "tensor_flops_per_launch": kd["tensor_flops"], "fp32_equivalent_tflops": kd["tflops"],
+                    "flops_per_launch": kd["flops"], "launch_ms": kd["ms"],
+                    "hbm": {"achieved": kd["gbs"], "peak": hbm_peak, "unit": "GB/s", "frac": kd["hbm_frac"],
+                            "algorithmic_bytes_per_launch": kd["bytes"], "peak_source": hbm_src}}
+        elif kd["bound"] == "fp32":
             roof = {"kernel": kd["name"], "bound": "fp32", "achieved": kd["tflops"], "peak": fp32_peak,
                     "unit": "TFLOP/s", "frac": kd["fp32_frac"], "traffic": traffic,
                     "peak_source": "cuBLAS SGEMM 8192^3, TF32 off, measured live in this run (CUDA-core FP32)",
@@ -394,7 +444,8 @@ def run_ours(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded %s pair per GPU)" % args.workload,
             "config": dict(info_cfg, parallelism="pair-parallel x%d (independent replicas, no collective)" % world,
-                           kernel_path="phase table" if info["path"] == 2 else "generic",
+                           kernel_path={1: "generic", 2: "phase table (CUDA-core GEMMs)",
+                                        3: "phase table (tcgen05 3xTF32 GEMMs)"}[info["path"]],
                            l2="flushed before every timed iteration (256 MB write outside the events)",
                            timing="CUDA events on the evaluator stream around each graph-replayed iteration",
                            arithmetic="FP32 kernel sums, FP64 global sums"),
@@ -405,6 +456,8 @@ def run_ours(args, rank, world, local_rank):
             "final_state": state,
             "roofline": roof,
             "roofline_kernels": kernels,
+            "peaks": {"hbm_gbs": hbm_peak, "hbm_source": hbm_src, "fp32_sgemm_tflops": fp32_peak,
+                      "tf32_gemm_tflops": tf32_peak},
             "e2e": {"value": e2e_rate, "unit": "iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps},
         }

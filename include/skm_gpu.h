@@ -131,16 +131,18 @@ int skm_evaluator_create(const skm_evaluator_desc *desc, skm_evaluator **out);
 int skm_evaluator_destroy(skm_evaluator *ev);
 
 /* Kernel path selection (no counterpart in the reference, which has one path).
- * request: -1 query only, 0 automatic (phase-table path where it applies), 1 generic
- * kernels only.  *active (may be NULL) receives the path MSE/NCC calls take:
+ * request: -1 query only, 0 automatic (phase-table path where it applies, its two GEMMs on
+ * the tensor cores where they fit), 1 generic kernels only, 2 phase-table path with its
+ * GEMMs on the CUDA cores.  *active (may be NULL) receives the path MSE/NCC calls take:
  * 1 generic, 2 phase table (stationary kernel, control spacing an integer multiple of
- * the fixed spacing, subsample 1).  Both paths compute the same sums. */
+ * the fixed spacing, subsample 1), 3 phase table with tensor-core GEMMs (3xTF32, FP32
+ * accuracy).  All paths compute the same sums. */
 int skm_evaluator_path(skm_evaluator *ev, int32_t request, int32_t *active);
 
 /* Work description of an evaluator (no counterpart in the reference): the kernel path and
  * the sizes that set the cost of one evaluation. */
 typedef struct skm_evaluator_info {
-    int32_t path;                     /* 1 generic kernels, 2 phase table */
+    int32_t path;                     /* 1 generic, 2 phase table, 3 phase table on tensor cores */
     int32_t dimensions;
     int64_t fixed_texels;
     int64_t samples;                  /* fixed texels / subsample^D */
@@ -150,6 +152,16 @@ typedef struct skm_evaluator_info {
     int32_t table_cells_per_axis[3];
     int64_t table_cells;
     int32_t table_regularizer_offsets;
+    /* tensor-core GEMMs of the table path (zero when they do not apply): M = 128 rows of
+     * (component, cell) per tile, N x K per MMA chain */
+    int32_t tc_cells_per_tile;
+    int32_t tc_brick[3];              /* cells per transform tile along x, y, z */
+    int64_t tc_transform_tiles;
+    int64_t tc_contrib_tiles;
+    int32_t tc_transform_n;           /* 2 x phases padded to 16 (tf32 part and remainder of the table) */
+    int32_t tc_transform_k;           /* taps padded to 8 */
+    int32_t tc_contrib_n;             /* taps padded to 16 */
+    int32_t tc_contrib_k;             /* phases padded to 8 */
 } skm_evaluator_info;
 int skm_evaluator_describe(skm_evaluator *ev, skm_evaluator_info *out);
 

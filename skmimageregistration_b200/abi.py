@@ -102,11 +102,20 @@ class EvaluatorInfo(C.Structure):
         ("table_cells_per_axis", C.c_int32 * 3),
         ("table_cells", C.c_int64),
         ("table_regularizer_offsets", C.c_int32),
+        ("tc_cells_per_tile", C.c_int32),
+        ("tc_brick", C.c_int32 * 3),
+        ("tc_transform_tiles", C.c_int64),
+        ("tc_contrib_tiles", C.c_int64),
+        ("tc_transform_n", C.c_int32),
+        ("tc_transform_k", C.c_int32),
+        ("tc_contrib_n", C.c_int32),
+        ("tc_contrib_k", C.c_int32),
     ]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
         d["table_cells_per_axis"] = list(self.table_cells_per_axis)
+        d["tc_brick"] = list(self.tc_brick)
         return d
 
 

@@ -6,6 +6,7 @@ object with the C-ABI of include/skm_gpu.h; Python reaches it through ctypes.
 """
 from __future__ import annotations
 
+import glob
 import os
 import subprocess
 import sys
@@ -14,8 +15,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libskm_b200.so")
 SOURCES = ["csrc/skm_capi.cu", "csrc/skm_noalloc.cu"]
-DEPS = ["csrc/skm_capi.cu", "csrc/skm_noalloc.cu", "csrc/skm_device.cuh", "csrc/skm_kernels.cuh", "csrc/skm_prefilter.cuh",
-        "csrc/skm_table.cuh", "csrc/skm_optimizer.cuh", "../include/skm_gpu.h"]
+
+def deps():
+    """Every source the library is compiled from: all of csrc/ and the C headers."""
+    files = glob.glob(os.path.join(HERE, "csrc", "*.cu")) + glob.glob(os.path.join(HERE, "csrc", "*.cuh"))
+    files += glob.glob(os.path.join(HERE, "..", "include", "*.h"))
+    return files + [os.path.abspath(__file__)]
+
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
@@ -30,7 +36,7 @@ def stale():
     if not os.path.exists(LIB_PATH):
         return True
     t = os.path.getmtime(LIB_PATH)
-    return any(os.path.getmtime(os.path.join(HERE, d)) > t for d in DEPS)
+    return any(os.path.getmtime(d) > t for d in deps())
 
 
 def build(force=False, verbose=False):

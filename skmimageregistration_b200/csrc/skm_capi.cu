@@ -17,6 +17,7 @@
 #include "skm_kernels.cuh"
 #include "skm_prefilter.cuh"
 #include "skm_table.cuh"
+#include "skm_table_tc.cuh"
 
 using namespace skm;
 
@@ -137,8 +138,10 @@ struct skm_evaluator {
     // pinned host staging
     double *h_in = nullptr, *h_out = nullptr;
 
-    // phase-table fast path (stationary kernel, integral spacing ratio)
+    // phase-table fast path (stationary kernel, integral spacing ratio) and its tensor-core GEMMs
     TablePlan table{};
+    TcPlan tc{};
+    bool use_tc = true;
 
     // state of GpuKernelEvaluator
     double reg_rkhs = 0, reg_rd = 0, rd_scaling = 1, reg_pg = 0, pg_scaling = 1;
@@ -155,12 +158,26 @@ struct skm_evaluator {
                         d_dense_sw_in, d_shifts, d_in, d_counters, d_part, d_stats, d_deriv, d_rpart, d_out};
         for (void *b : bufs)
             if (b) cudaFree(b);
+        table_tc_free(tc);
         table_free(table);
         if (h_in) cudaFreeHost(h_in);
         if (h_out) cudaFreeHost(h_out);
         if (stream) cudaStreamDestroy(stream);
     }
 };
+
+// 1 generic kernels, 2 phase table with CUDA-core GEMMs, 3 phase table with tensor-core GEMMs
+static int active_path(const skm_evaluator *e)
+{
+    if (!(e->use_table && e->table.enabled)) return 1;
+    return (e->use_tc && e->tc.enabled) ? 3 : 2;
+}
+
+// tensor-core GEMMs of the table path, when they apply and are selected
+static const TcPlan *tc_of(const skm_evaluator *e)
+{
+    return (e->use_tc && e->tc.enabled) ? &e->tc : nullptr;
+}
 
 // ------------------------------------------------------------------------------------------------
 // dispatch over dimension and kernel kind
@@ -413,6 +430,8 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         if (trc) return fail(SKM_ERR_CUDA, "table plan failed: %s", cudaGetErrorString(cudaGetLastError()));
         if (e->table.enabled && (table_set_attributes(e->table) || table_size_grids(e->table)))
             return fail(SKM_ERR_CUDA, "table kernel attributes: %s", cudaGetErrorString(cudaGetLastError()));
+        if (e->table.enabled && table_tc_plan(e->tc, e->table, e->stream))
+            return fail(SKM_ERR_CUDA, "tensor-core table plan: %s", cudaGetErrorString(cudaGetLastError()));
         return SKM_OK;
     }();
     if (rc) {
@@ -432,10 +451,18 @@ extern "C" int skm_evaluator_destroy(skm_evaluator *e)
 extern "C" int skm_evaluator_path(skm_evaluator *e, int32_t request, int32_t *active)
 {
     if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
-    if (request == 1) e->use_table = false;
-    else if (request == 0) e->use_table = true;
-    else if (request != -1) return fail(SKM_ERR_INVALID, "path request must be -1, 0 or 1");
-    if (active) *active = (e->use_table && e->table.enabled) ? 2 : 1;
+    if (request == 1) {
+        e->use_table = false;
+    } else if (request == 0) {
+        e->use_table = true;
+        e->use_tc = true;
+    } else if (request == 2) {
+        e->use_table = true;
+        e->use_tc = false;
+    } else if (request != -1) {
+        return fail(SKM_ERR_INVALID, "path request must be -1, 0, 1 or 2");
+    }
+    if (active) *active = active_path(e);
     return SKM_OK;
 }
 
@@ -444,7 +471,7 @@ extern "C" int skm_evaluator_describe(skm_evaluator *e, skm_evaluator_info *out)
     if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
     if (!out) return fail(SKM_ERR_INVALID, "out is NULL");
     skm_evaluator_info r{};
-    r.path = (e->use_table && e->table.enabled) ? 2 : 1;
+    r.path = active_path(e);
     r.dimensions = e->D;
     r.fixed_texels = e->N;
     r.samples = e->Ns;
@@ -456,6 +483,19 @@ extern "C" int skm_evaluator_describe(skm_evaluator *e, skm_evaluator_info *out)
         for (int d = 0; d < 3; ++d) r.table_cells_per_axis[d] = T.nq[d];
         r.table_cells = T.ncell;
         r.table_regularizer_offsets = T.nc[0] * T.nc[1] * T.nc[2];
+    }
+    if (e->table.enabled && e->tc.enabled) {
+        const TcDev &C = e->tc.dev;
+        r.tc_cells_per_tile = C.ct;
+        r.tc_brick[0] = C.bx;
+        r.tc_brick[1] = C.by;
+        r.tc_brick[2] = C.bz;
+        r.tc_transform_tiles = (int64_t)C.tiles[0] * C.tiles[1] * C.tiles[2];
+        r.tc_contrib_tiles = (e->table.dev.ncell + C.ct - 1) / C.ct;
+        r.tc_transform_n = 2 * C.np;
+        r.tc_transform_k = C.kp;
+        r.tc_contrib_n = C.npc;
+        r.tc_contrib_k = C.kpc;
     }
     *out = r;
     return SKM_OK;
@@ -575,7 +615,8 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     const bool tab = e->use_table && e->table.enabled && metric != SKM_LCC;
     if (metric != SKM_LCC) {
         if (tab) {
-            if (table_value(e->table, e->P, D, metric, e->d_stats, e->d_counters, e->stream, ev ? ev[0] : nullptr))
+            if (table_value(e->table, tc_of(e), e->P, D, metric, e->d_stats, e->d_counters, e->stream,
+                            ev ? ev[0] : nullptr))
                 return fail(SKM_ERR_CUDA, "table value pass: %s", cudaGetErrorString(cudaGetLastError()));
         } else if ((rc = dispatch<LaunchValue>(D, kind, e))) {
             return rc;
@@ -614,7 +655,7 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     bool any_reg = w.rkhs > 0 || w.rd > 0 || w.pg > 0 || w.with_metric;
     if (derivative) {
         if (tab) {
-            if (table_derivative(e->table, e->P, Q, D, e->gather_blocks, e->stream, ev ? ev[3] : nullptr))
+            if (table_derivative(e->table, tc_of(e), e->P, Q, D, e->gather_blocks, e->stream, ev ? ev[3] : nullptr))
                 return fail(SKM_ERR_CUDA, "table derivative: %s", cudaGetErrorString(cudaGetLastError()));
         } else {
             if (ev) SKM_CUDA(cudaEventRecord(ev[3], e->stream));
@@ -633,11 +674,32 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     if (ev) SKM_CUDA(cudaEventRecord(ev[4], e->stream));
     if (!((derivative || any_reg) && tab)) {    // the table gather computes the result itself
         result_kernel<<<1, 256, 0, e->stream>>>(e->d_stats, (derivative || any_reg) ? e->d_rpart : nullptr,
-                                               e->deriv_blocks, w.rkhs, w.rd, w.pg, w.l1, w.l21, w.l2, e->d_out);
+                                               e->deriv_blocks, w.rkhs, w.rd, w.pg, w.l1, w.l21, w.l2, e->d_out,
+                                               tab ? e->table.dev.tc_err : nullptr);
         SKM_CHECK_LAUNCH();
     }
     if (ev) SKM_CUDA(cudaEventRecord(ev[5], e->stream));
     return SKM_OK;
+}
+
+// A bounded wait of a tensor-core kernel gave up: reset the sticky word and report it.
+static int report_fault(skm_evaluator *e)
+{
+    if (e->tc.d_err) {
+        cudaMemsetAsync(e->tc.d_err, 0, sizeof(unsigned), e->stream);
+        cudaStreamSynchronize(e->stream);
+    }
+    return fail(SKM_ERR_TIMEOUT, "a tensor-core kernel gave up waiting for its MMAs; results discarded");
+}
+
+// Reads the sticky fault word (paths that do not copy the result vector back).
+static int check_fault(skm_evaluator *e)
+{
+    if (!e->tc.d_err) return SKM_OK;
+    unsigned f = 0;
+    SKM_CUDA(cudaMemcpyAsync(&f, e->tc.d_err, sizeof f, cudaMemcpyDeviceToHost, e->stream));
+    SKM_CUDA(cudaStreamSynchronize(e->stream));
+    return f ? report_fault(e) : SKM_OK;
 }
 
 static int fetch(skm_evaluator *e, double *derivative)
@@ -647,6 +709,7 @@ static int fetch(skm_evaluator *e, double *derivative)
         SKM_CUDA(cudaMemcpyAsync(e->h_out + NO, e->d_deriv, sizeof(double) * e->nparams, cudaMemcpyDeviceToHost,
                                  e->stream));
     SKM_CUDA(cudaStreamSynchronize(e->stream));
+    if (e->h_out[O_FAULT] != 0.0) return report_fault(e);
     if (derivative) std::memcpy(derivative, e->h_out + NO, sizeof(double) * e->nparams);
     return SKM_OK;
 }

@@ -24,7 +24,7 @@ enum {
 };
 // result vector written by result_kernel
 enum {
-    O_MEASURE = 0, O_RKHS, O_RD, O_PG, O_L1, O_L21, O_L2, O_REG, O_VALUE, O_COUNT, NO
+    O_MEASURE = 0, O_RKHS, O_RD, O_PG, O_L1, O_L21, O_L2, O_REG, O_VALUE, O_COUNT, O_FAULT, NO
 };
 
 struct EvalParams {
@@ -737,8 +737,11 @@ __global__ void __launch_bounds__(256) regvalue_kernel(EvalParams P, DerivParams
 }
 
 // final scalars: measure, regularizer values, weighted sum (metric hxx:531-538, 572)
+// fault: sticky failure word of the tensor-core kernels (NULL when none ran); copied to
+// out[O_FAULT] so that the host sees it with the result.
 __device__ inline void result_finalize(const double *stats, const double *v, double w_rkhs, double w_rd,
-                                       double w_pg, double w_l1, double w_l21, double w_l2, double *__restrict__ out)
+                                       double w_pg, double w_l1, double w_l21, double w_l2, double *__restrict__ out,
+                                       const unsigned *fault = nullptr)
 {
     double reg = 0.0;
     if (w_l1 > 0) reg += w_l1 * v[R_L1];
@@ -757,11 +760,13 @@ __device__ inline void result_finalize(const double *stats, const double *v, dou
     out[O_REG] = reg;
     out[O_VALUE] = stats[S_MEASURE] + reg;
     out[O_COUNT] = stats[S_COUNT];
+    out[O_FAULT] = fault ? (double)*(const volatile unsigned *)fault : 0.0;
 }
 
 static __global__ void __launch_bounds__(256) result_kernel(const double *__restrict__ stats, const double *__restrict__ rpart,
                                                      int nblocks, double w_rkhs, double w_rd, double w_pg, double w_l1,
-                                                     double w_l21, double w_l2, double *__restrict__ out)
+                                                     double w_l21, double w_l2, double *__restrict__ out,
+                                                     const unsigned *fault)
 {
     __shared__ double sh[NR * 32];
     double v[NR];
@@ -771,7 +776,7 @@ static __global__ void __launch_bounds__(256) result_kernel(const double *__rest
 #pragma unroll
         for (int k = 0; k < NR; ++k) v[k] = 0.0;
     }
-    if (threadIdx.x == 0) result_finalize(stats, v, w_rkhs, w_rd, w_pg, w_l1, w_l21, w_l2, out);
+    if (threadIdx.x == 0) result_finalize(stats, v, w_rkhs, w_rd, w_pg, w_l1, w_l21, w_l2, out, fault);
 }
 
 // ---- LCC: dense fields and per-sample values --------------------------------------------------

@@ -227,7 +227,7 @@ extern "C" int skm_optimizer_run(skm_optimizer *o, int32_t iterations)
     SKM_CUDA(cudaMemcpyAsync(&e->rng_state, o->d_rng, sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->stream));
     SKM_CUDA(cudaStreamSynchronize(e->stream));
     if (n > 0 && e->P.sub > 1) e->evaluated_once = true;
-    return SKM_OK;
+    return check_fault(e);
 }
 
 // Enqueue iterations without waiting (used for timing the device-resident loop).
@@ -263,6 +263,8 @@ extern "C" int skm_optimizer_get_state(skm_optimizer *o, skm_optimizer_state *ou
     SKM_CUDA(cudaSetDevice(e->device));
     SKM_CUDA(cudaMemcpyAsync(s, o->d_scal, sizeof s, cudaMemcpyDeviceToHost, e->stream));
     SKM_CUDA(cudaStreamSynchronize(e->stream));
+    int rc = check_fault(e);
+    if (rc) return rc;
     out->iteration = (int32_t)s[T_ITER];
     out->current_time = s[T_TIME];
     out->learning_rate = s[T_LR];

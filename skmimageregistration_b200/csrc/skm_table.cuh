@@ -50,10 +50,11 @@ struct TableDev {
     const float *tgemm;  // [phase][ntap_pad]
     const float *kcp;    // [nc0*nc1*nc2] kernel between control points at an offset
     float4 *rec;         // [cell][phase]: grad M, m
-    float4 *ucp;         // [cell][phase]: u = sum_t T w alpha
+    float *ucp;          // [comp][cell][phase]: u = sum_t T w alpha (planes of ncell*nph)
     const float *fixcp;  // [cell][phase]: fixed image value (0 outside)
     float *contrib;      // [3][ntap][ncell]
     double *part;        // [NQ][value blocks]
+    unsigned *tc_err;    // failure word of the tensor-core kernels (NULL without them)
     int value_blocks, tile_x, tile_y, tiles_x, tiles_y, tiles_z;
 };
 
@@ -61,11 +62,13 @@ struct TablePlan {
     bool enabled = false;
     TableDev dev{};
     float *d_tfwd = nullptr, *d_tgemm = nullptr, *d_kcp = nullptr, *d_fixcp = nullptr, *d_contrib = nullptr;
-    float4 *d_rec = nullptr, *d_ucp = nullptr;
+    float4 *d_rec = nullptr;
+    float *d_ucp = nullptr;
     double *d_part = nullptr;
     int hl = 1;          // z phases per thread in the transform kernel (template argument)
     int ncz = 1;         // cells per thread along z in the transform kernel
     int transform_blocks = 0, contrib_blocks = 0;
+    std::vector<float> h_tgemm;   // host copy of tgemm (operand tables of the tensor-core kernels)
 };
 
 // ------------------------------------------------------------------------------------------------
@@ -149,10 +152,13 @@ __global__ void __launch_bounds__(256, 2) table_transform_kernel(EvalParams P, T
             if (tz0 + c >= T.nq[2]) break;
             const long long cell =
                 (long long)(tx0 + cx) + (long long)T.nq[0] * ((ty0 + cy) + (long long)T.nq[1] * (tz0 + c));
+            const long long plane = T.ncell * T.nph;
 #pragma unroll
             for (int k = 0; k < HL; ++k) {
-                const int p_lin = px + T.h[0] * (py + T.h[1] * k);
-                T.ucp[cell * T.nph + p_lin] = make_float4(acc[c][k][0], acc[c][k][1], acc[c][k][2], 0.f);
+                const long long i = cell * T.nph + px + T.h[0] * (py + T.h[1] * k);
+                T.ucp[i] = acc[c][k][0];
+                T.ucp[i + plane] = acc[c][k][1];
+                if (T.D > 2) T.ucp[i + 2 * plane] = acc[c][k][2];
             }
         }
     }
@@ -186,7 +192,8 @@ __global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev 
         }
         float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ok) {
-            const float4 u = T.ucp[i];
+            const long long plane = T.ncell * T.nph;
+            const float u[3] = {T.ucp[i], T.ucp[i + plane], D > 2 ? T.ucp[i + 2 * plane] : 0.f};
             double fi[3] = {(double)x[0], (double)x[1], (double)x[2]}, p[3], mp[3], ml[3];
             to_global<D>(P.fixed, fi, p);
 #pragma unroll
@@ -200,9 +207,9 @@ __global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev 
                     if (D > 2) mp[2] += dv.z;
                 }
             }
-            mp[0] += (double)u.x;
-            if (D > 1) mp[1] += (double)u.y;
-            if (D > 2) mp[2] += (double)u.z;
+            mp[0] += (double)u[0];
+            if (D > 1) mp[1] += (double)u[1];
+            if (D > 2) mp[2] += (double)u[2];
             to_local<D>(P.mov, mp, ml);
             if (bspline_inside<D>(P.mov, ml)) {
                 float m, g[3] = {0.f, 0.f, 0.f};
@@ -500,7 +507,8 @@ __global__ void __launch_bounds__(256) table_gather_kernel(EvalParams P, TableDe
         double w[NR];
         sum_partials<NR>(Q.rpart, gridDim.x, w, shr);
         if (threadIdx.x == 0)
-            result_finalize(Q.stats, w, Q.reg_rkhs, Q.reg_rd, Q.reg_pg, Q.reg_l1, Q.reg_l21, Q.reg_l2, Q.out);
+            result_finalize(Q.stats, w, Q.reg_rkhs, Q.reg_rd, Q.reg_pg, Q.reg_l1, Q.reg_l21, Q.reg_l2, Q.out,
+                            T.tc_err);
     }
 }
 
@@ -711,9 +719,10 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
         return cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(float), cudaMemcpyHostToDevice, stream) ==
                cudaSuccess;
     };
+    pl.h_tgemm = tgemm;
     if (!up(&pl.d_tfwd, tfwd) || !up(&pl.d_tgemm, tgemm) || !up(&pl.d_kcp, kcp) || !up(&pl.d_fixcp, fix)) return 2;
     if (cudaMalloc((void **)&pl.d_rec, (size_t)T.ncell * T.nph * sizeof(float4)) != cudaSuccess) return 2;
-    if (cudaMalloc((void **)&pl.d_ucp, (size_t)T.ncell * T.nph * sizeof(float4)) != cudaSuccess) return 2;
+    if (cudaMalloc((void **)&pl.d_ucp, (size_t)D * T.ncell * T.nph * sizeof(float)) != cudaSuccess) return 2;
     if (cudaMalloc((void **)&pl.d_contrib, (size_t)3 * T.ntap * T.ncell * sizeof(float)) != cudaSuccess) return 2;
     if (cudaMalloc((void **)&pl.d_part, (size_t)NQ * T.value_blocks * sizeof(double)) != cudaSuccess) return 2;
     if (cudaStreamSynchronize(stream) != cudaSuccess) return 2;
@@ -790,62 +799,6 @@ inline int table_size_grids(TablePlan &pl)
     pl.transform_blocks = std::max(1, std::min(ntiles, std::max(1, bt) * sms));
     pl.contrib_blocks = (int)std::max<long long>(1, std::min<long long>(ctiles, (long long)std::max(1, bc) * sms));
     return 0;
-}
-
-template <int HL, int NCZ>
-inline int table_transform_launch(TablePlan &pl, const EvalParams &P, cudaStream_t s)
-{
-    table_transform_kernel<HL, NCZ><<<pl.transform_blocks, 256, table_value_smem(pl), s>>>(P, pl.dev);
-    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
-}
-
-// value pass of the table path: transform, then warp + statistics; writes its own partials
-// (pl.d_part, pl.dev.value_blocks blocks)
-inline int table_value(TablePlan &pl, const EvalParams &P, int D, int metric, double *stats, unsigned *counter,
-                       cudaStream_t s, cudaEvent_t mid = nullptr)
-{
-    int rc;
-    if (D == 3) {
-        switch (pl.hl) {
-        case 1: rc = table_transform_launch<1, 4>(pl, P, s); break;
-        case 2: rc = table_transform_launch<2, 4>(pl, P, s); break;
-        case 4: rc = table_transform_launch<4, 4>(pl, P, s); break;
-        default: rc = table_transform_launch<8, 4>(pl, P, s); break;
-        }
-    } else {
-        rc = table_transform_launch<1, 1>(pl, P, s);
-    }
-    if (rc) return rc;
-    if (mid && cudaEventRecord(mid, s) != cudaSuccess) return 2;
-    if (D == 3)
-        table_warp_kernel<3><<<pl.dev.value_blocks, 256, 0, s>>>(P, pl.dev, metric, stats, counter);
-    else
-        table_warp_kernel<2><<<pl.dev.value_blocks, 256, 0, s>>>(P, pl.dev, metric, stats, counter);
-    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
-}
-
-inline int table_derivative(TablePlan &pl, const EvalParams &P, const DerivParams &Q, int D, int gather_blocks,
-                            cudaStream_t s, cudaEvent_t mid = nullptr)
-{
-    const size_t smem = table_contrib_smem(pl.dev);
-    table_contrib_kernel<<<pl.contrib_blocks, kTabContribThreads, smem, s>>>(pl.dev, Q.stats);
-    if (cudaPeekAtLastError() != cudaSuccess) return 2;
-    if (mid && cudaEventRecord(mid, s) != cudaSuccess) return 2;
-    if (D == 3)
-        table_gather_kernel<3><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
-    else
-        table_gather_kernel<2><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
-    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
-}
-
-inline int table_derivative_gather_only(TablePlan &pl, const EvalParams &P, const DerivParams &Q, int D,
-                                        int gather_blocks, cudaStream_t s)
-{
-    if (D == 3)
-        table_gather_kernel<3><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
-    else
-        table_gather_kernel<2><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
-    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
 inline void table_free(TablePlan &pl)

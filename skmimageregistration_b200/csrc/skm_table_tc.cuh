@@ -1,0 +1,825 @@
+// skm_table_tc.cuh -- the two GEMM-shaped kernels of the phase-table path on the 5th-generation
+// tensor cores: tcgen05.mma kind::tf32 with FP32 accumulators in TMEM, FP32-accurate through a
+// hi/lo split of both operands (x = hi + lo, hi = tf32(x)).
+//
+// Rows of both GEMMs are (component, cell) pairs, component-major: row = comp * ct + c with
+// ct = 128 / D cells per tile (42 in 3-D, 64 in 2-D), so one M = 128 MMA serves all components.
+//
+//   transform  D[row][n] = sum_t A[row][t] B[n][t]  over taps t (K), phases n (N)
+//              A = im2col of w*alpha over a brick of cells, staged per tile as hi/lo planes,
+//              B = [T_hi ; T_lo]: n < np is the tf32 part of T[phase n][t], n >= np the rest;
+//              per K step  A_hi x [B_hi ; B_lo]  (N = 2 np)  and  A_lo x B_hi  (N = np), so
+//              u[row][p] = D[row][p] + D[row][np + p] = A_hi B_hi + A_lo B_hi + A_hi B_lo.
+//   contrib    D[row][tap] = sum_p G[row][p] T[p][tap],  G = (a f + b m + c) grad M per texel;
+//              per K step  G_hi T_hi + G_hi T_lo + G_lo T_hi  (N = taps padded to 16).
+//
+// One CTA per SM, persistent over tiles, warp-specialized: 8 producer warps build the A operand
+// of each K chunk in a ring of shared-memory stages (full/empty mbarriers), one thread issues the
+// MMAs of a chunk as soon as its stage is full and commits them to the stage's empty barrier, and
+// 4 epilogue warps drain the finished accumulator of a tile from TMEM (two accumulators, so the
+// MMAs of the next tile run meanwhile).  The transform's producers stage the control points of
+// the next brick with cp.async while they build the current one.  Operands use the K-major no-swizzle canonical layout
+// [K/4][rows][4 floats]: 8-row x 16-byte core matrices, SBO = 128 B between 8-row groups,
+// LBO = rows * 16 B between the two 4-element K halves of one MMA.
+// Every mbarrier wait is bounded; a wait that gives up sets *err and a CTA-wide abort flag that
+// ends the other roles' waits, the MMA thread waits (bounded) for its MMAs in flight, and the
+// CTA frees its TMEM and returns.
+#pragma once
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "skm_table.cuh"
+#include "skm_tc.cuh"
+
+namespace skm {
+
+constexpr int kTcEpiWarps = 4;                                   // warps 0-3: TMEM -> global
+constexpr int kTcMmaWarp = 4;                                    // warp 4: TMEM owner, lane 0 issues
+constexpr int kTcProdWarps = 8;                                  // warps 5-12: A operand stages
+constexpr int kTcProdThreads = kTcProdWarps * 32;
+constexpr int kTcProdBase = (kTcEpiWarps + 1) * 32;              // first producer thread
+constexpr int kTcThreads = kTcProdBase + kTcProdThreads;         // 416
+constexpr int kTcStages = 3;                                     // mbarrier slots (stages <= 3)
+constexpr int kTcKBlock = 32;                                    // K elements per 128-byte swizzle row
+constexpr int kTcRows = 128;
+constexpr int kTcProdBar = 1;                                    // named barrier of all producers
+constexpr int kTcGroupBar = 2;                                   // + group: named barriers of the groups
+constexpr int kTcGroupThreads = kTcProdThreads / 2;              // contrib: two producer groups
+static_assert(kTcProdThreads * 4 == kTcRows * (kTcKBlock / 4), "transform producers: 4 items per thread");
+constexpr int kTcNumBars = 2 * kTcStages + 5;
+constexpr int kTcMaxRegion = 4096;                               // staged control points per brick
+constexpr size_t kTcSmemMax = 227 * 1024;
+
+struct TcDev {
+    int ct;                  // cells per tile (rows per component)
+    // transform
+    int bx, by, bz;          // brick of cells per tile
+    int tiles[3];
+    int rx, ry, rz, rv;      // staged control-point region of a brick (rv padded to 4)
+    int kp;                  // taps padded to 32 (K)
+    int np;                  // phases padded to 16 (half of N)
+    int ns_tr;               // shared-memory stages (one 32-tap K block each)
+    int tr_stride, tr_cols;  // TMEM columns per accumulator, allocated columns
+    const float *btr;        // 2 np rows x kp, K-major 128-byte swizzled
+    // contrib
+    int kpc;                 // phases padded to 32 (K)
+    int npc;                 // taps padded to 16 (N)
+    int ns_con;              // shared-memory stages (one 32-phase K block each)
+    int con_stride, con_cols;
+    const float *bcon;       // npc rows x kpc, K-major 128-byte swizzled: hi, then lo
+    unsigned *err;           // sticky failure word of the bounded waits (read and reset by the host)
+};
+
+// mbarriers of one CTA: full[s] producers -> MMA (kTcProdThreads arrivals), empty[s] MMA ->
+// producers (commit), acc_full[b] MMA -> epilogue (commit), acc_empty[b] epilogue -> MMA
+// (kTcEpiWarps * 32 arrivals), drain (final commit of the MMA thread)
+struct TcBars {
+    uint64_t *full, *empty, *acc_full, *acc_empty, *drain;
+    __device__ explicit TcBars(uint64_t *b)
+        : full(b), empty(b + kTcStages), acc_full(b + 2 * kTcStages), acc_empty(b + 2 * kTcStages + 2),
+          drain(b + 2 * kTcStages + 4)
+    {
+    }
+    __device__ void init(int full_count) const
+    {
+        for (int s = 0; s < kTcStages; ++s) {     // stages beyond the kernel's count stay unused
+            tc::mbar_init(&full[s], full_count);
+            tc::mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            tc::mbar_init(&acc_full[b], 1);
+            tc::mbar_init(&acc_empty[b], kTcEpiWarps * 32);
+        }
+        tc::mbar_init(drain, 1);
+        tc::fence_mbarrier_init();
+    }
+};
+
+__device__ __forceinline__ void tc_fail(volatile int *abort, unsigned *err)
+{
+    *abort = 1;
+    atomicOr(err, 1u);
+}
+
+__device__ __forceinline__ void split4(const float *v, float4 &h, float4 &l)
+{
+    float hx, lx, hy, ly, hz, lz, hw, lw;
+    tc::split_tf32(v[0], hx, lx);
+    tc::split_tf32(v[1], hy, ly);
+    tc::split_tf32(v[2], hz, lz);
+    tc::split_tf32(v[3], hw, lw);
+    h = make_float4(hx, hy, hz, hw);
+    l = make_float4(lx, ly, lz, lw);
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(tc::smem_addr(dst)), "l"(src),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Teardown shared by both kernels: the MMA thread waits (bounded) until its MMAs have retired,
+// then the MMA warp frees the TMEM after every role has left its loop.
+__device__ __forceinline__ void tc_teardown(const TcBars &B, uint32_t tmem, uint32_t cols)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == kTcMmaWarp && lane == 0) {
+        tc::commit(B.drain);
+        tc::mbar_wait(B.drain, 0);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == kTcMmaWarp) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, cols);
+    }
+}
+
+// Shared-memory carve-up, in bytes from a 1024-byte-aligned base (the swizzle atoms need it):
+// A stages first (each [hi | lo], 128 rows x 32 K elements = 16 KB per half), then the table.
+constexpr int kTcStageBytes = 2 * kTcRows * kTcKBlock * 4;
+
+struct TcTransformLayout {
+    int a, b, raw, rg, tapoff, regxyz, bars, total_bytes;
+    __host__ __device__ explicit TcTransformLayout(const TcDev &C)
+    {
+        a = 0;
+        b = a + C.ns_tr * kTcStageBytes;
+        raw = b + C.kp * 2 * C.np * 4;                 // [rv] float4: staged w, alpha
+        rg = raw + 16 * C.rv;                          // [2][3][rv] floats: w * alpha planes, two tiles
+        tapoff = rg + 4 * 2 * 3 * C.rv;                // [kp] ints
+        regxyz = tapoff + 4 * C.kp;                    // [rv] ints: x | y << 10 | z << 20 of a region element
+        bars = regxyz + 4 * C.rv;                      // 16-byte aligned
+        total_bytes = bars + 8 * kTcNumBars + 8 + 1024;   // + alignment slack of the base
+    }
+};
+
+struct TcContribLayout {
+    int a, bhi, blo, bars, total_bytes;
+    __host__ __device__ explicit TcContribLayout(const TcDev &C)
+    {
+        a = 0;
+        bhi = a + C.ns_con * kTcStageBytes;
+        blo = bhi + C.kpc * C.npc * 4;
+        bars = blo + C.kpc * C.npc * 4;
+        total_bytes = bars + 8 * kTcNumBars + 8 + 1024;
+    }
+};
+
+__device__ __forceinline__ unsigned char *tc_aligned_smem(float4 *dyn)
+{
+    const uint32_t a = tc::smem_addr(dyn);
+    return reinterpret_cast<unsigned char *>(dyn) + (((a + 1023u) & ~1023u) - a);
+}
+
+// ------------------------------------------------------------------------------------------------
+// u(q, p) = sum_t T[p][t] (w alpha)[q + t] on the tensor cores; u planar [comp][cell][phase]
+__global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalParams P, TableDev T, TcDev C)
+{
+    extern __shared__ float4 tc_smem4[];
+    unsigned char *sm = tc_aligned_smem(tc_smem4);
+    const TcTransformLayout L(C);
+    unsigned char *As = sm + L.a;
+    float *Bs = reinterpret_cast<float *>(sm + L.b);
+    float4 *raw = reinterpret_cast<float4 *>(sm + L.raw);
+    float *Rg = reinterpret_cast<float *>(sm + L.rg);
+    int *tapoff = reinterpret_cast<int *>(sm + L.tapoff);
+    int *regxyz = reinterpret_cast<int *>(sm + L.regxyz);
+    uint64_t *barmem = reinterpret_cast<uint64_t *>(sm + L.bars);
+    const TcBars B(barmem);
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(barmem + kTcNumBars);
+    volatile int *abort = reinterpret_cast<volatile int *>(tmem_holder + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Kp = C.kp, Np = C.np, N2 = 2 * C.np, RV = C.rv, NS = C.ns_tr;
+    const int D = T.D;
+    const int ntiles = C.tiles[0] * C.tiles[1] * C.tiles[2];
+    const int nchunk = Kp / kTcKBlock;
+    const int brick = C.bx * C.by * C.bz;
+    const int rtotal = C.rx * C.ry * C.rz;
+
+    if (tid == 0) {
+        B.init(kTcProdThreads);
+        *abort = 0;
+    }
+    if (warp == kTcMmaWarp) tc::tmem_alloc(tmem_holder, (uint32_t)C.tr_cols);
+    for (int i = tid; i < Kp * N2 / 4; i += kTcThreads)
+        reinterpret_cast<float4 *>(Bs)[i] = __ldg(reinterpret_cast<const float4 *>(C.btr) + i);
+    const int nt0 = T.nt[0], nt01 = T.nt[0] * T.nt[1];
+    for (int t = tid; t < Kp; t += kTcThreads)
+        tapoff[t] = t < T.ntap ? (t % nt0) + C.rx * ((t / nt0) % T.nt[1] + C.ry * (t / nt01)) : -1;
+    for (int i = tid; i < rtotal; i += kTcThreads)
+        regxyz[i] = (i % C.rx) | (((i / C.rx) % C.ry) << 10) | ((i / (C.rx * C.ry)) << 20);
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tmem_holder;
+
+    if (warp >= kTcEpiWarps + 1) {
+        // ---------------- producers: staged region -> im2col hi/lo stages ----------------
+        // Thread pt owns row r = pt % 128 of every stage and its K groups pt / 128 + 2u, u < 4.
+        const int pt = tid - kTcProdBase;
+        const int r = pt & (kTcRows - 1), jg0 = pt >> 7;
+        const int comp = r / C.ct, c = r - comp * C.ct;
+        const bool row_exists = comp < D && c < brick;
+        const int cx = c % C.bx, cy = (c / C.bx) % C.by, cz = c / (C.bx * C.by);
+        const int rowoff = comp * RV + cx + C.rx * (cy + C.ry * cz);
+        auto tile_origin = [&](int tile, int *q0) {
+            const int t0 = tile % C.tiles[0], t12 = tile / C.tiles[0];
+            q0[0] = t0 * C.bx;
+            q0[1] = (t12 % C.tiles[1]) * C.by;
+            q0[2] = (t12 / C.tiles[1]) * C.bz;
+        };
+        // cp.async of the raw control points (w alpha computed on conversion) of a tile's region
+        auto fetch_region = [&](int tile) {
+            int q0[3];
+            tile_origin(tile, q0);
+            const int j0[3] = {T.qmin[0] + q0[0] + T.tlo[0], T.qmin[1] + q0[1] + T.tlo[1],
+                               T.qmin[2] + q0[2] + T.tlo[2]};
+            for (int i = pt; i < rtotal; i += kTcProdThreads) {
+                const int xyz = regxyz[i];
+                const int jx = j0[0] + (xyz & 1023), jy = j0[1] + ((xyz >> 10) & 1023), jz = j0[2] + (xyz >> 20);
+                const bool in = (unsigned)jx < (unsigned)P.cp.n[0] && (unsigned)jy < (unsigned)P.cp.n[1] &&
+                                (unsigned)jz < (unsigned)P.cp.n[2];
+                const float4 *src = in ? P.cpd + jx + P.cp.st[1] * jy + P.cp.st[2] * jz : P.cpd;
+                cp_async16(raw + i, src, in);
+            }
+            cp_async_commit();
+        };
+        // raw -> w alpha planes of buffer `buf`
+        auto convert_region = [&](int buf) {
+            float *R = Rg + buf * 3 * RV;
+            for (int i = pt; i < rtotal; i += kTcProdThreads) {
+                const float4 cv = raw[i];
+                R[i] = cv.w * cv.x;
+                R[RV + i] = cv.w * cv.y;
+                R[2 * RV + i] = cv.w * cv.z;
+            }
+        };
+        if ((int)blockIdx.x < ntiles) {
+            fetch_region(blockIdx.x);
+            cp_async_wait_all();
+            tc::bar_sync(kTcProdBar, kTcProdThreads);
+            convert_region(0);
+        }
+        tc::bar_sync(kTcProdBar, kTcProdThreads);
+        unsigned g = 0;
+        bool failed = false;
+        for (int it = 0; !failed; ++it) {
+            const int tile = blockIdx.x + it * gridDim.x;
+            if (tile >= ntiles) break;
+            const int buf = it & 1;
+            const int next = tile + gridDim.x;
+            if (next < ntiles) fetch_region(next);          // raw is free: converted before the last barrier
+            int q0[3];
+            tile_origin(tile, q0);
+            const bool valid = row_exists && q0[0] + cx < T.nq[0] && q0[1] + cy < T.nq[1] && q0[2] + cz < T.nq[2];
+            const float *Rrow = Rg + buf * 3 * RV + rowoff;
+            for (int kc = 0; kc < nchunk; ++kc, ++g) {
+                const int s = (int)(g % NS);
+                bool ok = true;
+                if (g >= (unsigned)NS) ok = tc::mbar_wait(&B.empty[s], ((g / NS) + 1) & 1, abort);
+                if (tc::bar_or(kTcProdBar, kTcProdThreads, !ok)) {
+                    if (pt == 0) tc_fail(abort, C.err);
+                    failed = true;
+                    break;
+                }
+                unsigned char *Ahi = As + s * kTcStageBytes, *Alo = Ahi + kTcStageBytes / 2;
+                const int4 *tap4 = reinterpret_cast<const int4 *>(tapoff + kc * kTcKBlock);
+                float v[4][4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int4 o = tap4[jg0 + 2 * u];
+                    v[u][0] = (valid && o.x >= 0) ? Rrow[o.x] : 0.f;
+                    v[u][1] = (valid && o.y >= 0) ? Rrow[o.y] : 0.f;
+                    v[u][2] = (valid && o.z >= 0) ? Rrow[o.z] : 0.f;
+                    v[u][3] = (valid && o.w >= 0) ? Rrow[o.w] : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    float4 h, l;
+                    split4(v[u], h, l);
+                    const uint32_t off = tc::sw128_offset(r, 4 * (jg0 + 2 * u), kTcRows);
+                    *reinterpret_cast<float4 *>(Ahi + off) = h;
+                    *reinterpret_cast<float4 *>(Alo + off) = l;
+                }
+                tc::fence_proxy_async();
+                tc::mbar_arrive(&B.full[s]);
+            }
+            if (failed) break;
+            if (next < ntiles) {
+                cp_async_wait_all();
+                tc::bar_sync(kTcProdBar, kTcProdThreads);   // every thread's copies have landed
+                convert_region(buf ^ 1);
+            }
+            tc::bar_sync(kTcProdBar, kTcProdThreads);
+        }
+        cp_async_wait_all();
+    } else if (warp == kTcMmaWarp) {
+        // ---------------- MMA issue (one thread) ----------------
+        if (lane == 0) {
+            const uint32_t idesc_cat = tc::idesc_tf32(kTcRows, N2), idesc_hi = tc::idesc_tf32(kTcRows, Np);
+            const uint32_t a_base = tc::smem_addr(As), b_base = tc::smem_addr(Bs);
+            unsigned g = 0;
+            for (int it = 0;; ++it) {
+                const int tile = blockIdx.x + it * gridDim.x;
+                if (tile >= ntiles) break;
+                const int b = it & 1;
+                if (it >= 2 && !tc::mbar_wait(&B.acc_empty[b], ((it >> 1) + 1) & 1, abort)) {
+                    tc_fail(abort, C.err);
+                    break;
+                }
+                tc::fence_after_sync();
+                bool failed = false;
+                for (int kc = 0; kc < nchunk; ++kc, ++g) {
+                    const int s = (int)(g % NS);
+                    if (!tc::mbar_wait(&B.full[s], (g / NS) & 1, abort)) {
+                        tc_fail(abort, C.err);
+                        failed = true;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const uint32_t dacc = tmem + (uint32_t)(b * C.tr_stride);
+                    const uint32_t ahi = a_base + (uint32_t)(s * kTcStageBytes);
+                    const uint32_t alo = ahi + (uint32_t)(kTcStageBytes / 2);
+                    const uint32_t bk = b_base + (uint32_t)kc * (uint32_t)N2 * 128u;   // K block kc of the table
+#pragma unroll
+                    for (int ks = 0; ks < kTcKBlock / 8; ++ks) {
+                        const uint64_t dah = tc::smem_desc_sw128(ahi + 32u * ks);
+                        const uint64_t dal = tc::smem_desc_sw128(alo + 32u * ks);
+                        const uint64_t db = tc::smem_desc_sw128(bk + 32u * ks);
+                        tc::mma_tf32(dacc, dah, db, idesc_cat, (kc | ks) != 0);
+                        tc::mma_tf32(dacc, dal, db, idesc_hi, 1);
+                    }
+                    tc::commit(&B.empty[s]);
+                }
+                if (failed) break;
+                tc::commit(&B.acc_full[b]);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------- epilogue: TMEM -> u (lane quarter = warp) ----------------
+        const long long plane = T.ncell * T.nph;
+        const int r = warp * 32 + lane;
+        const int comp = r / C.ct, c = r - comp * C.ct;
+        const int cx = c % C.bx, cy = (c / C.bx) % C.by, cz = c / (C.bx * C.by);
+        const bool row_ok = comp < D && c < brick;
+        for (int it = 0;; ++it) {
+            const int tile = blockIdx.x + it * gridDim.x;
+            if (tile >= ntiles) break;
+            const int b = it & 1;
+            // warp-uniform decision: tcgen05.ld below is a warp-wide instruction
+            if (!__all_sync(0xffffffffu, tc::mbar_wait(&B.acc_full[b], (it >> 1) & 1, abort))) {
+                if (lane == 0) tc_fail(abort, C.err);
+                break;
+            }
+            tc::fence_after_sync();
+            const int qx = (tile % C.tiles[0]) * C.bx + cx, qy = ((tile / C.tiles[0]) % C.tiles[1]) * C.by + cy,
+                      qz = (tile / (C.tiles[0] * C.tiles[1])) * C.bz + cz;
+            const bool valid = row_ok && qx < T.nq[0] && qy < T.nq[1] && qz < T.nq[2];
+            const long long cell = (long long)qx + (long long)T.nq[0] * (qy + (long long)T.nq[1] * qz);
+            const uint32_t tb = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * C.tr_stride);
+            for (int j = 0; j < (Np >> 4); ++j) {
+                float vh[16], vl[16];
+                tc::tmem_ld16(tb + (uint32_t)(16 * j), vh);
+                tc::tmem_ld16(tb + (uint32_t)(Np + 16 * j), vl);
+                if (valid) {
+                    float *dst = T.ucp + (long long)comp * plane + cell * T.nph + 16 * j;
+                    if (16 * j + 16 <= T.nph && (T.nph & 3) == 0) {
+#pragma unroll
+                        for (int v = 0; v < 4; ++v)
+                            reinterpret_cast<float4 *>(dst)[v] =
+                                make_float4(vh[4 * v] + vl[4 * v], vh[4 * v + 1] + vl[4 * v + 1],
+                                            vh[4 * v + 2] + vl[4 * v + 2], vh[4 * v + 3] + vl[4 * v + 3]);
+                    } else {
+                        for (int v = 0; v < 16; ++v)
+                            if (16 * j + v < T.nph) dst[v] = vh[v] + vl[v];
+                    }
+                }
+            }
+            tc::fence_before_sync();
+            tc::mbar_arrive(&B.acc_empty[b]);
+        }
+    }
+    tc_teardown(B, tmem, (uint32_t)C.tr_cols);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Contrib[comp][t][cell] = sum_p T[p][t] g(cell, p) on the tensor cores
+__global__ void __launch_bounds__(kTcThreads, 1) table_contrib_tc_kernel(TableDev T, TcDev C,
+                                                                        const double *__restrict__ stats)
+{
+    extern __shared__ float4 tc_smem4[];
+    unsigned char *sm = tc_aligned_smem(tc_smem4);
+    const TcContribLayout L(C);
+    unsigned char *As = sm + L.a;
+    float *Bhi = reinterpret_cast<float *>(sm + L.bhi), *Blo = reinterpret_cast<float *>(sm + L.blo);
+    uint64_t *barmem = reinterpret_cast<uint64_t *>(sm + L.bars);
+    const TcBars B(barmem);
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(barmem + kTcNumBars);
+    volatile int *abort = reinterpret_cast<volatile int *>(tmem_holder + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Kp = C.kpc, Np = C.npc, ct = C.ct, NS = C.ns_con;
+    const int D = T.D, nph = T.nph;
+    const long long ntiles = (T.ncell + ct - 1) / ct;
+    const int nchunk = Kp / kTcKBlock;
+
+    if (tid == 0) {
+        B.init(kTcGroupThreads);
+        *abort = 0;
+    }
+    if (warp == kTcMmaWarp) tc::tmem_alloc(tmem_holder, (uint32_t)C.con_cols);
+    for (int i = tid; i < 2 * Kp * Np / 4; i += kTcThreads)
+        reinterpret_cast<float4 *>(Bhi)[i] = __ldg(reinterpret_cast<const float4 *>(C.bcon) + i);
+    // rows past D * ct never receive data: zero their 128-byte rows once in every stage half
+    const int pad_rows = kTcRows - D * ct;
+    for (int i = tid; i < NS * 2 * pad_rows * 8; i += kTcThreads) {
+        const int half = i / (pad_rows * 8), r = D * ct + (i / 8) % pad_rows, c16 = i & 7;
+        *reinterpret_cast<float4 *>(As + half * (kTcStageBytes / 2) + (r >> 3) * 1024 + (r & 7) * 128 + c16 * 16) =
+            make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tmem_holder;
+
+    if (warp >= kTcEpiWarps + 1) {
+        // ---------------- producers: g = (a f + b m + c) grad M, hi/lo stages ----------------
+        // Two groups of 4 warps take alternate K chunks, so that one group's global loads are in
+        // flight while the other converts and stores.  Item = (cell c, 4 phases), lanes over cells.
+        const int pt = tid - kTcProdBase;
+        const int grp = pt / kTcGroupThreads, gt = pt - grp * kTcGroupThreads;
+        const float cf = (float)stats[S_COEF_F], cm = (float)stats[S_COEF_M], cc = (float)stats[S_COEF_C];
+        const int nitems = ct * (kTcKBlock / 4);
+        constexpr int kMaxItems = 3;                        // ceil(42 * 8 / 128); 2-D: 64 * 8 / 128 = 4
+        const bool vec = (nph & 3) == 0;
+        bool failed = false;
+        for (unsigned g = grp;; g += 2) {
+            const long long tile = blockIdx.x + (long long)(g / nchunk) * gridDim.x;
+            if (tile >= ntiles) break;
+            const int kc = (int)(g % nchunk);
+            const long long cell0 = tile * ct;
+            const int s = (int)(g % NS);
+            bool ok = true;
+            if (g >= (unsigned)NS) ok = tc::mbar_wait(&B.empty[s], ((g / NS) + 1) & 1, abort);
+            if (tc::bar_or(kTcGroupBar + grp, kTcGroupThreads, !ok)) {
+                if (gt == 0) tc_fail(abort, C.err);
+                failed = true;
+                break;
+            }
+            unsigned char *Ahi = As + s * kTcStageBytes, *Alo = Ahi + kTcStageBytes / 2;
+            const int k0 = kc * kTcKBlock;
+            for (int base = 0; base < nitems; base += kMaxItems * kTcGroupThreads) {
+                float4 rr[kMaxItems][4], ff[kMaxItems];
+#pragma unroll
+                for (int u = 0; u < kMaxItems; ++u) {           // all loads first
+                    const int i = base + gt + u * kTcGroupThreads;
+                    const int c = i % ct, jg = i / ct;
+                    const long long cell = cell0 + c;
+                    const int p0 = k0 + 4 * jg;
+                    const bool in = i < nitems && cell < T.ncell;
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        rr[u][e] = (in && p0 + e < nph) ? T.rec[cell * nph + p0 + e] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (in && vec && p0 < nph) {
+                        ff[u] = *reinterpret_cast<const float4 *>(T.fixcp + cell * nph + p0);
+                    } else {
+                        float f4[4];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) f4[e] = (in && p0 + e < nph) ? T.fixcp[cell * nph + p0 + e] : 0.f;
+                        ff[u] = make_float4(f4[0], f4[1], f4[2], f4[3]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kMaxItems; ++u) {
+                    const int i = base + gt + u * kTcGroupThreads;
+                    if (i >= nitems) break;
+                    const int c = i % ct, jg = i / ct;
+                    const float fv[4] = {ff[u].x, ff[u].y, ff[u].z, ff[u].w};
+                    float gv[3][4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const float coef = fmaf(cf, fv[e], fmaf(cm, rr[u][e].w, cc));
+                        gv[0][e] = coef * rr[u][e].x;
+                        gv[1][e] = coef * rr[u][e].y;
+                        gv[2][e] = coef * rr[u][e].z;
+                    }
+#pragma unroll
+                    for (int comp = 0; comp < 3; ++comp) {
+                        if (comp < D) {
+                            float4 h, l;
+                            split4(gv[comp], h, l);
+                            const uint32_t off = tc::sw128_offset(comp * ct + c, 4 * jg, kTcRows);
+                            *reinterpret_cast<float4 *>(Ahi + off) = h;
+                            *reinterpret_cast<float4 *>(Alo + off) = l;
+                        }
+                    }
+                }
+            }
+            tc::fence_proxy_async();
+            tc::mbar_arrive(&B.full[s]);
+        }
+    } else if (warp == kTcMmaWarp) {
+        // ---------------- MMA issue (one thread) ----------------
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_tf32(kTcRows, Np);
+            const uint32_t a_base = tc::smem_addr(As), bh_base = tc::smem_addr(Bhi), bl_base = tc::smem_addr(Blo);
+            unsigned g = 0;
+            for (int it = 0;; ++it) {
+                const long long tile = blockIdx.x + (long long)it * gridDim.x;
+                if (tile >= ntiles) break;
+                const int b = it & 1;
+                if (it >= 2 && !tc::mbar_wait(&B.acc_empty[b], ((it >> 1) + 1) & 1, abort)) {
+                    tc_fail(abort, C.err);
+                    break;
+                }
+                tc::fence_after_sync();
+                bool failed = false;
+                for (int kc = 0; kc < nchunk; ++kc, ++g) {
+                    const int s = (int)(g % NS);
+                    if (!tc::mbar_wait(&B.full[s], (g / NS) & 1, abort)) {
+                        tc_fail(abort, C.err);
+                        failed = true;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const uint32_t dacc = tmem + (uint32_t)(b * C.con_stride);
+                    const uint32_t ahi = a_base + (uint32_t)(s * kTcStageBytes);
+                    const uint32_t alo = ahi + (uint32_t)(kTcStageBytes / 2);
+                    const uint32_t bo = (uint32_t)kc * (uint32_t)Np * 128u;             // K block kc of the table
+#pragma unroll
+                    for (int ks = 0; ks < kTcKBlock / 8; ++ks) {
+                        const uint64_t dah = tc::smem_desc_sw128(ahi + 32u * ks);
+                        const uint64_t dal = tc::smem_desc_sw128(alo + 32u * ks);
+                        const uint64_t dbh = tc::smem_desc_sw128(bh_base + bo + 32u * ks);
+                        const uint64_t dbl = tc::smem_desc_sw128(bl_base + bo + 32u * ks);
+                        tc::mma_tf32(dacc, dah, dbh, idesc, (kc | ks) != 0);
+                        tc::mma_tf32(dacc, dah, dbl, idesc, 1);
+                        tc::mma_tf32(dacc, dal, dbh, idesc, 1);
+                    }
+                    tc::commit(&B.empty[s]);
+                }
+                if (failed) break;
+                tc::commit(&B.acc_full[b]);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------- epilogue: TMEM -> Contrib (lane quarter = warp) ----------------
+        const int r = warp * 32 + lane;
+        const int comp = r / ct, c = r - comp * ct;
+        for (int it = 0;; ++it) {
+            const long long tile = blockIdx.x + (long long)it * gridDim.x;
+            if (tile >= ntiles) break;
+            const int b = it & 1;
+            // warp-uniform decision: tcgen05.ld below is a warp-wide instruction
+            if (!__all_sync(0xffffffffu, tc::mbar_wait(&B.acc_full[b], (it >> 1) & 1, abort))) {
+                if (lane == 0) tc_fail(abort, C.err);
+                break;
+            }
+            tc::fence_after_sync();
+            const long long cell = tile * ct + c;
+            const bool valid = comp < D && cell < T.ncell;
+            const uint32_t tb = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * C.con_stride);
+            for (int j = 0; j < (Np >> 4); ++j) {
+                float v[16];
+                tc::tmem_ld16(tb + (uint32_t)(16 * j), v);
+                if (valid) {
+                    float *dst = T.contrib + ((long long)comp * T.ntap + 16 * j) * T.ncell + cell;
+#pragma unroll
+                    for (int e = 0; e < 16; ++e)
+                        if (16 * j + e < T.ntap) dst[(long long)e * T.ncell] = v[e];
+                }
+            }
+            tc::fence_before_sync();
+            tc::mbar_arrive(&B.acc_empty[b]);
+        }
+    }
+    tc_teardown(B, tmem, (uint32_t)C.con_cols);
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side
+
+// tf32 part of x (round to nearest, ties away from zero, as cvt.rna.tf32.f32)
+inline float tf32_hi_host(float x)
+{
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return x;
+    u = (u + 0x1000u) & 0xffffe000u;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+inline uint32_t pow2_at_least(uint32_t v)
+{
+    uint32_t p = 32;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+struct TcPlan {
+    bool enabled = false;
+    TcDev dev{};
+    float *d_btr = nullptr, *d_bcon = nullptr;
+    unsigned *d_err = nullptr;
+    int transform_blocks = 0, contrib_blocks = 0;
+    size_t transform_smem = 0, contrib_smem = 0;
+};
+
+// Decides whether the tensor-core kernels apply to a table plan and builds their operand
+// tables.  Returns 0 (tc.enabled says whether they apply) or 2 on a CUDA error.
+inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
+{
+    tc.enabled = false;
+    const TableDev &T = pl.dev;
+    const std::vector<float> &tgemm = pl.h_tgemm;
+    TcDev &C = tc.dev;
+    C = TcDev{};
+    if (T.D != 2 && T.D != 3) return 0;
+    C.ct = kTcRows / T.D;
+    C.np = (T.nph + 15) / 16 * 16;
+    C.kp = (T.ntap + kTcKBlock - 1) / kTcKBlock * kTcKBlock;
+    C.npc = (T.ntap + 15) / 16 * 16;
+    C.kpc = (T.nph + kTcKBlock - 1) / kTcKBlock * kTcKBlock;
+    if (2 * C.np > 256 || C.npc > 256) return 0;
+    // brick of at most ct cells with the fewest tiles (then the smallest staged region)
+    long long best_tiles = -1, best_rv = 0;
+    for (int bz = 1; bz <= std::min(C.ct, T.nq[2]); ++bz)
+        for (int by = 1; by <= std::min(C.ct / bz, T.nq[1]); ++by)
+            for (int bx = 1; bx <= std::min(C.ct / (bz * by), T.nq[0]); ++bx) {
+                const long long tiles = (long long)((T.nq[0] + bx - 1) / bx) * ((T.nq[1] + by - 1) / by) *
+                                        ((T.nq[2] + bz - 1) / bz);
+                const long long rv = (long long)(bx + T.nt[0] - 1) * (by + T.nt[1] - 1) * (bz + T.nt[2] - 1);
+                if (best_tiles < 0 || tiles < best_tiles || (tiles == best_tiles && rv < best_rv)) {
+                    best_tiles = tiles;
+                    best_rv = rv;
+                    C.bx = bx;
+                    C.by = by;
+                    C.bz = bz;
+                }
+            }
+    if (best_tiles <= 0 || best_tiles > (1LL << 30)) return 0;
+    C.tiles[0] = (T.nq[0] + C.bx - 1) / C.bx;
+    C.tiles[1] = (T.nq[1] + C.by - 1) / C.by;
+    C.tiles[2] = (T.nq[2] + C.bz - 1) / C.bz;
+    C.rx = C.bx + T.nt[0] - 1;
+    C.ry = C.by + T.nt[1] - 1;
+    C.rz = C.bz + T.nt[2] - 1;
+    if (C.rx * C.ry * C.rz > kTcMaxRegion || C.rx >= 1024 || C.ry >= 1024) return 0;
+    C.rv = (C.rx * C.ry * C.rz + 3) / 4 * 4;
+    C.tr_stride = (int)pow2_at_least(2 * C.np);
+    C.tr_cols = 2 * C.tr_stride;
+    C.con_stride = (int)pow2_at_least(C.npc);
+    C.con_cols = 2 * C.con_stride;
+    if (C.tr_cols > 512 || C.con_cols > 512) return 0;
+    // as many stages (up to 3, at least 2) as the shared memory holds
+    for (C.ns_tr = 3; C.ns_tr > 2 && (size_t)TcTransformLayout(C).total_bytes > kTcSmemMax; --C.ns_tr) {
+    }
+    for (C.ns_con = 3; C.ns_con > 2 && (size_t)TcContribLayout(C).total_bytes > kTcSmemMax; --C.ns_con) {
+    }
+    tc.transform_smem = (size_t)TcTransformLayout(C).total_bytes;
+    tc.contrib_smem = (size_t)TcContribLayout(C).total_bytes;
+    // both kernels must hold one CTA per SM alone (their TMEM allocations assume it)
+    if (tc.transform_smem > kTcSmemMax || tc.contrib_smem > kTcSmemMax) return 0;
+    if (tc.transform_smem < kTcSmemMax / 2 + 1024) tc.transform_smem = kTcSmemMax / 2 + 1024;
+    if (tc.contrib_smem < kTcSmemMax / 2 + 1024) tc.contrib_smem = kTcSmemMax / 2 + 1024;
+
+    // B operands, K-major 128-byte swizzled (float index of element (row, k))
+    auto kmaj = [](int row, int k, int rows) { return (size_t)tc::sw128_offset(row, k & ~3, rows) / 4 + (k & 3); };
+    std::vector<float> btr((size_t)C.kp * 2 * C.np, 0.f);
+    std::vector<float> bcon((size_t)2 * C.kpc * C.npc, 0.f);
+    const size_t lo_off = (size_t)C.kpc * C.npc;
+    for (int p = 0; p < T.nph; ++p)
+        for (int t = 0; t < T.ntap; ++t) {
+            const float v = tgemm[(size_t)p * T.ntap_pad + t];
+            const float hi = tf32_hi_host(v), lo = v - hi;
+            btr[kmaj(p, t, 2 * C.np)] = hi;
+            btr[kmaj(C.np + p, t, 2 * C.np)] = lo;
+            bcon[kmaj(t, p, C.npc)] = hi;
+            bcon[lo_off + kmaj(t, p, C.npc)] = lo;
+        }
+    if (cudaMalloc((void **)&tc.d_btr, btr.size() * sizeof(float)) != cudaSuccess) return 2;
+    if (cudaMalloc((void **)&tc.d_bcon, bcon.size() * sizeof(float)) != cudaSuccess) return 2;
+    if (cudaMalloc((void **)&tc.d_err, sizeof(unsigned)) != cudaSuccess) return 2;
+    if (cudaMemcpyAsync(tc.d_btr, btr.data(), btr.size() * sizeof(float), cudaMemcpyHostToDevice, stream) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(tc.d_bcon, bcon.data(), bcon.size() * sizeof(float), cudaMemcpyHostToDevice, stream) !=
+            cudaSuccess ||
+        cudaMemsetAsync(tc.d_err, 0, sizeof(unsigned), stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+        return 2;
+    C.btr = tc.d_btr;
+    C.bcon = tc.d_bcon;
+    C.err = tc.d_err;
+    pl.dev.tc_err = tc.d_err;
+
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 2;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 2;
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (cudaFuncSetAttribute(table_transform_tc_kernel, a, (int)tc.transform_smem) != cudaSuccess) return 2;
+    if (cudaFuncSetAttribute(table_contrib_tc_kernel, a, (int)tc.contrib_smem) != cudaSuccess) return 2;
+    const long long ttiles = (long long)C.tiles[0] * C.tiles[1] * C.tiles[2];
+    const long long ctiles = (T.ncell + C.ct - 1) / C.ct;
+    tc.transform_blocks = (int)std::max<long long>(1, std::min<long long>(ttiles, sms));
+    tc.contrib_blocks = (int)std::max<long long>(1, std::min<long long>(ctiles, sms));
+    tc.enabled = true;
+    return 0;
+}
+
+inline int table_transform_tc(const TcPlan &tc, const TablePlan &pl, const EvalParams &P, cudaStream_t s)
+{
+    table_transform_tc_kernel<<<tc.transform_blocks, kTcThreads, tc.transform_smem, s>>>(P, pl.dev, tc.dev);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
+}
+
+inline int table_contrib_tc(const TcPlan &tc, const TablePlan &pl, const double *stats, cudaStream_t s)
+{
+    table_contrib_tc_kernel<<<tc.contrib_blocks, kTcThreads, tc.contrib_smem, s>>>(pl.dev, tc.dev, stats);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
+}
+
+// ------------------------------------------------------------------------------------------------
+// launch sequences of the table path (tc: tensor-core GEMMs, or NULL for the CUDA-core ones)
+
+template <int HL, int NCZ>
+inline int table_transform_launch(TablePlan &pl, const EvalParams &P, cudaStream_t s)
+{
+    table_transform_kernel<HL, NCZ><<<pl.transform_blocks, 256, table_value_smem(pl), s>>>(P, pl.dev);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
+}
+
+// value pass of the table path: transform, then warp + statistics; writes its own partials
+// (pl.d_part, pl.dev.value_blocks blocks)
+inline int table_value(TablePlan &pl, const TcPlan *tc, const EvalParams &P, int D, int metric, double *stats,
+                       unsigned *counter, cudaStream_t s, cudaEvent_t mid = nullptr)
+{
+    int rc;
+    if (tc && tc->enabled) {
+        rc = table_transform_tc(*tc, pl, P, s);
+    } else if (D == 3) {
+        switch (pl.hl) {
+        case 1: rc = table_transform_launch<1, 4>(pl, P, s); break;
+        case 2: rc = table_transform_launch<2, 4>(pl, P, s); break;
+        case 4: rc = table_transform_launch<4, 4>(pl, P, s); break;
+        default: rc = table_transform_launch<8, 4>(pl, P, s); break;
+        }
+    } else {
+        rc = table_transform_launch<1, 1>(pl, P, s);
+    }
+    if (rc) return rc;
+    if (mid && cudaEventRecord(mid, s) != cudaSuccess) return 2;
+    if (D == 3)
+        table_warp_kernel<3><<<pl.dev.value_blocks, 256, 0, s>>>(P, pl.dev, metric, stats, counter);
+    else
+        table_warp_kernel<2><<<pl.dev.value_blocks, 256, 0, s>>>(P, pl.dev, metric, stats, counter);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
+}
+
+inline int table_derivative(TablePlan &pl, const TcPlan *tc, const EvalParams &P, const DerivParams &Q, int D,
+                            int gather_blocks, cudaStream_t s, cudaEvent_t mid = nullptr)
+{
+    if (tc && tc->enabled) {
+        if (table_contrib_tc(*tc, pl, Q.stats, s)) return 2;
+    } else {
+        const size_t smem = table_contrib_smem(pl.dev);
+        table_contrib_kernel<<<pl.contrib_blocks, kTabContribThreads, smem, s>>>(pl.dev, Q.stats);
+        if (cudaPeekAtLastError() != cudaSuccess) return 2;
+    }
+    if (mid && cudaEventRecord(mid, s) != cudaSuccess) return 2;
+    if (D == 3)
+        table_gather_kernel<3><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+    else
+        table_gather_kernel<2><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
+}
+
+inline int table_derivative_gather_only(TablePlan &pl, const EvalParams &P, const DerivParams &Q, int D,
+                                        int gather_blocks, cudaStream_t s)
+{
+    if (D == 3)
+        table_gather_kernel<3><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+    else
+        table_gather_kernel<2><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+    return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
+}
+
+inline void table_tc_free(TcPlan &tc)
+{
+    if (tc.d_btr) cudaFree(tc.d_btr);
+    if (tc.d_bcon) cudaFree(tc.d_bcon);
+    if (tc.d_err) cudaFree(tc.d_err);
+    tc = TcPlan{};
+}
+
+}  // namespace skm

@@ -117,10 +117,13 @@ class GpuKernelEvaluator:
         except Exception:
             pass
 
-    GENERIC, TABLE = 1, 2
+    GENERIC, TABLE, TABLE_TC = 1, 2, 3
+    # requests: -1 query, 0 automatic (table path, tensor-core GEMMs where they fit),
+    # 1 generic kernels, 2 table path with CUDA-core GEMMs
+    AUTO, REQ_GENERIC, REQ_TABLE_CUDA_CORES = 0, 1, 2
 
     def path(self, request=-1):
-        """Select (0 auto, 1 generic) and/or query the kernel path: returns 1 generic, 2 table."""
+        """Select and/or query the kernel path: returns 1 generic, 2 table, 3 table on tensor cores."""
         a = C.c_int32()
         check(lib().skm_evaluator_path(self.h, int(request), C.byref(a)))
         return a.value

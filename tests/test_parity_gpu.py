@@ -171,15 +171,24 @@ def _table_problem(D, h, shape, s4, s0, seed, **kw):
                         spacing=(1.0,) * D, origin=tuple([0.5, -1.0, 2.0][:D]), **kw)
 
 
+# GEMM engine of the table path: (path request, expected active path)
+ENGINES = {
+    "tensor": (GpuKernelEvaluator.AUTO, GpuKernelEvaluator.TABLE_TC),
+    "cuda": (GpuKernelEvaluator.REQ_TABLE_CUDA_CORES, GpuKernelEvaluator.TABLE),
+}
+
+
+@pytest.mark.parametrize("engine", sorted(ENGINES))
 @pytest.mark.parametrize("case", TABLE_CASES)
 @pytest.mark.parametrize("metric", [abi.MSE, abi.NCC])
 @pytest.mark.parametrize("with_df", [False, True])
-def test_table_path_matches_oracle_and_generic(case, metric, with_df):
+def test_table_path_matches_oracle_and_generic(case, metric, with_df, engine):
     D, h, shape, s4, s0 = case
     pb, cp, cpw = _table_problem(D, h, shape, s4, s0, seed=91)
     df = _df_for(pb, 9) if with_df else None
     ev = GpuKernelEvaluator(pb)
-    assert ev.path() == GpuKernelEvaluator.TABLE
+    request, expected = ENGINES[engine]
+    assert ev.path(request) == expected
     ev.SetRegularizerRD(0.05)
     ev.SetRegularizerRKHS(0.02)
     r, g = ev.getValueAndDerivative(metric, cp, cpw, df)
@@ -204,7 +213,7 @@ def test_table_path_metric_level_and_optimizer(case):
     params = np.ascontiguousarray(cp.T.reshape(-1))
     params[::5] = 0.0
     ev = GpuKernelEvaluator(pb)
-    assert ev.path() == GpuKernelEvaluator.TABLE
+    assert ev.path() == GpuKernelEvaluator.TABLE_TC
     orc = O.Oracle(pb)
     m = MetricDesc.make("ncc", l1=1e-3, l21=1e-3, l2=1e-3, rd=1e-2, pg=1e-3)
     v, g = ev.metric(m, params, cpw)

@@ -47,13 +47,15 @@ def test_matches_reference_evaluator(D, kind, metric, sub):
 
 
 @pytest.mark.parametrize("D", [2, 3])
-def test_table_path_matches_reference_evaluator(D):
+@pytest.mark.parametrize("request_, expected", [(GpuKernelEvaluator.AUTO, GpuKernelEvaluator.TABLE_TC),
+                                                (GpuKernelEvaluator.REQ_TABLE_CUDA_CORES, GpuKernelEvaluator.TABLE)])
+def test_table_path_matches_reference_evaluator(D, request_, expected):
     shape = (20, 22, 26) if D == 3 else (40, 44)
     pb, cp, cpw = make_problem(D, "stationary", shape=shape, seed=103, sigma_c4=9.0, sigma_c0=18.0, cp_spacing=4.0,
                                spacing=(1.0,) * D)
     ref = _ref(pb)
     ev = GpuKernelEvaluator(pb)
-    assert ev.path() == GpuKernelEvaluator.TABLE
+    assert ev.path(request_) == expected
     ev.SetRegularizerRD(0.05)
     ref.set_regularizers(rd=0.05)
     for metric in (abi.MSE, abi.NCC):

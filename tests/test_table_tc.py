@@ -1,0 +1,61 @@
+"""Tensor-core GEMMs of the phase-table path at the benchmark sizes.
+
+At these sizes every CTA of the persistent tensor-core kernels works through several tiles,
+so both TMEM accumulators, every shared-memory stage and both mbarrier parities are in use
+(the small parity cases run one tile per CTA).  The tensor-core path (3xTF32 products, FP32
+accumulation) is compared with the CUDA-core table path (FP32 FMA) on the same inputs:
+  * metric value: relative difference <= 1e-5, pixel counts exact
+  * derivative:   max |g_tc - g_cc| <= 1e-4 * max |g_cc|
+and both against the generic kernels with the same bounds.
+"""
+import numpy as np
+import pytest
+
+from helpers import max_rel, rel_err
+from skmimageregistration_b200 import workloads
+from skmimageregistration_b200.evaluator import GpuKernelEvaluator
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(pb, seed, scale):
+    rng = np.random.default_rng(seed)
+    cp = rng.normal(0.0, scale, (pb.C, pb.D))
+    cpw = rng.uniform(0.5, 1.5, pb.C)
+    return np.ascontiguousarray(cp), np.ascontiguousarray(cpw)
+
+
+@pytest.mark.parametrize("name", ["ncc128", "mse2d"])
+def test_tensor_core_table_matches_cuda_core_table_at_bench_size(name):
+    pb, m, _, _ = workloads.make(name, seed=0)
+    ev = GpuKernelEvaluator(pb)
+    if name == "ncc128":
+        ev.SetRegularizerRD(1e-3)
+    metric = m.metric
+    for seed, scale in ((1, 0.5), (2, 2.0)):
+        cp, cpw = _params(pb, seed, scale)
+        assert ev.path(GpuKernelEvaluator.AUTO) == GpuKernelEvaluator.TABLE_TC
+        r_tc, g_tc = ev.getValueAndDerivative(metric, cp, cpw)
+        assert ev.path(GpuKernelEvaluator.REQ_TABLE_CUDA_CORES) == GpuKernelEvaluator.TABLE
+        r_cc, g_cc = ev.getValueAndDerivative(metric, cp, cpw)
+        assert ev.path(GpuKernelEvaluator.REQ_GENERIC) == GpuKernelEvaluator.GENERIC
+        r_g, g_g = ev.getValueAndDerivative(metric, cp, cpw)
+        assert r_tc["num_pixels_counted"] == r_cc["num_pixels_counted"] == r_g["num_pixels_counted"]
+        assert rel_err(r_tc["measure"], r_cc["measure"]) <= 1e-5
+        assert rel_err(r_tc["measure"], r_g["measure"]) <= 1e-5
+        assert max_rel(g_tc, g_cc) <= 1e-4
+        assert max_rel(g_tc, g_g) <= 1e-4
+        assert np.all(np.isfinite(g_tc))
+
+
+def test_tensor_core_table_value_only_matches_derivative_call():
+    pb, m, _, _ = workloads.make("ncc128", seed=0)
+    ev = GpuKernelEvaluator(pb)
+    ev.SetRegularizerRD(1e-3)
+    cp, cpw = _params(pb, 4, 1.0)
+    assert ev.path() == GpuKernelEvaluator.TABLE_TC
+    r1 = ev.getValue(m.metric, cp, cpw)
+    r2, _ = ev.getValueAndDerivative(m.metric, cp, cpw)
+    assert r1["num_pixels_counted"] == r2["num_pixels_counted"]
+    assert r1["measure"] == r2["measure"]
+    assert r1["reg_value_rd"] == r2["reg_value_rd"]
