@@ -16,6 +16,20 @@ namespace skm {
 
 constexpr int kMaxDim = 3;
 
+// Division by a runtime constant d >= 1 for numerators below 2^31: q = (mulhi(n, m) + n) >> s with
+// s = ceil(log2 d) and m = floor(2^32 (2^s - d) / d) + 1 (the sum cannot overflow for n < 2^31).
+struct FastDiv {
+    uint32_t d = 1, m = 1, s = 0;
+    FastDiv() = default;
+    __host__ explicit FastDiv(uint32_t dv) : d(dv)
+    {
+        s = 0;
+        while ((1ull << s) < d) ++s;
+        m = (uint32_t)((((uint64_t)1 << 32) * (((uint64_t)1 << s) - d)) / d + 1);
+    }
+    __device__ __forceinline__ uint32_t div(uint32_t n) const { return (__umulhi(n, m) + n) >> s; }
+};
+
 // ImageBase (include/cuda/ImageBase.h:40-100): physical = o + s*idx, local = inv*(p - o).
 struct Geo {
     double o[3];

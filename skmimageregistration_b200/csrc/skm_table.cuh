@@ -56,6 +56,7 @@ struct TableDev {
     double *part;        // [NQ][value blocks]
     unsigned *tc_err;    // failure word of the tensor-core kernels (NULL without them)
     int value_blocks, tile_x, tile_y, tiles_x, tiles_y, tiles_z;
+    FastDiv div_nph, div_nq0, div_nq01, div_h0, div_h01;   // index decomposition (ncell * nph < 2^31)
 };
 
 struct TablePlan {
@@ -175,14 +176,14 @@ __global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev 
     float vf[NQ];                 // per-thread partials over a few texels; block sums in double
 #pragma unroll
     for (int k = 0; k < NQ; ++k) vf[k] = 0.f;
-    const long long total = T.ncell * T.nph;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const long long cell = i / T.nph;
-        const int p_lin = (int)(i - cell * T.nph);
-        const int cc[3] = {(int)(cell % T.nq[0]), (int)((cell / T.nq[0]) % T.nq[1]),
-                           (int)(cell / ((long long)T.nq[0] * T.nq[1]))};
-        const int ph[3] = {p_lin % T.h[0], (p_lin / T.h[0]) % T.h[1], p_lin / (T.h[0] * T.h[1])};
+    const int total = (int)(T.ncell * T.nph);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int cell = (int)T.div_nph.div((uint32_t)i);
+        const int p_lin = i - cell * T.nph;
+        const int cyz = (int)T.div_nq0.div((uint32_t)cell), cz = (int)T.div_nq01.div((uint32_t)cell);
+        const int cc[3] = {cell - cyz * T.nq[0], cyz - cz * T.nq[1], cz};
+        const int pyz = (int)T.div_h0.div((uint32_t)p_lin), pz = (int)T.div_h01.div((uint32_t)p_lin);
+        const int ph[3] = {p_lin - pyz * T.h[0], pyz - pz * T.h[1], pz};
         int x[3];
         bool ok = true;
 #pragma unroll
@@ -192,7 +193,7 @@ __global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev 
         }
         float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ok) {
-            const long long plane = T.ncell * T.nph;
+            const int plane = total;
             const float u[3] = {T.ucp[i], T.ucp[i + plane], D > 2 ? T.ucp[i + 2 * plane] : 0.f};
             double fi[3] = {(double)x[0], (double)x[1], (double)x[2]}, p[3], mp[3], ml[3];
             to_global<D>(P.fixed, fi, p);
@@ -654,7 +655,13 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     T.tiles_y = (T.nq[1] + T.tile_y - 1) / T.tile_y;
     T.tiles_z = (T.nq[2] + ncz - 1) / ncz;
     pl.transform_blocks = T.tiles_x * T.tiles_y * T.tiles_z;
+    if (T.ncell * T.nph >= (1LL << 31) || (long long)D * T.ncell * T.nph >= (1LL << 31)) return 0;
     T.value_blocks = (int)std::min<long long>((T.ncell * T.nph + 255) / 256, 148LL * 8);
+    T.div_nph = FastDiv((uint32_t)T.nph);
+    T.div_nq0 = FastDiv((uint32_t)T.nq[0]);
+    T.div_nq01 = FastDiv((uint32_t)(T.nq[0] * T.nq[1]));
+    T.div_h0 = FastDiv((uint32_t)T.h[0]);
+    T.div_h01 = FastDiv((uint32_t)(T.h[0] * T.h[1]));
     pl.hl = hl;
     pl.ncz = ncz;
 

@@ -1,6 +1,6 @@
 // skm_table_tc.cuh -- the two GEMM-shaped kernels of the phase-table path on the 5th-generation
 // tensor cores: tcgen05.mma kind::tf32 with FP32 accumulators in TMEM, FP32-accurate through a
-// hi/lo split of both operands (x = hi + lo, hi = tf32(x)).
+// hi/lo split of both operands (x = hi + lo, hi = x truncated to tf32).
 //
 // Rows of both GEMMs are (component, cell) pairs, component-major: row = comp * ct + c with
 // ct = 128 / D cells per tile (42 in 3-D, 64 in 2-D), so one M = 128 MMA serves all components.
@@ -18,9 +18,9 @@
 // MMAs of a chunk as soon as its stage is full and commits them to the stage's empty barrier, and
 // 4 epilogue warps drain the finished accumulator of a tile from TMEM (two accumulators, so the
 // MMAs of the next tile run meanwhile).  The transform's producers stage the control points of
-// the next brick with cp.async while they build the current one.  Operands use the K-major no-swizzle canonical layout
-// [K/4][rows][4 floats]: 8-row x 16-byte core matrices, SBO = 128 B between 8-row groups,
-// LBO = rows * 16 B between the two 4-element K halves of one MMA.
+// the next brick with cp.async while they build the current one.  Operands use the K-major
+// 128-byte-swizzled canonical layout (32 K elements per 128-byte row, 8-row atoms of 1024 bytes,
+// K blocks of 32 one after the other), which the tensor cores read at full rate.
 // Every mbarrier wait is bounded; a wait that gives up sets *err and a CTA-wide abort flag that
 // ends the other roles' waits, the MMA thread waits (bounded) for its MMAs in flight, and the
 // CTA frees its TMEM and returns.
