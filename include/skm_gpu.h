@@ -151,7 +151,7 @@ typedef struct skm_evaluator_info {
     int32_t table_taps;               /* control points per cell in the kernel support */
     int32_t table_cells_per_axis[3];
     int64_t table_cells;
-    int32_t table_regularizer_offsets;
+    int32_t table_regularizer_offsets;  /* control-point offsets with a nonzero kernel value */
     /* tensor-core GEMMs of the table path (zero when they do not apply): M = 128 rows of
      * (component, cell) per tile, N x K per MMA chain */
     int32_t tc_cells_per_tile;
@@ -159,9 +159,9 @@ typedef struct skm_evaluator_info {
     int64_t tc_transform_tiles;
     int64_t tc_contrib_tiles;
     int32_t tc_transform_n;           /* 2 x phases padded to 16 (tf32 part and remainder of the table) */
-    int32_t tc_transform_k;           /* taps padded to 8 */
+    int32_t tc_transform_k;           /* taps padded to 32 */
     int32_t tc_contrib_n;             /* taps padded to 16 */
-    int32_t tc_contrib_k;             /* phases padded to 8 */
+    int32_t tc_contrib_k;             /* phases padded to 32 */
 } skm_evaluator_info;
 int skm_evaluator_describe(skm_evaluator *ev, skm_evaluator_info *out);
 

@@ -482,7 +482,7 @@ extern "C" int skm_evaluator_describe(skm_evaluator *e, skm_evaluator_info *out)
         r.table_taps = T.ntap;
         for (int d = 0; d < 3; ++d) r.table_cells_per_axis[d] = T.nq[d];
         r.table_cells = T.ncell;
-        r.table_regularizer_offsets = T.nc[0] * T.nc[1] * T.nc[2];
+        r.table_regularizer_offsets = T.nkcp;
     }
     if (e->table.enabled && e->tc.enabled) {
         const TcDev &C = e->tc.dev;

@@ -48,7 +48,9 @@ struct TableDev {
     int clo[3], nc[3];           // control-point offsets of the regularizer box
     const float *tfwd;   // [tap][(px,py)][pz]
     const float *tgemm;  // [phase][ntap_pad]
-    const float *kcp;    // [nc0*nc1*nc2] kernel between control points at an offset
+    const float *kcp;    // [nkcp]: nonzero kernel values between control points at an offset ...
+    const int *kcpo;     // [nkcp]: ... and the offsets, (dx + 512) | (dy + 512) << 10 | (dz + 512) << 20
+    int nkcp;            // offsets of the regularizer box with a nonzero kernel value, in box order
     float4 *rec;         // [cell][phase]: grad M, m
     float *ucp;          // [comp][cell][phase]: u = sum_t T w alpha (planes of ncell*nph)
     const float *fixcp;  // [cell][phase]: fixed image value (0 outside)
@@ -63,6 +65,7 @@ struct TablePlan {
     bool enabled = false;
     TableDev dev{};
     float *d_tfwd = nullptr, *d_tgemm = nullptr, *d_kcp = nullptr, *d_fixcp = nullptr, *d_contrib = nullptr;
+    int *d_kcpo = nullptr;
     float4 *d_rec = nullptr;
     float *d_ucp = nullptr;
     double *d_part = nullptr;
@@ -316,15 +319,19 @@ __global__ void __launch_bounds__(kTabContribThreads) table_contrib_kernel(Table
 constexpr int kGatherGroups = 8;
 
 template <int D>
-__global__ void __launch_bounds__(256) table_gather_kernel(EvalParams P, TableDev T, DerivParams Q)
+__global__ void __launch_bounds__(256, 4) table_gather_kernel(EvalParams P, TableDev T, DerivParams Q)
 {
     __shared__ float sacc[kGatherGroups][3][32];
     __shared__ float sreg[kGatherGroups][9][32];
     __shared__ double sval[kGatherGroups][3][32];
     __shared__ float kcp_s[1024];
+    __shared__ int kcpo_s[1024];
     __shared__ int4 tapoff[kTabMaxTap * kTabMaxTap * kTabMaxTap];   // (tx+tlo, ty+tlo, tz+tlo) per tap
-    const int nkcp = T.nc[0] * T.nc[1] * T.nc[2];
-    for (int i = threadIdx.x; i < nkcp; i += blockDim.x) kcp_s[i] = T.kcp[i];
+    const int nkcp = T.nkcp;
+    for (int i = threadIdx.x; i < nkcp; i += blockDim.x) {
+        kcp_s[i] = T.kcp[i];
+        kcpo_s[i] = T.kcpo[i];
+    }
     for (int i = threadIdx.x; i < T.ntap; i += blockDim.x)
         tapoff[i] = make_int4(T.tlo[0] + T.qmin[0] + i % T.nt[0], T.tlo[1] + T.qmin[1] + (i / T.nt[0]) % T.nt[1],
                               T.tlo[2] + T.qmin[2] + i / (T.nt[0] * T.nt[1]), 0);
@@ -337,19 +344,29 @@ __global__ void __launch_bounds__(256) table_gather_kernel(EvalParams P, TableDe
     const float4 cj = active ? P.cpd[j_lin] : make_float4(0.f, 0.f, 0.f, 0.f);
     float acc[3] = {0.f, 0.f, 0.f};
     if (active && !Q.values_only) {
-        const int ntap = T.ntap;
-        const long long ncell = T.ncell;
-        const float *c0p = T.contrib, *c1p = T.contrib + (long long)ntap * ncell,
-                    *c2p = T.contrib + 2LL * ntap * ncell;
-#pragma unroll 4
-        for (int tap = grp; tap < ntap; tap += kGatherGroups) {
-            const int4 o = tapoff[tap];
-            const int qx = j[0] - o.x, qy = j[1] - o.y, qz = j[2] - o.z;
-            if ((unsigned)qx < (unsigned)T.nq[0] && (unsigned)qy < (unsigned)T.nq[1] && (unsigned)qz < (unsigned)T.nq[2]) {
-                const long long c = (long long)tap * ncell + ((long long)qz * T.nq[1] + qy) * T.nq[0] + qx;
-                acc[0] += __ldg(c0p + c);
-                acc[1] += __ldg(c1p + c);
-                if (D > 2) acc[2] += __ldg(c2p + c);
+        // groups of kU taps: all loads first (independent, predicated), then the sums in tap order
+        constexpr int kU = 8;
+        const int ntap = T.ntap, ncell = (int)T.ncell;
+        const float *c0p = T.contrib, *c1p = T.contrib + ntap * ncell, *c2p = T.contrib + 2 * ntap * ncell;
+        for (int base = grp; base < ntap; base += kGatherGroups * kU) {
+            float v[kU][3];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int tap = base + u * kGatherGroups;
+                const int4 o = tapoff[min(tap, ntap - 1)];
+                const int qx = j[0] - o.x, qy = j[1] - o.y, qz = j[2] - o.z;
+                const bool in = tap < ntap && (unsigned)qx < (unsigned)T.nq[0] && (unsigned)qy < (unsigned)T.nq[1] &&
+                                (unsigned)qz < (unsigned)T.nq[2];
+                const int c = in ? tap * ncell + (qz * T.nq[1] + qy) * T.nq[0] + qx : 0;
+                v[u][0] = in ? __ldg(c0p + c) : 0.f;
+                v[u][1] = in ? __ldg(c1p + c) : 0.f;
+                v[u][2] = (in && D > 2) ? __ldg(c2p + c) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                acc[0] += v[u][0];
+                acc[1] += v[u][1];
+                if (D > 2) acc[2] += v[u][2];
             }
         }
     }
@@ -361,13 +378,12 @@ __global__ void __launch_bounds__(256) table_gather_kernel(EvalParams P, TableDe
         const float wj = cj.w;
         const float cjv[3] = {cj.x, cj.y, cj.z};
         const float pgs = (float)Q.pg_scaling;
-        const int nc0 = T.nc[0], nc01 = T.nc[0] * T.nc[1];
         for (int o = grp; o < nkcp; o += kGatherGroups) {
             const float k = kcp_s[o];
-            if (k == 0.0f) continue;
-            const int ii[3] = {j[0] + T.clo[0] + o % nc0, j[1] + T.clo[1] + (o / nc0) % T.nc[1],
-                               j[2] + T.clo[2] + o / nc01};
-            if (ii[0] < 0 || ii[0] >= P.cp.n[0] || ii[1] < 0 || ii[1] >= P.cp.n[1] || ii[2] < 0 || ii[2] >= P.cp.n[2])
+            const int pk = kcpo_s[o];
+            const int ii[3] = {j[0] + (pk & 1023) - 512, j[1] + ((pk >> 10) & 1023) - 512, j[2] + (pk >> 20) - 512};
+            if ((unsigned)ii[0] >= (unsigned)P.cp.n[0] || (unsigned)ii[1] >= (unsigned)P.cp.n[1] ||
+                (unsigned)ii[2] >= (unsigned)P.cp.n[2])
                 continue;
             const float4 ci4 = __ldg(P.cpd + lin_of<D>(P.cp, ii));
             const float ci[3] = {ci4.x, ci4.y, ci4.z};
@@ -640,6 +656,8 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
         T.nc[d] = hi - lo + 1;
     }
     if (T.nc[0] * T.nc[1] * T.nc[2] > 1024) return 0;
+    for (int d = 0; d < 3; ++d)
+        if (T.clo[d] < -500 || T.clo[d] + T.nc[d] > 500) return 0;   // packed offsets of the gather
     // transform tiling: threads = (px,py) phases x cells; each thread HL z-phases of NCZ cells
     const int nphxy = T.h[0] * T.h[1];
     const int hl = T.h[2];
@@ -656,6 +674,7 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     T.tiles_z = (T.nq[2] + ncz - 1) / ncz;
     pl.transform_blocks = T.tiles_x * T.tiles_y * T.tiles_z;
     if (T.ncell * T.nph >= (1LL << 31) || (long long)D * T.ncell * T.nph >= (1LL << 31)) return 0;
+    if (3LL * T.ntap * T.ncell >= (1LL << 31)) return 0;          // 32-bit contribution indices
     T.value_blocks = (int)std::min<long long>((T.ncell * T.nph + 255) / 256, 148LL * 8);
     T.div_nph = FastDiv((uint32_t)T.nph);
     T.div_nq0 = FastDiv((uint32_t)T.nq[0]);
@@ -727,7 +746,22 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
                cudaSuccess;
     };
     pl.h_tgemm = tgemm;
-    if (!up(&pl.d_tfwd, tfwd) || !up(&pl.d_tgemm, tgemm) || !up(&pl.d_kcp, kcp) || !up(&pl.d_fixcp, fix)) return 2;
+    // nonzero entries of the regularizer box, in box order (the sums skip k = 0 terms anyway)
+    std::vector<float> kcpv;
+    std::vector<int> kcpo;
+    for (int oz = 0, o = 0; oz < T.nc[2]; ++oz)
+        for (int oy = 0; oy < T.nc[1]; ++oy)
+            for (int ox = 0; ox < T.nc[0]; ++ox, ++o) {
+                if (kcp[o] == 0.0f) continue;
+                kcpv.push_back(kcp[o]);
+                kcpo.push_back((T.clo[0] + ox + 512) | ((T.clo[1] + oy + 512) << 10) | ((T.clo[2] + oz + 512) << 20));
+            }
+    T.nkcp = (int)kcpv.size();
+    if (cudaMalloc((void **)&pl.d_kcpo, std::max<size_t>(1, kcpo.size()) * sizeof(int)) != cudaSuccess ||
+        cudaMemcpyAsync(pl.d_kcpo, kcpo.data(), kcpo.size() * sizeof(int), cudaMemcpyHostToDevice, stream) !=
+            cudaSuccess)
+        return 2;
+    if (!up(&pl.d_tfwd, tfwd) || !up(&pl.d_tgemm, tgemm) || !up(&pl.d_kcp, kcpv) || !up(&pl.d_fixcp, fix)) return 2;
     if (cudaMalloc((void **)&pl.d_rec, (size_t)T.ncell * T.nph * sizeof(float4)) != cudaSuccess) return 2;
     if (cudaMalloc((void **)&pl.d_ucp, (size_t)D * T.ncell * T.nph * sizeof(float)) != cudaSuccess) return 2;
     if (cudaMalloc((void **)&pl.d_contrib, (size_t)3 * T.ntap * T.ncell * sizeof(float)) != cudaSuccess) return 2;
@@ -736,6 +770,7 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     T.tfwd = pl.d_tfwd;
     T.tgemm = pl.d_tgemm;
     T.kcp = pl.d_kcp;
+    T.kcpo = pl.d_kcpo;
     T.fixcp = pl.d_fixcp;
     T.rec = pl.d_rec;
     T.ucp = pl.d_ucp;
@@ -811,6 +846,7 @@ inline int table_size_grids(TablePlan &pl)
 inline void table_free(TablePlan &pl)
 {
     float *f[] = {pl.d_tfwd, pl.d_tgemm, pl.d_kcp, pl.d_fixcp, pl.d_contrib};
+    if (pl.d_kcpo) cudaFree(pl.d_kcpo);
     for (float *p : f)
         if (p) cudaFree(p);
     if (pl.d_rec) cudaFree(pl.d_rec);

@@ -128,7 +128,10 @@ __device__ __forceinline__ unsigned long long globaltimer()
 }
 
 // Waits for the completion of the mbarrier phase with the given parity; false when the bound
-// runs out first or when *abort becomes nonzero (another role of the CTA gave up).
+// runs out first or when *abort becomes nonzero (another role of the CTA gave up).  try_wait
+// carries a suspend-time hint: a waiting thread sleeps in hardware until the phase completes (or
+// the hint elapses) instead of spinning, so waiting roles leave the issue slots to working ones.
+constexpr uint32_t kTcSuspendNs = 20000;
 __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, const volatile int *abort = nullptr)
 {
     const uint32_t a = smem_addr(mbar);
@@ -138,17 +141,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, const
         asm volatile(
             "{\n\t"
             ".reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t"
             "}\n"
-            : "=r"(done) : "r"(a), "r"(parity) : "memory");
+            : "=r"(done) : "r"(a), "r"(parity), "r"(kTcSuspendNs) : "memory");
         if (done) return true;
-        if ((i & 63) == 0) {
-            if (abort && *abort) return false;
-            const unsigned long long t = globaltimer();
-            if (i == 0) t0 = t;
-            else if (t - t0 > kTcWaitNs) return false;
-        }
+        if (abort && *abort) return false;
+        const unsigned long long t = globaltimer();
+        if (i == 0) t0 = t;
+        else if (t - t0 > kTcWaitNs) return false;
     }
     return false;
 }
