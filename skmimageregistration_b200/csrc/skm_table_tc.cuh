@@ -47,6 +47,12 @@ constexpr int kTcRows = 128;
 constexpr int kTcProdBar = 1;                                    // named barrier of all producers
 constexpr int kTcGroupBar = 2;                                   // + group: named barriers of the groups
 constexpr int kTcGroupThreads = kTcProdThreads / 2;              // contrib: two producer groups
+// contrib: 8 epilogue warps (two per TMEM lane quarter, alternate 16-column chunks), then the
+// MMA warp, then the producers
+constexpr int kConEpiWarps = 8;
+constexpr int kConMmaWarp = kConEpiWarps;
+constexpr int kConProdBase = (kConEpiWarps + 1) * 32;
+constexpr int kConThreads = kConProdBase + kTcProdThreads;     // 544
 static_assert(kTcProdThreads * 4 == kTcRows * (kTcKBlock / 4), "transform producers: 4 items per thread");
 constexpr int kTcNumBars = 2 * kTcStages + 5;
 constexpr int kTcMaxRegion = 4096;                               // staged control points per brick
@@ -82,7 +88,7 @@ struct TcBars {
           drain(b + 2 * kTcStages + 4)
     {
     }
-    __device__ void init(int full_count) const
+    __device__ void init(int full_count, int epi_threads = kTcEpiWarps * 32) const
     {
         for (int s = 0; s < kTcStages; ++s) {     // stages beyond the kernel's count stay unused
             tc::mbar_init(&full[s], full_count);
@@ -90,7 +96,7 @@ struct TcBars {
         }
         for (int b = 0; b < 2; ++b) {
             tc::mbar_init(&acc_full[b], 1);
-            tc::mbar_init(&acc_empty[b], kTcEpiWarps * 32);
+            tc::mbar_init(&acc_empty[b], epi_threads);
         }
         tc::mbar_init(drain, 1);
         tc::fence_mbarrier_init();
@@ -125,16 +131,16 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Teardown shared by both kernels: the MMA thread waits (bounded) until its MMAs have retired,
 // then the MMA warp frees the TMEM after every role has left its loop.
-__device__ __forceinline__ void tc_teardown(const TcBars &B, uint32_t tmem, uint32_t cols)
+__device__ __forceinline__ void tc_teardown(const TcBars &B, uint32_t tmem, uint32_t cols, int mma_warp = kTcMmaWarp)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp == kTcMmaWarp && lane == 0) {
+    if (warp == mma_warp && lane == 0) {
         tc::commit(B.drain);
         tc::mbar_wait(B.drain, 0);
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == kTcMmaWarp) {
+    if (warp == mma_warp) {
         tc::fence_after_sync();
         tc::tmem_dealloc(tmem, cols);
     }
@@ -412,7 +418,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
 
 // ------------------------------------------------------------------------------------------------
 // Contrib[comp][t][cell] = sum_p T[p][t] g(cell, p) on the tensor cores
-__global__ void __launch_bounds__(kTcThreads, 1) table_contrib_tc_kernel(TableDev T, TcDev C,
+__global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableDev T, TcDev C,
                                                                         const double *__restrict__ stats)
 {
     extern __shared__ float4 tc_smem4[];
@@ -431,15 +437,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_contrib_tc_kernel(TableDe
     const int nchunk = Kp / kTcKBlock;
 
     if (tid == 0) {
-        B.init(kTcGroupThreads);
+        B.init(kTcGroupThreads, kConEpiWarps * 32);
         *abort = 0;
     }
-    if (warp == kTcMmaWarp) tc::tmem_alloc(tmem_holder, (uint32_t)C.con_cols);
-    for (int i = tid; i < 2 * Kp * Np / 4; i += kTcThreads)
+    if (warp == kConMmaWarp) tc::tmem_alloc(tmem_holder, (uint32_t)C.con_cols);
+    for (int i = tid; i < 2 * Kp * Np / 4; i += kConThreads)
         reinterpret_cast<float4 *>(Bhi)[i] = __ldg(reinterpret_cast<const float4 *>(C.bcon) + i);
     // rows past D * ct never receive data: zero their 128-byte rows once in every stage half
     const int pad_rows = kTcRows - D * ct;
-    for (int i = tid; i < NS * 2 * pad_rows * 8; i += kTcThreads) {
+    for (int i = tid; i < NS * 2 * pad_rows * 8; i += kConThreads) {
         const int half = i / (pad_rows * 8), r = D * ct + (i / 8) % pad_rows, c16 = i & 7;
         *reinterpret_cast<float4 *>(As + half * (kTcStageBytes / 2) + (r >> 3) * 1024 + (r & 7) * 128 + c16 * 16) =
             make_float4(0.f, 0.f, 0.f, 0.f);
@@ -450,11 +456,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_contrib_tc_kernel(TableDe
     tc::fence_after_sync();
     const uint32_t tmem = *tmem_holder;
 
-    if (warp >= kTcEpiWarps + 1) {
+    if (warp >= kConEpiWarps + 1) {
         // ---------------- producers: g = (a f + b m + c) grad M, hi/lo stages ----------------
         // Two groups of 4 warps take alternate K chunks, so that one group's global loads are in
         // flight while the other converts and stores.  Item = (cell c, 4 phases), lanes over cells.
-        const int pt = tid - kTcProdBase;
+        const int pt = tid - kConProdBase;
         const int grp = pt / kTcGroupThreads, gt = pt - grp * kTcGroupThreads;
         const float cf = (float)stats[S_COEF_F], cm = (float)stats[S_COEF_M], cc = (float)stats[S_COEF_C];
         const int nitems = ct * (kTcKBlock / 4);
@@ -526,7 +532,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_contrib_tc_kernel(TableDe
             tc::fence_proxy_async();
             tc::mbar_arrive(&B.full[s]);
         }
-    } else if (warp == kTcMmaWarp) {
+    } else if (warp == kConMmaWarp) {
         // ---------------- MMA issue (one thread) ----------------
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_tf32(kTcRows, Np);
@@ -572,9 +578,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_contrib_tc_kernel(TableDe
         }
         __syncwarp();
     } else {
-        // ---------------- epilogue: TMEM -> Contrib (lane quarter = warp) ----------------
-        const int r = warp * 32 + lane;
+        // ---------------- epilogue: TMEM -> Contrib ----------------
+        // warp w reads TMEM lane quarter w % 4; warps w and w + 4 take alternate 16-column chunks
+        const int quarter = warp & 3, half = warp >> 2;
+        const int r = quarter * 32 + lane;
         const int comp = r / ct, c = r - comp * ct;
+        const int ncell = (int)T.ncell;
         for (int it = 0;; ++it) {
             const long long tile = blockIdx.x + (long long)it * gridDim.x;
             if (tile >= ntiles) break;
@@ -585,24 +594,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_contrib_tc_kernel(TableDe
                 break;
             }
             tc::fence_after_sync();
-            const long long cell = tile * ct + c;
-            const bool valid = comp < D && cell < T.ncell;
-            const uint32_t tb = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * C.con_stride);
-            for (int j = 0; j < (Np >> 4); ++j) {
+            const int cell = (int)(tile * ct) + c;
+            const bool valid = comp < D && cell < ncell;
+            const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * C.con_stride);
+            for (int j = half; j < (Np >> 4); j += kConEpiWarps / 4) {
                 float v[16];
                 tc::tmem_ld16(tb + (uint32_t)(16 * j), v);
                 if (valid) {
-                    float *dst = T.contrib + ((long long)comp * T.ntap + 16 * j) * T.ncell + cell;
+                    float *dst = T.contrib + (comp * T.ntap + 16 * j) * ncell + cell;
 #pragma unroll
                     for (int e = 0; e < 16; ++e)
-                        if (16 * j + e < T.ntap) dst[(long long)e * T.ncell] = v[e];
+                        if (16 * j + e < T.ntap) dst[e * ncell] = v[e];
                 }
             }
             tc::fence_before_sync();
             tc::mbar_arrive(&B.acc_empty[b]);
         }
     }
-    tc_teardown(B, tmem, (uint32_t)C.con_cols);
+    tc_teardown(B, tmem, (uint32_t)C.con_cols, kConMmaWarp);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -729,6 +738,14 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (cudaFuncSetAttribute(table_transform_tc_kernel, a, (int)tc.transform_smem) != cudaSuccess) return 2;
     if (cudaFuncSetAttribute(table_contrib_tc_kernel, a, (int)tc.contrib_smem) != cudaSuccess) return 2;
+    // both kernels must be launchable with their block sizes and shared memory (else: CUDA cores)
+    int occ_t = 0, occ_c = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, table_transform_tc_kernel, kTcThreads,
+                                                      tc.transform_smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, table_contrib_tc_kernel, kConThreads,
+                                                      tc.contrib_smem) != cudaSuccess)
+        return 2;
+    if (occ_t < 1 || occ_c < 1) return 0;
     const long long ttiles = (long long)C.tiles[0] * C.tiles[1] * C.tiles[2];
     const long long ctiles = (T.ncell + C.ct - 1) / C.ct;
     tc.transform_blocks = (int)std::max<long long>(1, std::min<long long>(ttiles, sms));
@@ -745,7 +762,7 @@ inline int table_transform_tc(const TcPlan &tc, const TablePlan &pl, const EvalP
 
 inline int table_contrib_tc(const TcPlan &tc, const TablePlan &pl, const double *stats, cudaStream_t s)
 {
-    table_contrib_tc_kernel<<<tc.contrib_blocks, kTcThreads, tc.contrib_smem, s>>>(pl.dev, tc.dev, stats);
+    table_contrib_tc_kernel<<<tc.contrib_blocks, kConThreads, tc.contrib_smem, s>>>(pl.dev, tc.dev, stats);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
