@@ -377,6 +377,9 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         for (long long i = 0; i < e->N; ++i) tmp[i] = (float)d->fixed_image[i];
         if (dalloc(&e->d_fixed, e->N)) return SKM_ERR_CUDA;
         SKM_CUDA(cudaMemcpy(e->d_fixed, tmp.data(), e->N * sizeof(float), cudaMemcpyHostToDevice));
+
+        if (ncoef >= (1LL << 31))
+            return fail(SKM_ERR_UNSUPPORTED, "moving image coefficients: %lld entries, at most 2^31 - 1", ncoef);
         for (long long i = 0; i < ncoef; ++i) tmp[i] = (float)d->moving_coefficients[i];
         if (dalloc(&e->d_coeffs, ncoef)) return SKM_ERR_CUDA;
         SKM_CUDA(cudaMemcpy(e->d_coeffs, tmp.data(), ncoef * sizeof(float), cudaMemcpyHostToDevice));

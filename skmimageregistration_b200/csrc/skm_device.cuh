@@ -345,14 +345,15 @@ __device__ __forceinline__ void bspline_derivs4(const float4 *__restrict__ c4, c
     }
     if (D == 3) {
         float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
-        const long long sy = mg.st[1], sz = mg.st[2];
-        const float4 *base = c4 + ii[0] + ii[1] * sy + ii[2] * sz;
+        // 32-bit offsets: the coefficient volume holds fewer than 2^31 entries (checked at creation)
+        const int sy = (int)mg.st[1], sz = (int)mg.st[2];
+        const float4 *base = c4 + (ii[0] + ii[1] * sy + ii[2] * sz);
 #pragma unroll
         for (int z = 0; z < 4; ++z) {
             float z0 = 0.f, z1 = 0.f, z3 = 0.f;
 #pragma unroll
             for (int y = 0; y < 4; ++y) {
-                const float4 r = __ldg(base + y * sy + z * sz);
+                const float4 r = __ldg(base + (y * sy + z * sz));
                 float dx = dW[0][0] * r.x + dW[1][0] * r.y + dW[2][0] * r.z + dW[3][0] * r.w;
                 float vx = W[0][0] * r.x + W[1][0] * r.y + W[2][0] * r.z + W[3][0] * r.w;
                 z0 += W[y][1] * dx;
@@ -370,8 +371,8 @@ __device__ __forceinline__ void bspline_derivs4(const float4 *__restrict__ c4, c
         grad[2] = c2 * (float)mg.inv[2];
     } else {
         float c0 = 0.f, c1 = 0.f, c2 = 0.f;
-        const long long sy = mg.st[1];
-        const float4 *base = c4 + ii[0] + ii[1] * sy;
+        const int sy = (int)mg.st[1];
+        const float4 *base = c4 + (ii[0] + ii[1] * sy);
 #pragma unroll
         for (int y = 0; y < 4; ++y) {
             const float4 r = __ldg(base + y * sy);
