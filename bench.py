@@ -366,8 +366,8 @@ def run_ours(args, rank, world, local_rank):
     ev2 = GpuKernelEvaluator(pb)
     ev2.path(gemm_request)
     params = np.zeros(P)
-    base = np.zeros(P)
-    prev = np.zeros(P)
+    step = np.zeros(P)
+    grad = [np.zeros(P), np.zeros(P)]               # this and the previous step's derivative
     t_sim = 0.0
     ev2.metric(mdesc, params, cpw)                  # warm-up
     e2e_s = 0.0
@@ -376,13 +376,14 @@ def run_ours(args, rank, world, local_rank):
             flush.fill_(float(i))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        v, g = ev2.metric(mdesc, params, cpw)
-        # AdaptiveStepGradientDescentOptimizerv4 update on the host (ITK glue path)
+        g, prev = grad[i & 1], grad[(i + 1) & 1]
+        v, _ = ev2.metric(mdesc, params, cpw, out_derivative=g)
+        # AdaptiveStepGradientDescentOptimizerv4 update on the host (ITK glue path), in place:
+        # the step base is the previous position, so params += lr * g
         lr = odesc.a / (odesc.A + t_sim + 1.0) ** odesc.alpha
-        sp = float(g @ prev)
-        prev = g
-        params = base + g * lr
-        base = params
+        sp = float(np.dot(g, prev))
+        np.multiply(g, lr, out=step)                # in place, no temporaries
+        np.add(params, step, out=params)
         x = -sp
         t_sim = max(0.0, t_sim + odesc.f_min + (odesc.f_max - odesc.f_min) /
                     (1.0 - (odesc.f_max / odesc.f_min) * math.exp(-x / odesc.omega)))

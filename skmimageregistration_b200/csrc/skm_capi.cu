@@ -137,6 +137,7 @@ struct skm_evaluator {
 
     // pinned host staging
     double *h_in = nullptr, *h_out = nullptr;
+    bool weights_uploaded = false;       // h_in's weight part is on the device (skip identical weights)
 
     // phase-table fast path (stationary kernel, integral spacing ratio) and its tensor-core GEMMs
     TablePlan table{};
@@ -560,9 +561,16 @@ static int upload_params(skm_evaluator *e, const double *cp, const double *cpw, 
 {
     if (!cp || !cpw) return fail(SKM_ERR_INVALID, "control points / weights are NULL");
     const long long C = e->C, n = C * e->D;
+    // (the previous call synchronised the stream, so the staging buffer is free)
     std::memcpy(e->h_in, cp, sizeof(double) * n);
-    std::memcpy(e->h_in + n, cpw, sizeof(double) * C);
-    SKM_CUDA(cudaMemcpyAsync(e->d_in, e->h_in, sizeof(double) * (n + C), cudaMemcpyHostToDevice, e->stream));
+    SKM_CUDA(cudaMemcpyAsync(e->d_in, e->h_in, sizeof(double) * n, cudaMemcpyHostToDevice, e->stream));
+    // weights: most callers pass the same weights every time; compare with the staged copy
+    if (!e->weights_uploaded || std::memcmp(e->h_in + n, cpw, sizeof(double) * C) != 0) {
+        e->weights_uploaded = false;
+        std::memcpy(e->h_in + n, cpw, sizeof(double) * C);
+        SKM_CUDA(cudaMemcpyAsync(e->d_in + n, e->h_in + n, sizeof(double) * C, cudaMemcpyHostToDevice, e->stream));
+        e->weights_uploaded = true;
+    }
     int blocks = (int)((C + 255) / 256);
     if (planar)
         pack_cp_planar<<<blocks, 256, 0, e->stream>>>(e->d_in, e->d_in + n, C, e->D, e->d_cpd);

@@ -182,12 +182,20 @@ class GpuKernelEvaluator:
         return out
 
     # --- metric level (RegularizedImageToImageMetricv4::GetValueAndDerivative)
-    def metric(self, mdesc: MetricDesc, params, cpw, df=None, df_geometry=None, derivative=True):
+    def metric(self, mdesc: MetricDesc, params, cpw, df=None, df_geometry=None, derivative=True, out_derivative=None):
+        """Metric value and (negated, regularized) derivative; `out_derivative` (float64, contiguous,
+        num_parameters) receives the derivative in place of a new array."""
         params = np.ascontiguousarray(params, np.float64)
         cpw = np.ascontiguousarray(cpw, np.float64)
         f = self._field(df, df_geometry)
         out = MetricValues()
-        der = np.zeros(self.problem.num_parameters) if derivative else None
+        if not derivative:
+            der = None
+        elif out_derivative is not None:
+            der = out_derivative
+            assert der.dtype == np.float64 and der.flags["C_CONTIGUOUS"] and der.size == self.problem.num_parameters
+        else:
+            der = np.zeros(self.problem.num_parameters)
         check(lib().skm_metric_evaluate(self.h, C.byref(mdesc), dptr(params), dptr(cpw), C.byref(f), dptr(der),
                                         C.byref(out)))
         return out.as_dict(), der
