@@ -291,6 +291,66 @@ int skm_bspline_coefficients(int32_t dimensions, const int32_t *size,
                              const double *image, double *coefficients);
 
 /* ------------------------------------------------------------------------- */
+/* Preprocessing and the multi-scale driver.                                   */
+
+/* GaussianSmoothing (include/itkUtils.h:139-150, ITK DiscreteGaussianImageFilter): discrete
+ * Gaussian e^-t I_n(t) per axis, t = variance / spacing^2 when use_image_spacing, kernel grown
+ * until it holds 1 - maximum_error of the mass (or half width > maximum_kernel_width), normalised,
+ * edge voxels repeated.  Host buffers, x fastest.  The reference passes maximum_error 0.01 and
+ * maximum_kernel_width 64. */
+int skm_gaussian_smooth(int32_t dimensions, const skm_geometry *geometry, double variance,
+                        int32_t use_image_spacing, double maximum_error, int32_t maximum_kernel_width,
+                        const double *src, double *dst);
+
+/* ThresholdImage + RescaleImage (include/itkUtils.h:45-110): with apply_threshold, clamp to
+ * [smallest value > threshold_min, largest value < threshold_max]; then map the range linearly
+ * onto [out_min, out_max].  SKM_ERR_INVALID when no value lies inside the thresholds. */
+int skm_threshold_rescale(int32_t dimensions, const int32_t *size, int32_t apply_threshold,
+                          double threshold_min, double threshold_max, double out_min, double out_max,
+                          const double *src, double *dst);
+
+#define SKM_MAX_SCALES 8
+
+/* Configuration of src/SKMReg.cxx (defaults in include/ConfigUtils.h:29-62); per-scale arrays
+ * hold num_scales entries (repeat the last one for "shorter lists", as CURRENT does). */
+typedef struct skm_register_desc {
+    int32_t dimensions;
+    int32_t num_scales;
+    int32_t metric;                   /* SKM_MSE / SKM_NCC / SKM_LCC */
+    double  cp_spacing_scaler;        /* control spacing = min(sigma_C4, sigma_C0) / scaler (1 below 1) */
+    int32_t apply_threshold;          /* intensity_thresholds given (2 entries) */
+    double  threshold_min, threshold_max;
+    double  sigma_c4[SKM_MAX_SCALES];
+    double  sigma_c0[SKM_MAX_SCALES];
+    double  smoothing_variance[SKM_MAX_SCALES];
+    double  initial_step_size[SKM_MAX_SCALES];
+    int32_t num_function_evaluations[SKM_MAX_SCALES];
+    int32_t sampling_rate[SKM_MAX_SCALES];
+    int32_t neighborhood_sampling[SKM_MAX_SCALES];
+    double  reg_l1[SKM_MAX_SCALES], reg_l21[SKM_MAX_SCALES], reg_l2[SKM_MAX_SCALES];
+    double  reg_rkhs[SKM_MAX_SCALES], reg_rd[SKM_MAX_SCALES], reg_rd_scaling[SKM_MAX_SCALES];
+    double  reg_pg[SKM_MAX_SCALES], reg_pg_scaling[SKM_MAX_SCALES];
+} skm_register_desc;
+
+typedef struct skm_register_report {
+    int32_t levels_done;
+    int32_t iterations[SKM_MAX_SCALES];
+    int64_t control_points[SKM_MAX_SCALES];
+    double  best_value[SKM_MAX_SCALES];   /* metric value (+ regularizers) at the returned parameters */
+    double  seconds[SKM_MAX_SCALES];
+} skm_register_report;
+
+/* The scale loop of src/SKMReg.cxx:84-500 (skmreg): threshold + rescale, then per level
+ * smoothing, B-spline prefilter, control-point grid, evaluator with the previous levels'
+ * displacement field, device-resident adaptive-step optimizer, summed displacement field.
+ * Reference (moving) and target (fixed) share `geometry` (the reference writes the field of the
+ * target grid into a reference-sized image, GenerateDisplacementFieldGpu, itkUtils.h:181-253).
+ * No weight image or covariance tensor (tensor_weights 0).  displacement: N x D doubles, x
+ * fastest, AoS. */
+int skm_register(const skm_register_desc *desc, const skm_geometry *geometry, const double *reference,
+                 const double *target, double *displacement, skm_register_report *report);
+
+/* ------------------------------------------------------------------------- */
 /* Metric value without any device allocation.  No counterpart in the reference.
  *
  * For callers that must not allocate device memory at evaluation time: frameworks that

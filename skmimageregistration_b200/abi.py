@@ -205,6 +205,45 @@ class OptimizerState(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+MAX_SCALES = 8
+
+
+class RegisterDesc(C.Structure):
+    """skm_register_desc: the configuration of the reference application (src/SKMReg.cxx)."""
+
+    _S = C.c_double * MAX_SCALES
+    _I = C.c_int32 * MAX_SCALES
+    _fields_ = [
+        ("dimensions", C.c_int32),
+        ("num_scales", C.c_int32),
+        ("metric", C.c_int32),
+        ("cp_spacing_scaler", C.c_double),
+        ("apply_threshold", C.c_int32),
+        ("threshold_min", C.c_double),
+        ("threshold_max", C.c_double),
+        ("sigma_c4", _S), ("sigma_c0", _S), ("smoothing_variance", _S), ("initial_step_size", _S),
+        ("num_function_evaluations", _I), ("sampling_rate", _I), ("neighborhood_sampling", _I),
+        ("reg_l1", _S), ("reg_l21", _S), ("reg_l2", _S), ("reg_rkhs", _S), ("reg_rd", _S),
+        ("reg_rd_scaling", _S), ("reg_pg", _S), ("reg_pg_scaling", _S),
+    ]
+
+
+class RegisterReport(C.Structure):
+    _fields_ = [
+        ("levels_done", C.c_int32),
+        ("iterations", C.c_int32 * MAX_SCALES),
+        ("control_points", C.c_int64 * MAX_SCALES),
+        ("best_value", C.c_double * MAX_SCALES),
+        ("seconds", C.c_double * MAX_SCALES),
+    ]
+
+    def as_dict(self):
+        n = self.levels_done
+        return {"levels_done": n, "iterations": list(self.iterations[:n]),
+                "control_points": list(self.control_points[:n]), "best_value": list(self.best_value[:n]),
+                "seconds": list(self.seconds[:n])}
+
+
 def dptr(a):
     """double* of a C-contiguous float64 numpy array (or NULL)."""
     if a is None:

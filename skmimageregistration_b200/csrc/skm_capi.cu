@@ -899,3 +899,4 @@ extern "C" int skm_bspline_coefficients(int32_t D, const int32_t *size, const do
 }
 
 #include "skm_optimizer.cuh"
+#include "skm_driver.cuh"

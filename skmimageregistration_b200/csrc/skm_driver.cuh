@@ -1,0 +1,348 @@
+// skm_driver.cuh -- preprocessing entry points and the multi-scale registration driver.
+//
+// skm_register restates the scale loop of the reference application (src/SKMReg.cxx:84-500):
+// threshold + rescale both images (:85-90), then per scale level
+//   smooth both images with the level's variance (:140-150),
+//   prefilter the smoothed reference (moving) image into B-spline coefficients,
+//   build the control-point grid with spacing min(sigma_C4, sigma_C0) / cp_spacing_scaler (:235-247,
+//   itkTransformAdapter.hxx:246-308),
+//   set up the evaluator (fixed = smoothed target, moving = smoothed reference) with the
+//   displacement field of the previous levels as the frozen front transform (:127-136),
+//   run the adaptive-step optimizer (a = initial step size, A = 20, alpha = 1, f_max = 1e7,
+//   f_min = -1e6, omega = 1, best parameters; orthant projection when L1 or L2,1 is the only
+//   regularizer) on the device (:392-442),
+//   and evaluate the summed displacement field on the reference grid (:452-460).
+// This file is included at the end of skm_capi.cu and uses its entry points.
+#pragma once
+
+#include <chrono>
+#include <vector>
+
+#include "skm_preprocess.cuh"
+
+namespace {
+
+struct DevBuf {
+    double *p = nullptr;
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+};
+
+int smooth_device(int D, const int *size, const double *spacing, double variance, int use_spacing,
+                  double maximum_error, int maximum_width, double *d_img, double *d_tmp, cudaStream_t s)
+{
+    const int X = size[0], Y = D > 1 ? size[1] : 1, Z = D > 2 ? size[2] : 1;
+    const long long n = (long long)X * Y * Z;
+    double *src = d_img, *dst = d_tmp;
+    for (int axis = 0; axis < D; ++axis) {
+        const double sp = use_spacing ? spacing[axis] : 1.0;
+        const std::vector<double> c = skm::gaussian_half_kernel(variance / (sp * sp), maximum_error, maximum_width);
+        const int r = (int)c.size() - 1;
+        if (r > skm::kSmoothMaxRadius) return fail(SKM_ERR_UNSUPPORTED, "smoothing kernel radius %d > %d", r,
+                                                  skm::kSmoothMaxRadius);
+        DevBuf dc;
+        SKM_CUDA(cudaMalloc((void **)&dc.p, c.size() * sizeof(double)));
+        SKM_CUDA(cudaMemcpyAsync(dc.p, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+        skm::smooth_axis_kernel<<<blocks, 256, 0, s>>>(src, dst, X, Y, Z, axis, dc.p, r);
+        SKM_CHECK_LAUNCH();
+        SKM_CUDA(cudaStreamSynchronize(s));     // dc is freed at the end of this iteration
+        std::swap(src, dst);
+    }
+    if (src != d_img) SKM_CUDA(cudaMemcpyAsync(d_img, src, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    return SKM_OK;
+}
+
+int threshold_rescale_device(long long n, int apply_threshold, double tmin, double tmax, double out_min,
+                             double out_max, double *d_img, cudaStream_t s)
+{
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 4);
+    DevBuf part, res;
+    SKM_CUDA(cudaMalloc((void **)&part.p, sizeof(double) * 4 * blocks));
+    SKM_CUDA(cudaMalloc((void **)&res.p, sizeof(double) * 4));
+    skm::range_kernel<<<blocks, 256, 0, s>>>(d_img, n, tmin, tmax, part.p);
+    SKM_CHECK_LAUNCH();
+    skm::range_finish_kernel<<<1, 32, 0, s>>>(part.p, blocks, res.p);
+    SKM_CHECK_LAUNCH();
+    double r[4];
+    SKM_CUDA(cudaMemcpyAsync(r, res.p, sizeof r, cudaMemcpyDeviceToHost, s));
+    SKM_CUDA(cudaStreamSynchronize(s));
+    double lo = r[0], hi = r[1];
+    if (apply_threshold) {
+        // largest value below tmax / smallest above tmin (itkUtils.h:50-62); none: nothing to keep
+        if (r[2] == -DBL_MAX || r[3] == DBL_MAX || r[3] > r[2])
+            return fail(SKM_ERR_INVALID, "no intensity inside the thresholds (%g, %g)", tmin, tmax);
+        lo = r[3];
+        hi = r[2];
+    }
+    // RescaleIntensityImageFilter: scale from the (thresholded) range, shift to out_min
+    double scale;
+    if (hi != lo) scale = (out_max - out_min) / (hi - lo);
+    else if (hi != 0.0) scale = (out_max - out_min) / hi;
+    else scale = 0.0;
+    const double shift = out_min - lo * scale;
+    skm::clamp_rescale_kernel<<<blocks, 256, 0, s>>>(d_img, n, lo, hi, scale, shift);
+    SKM_CHECK_LAUNCH();
+    return SKM_OK;
+}
+
+long long texel_count(int D, const int32_t *size)
+{
+    long long n = 1;
+    for (int d = 0; d < D; ++d) n *= size[d];
+    return n;
+}
+
+struct HostStream {
+    cudaStream_t s = nullptr;
+    ~HostStream()
+    {
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+}  // namespace
+
+extern "C" int skm_gaussian_smooth(int32_t dimensions, const skm_geometry *geometry, double variance,
+                                   int32_t use_image_spacing, double maximum_error, int32_t maximum_kernel_width,
+                                   const double *src, double *dst)
+{
+    if (dimensions != 2 && dimensions != 3) return fail(SKM_ERR_INVALID, "dimensions must be 2 or 3");
+    if (!geometry || !src || !dst) return fail(SKM_ERR_INVALID, "geometry / src / dst is NULL");
+    if (!(variance >= 0.0) || !(maximum_error > 0.0 && maximum_error < 1.0) || maximum_kernel_width < 1)
+        return fail(SKM_ERR_INVALID, "variance >= 0, 0 < maximum_error < 1 and maximum_kernel_width >= 1 required");
+    for (int d = 0; d < dimensions; ++d)
+        if (geometry->size[d] < 1 || (use_image_spacing && !(geometry->spacing[d] > 0.0)))
+            return fail(SKM_ERR_INVALID, "size and spacing must be positive");
+    const long long n = texel_count(dimensions, geometry->size);
+    HostStream hs;
+    SKM_CUDA(cudaStreamCreateWithFlags(&hs.s, cudaStreamNonBlocking));
+    DevBuf a, b;
+    SKM_CUDA(cudaMalloc((void **)&a.p, n * sizeof(double)));
+    SKM_CUDA(cudaMalloc((void **)&b.p, n * sizeof(double)));
+    SKM_CUDA(cudaMemcpyAsync(a.p, src, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
+    int rc = smooth_device(dimensions, geometry->size, geometry->spacing, variance, use_image_spacing, maximum_error,
+                           maximum_kernel_width, a.p, b.p, hs.s);
+    if (rc) return rc;
+    SKM_CUDA(cudaMemcpyAsync(dst, a.p, n * sizeof(double), cudaMemcpyDeviceToHost, hs.s));
+    SKM_CUDA(cudaStreamSynchronize(hs.s));
+    return SKM_OK;
+}
+
+extern "C" int skm_threshold_rescale(int32_t dimensions, const int32_t *size, int32_t apply_threshold,
+                                     double threshold_min, double threshold_max, double out_min, double out_max,
+                                     const double *src, double *dst)
+{
+    if (dimensions != 2 && dimensions != 3) return fail(SKM_ERR_INVALID, "dimensions must be 2 or 3");
+    if (!size || !src || !dst) return fail(SKM_ERR_INVALID, "size / src / dst is NULL");
+    for (int d = 0; d < dimensions; ++d)
+        if (size[d] < 1) return fail(SKM_ERR_INVALID, "size must be positive");
+    const long long n = texel_count(dimensions, size);
+    HostStream hs;
+    SKM_CUDA(cudaStreamCreateWithFlags(&hs.s, cudaStreamNonBlocking));
+    DevBuf a;
+    SKM_CUDA(cudaMalloc((void **)&a.p, n * sizeof(double)));
+    SKM_CUDA(cudaMemcpyAsync(a.p, src, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
+    int rc = threshold_rescale_device(n, apply_threshold, threshold_min, threshold_max, out_min, out_max, a.p, hs.s);
+    if (rc) return rc;
+    SKM_CUDA(cudaMemcpyAsync(dst, a.p, n * sizeof(double), cudaMemcpyDeviceToHost, hs.s));
+    SKM_CUDA(cudaStreamSynchronize(hs.s));
+    return SKM_OK;
+}
+
+namespace {
+
+// ComputeControlPointImage (itkTransformAdapter.hxx:246-308): size ceil(extent / spacing), the grid
+// centred on the image extent
+void control_grid(int D, const skm_geometry &img, double spacing, skm_geometry &cp)
+{
+    cp = skm_geometry{};
+    for (int d = 0; d < 3; ++d) {
+        if (d >= D) {
+            cp.origin[d] = 0.0;
+            cp.spacing[d] = 1.0;
+            cp.size[d] = 1;
+            continue;
+        }
+        const double lower = img.origin[d], upper = img.origin[d] + (img.size[d] - 1) * img.spacing[d];
+        const int n = (int)std::ceil(std::fabs((upper - lower) / spacing));
+        const double cp_upper = img.origin[d] + (n - 1) * spacing;
+        cp.size[d] = n;
+        cp.spacing[d] = spacing;
+        cp.origin[d] = img.origin[d] + std::fabs(upper - cp_upper) / 2.0;
+    }
+}
+
+int check_register_desc(const skm_register_desc *r)
+{
+    if (!r) return fail(SKM_ERR_INVALID, "register descriptor is NULL");
+    if (r->dimensions != 2 && r->dimensions != 3) return fail(SKM_ERR_INVALID, "dimensions must be 2 or 3");
+    if (r->num_scales < 1 || r->num_scales > SKM_MAX_SCALES)
+        return fail(SKM_ERR_INVALID, "num_scales must be in [1, %d]", SKM_MAX_SCALES);
+    if (r->metric != SKM_MSE && r->metric != SKM_NCC && r->metric != SKM_LCC)
+        return fail(SKM_ERR_INVALID, "unknown metric %d", r->metric);
+    for (int s = 0; s < r->num_scales; ++s) {
+        if (!(r->sigma_c4[s] > 0.0) || !(r->sigma_c0[s] > 0.0))
+            return fail(SKM_ERR_INVALID, "scale %d: sigma_C4 and sigma_C0 must be positive", s);
+        if (r->sampling_rate[s] < 1 || r->neighborhood_sampling[s] < 1)
+            return fail(SKM_ERR_INVALID, "scale %d: sampling rate and neighborhood sampling must be >= 1", s);
+        if (r->num_function_evaluations[s] < 0 || !(r->smoothing_variance[s] >= 0.0))
+            return fail(SKM_ERR_INVALID, "scale %d: negative iterations or smoothing variance", s);
+    }
+    return SKM_OK;
+}
+
+}  // namespace
+
+extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geometry, const double *reference,
+                            const double *target, double *displacement, skm_register_report *report)
+{
+    int rc;
+    if ((rc = check_register_desc(r))) return rc;
+    if (!geometry || !reference || !target || !displacement)
+        return fail(SKM_ERR_INVALID, "geometry / reference / target / displacement is NULL");
+    const int D = r->dimensions;
+    for (int d = 0; d < D; ++d)
+        if (geometry->size[d] < 4 || !(geometry->spacing[d] > 0.0))
+            return fail(SKM_ERR_INVALID, "image size must be >= 4 and spacing positive along every axis");
+    const long long n = texel_count(D, geometry->size);
+    skm_register_report rep{};
+    HostStream hs;
+    SKM_CUDA(cudaStreamCreateWithFlags(&hs.s, cudaStreamNonBlocking));
+
+    // preprocessing of both images (SKMReg.cxx:85-90)
+    DevBuf dref, dtar, dtmp;
+    SKM_CUDA(cudaMalloc((void **)&dref.p, n * sizeof(double)));
+    SKM_CUDA(cudaMalloc((void **)&dtar.p, n * sizeof(double)));
+    SKM_CUDA(cudaMalloc((void **)&dtmp.p, n * sizeof(double)));
+    SKM_CUDA(cudaMemcpyAsync(dref.p, reference, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
+    SKM_CUDA(cudaMemcpyAsync(dtar.p, target, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
+    if ((rc = threshold_rescale_device(n, r->apply_threshold, r->threshold_min, r->threshold_max, 0.0, 1.0, dref.p,
+                                       hs.s)))
+        return rc;
+    if ((rc = threshold_rescale_device(n, r->apply_threshold, r->threshold_min, r->threshold_max, 0.0, 1.0, dtar.p,
+                                       hs.s)))
+        return rc;
+
+    std::vector<double> ref_s((size_t)n), tar_s((size_t)n), past((size_t)n * D, 0.0), now((size_t)n * D);
+    long long ncoef = 1;
+    int32_t csize[3] = {1, 1, 1};
+    for (int d = 0; d < D; ++d) {
+        csize[d] = geometry->size[d];
+        ncoef *= geometry->size[d] + 3;
+    }
+    std::vector<double> coeffs((size_t)ncoef);
+    DevBuf dsm;
+    SKM_CUDA(cudaMalloc((void **)&dsm.p, n * sizeof(double)));
+
+    for (int s = 0; s < r->num_scales; ++s) {
+        const auto t0 = std::chrono::steady_clock::now();
+        // smoothed copies of both images (SKMReg.cxx:140-150)
+        for (int which = 0; which < 2; ++which) {
+            double *src = which == 0 ? dref.p : dtar.p;
+            SKM_CUDA(cudaMemcpyAsync(dsm.p, src, n * sizeof(double), cudaMemcpyDeviceToDevice, hs.s));
+            if (r->smoothing_variance[s] > 1e-5 &&
+                (rc = smooth_device(D, geometry->size, geometry->spacing, r->smoothing_variance[s], 1, 0.01, 64,
+                                    dsm.p, dtmp.p, hs.s)))
+                return rc;
+            SKM_CUDA(cudaMemcpyAsync(which == 0 ? ref_s.data() : tar_s.data(), dsm.p, n * sizeof(double),
+                                     cudaMemcpyDeviceToHost, hs.s));
+        }
+        SKM_CUDA(cudaStreamSynchronize(hs.s));
+        if ((rc = skm_bspline_coefficients(D, csize, ref_s.data(), coeffs.data()))) return rc;
+
+        // control-point grid (SKMReg.cxx:235-247)
+        // in float, as the reference computes it
+        const float smin = std::min((float)r->sigma_c4[s], (float)r->sigma_c0[s]);
+        const double cps = r->cp_spacing_scaler < 1.0 ? (double)(smin / 1.0f)
+                                                      : (double)(smin / (float)r->cp_spacing_scaler);
+        skm_geometry cpg;
+        control_grid(D, *geometry, cps, cpg);
+        const long long C = texel_count(D, cpg.size);
+        std::vector<double> cpw((size_t)C, 1.0), params((size_t)C * D, 0.0), best((size_t)C * D);
+
+        skm_evaluator_desc ed{};
+        ed.dimensions = D;
+        ed.num_parameters = (int32_t)(C * D);
+        ed.subsample = r->sampling_rate[s];
+        ed.subsample_neighborhood = r->neighborhood_sampling[s];
+        ed.sigma_c0 = r->sigma_c0[s];
+        ed.sigma_c4 = r->sigma_c4[s];
+        ed.use_weight_image = 0;
+        ed.use_weight_tensor = 0;
+        for (int d = 0; d < 3; ++d) {
+            ed.weight_image_geometry.size[d] = 1;
+            ed.weight_image_geometry.spacing[d] = 1.0;
+            ed.weight_tensor_geometry.size[d] = 1;
+            ed.weight_tensor_geometry.spacing[d] = 1.0;
+        }
+        ed.moving_coefficients = coeffs.data();
+        ed.moving_geometry = *geometry;
+        ed.fixed_image = tar_s.data();
+        ed.fixed_geometry = *geometry;
+        ed.cp_geometry = cpg;
+        ed.cpw_geometry = cpg;
+        skm_evaluator *ev = nullptr;
+        if ((rc = skm_evaluator_create(&ed, &ev))) return rc;
+
+        skm_metric_desc md{};
+        md.metric = r->metric;
+        md.reg_l1 = r->reg_l1[s];
+        md.reg_l21 = r->reg_l21[s];
+        md.reg_l2 = r->reg_l2[s];
+        md.reg_rkhs = r->reg_rkhs[s];
+        md.reg_rd = r->reg_rd[s];
+        md.reg_rd_scaling = r->reg_rd_scaling[s];
+        md.reg_pg = r->reg_pg[s];
+        md.reg_pg_scaling = r->reg_pg_scaling[s];
+        md.use_negative_gradient = 1;
+        md.do_resampling = 1;
+        const bool only_l1 = md.reg_l1 > 0 && md.reg_l21 <= 0 && md.reg_l2 <= 0 && md.reg_rkhs <= 0 &&
+                             md.reg_rd <= 0 && md.reg_pg <= 0;
+        const bool only_l21 = md.reg_l1 <= 0 && md.reg_l21 > 0 && md.reg_l2 <= 0 && md.reg_rkhs <= 0 &&
+                              md.reg_rd <= 0 && md.reg_pg <= 0;
+        skm_optimizer_desc od{};
+        od.a = r->initial_step_size[s];
+        od.A = 20.0;
+        od.alpha = 1.0;
+        od.f_max = 1e7;
+        od.f_min = -1e6;
+        od.omega = 1.0;
+        od.orthant_projection = (only_l1 || only_l21) ? 1 : 0;
+        od.number_of_iterations = r->num_function_evaluations[s];
+        od.return_best_parameters_and_value = 1;
+
+        skm_field df{};
+        df.data = s > 0 ? past.data() : nullptr;
+        df.geometry = *geometry;
+        skm_optimizer *opt = nullptr;
+        rc = skm_optimizer_create(ev, &od, &md, params.data(), cpw.data(), &df, &opt);
+        skm_optimizer_state st{};
+        if (!rc) rc = skm_optimizer_run(opt, r->num_function_evaluations[s]);
+        if (!rc) rc = skm_optimizer_get_parameters(opt, 1, best.data());
+        if (!rc) rc = skm_optimizer_get_state(opt, &st);
+        if (opt) skm_optimizer_destroy(opt);
+        if (rc) {
+            skm_evaluator_destroy(ev);
+            return rc;
+        }
+        // summed displacement field on the reference grid (SKMReg.cxx:452-460): planar -> AoS
+        std::vector<double> cp_aos((size_t)C * D);
+        for (long long i = 0; i < C; ++i)
+            for (int d = 0; d < D; ++d) cp_aos[(size_t)(i * D + d)] = best[(size_t)(d * C + i)];
+        rc = skm_evaluate_displacement_field(ev, cp_aos.data(), cpw.data(), &df, now.data());
+        skm_evaluator_destroy(ev);
+        if (rc) return rc;
+        past.swap(now);
+        rep.levels_done = s + 1;
+        rep.best_value[s] = st.best_value;
+        rep.iterations[s] = st.iteration;
+        rep.control_points[s] = C;
+        rep.seconds[s] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    std::memcpy(displacement, past.data(), sizeof(double) * n * D);
+    if (report) *report = rep;
+    return SKM_OK;
+}

@@ -68,6 +68,12 @@ def lib():
         L.skm_optimizer_get_state.argtypes = [C.c_void_p, C.POINTER(OptimizerState)]
         L.skm_optimizer_destroy.argtypes = [C.c_void_p]
         L.skm_bspline_coefficients.argtypes = [C.c_int32, C.POINTER(C.c_int32), _dp, _dp]
+        L.skm_gaussian_smooth.argtypes = [C.c_int32, C.POINTER(abi.Geometry), C.c_double, C.c_int32, C.c_double,
+                                          C.c_int32, _dp, _dp]
+        L.skm_threshold_rescale.argtypes = [C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_double,
+                                            C.c_double, C.c_double, _dp, _dp]
+        L.skm_register.argtypes = [C.POINTER(abi.RegisterDesc), C.POINTER(abi.Geometry), _dp, _dp, _dp,
+                                   C.POINTER(abi.RegisterReport)]
         _lib = L
     return _lib
 

@@ -1,0 +1,126 @@
+"""Multi-scale registration (the scale loop of src/SKMReg.cxx) and its preprocessing, on the GPU.
+
+``register(reference, target, spacing, origin, config)`` runs ``skm_register``: threshold +
+rescale, then per scale level Gaussian smoothing, B-spline prefilter, control-point grid,
+evaluator with the previous levels' displacement field and the device-resident adaptive-step
+optimizer.  ``config`` uses the reference's option names (include/ConfigUtils.h:29-62); a list
+value gives one entry per scale and its last entry repeats for later scales (the CURRENT macro,
+src/SKMReg.cxx:48-49).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .abi import Geometry, RegisterDesc, RegisterReport, dptr
+from .evaluator import check, lib
+
+# include/ConfigUtils.h:29-62, the options this driver uses (no weight image, no covariance tensor)
+DEFAULT_CONFIG = {
+    "sigma_C4": [64, 32, 16],
+    "sigma_C0": [128, 64, 32],
+    "cp_spacing_scaler": 4.0,
+    "reg_l1": [0, 0, 0],
+    "reg_l21": [0, 0, 0],
+    "reg_l2": [0, 0, 0],
+    "reg_rkhs": [0, 0, 0],
+    "reg_rd": [0, 0, 0],
+    "reg_rd_scaling": [1, 1, 1],
+    "reg_pg": [0, 0, 0],
+    "reg_pg_scaling": [1, 1, 1],
+    "num_scales": 3,
+    "num_function_evaluations": [500, 500, 500],
+    "initial_step_size": [0.1, 0.1, 0.1],
+    "metric": "mse",
+    "sampling_rate": [5, 4, 3],
+    "neighborhood_sampling": [15, 12, 9],
+    "intensity_thresholds": [-1500, 3500],
+    "smoothing_variance": [2, 1, 0],
+    "tensor_weights": [0, 0, 0],
+}
+
+PER_SCALE = ["sigma_C4", "sigma_C0", "reg_l1", "reg_l21", "reg_l2", "reg_rkhs", "reg_rd", "reg_rd_scaling", "reg_pg",
+             "reg_pg_scaling", "num_function_evaluations", "initial_step_size", "sampling_rate",
+             "neighborhood_sampling", "smoothing_variance", "tensor_weights"]
+_FIELD = {"sigma_C4": "sigma_c4", "sigma_C0": "sigma_c0"}
+
+
+def current(config, option, scale):
+    """config[option][min(scale, len - 1)] (src/SKMReg.cxx:48-49); scalars apply to every scale."""
+    v = config[option]
+    if isinstance(v, (list, tuple)):
+        return v[min(scale, len(v) - 1)]
+    return v
+
+
+def full_config(config=None):
+    c = dict(DEFAULT_CONFIG)
+    if config:
+        c.update(config)
+    return c
+
+
+def make_desc(config, D) -> RegisterDesc:
+    c = full_config(config)
+    n = int(c["num_scales"])
+    if not 1 <= n <= abi.MAX_SCALES:
+        raise ValueError("num_scales must be in [1, %d]" % abi.MAX_SCALES)
+    if any(current(c, "tensor_weights", s) != 0 for s in range(n)):
+        raise ValueError("tensor_weights > 0 needs the covariance-tensor builder (not available); set them to 0")
+    d = RegisterDesc()
+    d.dimensions = D
+    d.num_scales = n
+    d.metric = abi.METRICS[c["metric"]]
+    d.cp_spacing_scaler = float(c["cp_spacing_scaler"])
+    th = c.get("intensity_thresholds") or []
+    d.apply_threshold = int(len(th) == 2)
+    if len(th) == 2:
+        d.threshold_min, d.threshold_max = float(th[0]), float(th[1])
+    for opt in PER_SCALE:
+        if opt == "tensor_weights":
+            continue
+        arr = getattr(d, _FIELD.get(opt, opt))
+        for s in range(abi.MAX_SCALES):
+            arr[s] = current(c, opt, min(s, n - 1))
+    return d
+
+
+def register(reference, target, spacing=None, origin=None, config=None):
+    """Registers `reference` (moving) onto `target` (fixed); both arrays (Z, Y, X) or (Y, X) with
+    the same geometry.  Returns (displacement (..., D) on that grid, report dict)."""
+    ref = np.ascontiguousarray(reference, np.float64)
+    tar = np.ascontiguousarray(target, np.float64)
+    if ref.shape != tar.shape:
+        raise ValueError("reference and target must share their grid")
+    D = ref.ndim
+    geo = Geometry.make(tuple(reversed(ref.shape)), origin, spacing)
+    desc = make_desc(config, D)
+    disp = np.zeros(ref.shape + (D,))
+    rep = RegisterReport()
+    check(lib().skm_register(C.byref(desc), C.byref(geo), dptr(ref), dptr(tar), dptr(disp), C.byref(rep)))
+    return disp, rep.as_dict()
+
+
+def gaussian_smooth(image, spacing=None, variance=1.0, use_image_spacing=True, maximum_error=0.01,
+                    maximum_kernel_width=64):
+    """GaussianSmoothing (include/itkUtils.h:139-150) on the GPU."""
+    img = np.ascontiguousarray(image, np.float64)
+    geo = Geometry.make(tuple(reversed(img.shape)), None, spacing)
+    out = np.empty_like(img)
+    check(lib().skm_gaussian_smooth(img.ndim, C.byref(geo), float(variance), int(bool(use_image_spacing)),
+                                    float(maximum_error), int(maximum_kernel_width), dptr(img), dptr(out)))
+    return out
+
+
+def threshold_rescale(image, thresholds=(-1500, 3500), out_range=(0.0, 1.0)):
+    """ThresholdImage + RescaleImage (include/itkUtils.h:45-110) on the GPU; thresholds None: rescale only."""
+    img = np.ascontiguousarray(image, np.float64)
+    size = (C.c_int32 * 3)(*(list(reversed(img.shape)) + [1] * (3 - img.ndim)))
+    out = np.empty_like(img)
+    apply = thresholds is not None and len(thresholds) == 2
+    tmin, tmax = (float(thresholds[0]), float(thresholds[1])) if apply else (0.0, 0.0)
+    check(lib().skm_threshold_rescale(img.ndim, size, int(apply), tmin, tmax, float(out_range[0]),
+                                      float(out_range[1]), dptr(img), dptr(out)))
+    return out
