@@ -24,6 +24,7 @@ NCC statistics + control-point derivative + regularizer + parameter update.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import math
 import os
@@ -50,6 +51,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ncc128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-multiscale", action="store_true",
+                    help="skip the multi-scale registration comparison (s/pair)")
     ap.add_argument("--gemm", default="auto", choices=["auto", "cuda"],
                     help="table-path GEMMs: auto = tensor cores where they fit, cuda = CUDA-core kernels")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps (capped at 300)")
@@ -274,6 +277,113 @@ def reference_cuda_rate(pb, mdesc, budget_s=20.0, max_steps=50):
 
 
 # ------------------------------------------------------------------------------------------------
+# ------------------------------------------------------------------------------------------------
+# multi-scale registration of the ncc128 pair: ours (skm_register) against the same scale loop
+# driven by the reference's own GpuKernelEvaluator (host optimizer loop as in the ITK glue,
+# reference B-spline prefilter compiled for the host, FP64 smoothing / threshold restatements
+# standing in for the ITK filters)
+MS_CONFIG = dict(num_scales=3, sigma_C4=[48, 24, 12], sigma_C0=[96, 48, 24], cp_spacing_scaler=3.0,
+                 smoothing_variance=[2, 1, 0], sampling_rate=[1], neighborhood_sampling=[1],
+                 num_function_evaluations=[100, 100, 100], metric="ncc", reg_rd=[1e-3],
+                 initial_step_size=[1000.0], tensor_weights=[0])
+
+
+def final_ncc(fixed, moving, disp, spacing):
+    """NCC of the rescaled pair with the moving image warped by `disp` (our evaluator, subsample 1)."""
+    from skmimageregistration_b200 import register as R
+    from skmimageregistration_b200.evaluator import GpuKernelEvaluator, bspline_coefficients
+    from skmimageregistration_b200.problem import Problem
+    f = R.threshold_rescale(fixed, MS_CONFIG.get("intensity_thresholds", (-1500, 3500)))
+    m = R.threshold_rescale(moving, MS_CONFIG.get("intensity_thresholds", (-1500, 3500)))
+    pb = Problem(fixed=f, moving_coefficients=bspline_coefficients(m), spacing=spacing, origin=(0.0,) * f.ndim,
+                 sigma_c0=24.0, sigma_c4=12.0, cp_spacing=4.0)
+    ev = GpuKernelEvaluator(pb)
+    r = ev.getValue(GpuKernelEvaluator.NCC, np.zeros((pb.C, pb.D)), np.ones(pb.C),
+                    np.ascontiguousarray(disp.reshape(-1, f.ndim)))
+    ev.close()
+    return -float(r["measure"])
+
+
+def reference_multiscale(fixed, moving, spacing, config):
+    """The scale loop with the reference's GpuKernelEvaluator; returns (displacement, seconds)."""
+    from oracle import multiscale as M
+    from oracle import oracle as O
+    from skmimageregistration_b200.problem import Problem
+    from skmimageregistration_b200.register import current, full_config
+    c = full_config(config)
+    D = fixed.ndim
+    host = O.ref_host(D)
+    t0 = time.perf_counter()
+    th = c.get("intensity_thresholds") or []
+    ref = M.threshold_rescale(moving, th if len(th) == 2 else None)
+    tar = M.threshold_rescale(fixed, th if len(th) == 2 else None)
+    past = None
+    for s in range(int(c["num_scales"])):
+        var = float(current(c, "smoothing_variance", s))
+        ref_s = M.gaussian_smooth(ref, spacing, var) if var > 1e-5 else ref
+        tar_s = M.gaussian_smooth(tar, spacing, var) if var > 1e-5 else tar
+        coeffs = np.zeros(tuple(n + 3 for n in ref_s.shape))
+        size = (C.c_int32 * 3)(*(list(reversed(ref_s.shape)) + [1] * (3 - D)))
+        host.skmref_bspline_coefficients(size, ref_s.ctypes.data_as(C.POINTER(C.c_double)),
+                                         coeffs.ctypes.data_as(C.POINTER(C.c_double)))
+        s4, s0 = float(current(c, "sigma_C4", s)), float(current(c, "sigma_C0", s))
+        cps = float(np.float32(min(s4, s0)) / np.float32(c["cp_spacing_scaler"]))
+        pb = Problem(fixed=tar_s, moving_coefficients=coeffs, spacing=spacing, origin=(0.0,) * D, sigma_c0=s0,
+                     sigma_c4=s4, cp_spacing=cps, subsample=int(current(c, "sampling_rate", s)),
+                     subsample_neighborhood=int(current(c, "neighborhood_sampling", s)))
+        rg = O.RefGpu(pb, double=True)
+        w_rd = float(current(c, "reg_rd", s))
+        rg.set_regularizers(0.0, w_rd, float(current(c, "reg_rd_scaling", s)), 0.0, 1.0)
+        metric = {"mse": 0, "ncc": 1, "lcc": 2}[c["metric"]]
+        a, n_it = float(current(c, "initial_step_size", s)), int(current(c, "num_function_evaluations", s))
+        P, Cn = pb.num_parameters, pb.C
+        pos, base, prev, best = np.zeros(P), np.zeros(P), np.zeros(P), np.zeros(P)
+        t_sim, best_v, cpw = 0.0, np.inf, np.ones(Cn)
+        dfg = pb.fixed_geometry() if past is not None else None
+        for _ in range(n_it):                            # the ITK v4 loop with the adaptive step
+            r, g = rg.evaluate(metric, pos.reshape(D, Cn).T, cpw, past, dfg)
+            value = r["measure"] + w_rd * r["reg_value_rd"]
+            g = -g
+            lr = a / (20.0 + t_sim + 1.0)
+            sp = float(np.dot(g, prev))
+            prev = g
+            pos = base + g * lr
+            base = pos
+            t_sim = max(0.0, t_sim - 1e6 + (1e7 + 1e6) / (1.0 + 10.0 * math.exp(min(sp, 700.0))))
+            if value < best_v:
+                best_v, best = value, pos.copy()
+        past = rg.displacement_field(np.ascontiguousarray(best.reshape(D, Cn).T), cpw, past, dfg)
+        past = np.ascontiguousarray(past.reshape(fixed.shape + (D,)))
+        rg.close()
+    return past, time.perf_counter() - t0
+
+
+def multiscale_compare():
+    """s/pair of the multi-scale registration for both drivers and the NCC each reaches."""
+    from skmimageregistration_b200 import register as R
+    from skmimageregistration_b200 import synth
+    fixed, moving, _ = synth.ellipsoids3d(seed=0, shape=(96, 128, 128))
+    spacing = (1.0, 1.0, 1.0)
+    R.register(moving[::4, ::4, ::4].copy(), fixed[::4, ::4, ::4].copy(), spacing, None,
+               dict(MS_CONFIG, num_function_evaluations=[2], sigma_C4=[12], sigma_C0=[24]))   # warm-up
+    t0 = time.perf_counter()
+    disp, rep = R.register(moving, fixed, spacing, None, MS_CONFIG)
+    ours_s = time.perf_counter() - t0
+    out = {"config": dict(MS_CONFIG, volume="128x128x96"), "ours_s_per_pair": ours_s,
+           "ours_final_ncc": final_ncc(fixed, moving, disp, spacing), "ncc_before": final_ncc(fixed, moving,
+                                                                                              0 * disp, spacing),
+           "ours_levels": rep}
+    from oracle import oracle as O  # noqa: F401  (reference arm: needs the reference build)
+    if os.path.exists(O.ref_gpu_path(3, True)):
+        disp_r, ref_s = reference_multiscale(fixed, moving, spacing, MS_CONFIG)
+        out["reference_s_per_pair"] = ref_s
+        out["reference_final_ncc"] = final_ncc(fixed, moving, disp_r, spacing)
+        out["within_1e-3"] = bool(out["ours_final_ncc"] >= out["reference_final_ncc"] - 1e-3)
+        out["s_per_pair_to_reference_ncc"] = ours_s if out["within_1e-3"] else None
+        out["speedup"] = ref_s / ours_s
+    return out
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -465,6 +575,8 @@ def run_ours(args, rank, world, local_rank):
     opt.close()
     ev.close()
     ev2.close()
+    if rank == 0 and world == 1 and not args.no_multiscale:
+        line["multiscale"] = multiscale_compare()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O  # noqa: F401  (CPU baseline leg only)
         rate, steps, el, threads = cpu_port_rate(pb, mdesc, budget_s=15.0, max_steps=5)
