@@ -111,6 +111,7 @@ unsigned long long rng_advance_host(unsigned long long s, unsigned long long ste
 
 constexpr int kValueThreads = 256;
 constexpr int kDerivThreads = 256;     // 8 warps = 8 control points per block
+constexpr int kSplitBelowBlocks = 1024; // fewer derivative blocks than this: one block per control point
 
 }  // namespace
 
@@ -224,9 +225,12 @@ struct LaunchLccValue {
 
 template <int D, int KIND>
 struct LaunchDeriv {
-    static int run(skm_evaluator *e, DerivParams Q)
+    static int run(skm_evaluator *e, DerivParams Q, bool split)
     {
-        derivative_kernel<D, KIND><<<e->deriv_blocks, kDerivThreads, 0, e->stream>>>(e->P, Q);
+        if (split)
+            derivative_kernel<D, KIND, 8><<<(int)e->C, kDerivThreads, 0, e->stream>>>(e->P, Q);
+        else
+            derivative_kernel<D, KIND, 1><<<e->deriv_blocks, kDerivThreads, 0, e->stream>>>(e->P, Q);
         SKM_CHECK_LAUNCH();
         return SKM_OK;
     }
@@ -425,7 +429,8 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         if (dalloc(&e->d_counters, 4)) return SKM_ERR_CUDA;
         SKM_CUDA(cudaMemset(e->d_counters, 0, 4 * sizeof(unsigned)));
         if (dalloc(&e->d_deriv, e->nparams)) return SKM_ERR_CUDA;
-        if (dalloc(&e->d_rpart, (size_t)NR * std::max(e->deriv_blocks, e->gather_blocks))) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_rpart, (size_t)NR * std::max<long long>(e->C, std::max(e->deriv_blocks, e->gather_blocks))))
+            return SKM_ERR_CUDA;
         if (dalloc(&e->d_out, NO)) return SKM_ERR_CUDA;
         SKM_CUDA(cudaMallocHost((void **)&e->h_in, sizeof(double) * e->C * (D + 1)));
         SKM_CUDA(cudaMallocHost((void **)&e->h_out, sizeof(double) * (e->nparams + NO)));
@@ -664,13 +669,15 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     Q.out = e->d_out;
     Q.counter = e->d_counters + 1;
     bool any_reg = w.rkhs > 0 || w.rd > 0 || w.pg > 0 || w.with_metric;
+    // few control points (coarse levels): a block per control point keeps every SM busy
+    const bool split = derivative && !tab && metric != SKM_LCC && e->deriv_blocks < kSplitBelowBlocks;
     if (derivative) {
         if (tab) {
             if (table_derivative(e->table, tc_of(e), e->P, Q, D, e->gather_blocks, e->stream, ev ? ev[3] : nullptr))
                 return fail(SKM_ERR_CUDA, "table derivative: %s", cudaGetErrorString(cudaGetLastError()));
         } else {
             if (ev) SKM_CUDA(cudaEventRecord(ev[3], e->stream));
-            if ((rc = dispatch<LaunchDeriv>(D, kind, e, Q))) return rc;
+            if ((rc = dispatch<LaunchDeriv>(D, kind, e, Q, split))) return rc;
         }
     } else if (any_reg && tab) {
         // values only, through the same gather (and the same sums) as the derivative call, so
@@ -685,7 +692,8 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     if (ev) SKM_CUDA(cudaEventRecord(ev[4], e->stream));
     if (!((derivative || any_reg) && tab)) {    // the table gather computes the result itself
         result_kernel<<<1, 256, 0, e->stream>>>(e->d_stats, (derivative || any_reg) ? e->d_rpart : nullptr,
-                                               e->deriv_blocks, w.rkhs, w.rd, w.pg, w.l1, w.l21, w.l2, e->d_out,
+                                               split ? (int)e->C : e->deriv_blocks, w.rkhs, w.rd, w.pg, w.l1,
+                                               w.l21, w.l2, e->d_out,
                                                tab ? e->table.dev.tc_err : nullptr);
         SKM_CHECK_LAUNCH();
     }

@@ -509,12 +509,16 @@ __device__ __forceinline__ void lcc_sample_derivative(const EvalParams &P, const
     }
 }
 
-template <int D, int KIND>
+// SPLIT = 1: one warp per control point (8 per block).  SPLIT = 8 (few control points, MSE/NCC):
+// one block per control point, its 8 warps take interleaved z-planes of the support box and their
+// sums are combined in warp order, so results stay deterministic.
+template <int D, int KIND, int SPLIT = 1>
 __global__ void __launch_bounds__(256) derivative_kernel(EvalParams P, DerivParams Q)
 {
     __shared__ double shv[NR][8];
+    __shared__ float sacc[8][3];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const long long j_lin = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    const long long j_lin = SPLIT > 1 ? (long long)blockIdx.x : (long long)blockIdx.x * (blockDim.x >> 5) + wib;
     double val[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) val[k] = 0.0;
@@ -545,7 +549,7 @@ __global__ void __launch_bounds__(256) derivative_kernel(EvalParams P, DerivPara
                 base[d] = (float)(gp[d] - (P.fixed.o[d] + P.fixed.s[d] * (double)base_pos[d]));
                 hs[d] = (float)P.fixed.s[d];
             }
-            for (int zz = 0; zz < nz; ++zz) {
+            for (int zz = SPLIT > 1 ? wib : 0; zz < nz; zz += SPLIT) {
                 const int z = lo[2] + zz;
                 int x = lane % nx, y = lane / nx;              // lane position in the (y,x) plane
                 for (int t = lane; t < per_plane; t += 32) {
@@ -586,7 +590,7 @@ __global__ void __launch_bounds__(256) derivative_kernel(EvalParams P, DerivPara
                     while (x >= nx) { x -= nx; ++y; }
                 }
             }
-        } else {
+        } else if (SPLIT == 1) {
             // LCC: lanes over the samples of the box, each lane walks its sample's window
             to_local<D>(P.fixed, gp, ip);
             int lo[3], hi[3];
@@ -609,9 +613,21 @@ __global__ void __launch_bounds__(256) derivative_kernel(EvalParams P, DerivPara
         }
 #pragma unroll
         for (int d = 0; d < D; ++d) acc[d] = warp_sum(acc[d]);
+        if (SPLIT > 1) {                                   // the block's warps in a fixed order
+            if (lane == 0)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) sacc[wib][d] = acc[d];
+            __syncthreads();
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                float t = 0.f;
+                for (int w = 0; w < SPLIT; ++w) t += sacc[w][d];
+                acc[d] = t;
+            }
+        }
 
         float drk[3] = {0.f, 0.f, 0.f}, drd[3] = {0.f, 0.f, 0.f}, dpg[3] = {0.f, 0.f, 0.f};
-        if (Q.reg_rkhs > 0.0 || Q.reg_rd > 0.0 || Q.reg_pg > 0.0) {
+        if ((SPLIT == 1 || wib == 0) && (Q.reg_rkhs > 0.0 || Q.reg_rd > 0.0 || Q.reg_pg > 0.0)) {
             regularizers_of<D, KIND>(P, Q, j, j_lin, gp, pj, cj, lane, val, drk, drd, dpg);
 #pragma unroll
             for (int d = 0; d < D; ++d) {
@@ -622,7 +638,7 @@ __global__ void __launch_bounds__(256) derivative_kernel(EvalParams P, DerivPara
 #pragma unroll
             for (int k = R_RKHS; k <= R_PG; ++k) val[k] = warp_sum(val[k]);
         }
-        if (lane == 0) {
+        if (lane == 0 && (SPLIT == 1 || wib == 0)) {
             const double n = st[S_COUNT];
             double pc[3] = {0, 0, 0}, pn2 = 0.0;
             if (Q.with_metric) {
