@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define SKM_ABI_VERSION 1
+#define SKM_ABI_VERSION 2
 
 /* Status codes. */
 #define SKM_OK              0
@@ -330,6 +330,17 @@ typedef struct skm_register_desc {
     double  reg_l1[SKM_MAX_SCALES], reg_l21[SKM_MAX_SCALES], reg_l2[SKM_MAX_SCALES];
     double  reg_rkhs[SKM_MAX_SCALES], reg_rd[SKM_MAX_SCALES], reg_rd_scaling[SKM_MAX_SCALES];
     double  reg_pg[SKM_MAX_SCALES], reg_pg_scaling[SKM_MAX_SCALES];
+    /* kernel weighting (SKMReg.cxx:245-297; all images on the reference/target grid):
+     * tensor_weights[s] > 0: covariance tensor of level s computed by skm_anisotropic_tensor from
+     *   guidance_image (the reference's weight_tensor_filename read as an image, case 4) or, when
+     *   that is NULL, from the level's smoothed target (case 3);
+     * tensor_weights[s] == 0 and weight_tensor: that external tensor (case 2), N x D x D doubles;
+     * weight_image (the reference's weight_filename): N doubles > 1e-8, read by the kernel before
+     *   any tensor. */
+    double  tensor_weights[SKM_MAX_SCALES];
+    const double *guidance_image;
+    const double *weight_tensor;
+    const double *weight_image;
 } skm_register_desc;
 
 typedef struct skm_register_report {
@@ -345,10 +356,20 @@ typedef struct skm_register_report {
  * displacement field, device-resident adaptive-step optimizer, summed displacement field.
  * Reference (moving) and target (fixed) share `geometry` (the reference writes the field of the
  * target grid into a reference-sized image, GenerateDisplacementFieldGpu, itkUtils.h:181-253).
- * No weight image or covariance tensor (tensor_weights 0).  displacement: N x D doubles, x
- * fastest, AoS. */
+ * displacement: N x D doubles, x fastest, AoS. */
 int skm_register(const skm_register_desc *desc, const skm_geometry *geometry, const double *reference,
                  const double *target, double *displacement, skm_register_report *report);
+
+/* ComputeAnisotropicTensor (include/AnisotropicTensorUtils.h:37-371) with anisotropic_filtering
+ * false, as src/SKMReg.cxx:271 and :284 call it: weight * image smoothed with variance sigma,
+ * gradient outer product, each component smoothed with variance sigma / 4, eigen system ordered by
+ * magnitude, main direction damped by its alignment with axis alignment_direction (0 x, 1 y,
+ * 2 z; none when negative or >= dimensions), covariance U diag(s) U^T.  covariance: N x D x D
+ * doubles, row-major per texel.  maximum_tilt (may be NULL): the largest damped main eigenvalue
+ * over the texels whose eigenvalues all exceed 1e-8 in magnitude, -DBL_MAX when none do.
+ * SKM_ERR_INVALID where a covariance is not positive definite (the reference prints and stops). */
+int skm_anisotropic_tensor(int32_t dimensions, const skm_geometry *geometry, const double *image, double sigma,
+                           double weight, int32_t alignment_direction, double *covariance, double *maximum_tilt);
 
 /* ------------------------------------------------------------------------- */
 /* Metric value without any device allocation.  No counterpart in the reference.

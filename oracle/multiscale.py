@@ -6,7 +6,12 @@ product.  Follows
     discrete Gaussian e^-t I_n(t), t = variance / spacing^2, grown until 1 - maximum_error of the
     mass, half width <= maximum_kernel_width, normalised; edge voxels repeated);
   * ThresholdImage + RescaleImage, include/itkUtils.h:45-110;
-  * the scale loop of src/SKMReg.cxx:84-500 with the FP64 evaluator and optimizer of oracle.py.
+  * ComputeAnisotropicTensor, include/AnisotropicTensorUtils.h:37-371 (anisotropic_filtering false,
+    as src/SKMReg.cxx:271 calls it): structure tensor, eigen system ordered by magnitude
+    (include/itkSymmetricEigenDecompositionImageFilter.h, here numpy.linalg.eigh), direction
+    weighting and covariance;
+  * the scale loop of src/SKMReg.cxx:84-500 with the FP64 evaluator and optimizer of oracle.py,
+    including the kernel weighting of :245-297.
 ITK itself is not in this container: the ITK filters are restated from their published
 algorithms (exact Bessel values, scipy.special.ive), so agreement with ITK is unpinned.
 """
@@ -19,6 +24,7 @@ from scipy.special import ive
 
 from skmimageregistration_b200.abi import METRICS, MetricDesc, OptimizerDesc
 from skmimageregistration_b200.problem import Problem, control_point_grid
+from skmimageregistration_b200.register import current, full_config
 
 from . import oracle as O
 
@@ -79,9 +85,127 @@ def threshold_rescale(image, thresholds=(-1500, 3500), out_range=(0.0, 1.0)):
     return np.clip(v, lo, hi) * scale + (omin - lo * scale)
 
 
-def register(reference, target, spacing, origin, config):
+def image_gradient(image, spacing):
+    """itk::GradientImageFilter as ComputeAnisotropicTensor uses it (include/AnisotropicTensorUtils.h:65-68):
+    per axis (f[i+1] - f[i-1]) / (2 spacing), an edge texel's missing neighbour replaced by the
+    texel itself (zero-flux Neumann).  Returns (..., D), component 0 = x."""
+    f = np.asarray(image, np.float64)
+    D = f.ndim
+    g = np.empty(f.shape + (D,))
+    for d in range(D):
+        ax = D - 1 - d
+        n = f.shape[ax]
+        idx = np.arange(n)
+        hi = np.take(f, np.minimum(idx + 1, n - 1), axis=ax)
+        lo = np.take(f, np.maximum(idx - 1, 0), axis=ax)
+        g[..., d] = (hi - lo) / (2.0 * float(spacing[d]))
+    return g
+
+
+def structure_tensor(image, spacing, sigma, weight):
+    """K_{sigma/4} * (grad u_sigma grad u_sigma^T) of weight * image (AnisotropicTensorUtils.h:54-155):
+    smoothing with variance sigma, gradient, outer product, every component smoothed with variance
+    sigma / 4.  Returns (..., D, D)."""
+    f = np.asarray(image, np.float64) * float(weight)
+    D = f.ndim
+    g = image_gradient(gaussian_smooth(f, spacing, float(sigma)), spacing)
+    T = np.empty(f.shape + (D, D))
+    for i in range(D):
+        for j in range(i, D):
+            T[..., i, j] = gaussian_smooth(g[..., i] * g[..., j], spacing, float(sigma) / 4.0)
+            T[..., j, i] = T[..., i, j]
+    return T
+
+
+def covariance_from_structure(T, alignment_direction=2):
+    """The per-texel steps of ComputeAnisotropicTensor after the structure tensor
+    (AnisotropicTensorUtils.h:160-371), on (..., D, D) structure tensors.
+
+    Eigen decomposition ordered by magnitude, rows = eigenvalue * eigenvector
+    (include/itkSymmetricEigenDecompositionImageFilter.h); where every row is longer than 1e-8 the
+    main (largest) row is weighted by (|n x e_align| + 1e-10)^2 / sqrt(D) (only for an alignment
+    axis < D), p = |main row|^1.5, the main direction gets length 1/(1+p), the others
+    1 + p/(1+p), else the identity; then the rows are flipped and transposed and the covariance is
+    U diag(column norms) U^T (:316-360).  Returns (covariance (..., D, D), maximum tilt = the largest
+    |main row| over the texels that passed, -DBL_MAX when none did, number of non-positive
+    determinants)."""
+    T = np.asarray(T, np.float64)
+    D = T.shape[-1]
+    shape = T.shape[:-2]
+    flat = T.reshape(-1, D, D)
+    lam, vec = np.linalg.eigh(flat)                        # columns of vec are eigenvectors
+    order = np.argsort(np.abs(lam), axis=1, kind="stable")
+    lam = np.take_along_axis(lam, order, 1)
+    vec = np.take_along_axis(vec, order[:, None, :], 2)
+    rows = vec.transpose(0, 2, 1) * lam[:, :, None]        # row k = lam_k v_k, |lam| ascending
+    mag = np.linalg.norm(rows, axis=2)
+    ok = np.all(mag > 1e-8, axis=1)
+    safe = np.where(mag > 0, mag, 1.0)
+    normalized = rows[:, D - 1, :] / safe[:, D - 1:D]
+    main = rows[:, D - 1, :].copy()
+    if 0 <= alignment_direction < D:
+        md = np.zeros(D)
+        md[alignment_direction] = 1.0
+        if D == 2:
+            cross = np.abs(normalized[:, 0] * md[1] - normalized[:, 1] * md[0])
+        else:
+            cross = np.linalg.norm(np.cross(normalized, md), axis=1)
+        factor = (cross + 1e-10) ** 2 / math.sqrt(D)
+        main = main * factor[:, None]
+    rev = np.linalg.norm(main, axis=1)
+    p = rev ** 1.5
+    new = np.empty_like(rows)
+    new[:, D - 1, :] = normalized / (1.0 + p)[:, None]
+    for k in range(D - 1):
+        new[:, k, :] = rows[:, k, :] / safe[:, k:k + 1] * (1.0 + p / (1.0 + p))[:, None]
+    M = new[:, ::-1, :].transpose(0, 2, 1)                 # flipud().transpose(): column 0 = main
+    M = np.where(ok[:, None, None], M, np.eye(D)[None])
+    max_tilt = float(rev[ok].max()) if ok.any() else -np.finfo(np.float64).max
+    s = np.linalg.norm(M, axis=1)                          # column norms
+    U = M / np.where(s > 0, s, 1.0)[:, None, :]
+    cov = np.einsum("nik,nk,njk->nij", U, s, U)
+    cov = np.where((s[:, 0] < 1e-8)[:, None, None], np.eye(D)[None], cov)
+    bad = int(np.count_nonzero(~(np.linalg.det(cov) > 0)))
+    return cov.reshape(shape + (D, D)), max_tilt, bad
+
+
+def anisotropic_tensor(image, spacing, sigma, weight, alignment_direction=2):
+    """ComputeAnisotropicTensor (include/AnisotropicTensorUtils.h:37-371) with anisotropic_filtering
+    false, as src/SKMReg.cxx:271 and :284 call it: (covariance (..., D, D), maximum tilt)."""
+    cov, tilt, bad = covariance_from_structure(structure_tensor(image, spacing, sigma, weight), alignment_direction)
+    if bad:
+        raise ValueError("covariance tensor not positive definite at %d texels" % bad)
+    return cov, tilt
+
+
+def level_weighting(tar_s, spacing, c, s, guidance_image=None, weight_tensor=None, weight_image=None):
+    """Problem keyword arguments for the kernel weighting of level s (src/SKMReg.cxx:245-297 with
+    SetWeightingImage / SetWeightingTensor, include/itkTransformAdapter.hxx:312-365)."""
+    D = np.asarray(tar_s).ndim
+    tw = float(current(c, "tensor_weights", s))
+    tensor, weight, cov = None, None, None
+    if tw > 0:
+        src = tar_s if guidance_image is None else np.asarray(guidance_image, np.float64)
+        tensor, tilt = anisotropic_tensor(src, spacing, float(np.float32(current(c, "sigma_C4", s))), tw, 2)
+        weight, cov = (tilt, np.eye(D)) if tilt >= 0 else (1.0, np.eye(D))
+    elif tw == 0 and weight_tensor is not None:
+        tensor = np.asarray(weight_tensor, np.float64)
+        flat = tensor.reshape(-1, D, D)
+        if np.any(~(np.linalg.det(flat) > 0)):
+            raise ValueError("weighting tensors must be positive definite")
+        ev = np.abs(np.linalg.eigvalsh(flat)[:, -1])
+        k = int(np.argmax(ev))
+        weight, cov = float(ev[k]), flat[k].copy()
+    if weight_image is not None:
+        wi = np.asarray(weight_image, np.float64)
+        return dict(weight_image=wi, maximum_weight=weight if tensor is not None else float(wi.max()))
+    if tensor is not None:
+        return dict(weight_tensor=tensor, maximum_weight=weight, maximum_eigenvalue_covariance=cov)
+    return {}
+
+
+def register(reference, target, spacing, origin, config, guidance_image=None, weight_tensor=None, weight_image=None):
     """The scale loop with the FP64 evaluator / optimizer; returns (displacement, per-level best values)."""
-    from skmimageregistration_b200.register import current, full_config
     c = full_config(config)
     ref = np.asarray(reference, np.float64)
     tar = np.asarray(target, np.float64)
@@ -103,7 +227,8 @@ def register(reference, target, spacing, origin, config):
         cps = float(smin / np.float32(1.0)) if scaler < 1 else float(smin / np.float32(scaler))
         pb = Problem(fixed=tar_s, moving_coefficients=O.bspline_coefficients(ref_s), spacing=spacing, origin=origin,
                      sigma_c0=s0, sigma_c4=s4, cp_spacing=cps, subsample=int(current(c, "sampling_rate", s)),
-                     subsample_neighborhood=int(current(c, "neighborhood_sampling", s)))
+                     subsample_neighborhood=int(current(c, "neighborhood_sampling", s)),
+                     **level_weighting(tar_s, spacing, c, s, guidance_image, weight_tensor, weight_image))
         assert pb.cp_size == control_point_grid(tuple(reversed(ref.shape)), spacing, origin, cps)[0]
         regs = {k: float(current(c, "reg_" + k, s)) for k in ("l1", "l21", "l2", "rkhs", "rd", "rd_scaling", "pg",
                                                                "pg_scaling")}

@@ -225,6 +225,10 @@ class RegisterDesc(C.Structure):
         ("num_function_evaluations", _I), ("sampling_rate", _I), ("neighborhood_sampling", _I),
         ("reg_l1", _S), ("reg_l21", _S), ("reg_l2", _S), ("reg_rkhs", _S), ("reg_rd", _S),
         ("reg_rd_scaling", _S), ("reg_pg", _S), ("reg_pg_scaling", _S),
+        ("tensor_weights", _S),
+        ("guidance_image", C.POINTER(C.c_double)),
+        ("weight_tensor", C.POINTER(C.c_double)),
+        ("weight_image", C.POINTER(C.c_double)),
     ]
 
 

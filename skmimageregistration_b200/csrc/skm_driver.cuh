@@ -95,6 +95,118 @@ long long texel_count(int D, const int32_t *size)
     return n;
 }
 
+int grid_blocks(long long n, int per_sm)
+{
+    return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * per_sm));
+}
+
+// largest value of d_v[0..n) (the max of range_kernel)
+int device_max(const double *d_v, long long n, double *out, cudaStream_t s)
+{
+    const int blocks = grid_blocks(n, 4);
+    DevBuf part, res;
+    SKM_CUDA(cudaMalloc((void **)&part.p, sizeof(double) * 4 * blocks));
+    SKM_CUDA(cudaMalloc((void **)&res.p, sizeof(double) * 4));
+    skm::range_kernel<<<blocks, 256, 0, s>>>(d_v, n, 0.0, 0.0, part.p);
+    SKM_CHECK_LAUNCH();
+    skm::range_finish_kernel<<<1, 32, 0, s>>>(part.p, blocks, res.p);
+    SKM_CHECK_LAUNCH();
+    double r[4];
+    SKM_CUDA(cudaMemcpyAsync(r, res.p, sizeof r, cudaMemcpyDeviceToHost, s));
+    SKM_CUDA(cudaStreamSynchronize(s));
+    *out = r[1];
+    return SKM_OK;
+}
+
+// ComputeAnisotropicTensor (include/AnisotropicTensorUtils.h:37-371) with anisotropic_filtering
+// false, the form src/SKMReg.cxx:271 and :284 call: d_img (n texels, unchanged) -> d_cov (n x D x D
+// row-major) and the maximum tilt (largest |main row| after the alignment weighting over the texels
+// that passed the 1e-8 test; -DBL_MAX when none did).
+int anisotropic_tensor_device(int D, const int32_t *size, const double *spacing, const double *d_img, double sigma,
+                              double weight, int alignment, double *d_cov, double *max_tilt, cudaStream_t s)
+{
+    const int X = size[0], Y = D > 1 ? size[1] : 1, Z = D > 2 ? size[2] : 1;
+    const long long n = (long long)X * Y * Z;
+    const int nc = skm::tensor_components(D);
+    const int blocks = grid_blocks(n, 16);
+    DevBuf f, tmp, comp, tilt;
+    SKM_CUDA(cudaMalloc((void **)&f.p, n * sizeof(double)));
+    SKM_CUDA(cudaMalloc((void **)&tmp.p, n * sizeof(double)));
+    SKM_CUDA(cudaMalloc((void **)&comp.p, nc * n * sizeof(double)));
+    SKM_CUDA(cudaMalloc((void **)&tilt.p, n * sizeof(double)));
+    unsigned *d_bad = nullptr;
+    SKM_CUDA(cudaMalloc((void **)&d_bad, sizeof(unsigned)));
+    struct FreeBad {
+        unsigned *p;
+        ~FreeBad() { cudaFree(p); }
+    } free_bad{d_bad};
+    SKM_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(unsigned), s));
+    // weight * image, smoothed with variance sigma (:54-64)
+    skm::scale_kernel<<<blocks, 256, 0, s>>>(d_img, f.p, n, weight);
+    SKM_CHECK_LAUNCH();
+    int rc = smooth_device(D, size, spacing, sigma, 1, 0.01, 64, f.p, tmp.p, s);
+    if (rc) return rc;
+    // gradient outer product (:65-103), every component smoothed with variance sigma / 4 (:106-155)
+    if (D == 2)
+        skm::gradient_outer_kernel<2><<<blocks, 256, 0, s>>>(f.p, X, Y, Z, 2.0 * spacing[0], 2.0 * spacing[1], 1.0,
+                                                              comp.p);
+    else
+        skm::gradient_outer_kernel<3><<<blocks, 256, 0, s>>>(f.p, X, Y, Z, 2.0 * spacing[0], 2.0 * spacing[1],
+                                                              2.0 * spacing[2], comp.p);
+    SKM_CHECK_LAUNCH();
+    for (int k = 0; k < nc; ++k)
+        if ((rc = smooth_device(D, size, spacing, sigma / 4.0, 1, 0.01, 64, comp.p + k * n, tmp.p, s))) return rc;
+    // eigen analysis, direction weighting and covariance (:160-371)
+    if (D == 2)
+        skm::covariance_kernel<2><<<blocks, 256, 0, s>>>(comp.p, n, alignment, d_cov, tilt.p, d_bad);
+    else
+        skm::covariance_kernel<3><<<blocks, 256, 0, s>>>(comp.p, n, alignment, d_cov, tilt.p, d_bad);
+    SKM_CHECK_LAUNCH();
+    unsigned bad = 0;
+    SKM_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, s));
+    if ((rc = device_max(tilt.p, n, max_tilt, s))) return rc;
+    if (bad) return fail(SKM_ERR_INVALID, "covariance tensor not positive definite at %u texels", bad);
+    return SKM_OK;
+}
+
+// SetWeightingTensor with a negative tilt (itkTransformAdapter.hxx:341-361): the tensor whose
+// largest eigenvalue has the largest magnitude (the first such texel), after the determinant test.
+int max_eigenvalue_tensor(int D, long long n, const double *d_tensor, const double *h_tensor, double *maximum,
+                          double *cov_out, cudaStream_t s)
+{
+    DevBuf ev;
+    SKM_CUDA(cudaMalloc((void **)&ev.p, n * sizeof(double)));
+    unsigned *d_bad = nullptr;
+    SKM_CUDA(cudaMalloc((void **)&d_bad, sizeof(unsigned)));
+    struct FreeBad {
+        unsigned *p;
+        ~FreeBad() { cudaFree(p); }
+    } free_bad{d_bad};
+    SKM_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(unsigned), s));
+    const int blocks = grid_blocks(n, 16);
+    if (D == 2) skm::max_eigenvalue_kernel<2><<<blocks, 256, 0, s>>>(d_tensor, n, ev.p, d_bad);
+    else skm::max_eigenvalue_kernel<3><<<blocks, 256, 0, s>>>(d_tensor, n, ev.p, d_bad);
+    SKM_CHECK_LAUNCH();
+    std::vector<double> h((size_t)n);
+    unsigned bad = 0;
+    SKM_CUDA(cudaMemcpyAsync(h.data(), ev.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    SKM_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, s));
+    SKM_CUDA(cudaStreamSynchronize(s));
+    if (bad) return fail(SKM_ERR_INVALID, "weighting tensors must be positive definite (%u texels are not)", bad);
+    long long best = 0;
+    double mx = -DBL_MAX;
+    for (long long i = 0; i < n; ++i)
+        if (h[(size_t)i] > mx) {
+            mx = h[(size_t)i];
+            best = i;
+        }
+    *maximum = mx;
+    for (int k = 0; k < 9; ++k) cov_out[k] = 0.0;
+    for (int r = 0; r < D; ++r)
+        for (int c = 0; c < D; ++c) cov_out[r * D + c] = h_tensor[best * D * D + r * D + c];
+    return SKM_OK;
+}
+
 struct HostStream {
     cudaStream_t s = nullptr;
     ~HostStream()
@@ -149,6 +261,35 @@ extern "C" int skm_threshold_rescale(int32_t dimensions, const int32_t *size, in
     if (rc) return rc;
     SKM_CUDA(cudaMemcpyAsync(dst, a.p, n * sizeof(double), cudaMemcpyDeviceToHost, hs.s));
     SKM_CUDA(cudaStreamSynchronize(hs.s));
+    return SKM_OK;
+}
+
+extern "C" int skm_anisotropic_tensor(int32_t dimensions, const skm_geometry *geometry, const double *image,
+                                      double sigma, double weight, int32_t alignment_direction, double *covariance,
+                                      double *maximum_tilt)
+{
+    if (dimensions != 2 && dimensions != 3) return fail(SKM_ERR_INVALID, "dimensions must be 2 or 3");
+    if (!geometry || !image || !covariance) return fail(SKM_ERR_INVALID, "geometry / image / covariance is NULL");
+    if (!(sigma >= 0.0) || !std::isfinite(sigma) || !std::isfinite(weight))
+        return fail(SKM_ERR_INVALID, "sigma must be finite and >= 0, weight finite");
+    for (int d = 0; d < dimensions; ++d)
+        if (geometry->size[d] < 1 || !(geometry->spacing[d] > 0.0))
+            return fail(SKM_ERR_INVALID, "size and spacing must be positive");
+    const long long n = texel_count(dimensions, geometry->size);
+    const long long nt = n * dimensions * dimensions;
+    HostStream hs;
+    SKM_CUDA(cudaStreamCreateWithFlags(&hs.s, cudaStreamNonBlocking));
+    DevBuf img, cov;
+    SKM_CUDA(cudaMalloc((void **)&img.p, n * sizeof(double)));
+    SKM_CUDA(cudaMalloc((void **)&cov.p, nt * sizeof(double)));
+    SKM_CUDA(cudaMemcpyAsync(img.p, image, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
+    double tilt = -DBL_MAX;
+    int rc = anisotropic_tensor_device(dimensions, geometry->size, geometry->spacing, img.p, sigma, weight,
+                                       alignment_direction, cov.p, &tilt, hs.s);
+    if (rc) return rc;
+    SKM_CUDA(cudaMemcpyAsync(covariance, cov.p, nt * sizeof(double), cudaMemcpyDeviceToHost, hs.s));
+    SKM_CUDA(cudaStreamSynchronize(hs.s));
+    if (maximum_tilt) *maximum_tilt = tilt;
     return SKM_OK;
 }
 
@@ -237,6 +378,27 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
     DevBuf dsm;
     SKM_CUDA(cudaMalloc((void **)&dsm.p, n * sizeof(double)));
 
+    // kernel weighting (SKMReg.cxx:245-297): a weight image, or per level a covariance tensor built
+    // from the guidance image / the smoothed target, or an external tensor where the weight is 0
+    double max_weight_image = 0.0;
+    if (r->weight_image)
+        for (long long i = 0; i < n; ++i) max_weight_image = std::max(max_weight_image, r->weight_image[i]);
+    bool any_tensor = false;
+    for (int s = 0; s < r->num_scales; ++s) any_tensor = any_tensor || r->tensor_weights[s] > 0.0;
+    DevBuf dguide, dcov, dext;
+    std::vector<double> tensor;
+    const long long nt = n * D * D;
+    if (any_tensor) {
+        SKM_CUDA(cudaMalloc((void **)&dcov.p, nt * sizeof(double)));
+        if (r->guidance_image) {
+            SKM_CUDA(cudaMalloc((void **)&dguide.p, n * sizeof(double)));
+            SKM_CUDA(cudaMemcpyAsync(dguide.p, r->guidance_image, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
+        }
+        tensor.resize((size_t)nt);
+    }
+    double ext_maximum = 0.0, ext_cov[9] = {};
+    bool ext_ready = false;
+
     for (int s = 0; s < r->num_scales; ++s) {
         const auto t0 = std::chrono::steady_clock::now();
         // smoothed copies of both images (SKMReg.cxx:140-150)
@@ -277,6 +439,58 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
             ed.weight_image_geometry.spacing[d] = 1.0;
             ed.weight_tensor_geometry.size[d] = 1;
             ed.weight_tensor_geometry.spacing[d] = 1.0;
+        }
+        // kernel weighting of this level (SKMReg.cxx:245-297)
+        const double tw = r->tensor_weights[s];
+        bool has_tensor = false;
+        const double *tensor_ptr = nullptr;
+        double tensor_weight = 1.0, tensor_cov[9] = {};
+        for (int d = 0; d < D; ++d) tensor_cov[d * D + d] = 1.0;
+        if (tw > 0.0) {
+            // cases 3 and 4 (:269-286): tensor from the guidance image or the smoothed target with
+            // sigma_C4 and this level's weight, alignment axis z.  SetWeightingTensor with the tilt
+            // it returns (itkTransformAdapter.hxx:341-365): tilt >= 0 becomes the maximum weight and
+            // the support covariance stays the identity; a negative tilt means no texel passed, every
+            // tensor is the identity and so is the one with the largest eigenvalue (weight 1)
+            double tilt = -DBL_MAX;
+            if ((rc = anisotropic_tensor_device(D, geometry->size, geometry->spacing, dguide.p ? dguide.p : dsm.p,
+                                                (double)(float)r->sigma_c4[s], tw, 2, dcov.p, &tilt, hs.s)))
+                return rc;
+            SKM_CUDA(cudaMemcpyAsync(tensor.data(), dcov.p, nt * sizeof(double), cudaMemcpyDeviceToHost, hs.s));
+            SKM_CUDA(cudaStreamSynchronize(hs.s));
+            has_tensor = true;
+            tensor_ptr = tensor.data();
+            tensor_weight = tilt >= 0.0 ? tilt : 1.0;
+        } else if (tw == 0.0 && r->weight_tensor) {
+            // case 2 (:259-268): external tensor with tilt -1: the tensor whose largest eigenvalue is
+            // largest gives the support covariance and the maximum weight
+            if (!ext_ready) {
+                SKM_CUDA(cudaMalloc((void **)&dext.p, nt * sizeof(double)));
+                SKM_CUDA(cudaMemcpyAsync(dext.p, r->weight_tensor, nt * sizeof(double), cudaMemcpyHostToDevice,
+                                         hs.s));
+                if ((rc = max_eigenvalue_tensor(D, n, dext.p, r->weight_tensor, &ext_maximum, ext_cov, hs.s)))
+                    return rc;
+                ext_ready = true;
+            }
+            has_tensor = true;
+            tensor_ptr = r->weight_tensor;
+            tensor_weight = ext_maximum;
+            for (int k = 0; k < 9; ++k) tensor_cov[k] = ext_cov[k];
+        }
+        if (r->weight_image) {
+            // SetWeightingImage (itkTransformAdapter.hxx:312-331) sets the maximum weight, which a
+            // later SetWeightingTensor overwrites; every kernel reads the weight image before any
+            // tensor (GpuEvaluatorDisplacementField.cu:43-50), so the tensor itself goes unused
+            ed.use_weight_image = 1;
+            ed.maximum_weight = has_tensor ? tensor_weight : max_weight_image;
+            ed.weight_image = r->weight_image;
+            ed.weight_image_geometry = *geometry;
+        } else if (has_tensor) {
+            ed.use_weight_tensor = 1;
+            ed.maximum_weight = tensor_weight;
+            ed.weight_tensor = tensor_ptr;
+            ed.weight_tensor_geometry = *geometry;
+            for (int k = 0; k < 9; ++k) ed.maximum_eigenvalue_covariance[k] = tensor_cov[k];
         }
         ed.moving_coefficients = coeffs.data();
         ed.moving_geometry = *geometry;

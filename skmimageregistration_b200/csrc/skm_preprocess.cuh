@@ -130,4 +130,252 @@ __global__ void clamp_rescale_kernel(double *__restrict__ v, long long n, double
         v[i] = fmin(fmax(v[i], lo), hi) * scale + shift;
 }
 
+__global__ void scale_kernel(const double *__restrict__ in, double *__restrict__ out, long long n, double w)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = in[i] * w;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Anisotropic covariance tensor (ComputeAnisotropicTensor, include/AnisotropicTensorUtils.h:37-371).
+//
+// Structure tensor components are stored as D(D+1)/2 planes of n texels, upper triangle row by
+// row: 2-D xx, xy, yy; 3-D xx, xy, xz, yy, yz, zz.
+
+__host__ __device__ constexpr int tensor_components(int D) { return D * (D + 1) / 2; }
+
+template <int D>
+__host__ __device__ constexpr int tensor_slot(int i, int j)
+{
+    return i <= j ? i * D - i * (i - 1) / 2 + (j - i) : j * D - j * (j - 1) / 2 + (i - j);
+}
+
+// Outer product of the image gradient (itk::GradientImageFilter: (f[i+1] - f[i-1]) / (2 spacing)
+// per axis, an edge texel's missing neighbour replaced by the texel itself).
+template <int D>
+__global__ void gradient_outer_kernel(const double *__restrict__ f, int X, int Y, int Z, double hx, double hy,
+                                      double hz, double *__restrict__ comp)
+{
+    const long long n = (long long)X * Y * Z;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % X), y = (int)((i / X) % Y), z = (int)(i / ((long long)X * Y));
+        const long long sy = X, sz = (long long)X * Y;
+        double g[3];
+        g[0] = (f[i + (x < X - 1 ? 1 : 0)] - f[i - (x > 0 ? 1 : 0)]) / hx;
+        g[1] = (f[i + (y < Y - 1 ? sy : 0)] - f[i - (y > 0 ? sy : 0)]) / hy;
+        if (D == 3) g[2] = (f[i + (z < Z - 1 ? sz : 0)] - f[i - (z > 0 ? sz : 0)]) / hz;
+#pragma unroll
+        for (int a = 0; a < D; ++a)
+#pragma unroll
+            for (int b = a; b < D; ++b) comp[(long long)tensor_slot<D>(a, b) * n + i] = g[a] * g[b];
+    }
+}
+
+// Cyclic Jacobi eigen decomposition of a symmetric D x D matrix (Golub & Van Loan, Matrix
+// Computations, 4th ed., algorithms 8.5.1-8.5.3): a is overwritten, w[k] = a[k][k] at the end,
+// column k of v the unit eigenvector of w[k].
+template <int D>
+__device__ void jacobi_eigen(double (&a)[3][3], double (&w)[3], double (&v)[3][3])
+{
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[r][c] = r == c ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 32; ++sweep) {
+        double off = 0.0, diag = 0.0;
+#pragma unroll
+        for (int p = 0; p < D; ++p) {
+            diag += a[p][p] * a[p][p];
+#pragma unroll
+            for (int q = p + 1; q < D; ++q) off += a[p][q] * a[p][q];
+        }
+        if (off <= 1e-36 * diag || off == 0.0) break;
+#pragma unroll
+        for (int p = 0; p < D - 1; ++p)
+#pragma unroll
+            for (int q = p + 1; q < D; ++q) {
+                const double apq = a[p][q];
+                if (apq == 0.0) continue;
+                // 2x2 symmetric Schur decomposition: tan of the angle that zeroes a[p][q]
+                const double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
+                const double t = fabs(theta) > 1e150 ? 0.5 / theta
+                                                     : copysign(1.0, theta) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                a[p][p] -= t * apq;
+                a[q][q] += t * apq;
+                a[p][q] = a[q][p] = 0.0;
+#pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    if (r == p || r == q) continue;
+                    const double arp = a[r][p], arq = a[r][q];
+                    a[r][p] = a[p][r] = c * arp - s * arq;
+                    a[r][q] = a[q][r] = s * arp + c * arq;
+                }
+#pragma unroll
+                for (int r = 0; r < D; ++r) {
+                    const double vp = v[r][p], vq = v[r][q];
+                    v[r][p] = c * vp - s * vq;
+                    v[r][q] = s * vp + c * vq;
+                }
+            }
+    }
+#pragma unroll
+    for (int k = 0; k < D; ++k) w[k] = a[k][k];
+}
+
+template <int D>
+__device__ __forceinline__ double row_norm(const double (&r)[3])
+{
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) s += r[k] * r[k];
+    return sqrt(s);
+}
+
+// Per texel: eigen system of the smoothed structure tensor ordered by magnitude with rows
+// eigenvalue * eigenvector (include/itkSymmetricEigenDecompositionImageFilter.h), the direction
+// weighting (AnisotropicTensorUtils.h:181-300) and the covariance U diag(column norms) U^T
+// (:316-360).  tilt[i] = |main row| after the alignment weighting where the texel passed the
+// 1e-8 test, else -DBL_MAX; bad counts texels whose covariance has a non-positive determinant.
+template <int D>
+__global__ void covariance_kernel(const double *__restrict__ comp, long long n, int alignment,
+                                  double *__restrict__ cov, double *__restrict__ tilt, unsigned *__restrict__ bad)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double a[3][3] = {}, w[3] = {}, v[3][3];
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) a[r][c] = comp[(long long)tensor_slot<D>(r, c) * n + i];
+        jacobi_eigen<D>(a, w, v);
+        // order by |eigenvalue| ascending (stable), rows[k] = w * eigenvector
+        int ord[3] = {0, 1, 2};
+#pragma unroll
+        for (int p = 1; p < D; ++p)
+#pragma unroll
+            for (int q = p; q > 0; --q)
+                if (fabs(w[ord[q]]) < fabs(w[ord[q - 1]])) {
+                    const int t = ord[q];
+                    ord[q] = ord[q - 1];
+                    ord[q - 1] = t;
+                }
+        double rows[3][3] = {}, mag[3];
+        bool ok = true;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+#pragma unroll
+            for (int c = 0; c < D; ++c) rows[k][c] = w[ord[k]] * v[c][ord[k]];
+            mag[k] = row_norm<D>(rows[k]);
+            ok = ok && mag[k] > 1e-8;
+        }
+        double M[3][3] = {};
+        double rev = -DBL_MAX;
+        if (ok) {
+            double nrm[3] = {}, main[3] = {};
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                nrm[c] = rows[D - 1][c] / mag[D - 1];
+                main[c] = rows[D - 1][c];
+            }
+            if (alignment >= 0 && alignment < D) {
+                double cr;
+                if (D == 2) {
+                    const double m0 = alignment == 0 ? 1.0 : 0.0, m1 = alignment == 1 ? 1.0 : 0.0;
+                    cr = fabs(nrm[0] * m1 - nrm[1] * m0);
+                } else {
+                    double m[3] = {0.0, 0.0, 0.0};
+                    m[alignment] = 1.0;
+                    const double c0 = nrm[1] * m[2] - nrm[2] * m[1], c1 = nrm[2] * m[0] - nrm[0] * m[2],
+                                 c2 = nrm[0] * m[1] - nrm[1] * m[0];
+                    cr = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+                }
+                double factor = cr + 1e-10;
+                factor = factor * factor / sqrt((double)D);
+#pragma unroll
+                for (int c = 0; c < D; ++c) main[c] *= factor;
+            }
+            rev = row_norm<D>(main);
+            const double p = pow(rev, 1.5);
+            double out[3][3] = {};
+#pragma unroll
+            for (int c = 0; c < D; ++c) out[D - 1][c] = nrm[c] / (1.0 + p);
+#pragma unroll
+            for (int k = 0; k < D - 1; ++k)
+#pragma unroll
+                for (int c = 0; c < D; ++c) out[k][c] = rows[k][c] / mag[k] * (1.0 + p / (1.0 + p));
+            // flipud().transpose(): M[r][c] = out[D - 1 - c][r]
+#pragma unroll
+            for (int r = 0; r < D; ++r)
+#pragma unroll
+                for (int c = 0; c < D; ++c) M[r][c] = out[D - 1 - c][r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < D; ++r) M[r][r] = 1.0;
+        }
+        // covariance from the scaled eigenvectors (columns of M)
+        double s[3], C[3][3] = {};
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+            double q = 0.0;
+#pragma unroll
+            for (int r = 0; r < D; ++r) q += M[r][c] * M[r][c];
+            s[c] = sqrt(q);
+        }
+        if (s[0] < 1e-8) {
+#pragma unroll
+            for (int r = 0; r < D; ++r) C[r][r] = 1.0;
+        } else {
+#pragma unroll
+            for (int r = 0; r < D; ++r)
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int k = 0; k < D; ++k) acc += (M[r][k] / s[k]) * s[k] * (M[c][k] / s[k]);
+                    C[r][c] = acc;
+                }
+        }
+        const double det = D == 2 ? C[0][0] * C[1][1] - C[0][1] * C[1][0]
+                                  : C[0][0] * (C[1][1] * C[2][2] - C[1][2] * C[2][1]) -
+                                        C[0][1] * (C[1][0] * C[2][2] - C[1][2] * C[2][0]) +
+                                        C[0][2] * (C[1][0] * C[2][1] - C[1][1] * C[2][0]);
+        if (!(det > 0.0)) atomicAdd(bad, 1u);
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) cov[i * D * D + r * D + c] = C[r][c];
+        tilt[i] = rev;
+    }
+}
+
+// |largest eigenvalue| of each D x D tensor (vnl_symmetric_eigensystem's last eigenvalue, as
+// itkTransformAdapter.hxx:352-358 compares it), and the determinant test of :348-350.
+template <int D>
+__global__ void max_eigenvalue_kernel(const double *__restrict__ tensor, long long n, double *__restrict__ out,
+                                      unsigned *__restrict__ bad)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double a[3][3] = {}, w[3] = {}, v[3][3];
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) a[r][c] = tensor[i * D * D + r * D + c];
+        const double det = D == 2 ? a[0][0] * a[1][1] - a[0][1] * a[1][0]
+                                  : a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) -
+                                        a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+                                        a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+        if (!(det > 0.0)) atomicAdd(bad, 1u);
+        // symmetrise the way the eigen solver reads the matrix (upper triangle)
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < r; ++c) a[r][c] = a[c][r];
+        jacobi_eigen<D>(a, w, v);
+        double mx = w[0];
+#pragma unroll
+        for (int k = 1; k < D; ++k) mx = fmax(mx, w[k]);
+        out[i] = fabs(mx);
+    }
+}
+
 }  // namespace skm

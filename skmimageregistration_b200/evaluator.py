@@ -74,6 +74,8 @@ def lib():
                                             C.c_double, C.c_double, _dp, _dp]
         L.skm_register.argtypes = [C.POINTER(abi.RegisterDesc), C.POINTER(abi.Geometry), _dp, _dp, _dp,
                                    C.POINTER(abi.RegisterReport)]
+        L.skm_anisotropic_tensor.argtypes = [C.c_int32, C.POINTER(abi.Geometry), _dp, C.c_double, C.c_double,
+                                             C.c_int32, _dp, _dp]
         _lib = L
     return _lib
 

@@ -17,7 +17,8 @@ from . import abi
 from .abi import Geometry, RegisterDesc, RegisterReport, dptr
 from .evaluator import check, lib
 
-# include/ConfigUtils.h:29-62, the options this driver uses (no weight image, no covariance tensor)
+# include/ConfigUtils.h:29-62, the options this driver uses; weight_filename and
+# weight_tensor_filename become the weight_image / weight_tensor / guidance_image arrays of register()
 DEFAULT_CONFIG = {
     "sigma_C4": [64, 32, 16],
     "sigma_C0": [128, 64, 32],
@@ -38,7 +39,7 @@ DEFAULT_CONFIG = {
     "neighborhood_sampling": [15, 12, 9],
     "intensity_thresholds": [-1500, 3500],
     "smoothing_variance": [2, 1, 0],
-    "tensor_weights": [0, 0, 0],
+    "tensor_weights": [400, 200, 100],
 }
 
 PER_SCALE = ["sigma_C4", "sigma_C0", "reg_l1", "reg_l21", "reg_l2", "reg_rkhs", "reg_rd", "reg_rd_scaling", "reg_pg",
@@ -67,8 +68,6 @@ def make_desc(config, D) -> RegisterDesc:
     n = int(c["num_scales"])
     if not 1 <= n <= abi.MAX_SCALES:
         raise ValueError("num_scales must be in [1, %d]" % abi.MAX_SCALES)
-    if any(current(c, "tensor_weights", s) != 0 for s in range(n)):
-        raise ValueError("tensor_weights > 0 needs the covariance-tensor builder (not available); set them to 0")
     d = RegisterDesc()
     d.dimensions = D
     d.num_scales = n
@@ -79,17 +78,22 @@ def make_desc(config, D) -> RegisterDesc:
     if len(th) == 2:
         d.threshold_min, d.threshold_max = float(th[0]), float(th[1])
     for opt in PER_SCALE:
-        if opt == "tensor_weights":
-            continue
         arr = getattr(d, _FIELD.get(opt, opt))
         for s in range(abi.MAX_SCALES):
             arr[s] = current(c, opt, min(s, n - 1))
     return d
 
 
-def register(reference, target, spacing=None, origin=None, config=None):
+def register(reference, target, spacing=None, origin=None, config=None, guidance_image=None, weight_tensor=None,
+             weight_image=None):
     """Registers `reference` (moving) onto `target` (fixed); both arrays (Z, Y, X) or (Y, X) with
-    the same geometry.  Returns (displacement (..., D) on that grid, report dict)."""
+    the same geometry.  Returns (displacement (..., D) on that grid, report dict).
+
+    Kernel weighting as src/SKMReg.cxx:245-297, all images on the same grid: per level with
+    tensor_weights > 0 a covariance tensor from `guidance_image` (the reference's
+    weight_tensor_filename read as an image) or, without one, from the smoothed target; with
+    tensor_weights == 0 the external `weight_tensor` (..., D, D) when given; `weight_image`
+    (the reference's weight_filename) takes precedence in the kernel."""
     ref = np.ascontiguousarray(reference, np.float64)
     tar = np.ascontiguousarray(target, np.float64)
     if ref.shape != tar.shape:
@@ -97,10 +101,33 @@ def register(reference, target, spacing=None, origin=None, config=None):
     D = ref.ndim
     geo = Geometry.make(tuple(reversed(ref.shape)), origin, spacing)
     desc = make_desc(config, D)
+    keep = []
+    for name, arr, shape in (("guidance_image", guidance_image, ref.shape),
+                             ("weight_tensor", weight_tensor, ref.shape + (D, D)),
+                             ("weight_image", weight_image, ref.shape)):
+        if arr is not None:
+            a = np.ascontiguousarray(arr, np.float64)
+            if a.shape != shape:
+                raise ValueError("%s must have shape %s" % (name, shape))
+            keep.append(a)
+            setattr(desc, name, dptr(a))
     disp = np.zeros(ref.shape + (D,))
     rep = RegisterReport()
     check(lib().skm_register(C.byref(desc), C.byref(geo), dptr(ref), dptr(tar), dptr(disp), C.byref(rep)))
     return disp, rep.as_dict()
+
+
+def anisotropic_tensor(image, spacing=None, sigma=64.0, weight=400.0, alignment_direction=2):
+    """ComputeAnisotropicTensor (include/AnisotropicTensorUtils.h:37-371, anisotropic_filtering
+    false) on the GPU: (covariance (..., D, D), maximum tilt)."""
+    img = np.ascontiguousarray(image, np.float64)
+    D = img.ndim
+    geo = Geometry.make(tuple(reversed(img.shape)), None, spacing)
+    cov = np.empty(img.shape + (D, D))
+    tilt = C.c_double(0.0)
+    check(lib().skm_anisotropic_tensor(D, C.byref(geo), dptr(img), float(sigma), float(weight),
+                                       int(alignment_direction), dptr(cov), C.byref(tilt)))
+    return cov, tilt.value
 
 
 def gaussian_smooth(image, spacing=None, variance=1.0, use_image_spacing=True, maximum_error=0.01,

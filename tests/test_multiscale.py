@@ -60,5 +60,78 @@ def test_current_repeats_the_last_entry():
     assert list(d.sigma_c4[:4]) == [32.0, 16.0, 16.0, 16.0]
     assert list(d.sampling_rate[:4]) == [5, 4, 3, 3]
     assert d.apply_threshold == 1 and d.threshold_min == -1500 and d.threshold_max == 3500
-    with pytest.raises(ValueError):
-        make_desc(dict(c, tensor_weights=[400]), 3)
+    assert list(d.tensor_weights[:4]) == [400.0, 200.0, 100.0, 100.0]   # the reference's defaults
+    d = make_desc(dict(c, tensor_weights=[0]), 3)
+    assert list(d.tensor_weights[:4]) == [0.0] * 4
+    assert not d.guidance_image and not d.weight_tensor and not d.weight_image
+
+
+# --- anisotropic covariance tensor (include/AnisotropicTensorUtils.h) ------------------------
+
+def test_image_gradient_central_differences_with_repeated_edges():
+    f = np.array([[0.0, 1.0, 4.0, 9.0]])                  # one row, x = 0..3
+    g = M.image_gradient(f, (0.5, 1.0))
+    assert np.allclose(g[0, :, 0], [(1 - 0) / 1.0, (4 - 0) / 1.0, (9 - 1) / 1.0, (9 - 4) / 1.0])
+    assert np.allclose(g[..., 1], 0.0)                    # a single row: y neighbours are the texel itself
+
+
+def _cov_known(lams, D, align):
+    """Covariance the reference builds for a diagonal structure tensor diag(lams)."""
+    order = np.argsort(np.abs(lams), kind="stable")
+    main = order[-1]
+    n = np.zeros(D)
+    n[main] = 1.0
+    lam = abs(lams[main])
+    if 0 <= align < D:
+        m = np.zeros(D)
+        m[align] = 1.0
+        cr = abs(n[0] * m[1] - n[1] * m[0]) if D == 2 else np.linalg.norm(np.cross(n, m))
+        lam *= (cr + 1e-10) ** 2 / np.sqrt(D)
+    p = lam ** 1.5
+    cov = np.diag([1.0 + p / (1.0 + p)] * D)
+    cov[main, main] = 1.0 / (1.0 + p)
+    return cov, lam
+
+
+@pytest.mark.parametrize("lams,align", [((4.0, 1.0), 2), ((1.0, 4.0), 2), ((4.0, 1.0), 1), ((9.0, 4.0, 1.0), 2),
+                                        ((1.0, 9.0, 4.0), 2), ((1.0, 4.0, 9.0), 2), ((9.0, 4.0, 1.0), 0),
+                                        ((2.0, 3.0, 5.0), -1)])
+def test_covariance_known_answers_on_diagonal_tensors(lams, align):
+    D = len(lams)
+    cov, tilt, bad = M.covariance_from_structure(np.diag(lams)[None], align)
+    ref, lam = _cov_known(np.asarray(lams), D, align)
+    assert bad == 0
+    assert np.allclose(cov[0], ref, rtol=0, atol=1e-14)
+    assert abs(tilt - lam) <= 1e-14 * max(1.0, lam)
+
+
+def test_covariance_identity_where_an_eigenvalue_vanishes():
+    T = np.zeros((3, 3, 3))
+    T[0] = np.diag([5.0, 2.0, 0.0])                       # rank 2
+    T[1] = np.diag([5.0, 2.0, 5e-9])                      # below the 1e-8 test
+    T[2] = np.diag([5.0, 2.0, 2e-8])                      # passes
+    cov, tilt, bad = M.covariance_from_structure(T, 2)
+    assert np.allclose(cov[0], np.eye(3)) and np.allclose(cov[1], np.eye(3))
+    assert not np.allclose(cov[2], np.eye(3))
+    _, none, _ = M.covariance_from_structure(np.zeros((2, 2, 2)), 2)
+    assert none == -np.finfo(np.float64).max
+
+
+def test_covariance_rotates_with_the_structure_tensor_in_2d():
+    rng = np.random.default_rng(4)
+    A = rng.normal(size=(50, 2, 2))
+    T = A @ A.transpose(0, 2, 1) + 0.1 * np.eye(2)
+    th = 0.7
+    R = np.array([[np.cos(th), -np.sin(th)], [np.sin(th), np.cos(th)]])
+    cov, _, _ = M.covariance_from_structure(T, -1)
+    cov_r, _, _ = M.covariance_from_structure(R @ T @ R.T, -1)
+    assert np.allclose(cov_r, R @ cov @ R.T, atol=1e-12)
+    ev = np.linalg.eigvalsh(cov)
+    assert ev.min() > 0 and ev.max() < 2                  # 1/(1+p) and 1 + p/(1+p)
+
+
+def test_anisotropic_tensor_constant_and_ramp_images_give_identity():
+    for img in (np.full((9, 10, 11), 0.7), np.broadcast_to(np.arange(11.0), (9, 10, 11))):
+        cov, tilt = M.anisotropic_tensor(img, (1.0, 1.0, 1.0), 8.0, 400.0, 2)
+        assert np.allclose(cov, np.eye(3), atol=1e-12)       # rank <= 1 structure: identity
+        assert tilt == -np.finfo(np.float64).max

@@ -43,12 +43,12 @@ CASES = {
     "2d_ncc_generic": dict(shape=(40, 44), spacing=(1.0, 1.0), config=dict(
         num_scales=2, sigma_C4=[8, 6], sigma_C0=[16, 12], cp_spacing_scaler=2.0, smoothing_variance=[1.0, 0],
         sampling_rate=[2, 1], neighborhood_sampling=[1], num_function_evaluations=[4, 3], metric="ncc",
-        reg_rd=[1e-3], initial_step_size=[1000.0])),
+        reg_rd=[1e-3], initial_step_size=[1000.0], tensor_weights=[0])),
     # phase-table path with the tensor-core GEMMs (control spacing 2 voxels, every voxel sampled)
     "3d_mse_table": dict(shape=(20, 22, 26), spacing=(1.0, 1.0, 1.0), config=dict(
         num_scales=2, sigma_C4=[8, 8], sigma_C0=[16, 16], cp_spacing_scaler=4.0, smoothing_variance=[2.0, 0],
         sampling_rate=[1], neighborhood_sampling=[1], num_function_evaluations=[3, 3], metric="mse",
-        initial_step_size=[400.0])),
+        initial_step_size=[400.0], tensor_weights=[0])),
 }
 
 
