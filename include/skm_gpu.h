@@ -341,10 +341,20 @@ typedef struct skm_register_desc {
     const double *guidance_image;
     const double *weight_tensor;
     const double *weight_image;
+    /* restart (SKMReg's restart_at, src/SKMReg.cxx:96-123): with 1 < restart_at <= num_scales and
+     * initial_displacement (N x D, the summed field after level restart_at - 1) the levels
+     * restart_at..num_scales run on top of that field; otherwise every level runs from zero. */
+    int32_t restart_at;
+    const double *initial_displacement;
+    /* optional: called after every level with the summed displacement field so far (N x D, valid
+     * during the call) -- the df-full-<level> checkpoint SKMReg writes (src/SKMReg.cxx:468). */
+    void (*level_done)(int32_t level, const double *displacement, void *user);
+    void *level_user;
 } skm_register_desc;
 
 typedef struct skm_register_report {
-    int32_t levels_done;
+    int32_t levels_done;              /* index of the last level run + 1 */
+    int32_t first_level;              /* 0, or restart_at - 1 after a restart */
     int32_t iterations[SKM_MAX_SCALES];
     int64_t control_points[SKM_MAX_SCALES];
     double  best_value[SKM_MAX_SCALES];   /* metric value (+ regularizers) at the returned parameters */
@@ -370,6 +380,18 @@ int skm_register(const skm_register_desc *desc, const skm_geometry *geometry, co
  * SKM_ERR_INVALID where a covariance is not positive definite (the reference prints and stops). */
 int skm_anisotropic_tensor(int32_t dimensions, const skm_geometry *geometry, const double *image, double sigma,
                            double weight, int32_t alignment_direction, double *covariance, double *maximum_tilt);
+
+/* Warped image: out(i) = I(p_i + u_i) on the field's grid (u: N x D doubles, AoS), I the image
+ * interpolated with order 1 (multilinear, the final resampling of src/SKMReg.cxx:504-522) or
+ * order 3 (cubic B-spline, WarpImage of include/itkUtils.h:163-178); default_value where the
+ * continuous index leaves [-0.5, size - 0.5) on an axis. */
+int skm_warp_image(int32_t dimensions, const skm_geometry *image_geometry, const double *image,
+                   const skm_geometry *field_geometry, const double *field, int32_t order, double default_value,
+                   double *out);
+
+/* JacobianDeterminant (include/itkUtils.h:153-161): det(I + du/dx) per texel with central
+ * differences over 2 spacing, edge texels repeated.  field: N x D doubles (AoS), out: N. */
+int skm_jacobian_determinant(int32_t dimensions, const skm_geometry *geometry, const double *field, double *out);
 
 /* ------------------------------------------------------------------------- */
 /* Metric value without any device allocation.  No counterpart in the reference.

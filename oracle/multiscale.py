@@ -204,7 +204,78 @@ def level_weighting(tar_s, spacing, c, s, guidance_image=None, weight_tensor=Non
     return {}
 
 
-def register(reference, target, spacing, origin, config, guidance_image=None, weight_tensor=None, weight_image=None):
+def _mirror(k, n):
+    period = 2 * (n - 1)
+    if period <= 0:
+        return np.zeros_like(k)
+    k = np.mod(k, period)
+    return np.where(k < n, k, period - k)
+
+
+def warp_image(image, displacement, image_spacing, image_origin, field_spacing, field_origin, order=3,
+               default_value=0.0):
+    """I(p + u(p)) on the field's grid (WarpImage, include/itkUtils.h:163-178, order 3; the final
+    resampling of src/SKMReg.cxx:504-522, order 1).  Outside [-0.5, size - 0.5) in continuous index:
+    default_value.  Order 1: multilinear with clamped neighbours; order 3: cubic B-spline of the
+    evaluator's prefiltered coefficients at floor(x) - 1 .. floor(x) + 2, whole-sample mirrored."""
+    img = np.asarray(image, np.float64)
+    u = np.asarray(displacement, np.float64)
+    D = img.ndim
+    isize = tuple(reversed(img.shape))
+    fgrid = u.shape[:-1]
+    idx = np.indices(fgrid, dtype=np.float64)             # numpy order: axis 0 = z (or y)
+    ci, inside = [], np.ones(fgrid, bool)
+    for d in range(D):
+        p = field_origin[d] + field_spacing[d] * idx[D - 1 - d] + u[..., d]
+        c = (p - image_origin[d]) / image_spacing[d]
+        inside &= (c >= -0.5) & (c < isize[d] - 0.5)
+        ci.append(c)
+    if order == 3:
+        coef = O.bspline_coefficients(img)[tuple(slice(1, n + 1) for n in img.shape)]
+    else:
+        coef = img
+    taps = 2 if order == 1 else 4
+    W, I = [], []
+    for d in range(D):
+        b = np.floor(ci[d])
+        t = ci[d] - b
+        b = b.astype(np.int64)
+        if order == 1:
+            W.append([1.0 - t, t])
+            I.append([np.clip(b, 0, isize[d] - 1), np.clip(b + 1, 0, isize[d] - 1)])
+        else:
+            s = 1.0 - t
+            W.append([s ** 3 / 6.0, 2.0 / 3.0 - t * t + 0.5 * t ** 3, 2.0 / 3.0 - s * s + 0.5 * s ** 3, t ** 3 / 6.0])
+            I.append([_mirror(b - 1 + k, isize[d]) for k in range(4)])
+    out = np.zeros(fgrid)
+    for corner in np.ndindex(*([taps] * D)):
+        w = np.ones(fgrid)
+        for d in range(D):
+            w = w * W[d][corner[d]]
+        sel = tuple(I[d][corner[d]] for d in reversed(range(D)))
+        out += w * coef[sel]
+    return np.where(inside, out, default_value)
+
+
+def jacobian_determinant(field, spacing):
+    """JacobianDeterminant (include/itkUtils.h:153-161): det(I + du/dx), central differences over
+    2 spacing with edge texels repeated."""
+    u = np.asarray(field, np.float64)
+    D = u.shape[-1]
+    J = np.zeros(u.shape[:-1] + (D, D))
+    for j in range(D):
+        ax = D - 1 - j
+        n = u.shape[ax]
+        k = np.arange(n)
+        hi = np.take(u, np.minimum(k + 1, n - 1), axis=ax)
+        lo = np.take(u, np.maximum(k - 1, 0), axis=ax)
+        J[..., :, j] = (hi - lo) / (2.0 * float(spacing[j]))
+    J += np.eye(D)
+    return np.linalg.det(J)
+
+
+def register(reference, target, spacing, origin, config, guidance_image=None, weight_tensor=None, weight_image=None,
+             initial_displacement=None):
     """The scale loop with the FP64 evaluator / optimizer; returns (displacement, per-level best values)."""
     c = full_config(config)
     ref = np.asarray(reference, np.float64)
@@ -217,7 +288,12 @@ def register(reference, target, spacing, origin, config, guidance_image=None, we
     tar = threshold_rescale(tar, th if len(th) == 2 else None)
     past = None
     best = []
-    for s in range(int(c["num_scales"])):
+    first = 0
+    ra = int(c.get("restart_at", 0))
+    if 1 < ra <= int(c["num_scales"]) and initial_displacement is not None:
+        first = ra - 1
+        past = np.ascontiguousarray(np.asarray(initial_displacement, np.float64))
+    for s in range(first, int(c["num_scales"])):
         var = float(current(c, "smoothing_variance", s))
         ref_s = gaussian_smooth(ref, spacing, var) if var > 1e-5 else ref
         tar_s = gaussian_smooth(tar, spacing, var) if var > 1e-5 else tar

@@ -208,6 +208,9 @@ class OptimizerState(C.Structure):
 MAX_SCALES = 8
 
 
+LEVEL_CALLBACK = C.CFUNCTYPE(None, C.c_int32, C.POINTER(C.c_double), C.c_void_p)
+
+
 class RegisterDesc(C.Structure):
     """skm_register_desc: the configuration of the reference application (src/SKMReg.cxx)."""
 
@@ -229,12 +232,17 @@ class RegisterDesc(C.Structure):
         ("guidance_image", C.POINTER(C.c_double)),
         ("weight_tensor", C.POINTER(C.c_double)),
         ("weight_image", C.POINTER(C.c_double)),
+        ("restart_at", C.c_int32),
+        ("initial_displacement", C.POINTER(C.c_double)),
+        ("level_done", LEVEL_CALLBACK),
+        ("level_user", C.c_void_p),
     ]
 
 
 class RegisterReport(C.Structure):
     _fields_ = [
         ("levels_done", C.c_int32),
+        ("first_level", C.c_int32),
         ("iterations", C.c_int32 * MAX_SCALES),
         ("control_points", C.c_int64 * MAX_SCALES),
         ("best_value", C.c_double * MAX_SCALES),
@@ -243,7 +251,7 @@ class RegisterReport(C.Structure):
 
     def as_dict(self):
         n = self.levels_done
-        return {"levels_done": n, "iterations": list(self.iterations[:n]),
+        return {"levels_done": n, "first_level": self.first_level, "iterations": list(self.iterations[:n]),
                 "control_points": list(self.control_points[:n]), "best_value": list(self.best_value[:n]),
                 "seconds": list(self.seconds[:n])}
 

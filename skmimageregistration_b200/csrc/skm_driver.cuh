@@ -18,6 +18,7 @@
 #include <chrono>
 #include <vector>
 
+#include "skm_output.cuh"
 #include "skm_preprocess.cuh"
 
 namespace {
@@ -295,6 +296,101 @@ extern "C" int skm_anisotropic_tensor(int32_t dimensions, const skm_geometry *ge
 
 namespace {
 
+skm::OutGeo out_geo(int D, const skm_geometry &g)
+{
+    skm::OutGeo o{};
+    for (int d = 0; d < 3; ++d) {
+        o.o[d] = d < D ? g.origin[d] : 0.0;
+        o.s[d] = d < D ? g.spacing[d] : 1.0;
+        o.n[d] = d < D ? g.size[d] : 1;
+    }
+    return o;
+}
+
+bool out_geometry_ok(int D, const skm_geometry *g)
+{
+    if (!g) return false;
+    for (int d = 0; d < D; ++d)
+        if (g->size[d] < 1 || !(g->spacing[d] > 0.0) || !std::isfinite(g->origin[d])) return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" int skm_warp_image(int32_t dimensions, const skm_geometry *image_geometry, const double *image,
+                              const skm_geometry *field_geometry, const double *field, int32_t order,
+                              double default_value, double *out)
+{
+    if (dimensions != 2 && dimensions != 3) return fail(SKM_ERR_INVALID, "dimensions must be 2 or 3");
+    if (!image || !field || !out) return fail(SKM_ERR_INVALID, "image / field / out is NULL");
+    if (!out_geometry_ok(dimensions, image_geometry) || !out_geometry_ok(dimensions, field_geometry))
+        return fail(SKM_ERR_INVALID, "invalid geometry (size < 1, spacing <= 0 or origin not finite)");
+    if (order != 1 && order != 3) return fail(SKM_ERR_UNSUPPORTED, "interpolation order %d (1 or 3)", order);
+    const int D = dimensions;
+    if (order == 3)
+        for (int d = 0; d < D; ++d)
+            if (image_geometry->size[d] < 2)
+                return fail(SKM_ERR_INVALID, "cubic interpolation needs at least 2 texels per axis");
+    const long long ni = texel_count(D, image_geometry->size), nf = texel_count(D, field_geometry->size);
+    HostStream hs;
+    SKM_CUDA(cudaStreamCreateWithFlags(&hs.s, cudaStreamNonBlocking));
+    DevBuf di, df, dout;
+    SKM_CUDA(cudaMalloc((void **)&di.p, ni * sizeof(double)));
+    SKM_CUDA(cudaMalloc((void **)&df.p, nf * D * sizeof(double)));
+    SKM_CUDA(cudaMalloc((void **)&dout.p, nf * sizeof(double)));
+    SKM_CUDA(cudaMemcpyAsync(di.p, image, ni * sizeof(double), cudaMemcpyHostToDevice, hs.s));
+    SKM_CUDA(cudaMemcpyAsync(df.p, field, nf * D * sizeof(double), cudaMemcpyHostToDevice, hs.s));
+    const skm::OutGeo gi = out_geo(D, *image_geometry), gf = out_geo(D, *field_geometry);
+    if (order == 3) {
+        // the evaluator's prefilter, in place, without the mirror padding
+        const int X = gi.n[0], Y = gi.n[1], Z = gi.n[2];
+        const double pole = std::sqrt(3.0) - 2.0;
+        if (D == 3) {
+            skm::bs_prefilter_axis<<<(int)(((long long)X * Y + 127) / 128), 128, 0, hs.s>>>(di.p, X, Y, Z, 2, pole);
+            skm::bs_prefilter_axis<<<(int)(((long long)X * Z + 127) / 128), 128, 0, hs.s>>>(di.p, X, Y, Z, 1, pole);
+            skm::bs_prefilter_axis<<<(int)(((long long)Y * Z + 127) / 128), 128, 0, hs.s>>>(di.p, X, Y, Z, 0, pole);
+        } else {
+            skm::bs_prefilter_axis<<<(Y + 127) / 128, 128, 0, hs.s>>>(di.p, X, Y, 1, 0, pole);
+            skm::bs_prefilter_axis<<<(X + 127) / 128, 128, 0, hs.s>>>(di.p, X, Y, 1, 1, pole);
+        }
+        SKM_CHECK_LAUNCH();
+    }
+    const int blocks = grid_blocks(nf, 16);
+    if (D == 2 && order == 1) skm::warp_kernel<2, 1><<<blocks, 256, 0, hs.s>>>(di.p, gi, df.p, gf, default_value, dout.p);
+    if (D == 2 && order == 3) skm::warp_kernel<2, 3><<<blocks, 256, 0, hs.s>>>(di.p, gi, df.p, gf, default_value, dout.p);
+    if (D == 3 && order == 1) skm::warp_kernel<3, 1><<<blocks, 256, 0, hs.s>>>(di.p, gi, df.p, gf, default_value, dout.p);
+    if (D == 3 && order == 3) skm::warp_kernel<3, 3><<<blocks, 256, 0, hs.s>>>(di.p, gi, df.p, gf, default_value, dout.p);
+    SKM_CHECK_LAUNCH();
+    SKM_CUDA(cudaMemcpyAsync(out, dout.p, nf * sizeof(double), cudaMemcpyDeviceToHost, hs.s));
+    SKM_CUDA(cudaStreamSynchronize(hs.s));
+    return SKM_OK;
+}
+
+extern "C" int skm_jacobian_determinant(int32_t dimensions, const skm_geometry *geometry, const double *field,
+                                        double *out)
+{
+    if (dimensions != 2 && dimensions != 3) return fail(SKM_ERR_INVALID, "dimensions must be 2 or 3");
+    if (!field || !out) return fail(SKM_ERR_INVALID, "field / out is NULL");
+    if (!out_geometry_ok(dimensions, geometry)) return fail(SKM_ERR_INVALID, "invalid geometry");
+    const int D = dimensions;
+    const long long n = texel_count(D, geometry->size);
+    HostStream hs;
+    SKM_CUDA(cudaStreamCreateWithFlags(&hs.s, cudaStreamNonBlocking));
+    DevBuf du, dout;
+    SKM_CUDA(cudaMalloc((void **)&du.p, n * D * sizeof(double)));
+    SKM_CUDA(cudaMalloc((void **)&dout.p, n * sizeof(double)));
+    SKM_CUDA(cudaMemcpyAsync(du.p, field, n * D * sizeof(double), cudaMemcpyHostToDevice, hs.s));
+    const skm::OutGeo g = out_geo(D, *geometry);
+    if (D == 2) skm::jacobian_determinant_kernel<2><<<grid_blocks(n, 16), 256, 0, hs.s>>>(du.p, g, dout.p);
+    else skm::jacobian_determinant_kernel<3><<<grid_blocks(n, 16), 256, 0, hs.s>>>(du.p, g, dout.p);
+    SKM_CHECK_LAUNCH();
+    SKM_CUDA(cudaMemcpyAsync(out, dout.p, n * sizeof(double), cudaMemcpyDeviceToHost, hs.s));
+    SKM_CUDA(cudaStreamSynchronize(hs.s));
+    return SKM_OK;
+}
+
+namespace {
+
 // ComputeControlPointImage (itkTransformAdapter.hxx:246-308): size ceil(extent / spacing), the grid
 // centred on the image extent
 void control_grid(int D, const skm_geometry &img, double spacing, skm_geometry &cp)
@@ -399,7 +495,15 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
     double ext_maximum = 0.0, ext_cov[9] = {};
     bool ext_ready = false;
 
-    for (int s = 0; s < r->num_scales; ++s) {
+    // restart on a later level with the field of the levels before it (SKMReg.cxx:96-123)
+    int first = 0;
+    if (r->restart_at > 1 && r->restart_at <= r->num_scales && r->initial_displacement) {
+        first = r->restart_at - 1;
+        std::memcpy(past.data(), r->initial_displacement, sizeof(double) * n * D);
+    }
+    rep.first_level = first;
+
+    for (int s = first; s < r->num_scales; ++s) {
         const auto t0 = std::chrono::steady_clock::now();
         // smoothed copies of both images (SKMReg.cxx:140-150)
         for (int which = 0; which < 2; ++which) {
@@ -555,6 +659,7 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
         rep.iterations[s] = st.iteration;
         rep.control_points[s] = C;
         rep.seconds[s] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (r->level_done) r->level_done(s, past.data(), r->level_user);     // df-full-<s> (SKMReg.cxx:468)
     }
     std::memcpy(displacement, past.data(), sizeof(double) * n * D);
     if (report) *report = rep;

@@ -76,6 +76,9 @@ def lib():
                                    C.POINTER(abi.RegisterReport)]
         L.skm_anisotropic_tensor.argtypes = [C.c_int32, C.POINTER(abi.Geometry), _dp, C.c_double, C.c_double,
                                              C.c_int32, _dp, _dp]
+        L.skm_warp_image.argtypes = [C.c_int32, C.POINTER(abi.Geometry), _dp, C.POINTER(abi.Geometry), _dp, C.c_int32,
+                                     C.c_double, _dp]
+        L.skm_jacobian_determinant.argtypes = [C.c_int32, C.POINTER(abi.Geometry), _dp, _dp]
         _lib = L
     return _lib
 

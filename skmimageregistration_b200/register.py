@@ -40,6 +40,7 @@ DEFAULT_CONFIG = {
     "intensity_thresholds": [-1500, 3500],
     "smoothing_variance": [2, 1, 0],
     "tensor_weights": [400, 200, 100],
+    "restart_at": 0,
 }
 
 PER_SCALE = ["sigma_C4", "sigma_C0", "reg_l1", "reg_l21", "reg_l2", "reg_rkhs", "reg_rd", "reg_rd_scaling", "reg_pg",
@@ -74,6 +75,7 @@ def make_desc(config, D) -> RegisterDesc:
     d.metric = abi.METRICS[c["metric"]]
     d.cp_spacing_scaler = float(c["cp_spacing_scaler"])
     th = c.get("intensity_thresholds") or []
+    d.restart_at = int(c.get("restart_at", 0))
     d.apply_threshold = int(len(th) == 2)
     if len(th) == 2:
         d.threshold_min, d.threshold_max = float(th[0]), float(th[1])
@@ -85,7 +87,7 @@ def make_desc(config, D) -> RegisterDesc:
 
 
 def register(reference, target, spacing=None, origin=None, config=None, guidance_image=None, weight_tensor=None,
-             weight_image=None):
+             weight_image=None, initial_displacement=None, on_level=None):
     """Registers `reference` (moving) onto `target` (fixed); both arrays (Z, Y, X) or (Y, X) with
     the same geometry.  Returns (displacement (..., D) on that grid, report dict).
 
@@ -93,7 +95,12 @@ def register(reference, target, spacing=None, origin=None, config=None, guidance
     tensor_weights > 0 a covariance tensor from `guidance_image` (the reference's
     weight_tensor_filename read as an image) or, without one, from the smoothed target; with
     tensor_weights == 0 the external `weight_tensor` (..., D, D) when given; `weight_image`
-    (the reference's weight_filename) takes precedence in the kernel."""
+    (the reference's weight_filename) takes precedence in the kernel.
+
+    Restart (config "restart_at" > 1, src/SKMReg.cxx:96-123): `initial_displacement` (..., D) is
+    the summed field after level restart_at - 1; without it every level runs.  `on_level(level,
+    displacement)` is called after each level with a copy of the summed field so far (the
+    df-full-<level> checkpoint of the reference)."""
     ref = np.ascontiguousarray(reference, np.float64)
     tar = np.ascontiguousarray(target, np.float64)
     if ref.shape != tar.shape:
@@ -104,13 +111,19 @@ def register(reference, target, spacing=None, origin=None, config=None, guidance
     keep = []
     for name, arr, shape in (("guidance_image", guidance_image, ref.shape),
                              ("weight_tensor", weight_tensor, ref.shape + (D, D)),
-                             ("weight_image", weight_image, ref.shape)):
+                             ("weight_image", weight_image, ref.shape),
+                             ("initial_displacement", initial_displacement, ref.shape + (D,))):
         if arr is not None:
             a = np.ascontiguousarray(arr, np.float64)
             if a.shape != shape:
                 raise ValueError("%s must have shape %s" % (name, shape))
             keep.append(a)
             setattr(desc, name, dptr(a))
+    if on_level is not None:
+        def _level(level, ptr, _user):
+            on_level(int(level), np.ctypeslib.as_array(ptr, shape=ref.shape + (D,)).copy())
+        desc.level_done = abi.LEVEL_CALLBACK(_level)
+        keep.append(desc.level_done)
     disp = np.zeros(ref.shape + (D,))
     rep = RegisterReport()
     check(lib().skm_register(C.byref(desc), C.byref(geo), dptr(ref), dptr(tar), dptr(disp), C.byref(rep)))
@@ -150,4 +163,34 @@ def threshold_rescale(image, thresholds=(-1500, 3500), out_range=(0.0, 1.0)):
     tmin, tmax = (float(thresholds[0]), float(thresholds[1])) if apply else (0.0, 0.0)
     check(lib().skm_threshold_rescale(img.ndim, size, int(apply), tmin, tmax, float(out_range[0]),
                                       float(out_range[1]), dptr(img), dptr(out)))
+    return out
+
+
+def warp_image(image, displacement, image_spacing=None, image_origin=None, field_spacing=None, field_origin=None,
+               order=3, default_value=0.0):
+    """I(p + u(p)) on the displacement field's grid (WarpImage, include/itkUtils.h:163-178, order 3;
+    the final resampling of src/SKMReg.cxx:504-522, order 1) on the GPU."""
+    img = np.ascontiguousarray(image, np.float64)
+    u = np.ascontiguousarray(displacement, np.float64)
+    D = img.ndim
+    if u.ndim != D + 1 or u.shape[-1] != D:
+        raise ValueError("displacement must have shape (..., %d)" % D)
+    gi = Geometry.make(tuple(reversed(img.shape)), image_origin, image_spacing)
+    gf = Geometry.make(tuple(reversed(u.shape[:-1])), field_origin if field_origin is not None else image_origin,
+                       field_spacing if field_spacing is not None else image_spacing)
+    out = np.empty(u.shape[:-1])
+    check(lib().skm_warp_image(D, C.byref(gi), dptr(img), C.byref(gf), dptr(u), int(order), float(default_value),
+                               dptr(out)))
+    return out
+
+
+def jacobian_determinant(field, spacing=None):
+    """JacobianDeterminant (include/itkUtils.h:153-161) of a (..., D) vector field on the GPU."""
+    u = np.ascontiguousarray(field, np.float64)
+    D = u.ndim - 1
+    if D not in (2, 3) or u.shape[-1] != D:
+        raise ValueError("field must have shape (Y, X, 2) or (Z, Y, X, 3)")
+    geo = Geometry.make(tuple(reversed(u.shape[:-1])), None, spacing)
+    out = np.empty(u.shape[:-1])
+    check(lib().skm_jacobian_determinant(D, C.byref(geo), dptr(u), dptr(out)))
     return out
