@@ -30,6 +30,10 @@
 
 namespace skm {
 
+#ifndef SKM_WARP_HOIST
+#define SKM_WARP_HOIST 1
+#endif
+
 constexpr int kTabMaxPhase = 8;      // phases per axis
 constexpr int kTabMaxTap = 10;       // taps per axis
 constexpr int kTabContribThreads = 288;   // 9 warps
@@ -180,7 +184,38 @@ __global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev 
 #pragma unroll
     for (int k = 0; k < NQ; ++k) vf[k] = 0.f;
     const int total = (int)(T.ncell * T.nph);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const int stride = gridDim.x * blockDim.x;
+#if SKM_WARP_HOIST
+    // the grid stride is a multiple of the phase count (checked by the host): every texel of this
+    // thread has the same phase, so its offsets are computed once
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p_fix = i0 % T.nph;
+    int ph[3], xo[3];
+    {
+        const int pyz = p_fix / T.h[0], pz = pyz / T.h[1];
+        ph[0] = p_fix - pyz * T.h[0];
+        ph[1] = pyz - pz * T.h[1];
+        ph[2] = pz;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) xo[d] = T.h[d] * (T.qmin[d] - T.qoff[d][ph[d]]) + ph[d];
+    }
+    const int fn[3] = {P.fixed.n[0], P.fixed.n[1], P.fixed.n[2]};
+    const int hh[3] = {T.h[0], T.h[1], T.h[2]};
+    const int nq0 = T.nq[0], nq1 = T.nq[1];
+    const FastDiv dq0 = T.div_nq0, dq01 = T.div_nq01;
+    const int nphv = T.nph;
+    for (int i = i0, cell = i0 / nphv; i < total; i += stride, cell += stride / nphv) {
+        const int cyz = (int)dq0.div((uint32_t)cell), cz = (int)dq01.div((uint32_t)cell);
+        const int cc[3] = {cell - cyz * nq0, cyz - cz * nq1, cz};
+        int x[3];
+        bool ok = true;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            x[d] = hh[d] * cc[d] + xo[d];
+            if (x[d] < 0 || x[d] >= fn[d]) ok = false;
+        }
+#else
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
         const int cell = (int)T.div_nph.div((uint32_t)i);
         const int p_lin = i - cell * T.nph;
         const int cyz = (int)T.div_nq0.div((uint32_t)cell), cz = (int)T.div_nq01.div((uint32_t)cell);
@@ -194,6 +229,7 @@ __global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev 
             x[d] = T.h[d] * (T.qmin[d] + cc[d] - T.qoff[d][ph[d]]) + ph[d];
             if (x[d] < 0 || x[d] >= P.fixed.n[d]) ok = false;
         }
+#endif
         float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ok) {
             const int plane = total;
@@ -316,10 +352,17 @@ __global__ void __launch_bounds__(kTabContribThreads) table_contrib_kernel(Table
 // consecutive control points; its 8 warps split the taps (and the regularizer offsets) so that
 // every warp load reads 32 consecutive cells of one Contrib row; warp 0 then combines the 8
 // partial sums in a fixed order -- deterministic, no atomics.
-constexpr int kGatherGroups = 8;
+#ifndef SKM_GATHER_GROUPS
+#define SKM_GATHER_GROUPS 8
+#endif
+#ifndef SKM_GATHER_MINB
+#define SKM_GATHER_MINB 4
+#endif
+constexpr int kGatherGroups = SKM_GATHER_GROUPS;    // warps per block, each over a share of the taps
+constexpr int kGatherThreads = 32 * kGatherGroups;
 
 template <int D>
-__global__ void __launch_bounds__(256, 4) table_gather_kernel(EvalParams P, TableDev T, DerivParams Q)
+__global__ void __launch_bounds__(kGatherThreads, SKM_GATHER_MINB) table_gather_kernel(EvalParams P, TableDev T, DerivParams Q)
 {
     __shared__ float sacc[kGatherGroups][3][32];
     __shared__ float sreg[kGatherGroups][9][32];
@@ -675,7 +718,18 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     pl.transform_blocks = T.tiles_x * T.tiles_y * T.tiles_z;
     if (T.ncell * T.nph >= (1LL << 31) || (long long)D * T.ncell * T.nph >= (1LL << 31)) return 0;
     if (3LL * T.ntap * T.ncell >= (1LL << 31)) return 0;          // 32-bit contribution indices
-    T.value_blocks = (int)std::min<long long>((T.ncell * T.nph + 255) / 256, 148LL * 8);
+    {
+        // a grid stride that is a multiple of the phase count keeps every thread on one phase
+        long long vb = std::min<long long>((T.ncell * T.nph + 255) / 256, 148LL * 8);
+        int g = T.nph, b = 256;
+        while (b) {
+            const int t = g % b;
+            g = b;
+            b = t;
+        }
+        const long long m = T.nph / g;
+        T.value_blocks = (int)std::max<long long>(m, (vb / m) * m);
+    }
     T.div_nph = FastDiv((uint32_t)T.nph);
     T.div_nq0 = FastDiv((uint32_t)T.nq[0]);
     T.div_nq01 = FastDiv((uint32_t)(T.nq[0] * T.nq[1]));

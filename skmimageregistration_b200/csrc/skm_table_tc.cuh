@@ -37,11 +37,13 @@ namespace skm {
 
 constexpr int kTcEpiWarps = 4;                                   // warps 0-3: TMEM -> global
 constexpr int kTcMmaWarp = 4;                                    // warp 4: TMEM owner, lane 0 issues
-constexpr int kTcProdWarps = 8;                                  // warps 5-12: A operand stages
+constexpr int kTcProdWarps = 8;                                  // contrib producers
 constexpr int kTcProdThreads = kTcProdWarps * 32;
 constexpr int kTcProdBase = (kTcEpiWarps + 1) * 32;              // first producer thread
-constexpr int kTcThreads = kTcProdBase + kTcProdThreads;         // 416
-constexpr int kTcStages = 3;                                     // mbarrier slots (stages <= 3)
+constexpr int kTrProdWarps = 8;                                  // transform producers: warps 5-12,
+constexpr int kTrProdThreads = kTrProdWarps * 32;                // two per TMEM lane quarter
+constexpr int kTcThreads = kTcProdBase + kTrProdThreads;         // 416
+constexpr int kTcStages = 4;                                     // mbarrier slots (stages <= 4)
 constexpr int kTcKBlock = 32;                                    // K elements per 128-byte swizzle row
 constexpr int kTcRows = 128;
 constexpr int kTcProdBar = 1;                                    // named barrier of all producers
@@ -53,8 +55,8 @@ constexpr int kConEpiWarps = 8;
 constexpr int kConMmaWarp = kConEpiWarps;
 constexpr int kConProdBase = (kConEpiWarps + 1) * 32;
 constexpr int kConThreads = kConProdBase + kTcProdThreads;     // 544
-static_assert(kTcProdThreads * 4 == kTcRows * (kTcKBlock / 4), "transform producers: 4 items per thread");
-constexpr int kTcNumBars = 2 * kTcStages + 5;
+static_assert(kTrProdWarps == 8 && (kTcEpiWarps + 1) % 4 == 1, "transform producers: (lane quarter, K half) pairs");
+constexpr int kTcNumBars = 2 * kTcStages + 6;
 constexpr int kTcMaxRegion = 4096;                               // staged control points per brick
 constexpr size_t kTcSmemMax = 227 * 1024;
 
@@ -64,10 +66,14 @@ struct TcDev {
     int bx, by, bz;          // brick of cells per tile
     int tiles[3];
     int rx, ry, rz, rv;      // staged control-point region of a brick (rv padded to 4)
-    int kp;                  // taps padded to 32 (K)
+    int rvp;                 // region plane length (rx ry rz + 2, padded to 4)
+    int pairs_x;             // tap pairs per x row: ceil(nt0 / 2)
+    int npairs;              // tap pairs (two x-neighbouring taps, the second virtual when nt0 is odd)
+    int kp;                  // 4 * ceil(npairs / 2) padded to 32 (K): k = 4 u + j, unit u = pairs 2u, 2u + 1
     int np;                  // phases padded to 16 (half of N)
-    int ns_tr;               // shared-memory stages (one 32-tap K block each)
+    int ns_tr;               // A stages in TMEM (one 32-tap K block each: 32 hi + 32 lo columns)
     int tr_stride, tr_cols;  // TMEM columns per accumulator, allocated columns
+    int tr_abase;            // first TMEM column of the A stages
     const float *btr;        // 2 np rows x kp, K-major 128-byte swizzled
     // contrib
     int kpc;                 // phases padded to 32 (K)
@@ -82,10 +88,10 @@ struct TcDev {
 // producers (commit), acc_full[b] MMA -> epilogue (commit), acc_empty[b] epilogue -> MMA
 // (kTcEpiWarps * 32 arrivals), drain (final commit of the MMA thread)
 struct TcBars {
-    uint64_t *full, *empty, *acc_full, *acc_empty, *drain;
+    uint64_t *full, *empty, *acc_full, *acc_empty, *drain, *table;
     __device__ explicit TcBars(uint64_t *b)
         : full(b), empty(b + kTcStages), acc_full(b + 2 * kTcStages), acc_empty(b + 2 * kTcStages + 2),
-          drain(b + 2 * kTcStages + 4)
+          drain(b + 2 * kTcStages + 4), table(b + 2 * kTcStages + 5)
     {
     }
     __device__ void init(int full_count, int epi_threads = kTcEpiWarps * 32) const
@@ -99,6 +105,7 @@ struct TcBars {
             tc::mbar_init(&acc_empty[b], epi_threads);
         }
         tc::mbar_init(drain, 1);
+        tc::mbar_init(table, 1);
         tc::fence_mbarrier_init();
     }
 };
@@ -150,17 +157,19 @@ __device__ __forceinline__ void tc_teardown(const TcBars &B, uint32_t tmem, uint
 // A stages first (each [hi | lo], 128 rows x 32 K elements = 16 KB per half), then the table.
 constexpr int kTcStageBytes = 2 * kTcRows * kTcKBlock * 4;
 
+// Transform region: w * alpha of the brick's control points, split into tf32 hi and lo parts, each
+// in two copies (even: E[i] = R[i]; odd: O[i] = R[i + 1]) so that any two neighbouring elements
+// R[a], R[a + 1] are one aligned 8-byte load: plane (hilo * 2 + (a & 1)) * 3 + comp at a & ~1.
 struct TcTransformLayout {
-    int a, b, raw, rg, tapoff, regxyz, bars, total_bytes;
+    int b, raw, reg, pairoff, regxyz, bars, total_bytes;
     __host__ __device__ explicit TcTransformLayout(const TcDev &C)
     {
-        a = 0;
-        b = a + C.ns_tr * kTcStageBytes;
-        raw = b + C.kp * 2 * C.np * 4;                 // [rv] float4: staged w, alpha
-        rg = raw + 16 * C.rv;                          // [2][3][rv] floats: w * alpha planes, two tiles
-        tapoff = rg + 4 * 2 * 3 * C.rv;                // [kp] ints
-        regxyz = tapoff + 4 * C.kp;                    // [rv] ints: x | y << 10 | z << 20 of a region element
-        bars = regxyz + 4 * C.rv;                      // 16-byte aligned
+        b = 0;                                         // the table (A stages live in TMEM)
+        raw = b + C.kp * 2 * C.np * 4;                 // [rv] float4: staged alpha, w
+        reg = raw + 16 * C.rv;                         // [hi, lo][even, odd][3][rvp] floats
+        pairoff = reg + 4 * 4 * 3 * C.rvp;             // [kp / 4] int2: region offsets of a unit's pairs
+        regxyz = pairoff + 8 * (C.kp / 4);             // [rv] ints: x | y << 10 | z << 20 of a region element
+        bars = (regxyz + 4 * C.rv + 15) / 16 * 16;
         total_bytes = bars + 8 * kTcNumBars + 8 + 1024;   // + alignment slack of the base
     }
 };
@@ -184,70 +193,88 @@ __device__ __forceinline__ unsigned char *tc_aligned_smem(float4 *dyn)
 }
 
 // ------------------------------------------------------------------------------------------------
-// u(q, p) = sum_t T[p][t] (w alpha)[q + t] on the tensor cores; u planar [comp][cell][phase]
+// u(q, p) = sum_t T[p][t] (w alpha)[q + t] on the tensor cores; u planar [comp][cell][phase].
+// The A operand (im2col of the split region) goes from registers straight into TMEM stages
+// (tcgen05.st) and the MMAs read it there, so shared memory carries only the region reads and
+// the table reads of the tensor cores.
 __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalParams P, TableDev T, TcDev C)
 {
     extern __shared__ float4 tc_smem4[];
     unsigned char *sm = tc_aligned_smem(tc_smem4);
     const TcTransformLayout L(C);
-    unsigned char *As = sm + L.a;
     float *Bs = reinterpret_cast<float *>(sm + L.b);
     float4 *raw = reinterpret_cast<float4 *>(sm + L.raw);
-    float *Rg = reinterpret_cast<float *>(sm + L.rg);
-    int *tapoff = reinterpret_cast<int *>(sm + L.tapoff);
+    float *Reg = reinterpret_cast<float *>(sm + L.reg);
+    int2 *pairoff = reinterpret_cast<int2 *>(sm + L.pairoff);
     int *regxyz = reinterpret_cast<int *>(sm + L.regxyz);
     uint64_t *barmem = reinterpret_cast<uint64_t *>(sm + L.bars);
     const TcBars B(barmem);
     uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(barmem + kTcNumBars);
     volatile int *abort = reinterpret_cast<volatile int *>(tmem_holder + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int Kp = C.kp, Np = C.np, N2 = 2 * C.np, RV = C.rv, NS = C.ns_tr;
+    const int Kp = C.kp, Np = C.np, N2 = 2 * C.np, RVP = C.rvp, NS = C.ns_tr;
+    const int PS = 3 * RVP;                                  // floats per (hilo, parity) plane set
     const int D = T.D;
     const int ntiles = C.tiles[0] * C.tiles[1] * C.tiles[2];
     const int nchunk = Kp / kTcKBlock;
     const int brick = C.bx * C.by * C.bz;
     const int rtotal = C.rx * C.ry * C.rz;
+    const uint32_t table_bytes = (uint32_t)(Kp * N2 * 4);
 
     if (tid == 0) {
-        B.init(kTcProdThreads);
+        B.init(kTrProdThreads);
         *abort = 0;
     }
     if (warp == kTcMmaWarp) tc::tmem_alloc(tmem_holder, (uint32_t)C.tr_cols);
-    for (int i = tid; i < Kp * N2 / 4; i += kTcThreads)
-        reinterpret_cast<float4 *>(Bs)[i] = __ldg(reinterpret_cast<const float4 *>(C.btr) + i);
-    const int nt0 = T.nt[0], nt01 = T.nt[0] * T.nt[1];
-    for (int t = tid; t < Kp; t += kTcThreads)
-        tapoff[t] = t < T.ntap ? (t % nt0) + C.rx * ((t / nt0) % T.nt[1] + C.ry * (t / nt01)) : -1;
+    // unit u of the K axis = tap pairs 2u and 2u + 1 (pairs: x-neighbouring taps of one x row)
+    for (int u = tid; u < Kp / 4; u += kTcThreads) {
+        int off[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int pi = 2 * u + h;
+            const int tx = 2 * (pi % C.pairs_x), ty = (pi / C.pairs_x) % T.nt[1], tz = pi / (C.pairs_x * T.nt[1]);
+            off[h] = pi < C.npairs ? tx + C.rx * (ty + C.ry * tz) : 0;
+        }
+        pairoff[u] = make_int2(off[0], off[1]);
+    }
     for (int i = tid; i < rtotal; i += kTcThreads)
         regxyz[i] = (i % C.rx) | (((i / C.rx) % C.ry) << 10) | ((i / (C.rx * C.ry)) << 20);
-    tc::fence_proxy_async();
+    for (int i = tid; i < 4 * PS; i += kTcThreads) Reg[i] = 0.f;   // the padding stays zero
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tmem_holder;
+    if (tid == 0) {                                          // the table: one bulk copy
+        tc::mbar_expect_tx(B.table, table_bytes);
+        tc::bulk_g2s(Bs, C.btr, table_bytes, B.table);
+    }
 
     if (warp >= kTcEpiWarps + 1) {
-        // ---------------- producers: staged region -> im2col hi/lo stages ----------------
-        // Thread pt owns row r = pt % 128 of every stage and its K groups pt / 128 + 2u, u < 4.
+        // ---------------- producers: split region -> im2col hi/lo stages in TMEM ----------------
+        // A warp writes the TMEM lanes of its quarter (warp % 4): thread = row r, and half h of
+        // each 32-column K block (4 units of 4 columns), hi and lo.
+        const int q = warp & 3, h = (warp - (kTcEpiWarps + 1)) >> 2;
         const int pt = tid - kTcProdBase;
-        const int r = pt & (kTcRows - 1), jg0 = pt >> 7;
+        const int r = 32 * q + lane;
         const int comp = r / C.ct, c = r - comp * C.ct;
         const bool row_exists = comp < D && c < brick;
         const int cx = c % C.bx, cy = (c / C.bx) % C.by, cz = c / (C.bx * C.by);
-        const int rowoff = comp * RV + cx + C.rx * (cy + C.ry * cz);
+        // rows without a cell read real region data; the epilogue never stores them
+        const int rowbase = row_exists ? comp * RVP + cx + C.rx * (cy + C.ry * cz) : 0;
+        const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
         auto tile_origin = [&](int tile, int *q0) {
             const int t0 = tile % C.tiles[0], t12 = tile / C.tiles[0];
             q0[0] = t0 * C.bx;
             q0[1] = (t12 % C.tiles[1]) * C.by;
             q0[2] = (t12 / C.tiles[1]) * C.bz;
         };
-        // cp.async of the raw control points (w alpha computed on conversion) of a tile's region
+        // cp.async of the raw control points (alpha, w) of a tile's region
         auto fetch_region = [&](int tile) {
             int q0[3];
             tile_origin(tile, q0);
             const int j0[3] = {T.qmin[0] + q0[0] + T.tlo[0], T.qmin[1] + q0[1] + T.tlo[1],
                                T.qmin[2] + q0[2] + T.tlo[2]};
-            for (int i = pt; i < rtotal; i += kTcProdThreads) {
+            for (int i = pt; i < rtotal; i += kTrProdThreads) {
                 const int xyz = regxyz[i];
                 const int jx = j0[0] + (xyz & 1023), jy = j0[1] + ((xyz >> 10) & 1023), jz = j0[2] + (xyz >> 20);
                 const bool in = (unsigned)jx < (unsigned)P.cp.n[0] && (unsigned)jy < (unsigned)P.cp.n[1] &&
@@ -257,82 +284,105 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
             }
             cp_async_commit();
         };
-        // raw -> w alpha planes of buffer `buf`
-        auto convert_region = [&](int buf) {
-            float *R = Rg + buf * 3 * RV;
-            for (int i = pt; i < rtotal; i += kTcProdThreads) {
+        // raw -> w alpha, split into hi / lo, written to the even and odd copies
+        auto convert_region = [&]() {
+            for (int i = pt; i < rtotal; i += kTrProdThreads) {
                 const float4 cv = raw[i];
-                R[i] = cv.w * cv.x;
-                R[RV + i] = cv.w * cv.y;
-                R[2 * RV + i] = cv.w * cv.z;
+                const float v[3] = {cv.w * cv.x, cv.w * cv.y, cv.w * cv.z};
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    float hi, lo;
+                    tc::split_tf32(v[k], hi, lo);
+                    float *E = Reg + k * RVP;
+                    E[i] = hi;                               // hi, even
+                    E[2 * PS + i] = lo;                      // lo, even
+                    if (i > 0) {
+                        E[PS + i - 1] = hi;                  // hi, odd
+                        E[3 * PS + i - 1] = lo;              // lo, odd
+                    }
+                }
             }
         };
         if ((int)blockIdx.x < ntiles) {
             fetch_region(blockIdx.x);
             cp_async_wait_all();
-            tc::bar_sync(kTcProdBar, kTcProdThreads);
-            convert_region(0);
+            tc::bar_sync(kTcProdBar, kTrProdThreads);
+            convert_region();
         }
-        tc::bar_sync(kTcProdBar, kTcProdThreads);
+        tc::bar_sync(kTcProdBar, kTrProdThreads);
+        int s = 0;
+        uint32_t phase = 0;                                  // parity of stage s's current use
         unsigned g = 0;
         bool failed = false;
-        for (int it = 0; !failed; ++it) {
+        for (int it = 0;; ++it) {
             const int tile = blockIdx.x + it * gridDim.x;
             if (tile >= ntiles) break;
-            const int buf = it & 1;
             const int next = tile + gridDim.x;
             if (next < ntiles) fetch_region(next);          // raw is free: converted before the last barrier
-            int q0[3];
-            tile_origin(tile, q0);
-            const bool valid = row_exists && q0[0] + cx < T.nq[0] && q0[1] + cy < T.nq[1] && q0[2] + cz < T.nq[2];
-            const float *Rrow = Rg + buf * 3 * RV + rowoff;
             for (int kc = 0; kc < nchunk; ++kc, ++g) {
-                const int s = (int)(g % NS);
-                bool ok = true;
-                if (g >= (unsigned)NS) ok = tc::mbar_wait(&B.empty[s], ((g / NS) + 1) & 1, abort);
-                if (tc::bar_or(kTcProdBar, kTcProdThreads, !ok)) {
-                    if (pt == 0) tc_fail(abort, C.err);
-                    failed = true;
-                    break;
+                // a failed wait skips the rest of the tile (warp-uniform: tcgen05.st is warp-wide);
+                // the decision is made uniform across the producers at the tile's end
+                if (!failed && g >= (unsigned)NS) {
+                    const bool ok = tc::mbar_wait(&B.empty[s], phase ^ 1u, abort);
+                    if (__any_sync(0xffffffffu, !ok)) {
+                        if (lane == 0) tc_fail(abort, C.err);
+                        failed = true;
+                    }
                 }
-                unsigned char *Ahi = As + s * kTcStageBytes, *Alo = Ahi + kTcStageBytes / 2;
-                const int4 *tap4 = reinterpret_cast<const int4 *>(tapoff + kc * kTcKBlock);
-                float v[4][4];
+                if (!failed) {
+                    tc::fence_after_sync();
+                    float vh[16], vl[16];
+                    const int2 *po = pairoff + kc * (kTcKBlock / 4) + 4 * h;
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int4 o = tap4[jg0 + 2 * u];
-                    v[u][0] = (valid && o.x >= 0) ? Rrow[o.x] : 0.f;
-                    v[u][1] = (valid && o.y >= 0) ? Rrow[o.y] : 0.f;
-                    v[u][2] = (valid && o.z >= 0) ? Rrow[o.z] : 0.f;
-                    v[u][3] = (valid && o.w >= 0) ? Rrow[o.w] : 0.f;
+                    for (int u = 0; u < 4; ++u) {
+                        const int2 o = po[u];
+                        const int a0 = rowbase + o.x, a1 = rowbase + o.y;
+                        const int e0 = (a0 & 1) * PS + (a0 & ~1), e1 = (a1 & 1) * PS + (a1 & ~1);
+                        const float2 h0 = *reinterpret_cast<const float2 *>(Reg + e0);
+                        const float2 h1 = *reinterpret_cast<const float2 *>(Reg + e1);
+                        const float2 l0 = *reinterpret_cast<const float2 *>(Reg + 2 * PS + e0);
+                        const float2 l1 = *reinterpret_cast<const float2 *>(Reg + 2 * PS + e1);
+                        vh[4 * u] = h0.x;
+                        vh[4 * u + 1] = h0.y;
+                        vh[4 * u + 2] = h1.x;
+                        vh[4 * u + 3] = h1.y;
+                        vl[4 * u] = l0.x;
+                        vl[4 * u + 1] = l0.y;
+                        vl[4 * u + 2] = l1.x;
+                        vl[4 * u + 3] = l1.y;
+                    }
+                    const uint32_t col = (uint32_t)(C.tr_abase + 2 * kTcKBlock * s + 16 * h);
+                    tc::tmem_st16(tmem + lane_addr + col, vh);
+                    tc::tmem_st16(tmem + lane_addr + col + kTcKBlock, vl);
+                    tc::tmem_wait_st();
+                    tc::fence_before_sync();
+                    tc::mbar_arrive(&B.full[s]);
                 }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    float4 h, l;
-                    split4(v[u], h, l);
-                    const uint32_t off = tc::sw128_offset(r, 4 * (jg0 + 2 * u), kTcRows);
-                    *reinterpret_cast<float4 *>(Ahi + off) = h;
-                    *reinterpret_cast<float4 *>(Alo + off) = l;
+                if (++s == NS) {
+                    s = 0;
+                    phase ^= 1u;
                 }
-                tc::fence_proxy_async();
-                tc::mbar_arrive(&B.full[s]);
             }
-            if (failed) break;
+            // every producer has finished the tile (and read the region for the last time)
+            if (tc::bar_or(kTcProdBar, kTrProdThreads, failed)) break;
             if (next < ntiles) {
                 cp_async_wait_all();
-                tc::bar_sync(kTcProdBar, kTcProdThreads);   // every thread's copies have landed
-                convert_region(buf ^ 1);
+                tc::bar_sync(kTcProdBar, kTrProdThreads);   // every thread's copies have landed
+                convert_region();
             }
-            tc::bar_sync(kTcProdBar, kTcProdThreads);
+            tc::bar_sync(kTcProdBar, kTrProdThreads);
         }
         cp_async_wait_all();
     } else if (warp == kTcMmaWarp) {
         // ---------------- MMA issue (one thread) ----------------
         if (lane == 0) {
             const uint32_t idesc_cat = tc::idesc_tf32(kTcRows, N2), idesc_hi = tc::idesc_tf32(kTcRows, Np);
-            const uint32_t a_base = tc::smem_addr(As), b_base = tc::smem_addr(Bs);
-            unsigned g = 0;
-            for (int it = 0;; ++it) {
+            const uint32_t b_base = tc::smem_addr(Bs);
+            bool ok = tc::mbar_wait(B.table, 0, abort);      // the table has landed
+            if (!ok) tc_fail(abort, C.err);
+            int s = 0;
+            uint32_t phase = 0;
+            for (int it = 0; ok; ++it) {
                 const int tile = blockIdx.x + it * gridDim.x;
                 if (tile >= ntiles) break;
                 const int b = it & 1;
@@ -342,27 +392,28 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
                 }
                 tc::fence_after_sync();
                 bool failed = false;
-                for (int kc = 0; kc < nchunk; ++kc, ++g) {
-                    const int s = (int)(g % NS);
-                    if (!tc::mbar_wait(&B.full[s], (g / NS) & 1, abort)) {
+                for (int kc = 0; kc < nchunk; ++kc) {
+                    if (!tc::mbar_wait(&B.full[s], phase, abort)) {
                         tc_fail(abort, C.err);
                         failed = true;
                         break;
                     }
                     tc::fence_after_sync();
                     const uint32_t dacc = tmem + (uint32_t)(b * C.tr_stride);
-                    const uint32_t ahi = a_base + (uint32_t)(s * kTcStageBytes);
-                    const uint32_t alo = ahi + (uint32_t)(kTcStageBytes / 2);
+                    const uint32_t ahi = tmem + (uint32_t)(C.tr_abase + 2 * kTcKBlock * s);
+                    const uint32_t alo = ahi + (uint32_t)kTcKBlock;
                     const uint32_t bk = b_base + (uint32_t)kc * (uint32_t)N2 * 128u;   // K block kc of the table
 #pragma unroll
                     for (int ks = 0; ks < kTcKBlock / 8; ++ks) {
-                        const uint64_t dah = tc::smem_desc_sw128(ahi + 32u * ks);
-                        const uint64_t dal = tc::smem_desc_sw128(alo + 32u * ks);
                         const uint64_t db = tc::smem_desc_sw128(bk + 32u * ks);
-                        tc::mma_tf32(dacc, dah, db, idesc_cat, (kc | ks) != 0);
-                        tc::mma_tf32(dacc, dal, db, idesc_hi, 1);
+                        tc::mma_tf32_tmem_a(dacc, ahi + 8u * ks, db, idesc_cat, (kc | ks) != 0);
+                        tc::mma_tf32_tmem_a(dacc, alo + 8u * ks, db, idesc_hi, 1);
                     }
                     tc::commit(&B.empty[s]);
+                    if (++s == NS) {
+                        s = 0;
+                        phase ^= 1u;
+                    }
                 }
                 if (failed) break;
                 tc::commit(&B.acc_full[b]);
@@ -413,6 +464,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
             tc::mbar_arrive(&B.acc_empty[b]);
         }
     }
+    // the table copy has completed before the teardown frees nothing in shared memory it writes:
+    // the MMA thread waited for it, or (no tile) wait here (bounded)
+    if (tid == 0 && (int)blockIdx.x >= ntiles) tc::mbar_wait(B.table, 0, abort);
     tc_teardown(B, tmem, (uint32_t)C.tr_cols);
 }
 
@@ -657,18 +711,30 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
     if (T.D != 2 && T.D != 3) return 0;
     C.ct = kTcRows / T.D;
     C.np = (T.nph + 15) / 16 * 16;
-    C.kp = (T.ntap + kTcKBlock - 1) / kTcKBlock * kTcKBlock;
+    // transform K axis: x-neighbouring tap pairs (the second tap of a row's last pair is virtual
+    // when nt0 is odd), two pairs per 16-byte unit
+    C.pairs_x = (T.nt[0] + 1) / 2;
+    C.npairs = C.pairs_x * T.nt[1] * T.nt[2];
+    C.kp = (4 * ((C.npairs + 1) / 2) + kTcKBlock - 1) / kTcKBlock * kTcKBlock;
     C.npc = (T.ntap + 15) / 16 * 16;
     C.kpc = (T.nph + kTcKBlock - 1) / kTcKBlock * kTcKBlock;
     if (2 * C.np > 256 || C.npc > 256) return 0;
-    // brick of at most ct cells with the fewest tiles (then the smallest staged region)
+    const int xpad = 2 * C.pairs_x - T.nt[0];                    // virtual column of odd tap rows
+    // brick of at most ct cells with the fewest tiles (then the smallest staged region), whose
+    // transform layout fits the shared memory with two stages
     long long best_tiles = -1, best_rv = 0;
     for (int bz = 1; bz <= std::min(C.ct, T.nq[2]); ++bz)
         for (int by = 1; by <= std::min(C.ct / bz, T.nq[1]); ++by)
             for (int bx = 1; bx <= std::min(C.ct / (bz * by), T.nq[0]); ++bx) {
                 const long long tiles = (long long)((T.nq[0] + bx - 1) / bx) * ((T.nq[1] + by - 1) / by) *
                                         ((T.nq[2] + bz - 1) / bz);
-                const long long rv = (long long)(bx + T.nt[0] - 1) * (by + T.nt[1] - 1) * (bz + T.nt[2] - 1);
+                const long long rv =
+                    (long long)(bx + T.nt[0] - 1 + xpad) * (by + T.nt[1] - 1) * (bz + T.nt[2] - 1);
+                if (rv > kTcMaxRegion) continue;
+                TcDev probe = C;
+                probe.rv = (int)((rv + 3) / 4 * 4);
+                probe.rvp = (int)((rv + 2 + 3) / 4 * 4);
+                if ((size_t)TcTransformLayout(probe).total_bytes > kTcSmemMax) continue;
                 if (best_tiles < 0 || tiles < best_tiles || (tiles == best_tiles && rv < best_rv)) {
                     best_tiles = tiles;
                     best_rv = rv;
@@ -681,19 +747,21 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
     C.tiles[0] = (T.nq[0] + C.bx - 1) / C.bx;
     C.tiles[1] = (T.nq[1] + C.by - 1) / C.by;
     C.tiles[2] = (T.nq[2] + C.bz - 1) / C.bz;
-    C.rx = C.bx + T.nt[0] - 1;
+    C.rx = C.bx + T.nt[0] - 1 + xpad;
     C.ry = C.by + T.nt[1] - 1;
     C.rz = C.bz + T.nt[2] - 1;
     if (C.rx * C.ry * C.rz > kTcMaxRegion || C.rx >= 1024 || C.ry >= 1024) return 0;
     C.rv = (C.rx * C.ry * C.rz + 3) / 4 * 4;
+    C.rvp = (C.rx * C.ry * C.rz + 2 + 3) / 4 * 4;
     C.tr_stride = (int)pow2_at_least(2 * C.np);
-    C.tr_cols = 2 * C.tr_stride;
+    C.tr_abase = 2 * C.tr_stride;                            // then the A stages: 64 columns each
+    C.tr_cols = 512;
+    C.ns_tr = std::min(kTcStages, (C.tr_cols - C.tr_abase) / (2 * kTcKBlock));
+    if (C.ns_tr < 2) return 0;
     C.con_stride = (int)pow2_at_least(C.npc);
     C.con_cols = 2 * C.con_stride;
     if (C.tr_cols > 512 || C.con_cols > 512) return 0;
     // as many stages (up to 3, at least 2) as the shared memory holds
-    for (C.ns_tr = 3; C.ns_tr > 2 && (size_t)TcTransformLayout(C).total_bytes > kTcSmemMax; --C.ns_tr) {
-    }
     for (C.ns_con = 3; C.ns_con > 2 && (size_t)TcContribLayout(C).total_bytes > kTcSmemMax; --C.ns_con) {
     }
     tc.transform_smem = (size_t)TcTransformLayout(C).total_bytes;
@@ -712,11 +780,25 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
         for (int t = 0; t < T.ntap; ++t) {
             const float v = tgemm[(size_t)p * T.ntap_pad + t];
             const float hi = tf32_hi_host(v), lo = v - hi;
-            btr[kmaj(p, t, 2 * C.np)] = hi;
-            btr[kmaj(C.np + p, t, 2 * C.np)] = lo;
             bcon[kmaj(t, p, C.npc)] = hi;
             bcon[lo_off + kmaj(t, p, C.npc)] = lo;
         }
+    // transform table in the pair order of the K axis: k = 4 u + j is tap (tx + (j & 1), ty, tz) of
+    // pair 2 u + (j >> 1) = (tx / 2, ty, tz); virtual taps and padding stay zero
+    for (int k = 0; k < C.kp; ++k) {
+        const int pi = 2 * (k / 4) + ((k & 3) >> 1);
+        if (pi >= C.npairs) continue;
+        const int tx = 2 * (pi % C.pairs_x) + (k & 1), ty = (pi / C.pairs_x) % T.nt[1],
+                  tz = pi / (C.pairs_x * T.nt[1]);
+        if (tx >= T.nt[0]) continue;
+        const int t = tx + T.nt[0] * (ty + T.nt[1] * tz);
+        for (int p = 0; p < T.nph; ++p) {
+            const float v = tgemm[(size_t)p * T.ntap_pad + t];
+            const float hi = tf32_hi_host(v), lo = v - hi;
+            btr[kmaj(p, k, 2 * C.np)] = hi;
+            btr[kmaj(C.np + p, k, 2 * C.np)] = lo;
+        }
+    }
     if (cudaMalloc((void **)&tc.d_btr, btr.size() * sizeof(float)) != cudaSuccess) return 2;
     if (cudaMalloc((void **)&tc.d_bcon, bcon.size() * sizeof(float)) != cudaSuccess) return 2;
     if (cudaMalloc((void **)&tc.d_err, sizeof(unsigned)) != cudaSuccess) return 2;
@@ -815,9 +897,9 @@ inline int table_derivative(TablePlan &pl, const TcPlan *tc, const EvalParams &P
     }
     if (mid && cudaEventRecord(mid, s) != cudaSuccess) return 2;
     if (D == 3)
-        table_gather_kernel<3><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+        table_gather_kernel<3><<<gather_blocks, kGatherThreads, 0, s>>>(P, pl.dev, Q);
     else
-        table_gather_kernel<2><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+        table_gather_kernel<2><<<gather_blocks, kGatherThreads, 0, s>>>(P, pl.dev, Q);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
@@ -825,9 +907,9 @@ inline int table_derivative_gather_only(TablePlan &pl, const EvalParams &P, cons
                                         int gather_blocks, cudaStream_t s)
 {
     if (D == 3)
-        table_gather_kernel<3><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+        table_gather_kernel<3><<<gather_blocks, kGatherThreads, 0, s>>>(P, pl.dev, Q);
     else
-        table_gather_kernel<2><<<gather_blocks, 256, 0, s>>>(P, pl.dev, Q);
+        table_gather_kernel<2><<<gather_blocks, kGatherThreads, 0, s>>>(P, pl.dev, Q);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
