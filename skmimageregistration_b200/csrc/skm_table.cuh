@@ -30,9 +30,6 @@
 
 namespace skm {
 
-#ifndef SKM_WARP_HOIST
-#define SKM_WARP_HOIST 1
-#endif
 
 constexpr int kTabMaxPhase = 8;      // phases per axis
 constexpr int kTabMaxTap = 10;       // taps per axis
@@ -58,7 +55,9 @@ struct TableDev {
     float4 *rec;         // [cell][phase]: grad M, m
     float *ucp;          // [comp][cell][phase]: u = sum_t T w alpha (planes of ncell*nph)
     const float *fixcp;  // [cell][phase]: fixed image value (0 outside)
-    float *contrib;      // [3][ntap][ncell]
+    float *contrib;      // [3][ngtap][ncell]
+    const int *gtap;     // contrib tap k -> box tap index (NULL: identity, all ntap box taps)
+    int ngtap;           // taps in the contrib layout
     double *part;        // [NQ][value blocks]
     unsigned *tc_err;    // failure word of the tensor-core kernels (NULL without them)
     int value_blocks, tile_x, tile_y, tiles_x, tiles_y, tiles_z;
@@ -176,7 +175,7 @@ __global__ void __launch_bounds__(256, 2) table_transform_kernel(EvalParams P, T
 // metric statistics (FP64 block partials) and the (grad M, m) record, all in cell-phase order
 // so that a warp covers a compact brick of texels.
 template <int D>
-__global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev T, int metric, double *stats,
+__global__ void __launch_bounds__(256, 4) table_warp_kernel(EvalParams P, TableDev T, int metric, double *stats,
                                                          unsigned *counter)
 {
     __shared__ double sh[NQ * 32];
@@ -185,7 +184,6 @@ __global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev 
     for (int k = 0; k < NQ; ++k) vf[k] = 0.f;
     const int total = (int)(T.ncell * T.nph);
     const int stride = gridDim.x * blockDim.x;
-#if SKM_WARP_HOIST
     // the grid stride is a multiple of the phase count (checked by the host): every texel of this
     // thread has the same phase, so its offsets are computed once
     const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
@@ -214,22 +212,6 @@ __global__ void __launch_bounds__(256) table_warp_kernel(EvalParams P, TableDev 
             x[d] = hh[d] * cc[d] + xo[d];
             if (x[d] < 0 || x[d] >= fn[d]) ok = false;
         }
-#else
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        const int cell = (int)T.div_nph.div((uint32_t)i);
-        const int p_lin = i - cell * T.nph;
-        const int cyz = (int)T.div_nq0.div((uint32_t)cell), cz = (int)T.div_nq01.div((uint32_t)cell);
-        const int cc[3] = {cell - cyz * T.nq[0], cyz - cz * T.nq[1], cz};
-        const int pyz = (int)T.div_h0.div((uint32_t)p_lin), pz = (int)T.div_h01.div((uint32_t)p_lin);
-        const int ph[3] = {p_lin - pyz * T.h[0], pyz - pz * T.h[1], pz};
-        int x[3];
-        bool ok = true;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            x[d] = T.h[d] * (T.qmin[d] + cc[d] - T.qoff[d][ph[d]]) + ph[d];
-            if (x[d] < 0 || x[d] >= P.fixed.n[d]) ok = false;
-        }
-#endif
         float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ok) {
             const int plane = total;
@@ -352,17 +334,11 @@ __global__ void __launch_bounds__(kTabContribThreads) table_contrib_kernel(Table
 // consecutive control points; its 8 warps split the taps (and the regularizer offsets) so that
 // every warp load reads 32 consecutive cells of one Contrib row; warp 0 then combines the 8
 // partial sums in a fixed order -- deterministic, no atomics.
-#ifndef SKM_GATHER_GROUPS
-#define SKM_GATHER_GROUPS 8
-#endif
-#ifndef SKM_GATHER_MINB
-#define SKM_GATHER_MINB 4
-#endif
-constexpr int kGatherGroups = SKM_GATHER_GROUPS;    // warps per block, each over a share of the taps
+constexpr int kGatherGroups = 8;                    // warps per block, each over a share of the taps
 constexpr int kGatherThreads = 32 * kGatherGroups;
 
 template <int D>
-__global__ void __launch_bounds__(kGatherThreads, SKM_GATHER_MINB) table_gather_kernel(EvalParams P, TableDev T, DerivParams Q)
+__global__ void __launch_bounds__(kGatherThreads, 4) table_gather_kernel(EvalParams P, TableDev T, DerivParams Q)
 {
     __shared__ float sacc[kGatherGroups][3][32];
     __shared__ float sreg[kGatherGroups][9][32];
@@ -375,9 +351,11 @@ __global__ void __launch_bounds__(kGatherThreads, SKM_GATHER_MINB) table_gather_
         kcp_s[i] = T.kcp[i];
         kcpo_s[i] = T.kcpo[i];
     }
-    for (int i = threadIdx.x; i < T.ntap; i += blockDim.x)
-        tapoff[i] = make_int4(T.tlo[0] + T.qmin[0] + i % T.nt[0], T.tlo[1] + T.qmin[1] + (i / T.nt[0]) % T.nt[1],
+    for (int k = threadIdx.x; k < T.ngtap; k += blockDim.x) {
+        const int i = T.gtap ? T.gtap[k] : k;
+        tapoff[k] = make_int4(T.tlo[0] + T.qmin[0] + i % T.nt[0], T.tlo[1] + T.qmin[1] + (i / T.nt[0]) % T.nt[1],
                               T.tlo[2] + T.qmin[2] + i / (T.nt[0] * T.nt[1]), 0);
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31, grp = threadIdx.x >> 5;
     const long long j_lin = (long long)blockIdx.x * 32 + lane;
@@ -389,7 +367,7 @@ __global__ void __launch_bounds__(kGatherThreads, SKM_GATHER_MINB) table_gather_
     if (active && !Q.values_only) {
         // groups of kU taps: all loads first (independent, predicated), then the sums in tap order
         constexpr int kU = 8;
-        const int ntap = T.ntap, ncell = (int)T.ncell;
+        const int ntap = T.ngtap, ncell = (int)T.ncell;
         const float *c0p = T.contrib, *c1p = T.contrib + ntap * ncell, *c2p = T.contrib + 2 * ntap * ncell;
         for (int base = grp; base < ntap; base += kGatherGroups * kU) {
             float v[kU][3];
@@ -661,6 +639,8 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     }
     T.ntap = T.nt[0] * T.nt[1] * T.nt[2];
     T.ntap_pad = ((T.ntap + kTabTapChunk - 1) / kTabTapChunk) * kTabTapChunk;
+    T.gtap = nullptr;
+    T.ngtap = T.ntap;
     // cells covering the fixed image
     long long ncell = 1;
     for (int d = 0; d < 3; ++d) {

@@ -40,9 +40,11 @@ constexpr int kTcMmaWarp = 4;                                    // warp 4: TMEM
 constexpr int kTcProdWarps = 8;                                  // contrib producers
 constexpr int kTcProdThreads = kTcProdWarps * 32;
 constexpr int kTcProdBase = (kTcEpiWarps + 1) * 32;              // first producer thread
-constexpr int kTrProdWarps = 8;                                  // transform producers: warps 5-12,
-constexpr int kTrProdThreads = kTrProdWarps * 32;                // two per TMEM lane quarter
-constexpr int kTcThreads = kTcProdBase + kTrProdThreads;         // 416
+constexpr int kTrProdWarps = 8;                                  // transform producers: warps 5.., a
+constexpr int kTrProdThreads = kTrProdWarps * 32;                // K slice of one TMEM lane quarter each
+constexpr int kTrSlices = kTrProdWarps / 4;                      // K slices of a 32-column block
+constexpr int kTrCols = 32 / kTrSlices;                          // columns per producer warp and K block
+constexpr int kTcThreads = kTcProdBase + kTrProdThreads;
 constexpr int kTcStages = 4;                                     // mbarrier slots (stages <= 4)
 constexpr int kTcKBlock = 32;                                    // K elements per 128-byte swizzle row
 constexpr int kTcRows = 128;
@@ -55,7 +57,8 @@ constexpr int kConEpiWarps = 8;
 constexpr int kConMmaWarp = kConEpiWarps;
 constexpr int kConProdBase = (kConEpiWarps + 1) * 32;
 constexpr int kConThreads = kConProdBase + kTcProdThreads;     // 544
-static_assert(kTrProdWarps == 8 && (kTcEpiWarps + 1) % 4 == 1, "transform producers: (lane quarter, K half) pairs");
+static_assert((kTrProdWarps == 8 || kTrProdWarps == 16) && (kTcEpiWarps + 1) % 4 == 1,
+              "transform producers: (lane quarter, K slice) pairs");
 constexpr int kTcNumBars = 2 * kTcStages + 6;
 constexpr int kTcMaxRegion = 4096;                               // staged control points per brick
 constexpr size_t kTcSmemMax = 227 * 1024;
@@ -69,6 +72,7 @@ struct TcDev {
     int rvp;                 // region plane length (rx ry rz + 2, padded to 4)
     int pairs_x;             // tap pairs per x row: ceil(nt0 / 2)
     int npairs;              // tap pairs (two x-neighbouring taps, the second virtual when nt0 is odd)
+                             // with a nonzero table column
     int kp;                  // 4 * ceil(npairs / 2) padded to 32 (K): k = 4 u + j, unit u = pairs 2u, 2u + 1
     int np;                  // phases padded to 16 (half of N)
     int ns_tr;               // A stages in TMEM (one 32-tap K block each: 32 hi + 32 lo columns)
@@ -76,8 +80,10 @@ struct TcDev {
     int tr_abase;            // first TMEM column of the A stages
     const float *btr;        // 2 np rows x kp, K-major 128-byte swizzled
     // contrib
+    const int2 *pairoff;     // [kp / 4]: region offsets (tx + rx (ty + ry tz)) of a unit's two pairs
     int kpc;                 // phases padded to 32 (K)
-    int npc;                 // taps padded to 16 (N)
+    int nct;                 // contrib taps: the box taps with a nonzero table column
+    int npc;                 // nct padded to 16 (N)
     int ns_con;              // shared-memory stages (one 32-phase K block each)
     int con_stride, con_cols;
     const float *bcon;       // npc rows x kpc, K-major 128-byte swizzled: hi, then lo
@@ -227,16 +233,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
     }
     if (warp == kTcMmaWarp) tc::tmem_alloc(tmem_holder, (uint32_t)C.tr_cols);
     // unit u of the K axis = tap pairs 2u and 2u + 1 (pairs: x-neighbouring taps of one x row)
-    for (int u = tid; u < Kp / 4; u += kTcThreads) {
-        int off[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int pi = 2 * u + h;
-            const int tx = 2 * (pi % C.pairs_x), ty = (pi / C.pairs_x) % T.nt[1], tz = pi / (C.pairs_x * T.nt[1]);
-            off[h] = pi < C.npairs ? tx + C.rx * (ty + C.ry * tz) : 0;
-        }
-        pairoff[u] = make_int2(off[0], off[1]);
-    }
+    for (int u = tid; u < Kp / 4; u += kTcThreads) pairoff[u] = C.pairoff[u];
     for (int i = tid; i < rtotal; i += kTcThreads)
         regxyz[i] = (i % C.rx) | (((i / C.rx) % C.ry) << 10) | ((i / (C.rx * C.ry)) << 20);
     for (int i = tid; i < 4 * PS; i += kTcThreads) Reg[i] = 0.f;   // the padding stays zero
@@ -251,8 +248,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
 
     if (warp >= kTcEpiWarps + 1) {
         // ---------------- producers: split region -> im2col hi/lo stages in TMEM ----------------
-        // A warp writes the TMEM lanes of its quarter (warp % 4): thread = row r, and half h of
-        // each 32-column K block (4 units of 4 columns), hi and lo.
+        // A warp writes the TMEM lanes of its quarter (warp % 4): thread = row r, and slice h of
+        // each 32-column K block (kTrCols / 4 units of 4 columns), hi and lo.
         const int q = warp & 3, h = (warp - (kTcEpiWarps + 1)) >> 2;
         const int pt = tid - kTcProdBase;
         const int r = 32 * q + lane;
@@ -331,10 +328,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
                 }
                 if (!failed) {
                     tc::fence_after_sync();
-                    float vh[16], vl[16];
-                    const int2 *po = pairoff + kc * (kTcKBlock / 4) + 4 * h;
+                    float vh[kTrCols], vl[kTrCols];
+                    const int2 *po = pairoff + kc * (kTcKBlock / 4) + (kTrCols / 4) * h;
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
+                    for (int u = 0; u < kTrCols / 4; ++u) {
                         const int2 o = po[u];
                         const int a0 = rowbase + o.x, a1 = rowbase + o.y;
                         const int e0 = (a0 & 1) * PS + (a0 & ~1), e1 = (a1 & 1) * PS + (a1 & ~1);
@@ -351,9 +348,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
                         vl[4 * u + 2] = l1.x;
                         vl[4 * u + 3] = l1.y;
                     }
-                    const uint32_t col = (uint32_t)(C.tr_abase + 2 * kTcKBlock * s + 16 * h);
-                    tc::tmem_st16(tmem + lane_addr + col, vh);
-                    tc::tmem_st16(tmem + lane_addr + col + kTcKBlock, vl);
+                    const uint32_t col = (uint32_t)(C.tr_abase + 2 * kTcKBlock * s + kTrCols * h);
+                    if (kTrCols == 16) {
+                        tc::tmem_st16(tmem + lane_addr + col, vh);
+                        tc::tmem_st16(tmem + lane_addr + col + kTcKBlock, vl);
+                    } else {
+                        tc::tmem_st8(tmem + lane_addr + col, vh);
+                        tc::tmem_st8(tmem + lane_addr + col + kTcKBlock, vl);
+                    }
                     tc::tmem_wait_st();
                     tc::fence_before_sync();
                     tc::mbar_arrive(&B.full[s]);
@@ -655,10 +657,10 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
                 float v[16];
                 tc::tmem_ld16(tb + (uint32_t)(16 * j), v);
                 if (valid) {
-                    float *dst = T.contrib + (comp * T.ntap + 16 * j) * ncell + cell;
+                    float *dst = T.contrib + (comp * C.nct + 16 * j) * ncell + cell;
 #pragma unroll
                     for (int e = 0; e < 16; ++e)
-                        if (16 * j + e < T.ntap) dst[e * ncell] = v[e];
+                        if (16 * j + e < C.nct) dst[e * ncell] = v[e];
                 }
             }
             tc::fence_before_sync();
@@ -694,6 +696,8 @@ struct TcPlan {
     bool enabled = false;
     TcDev dev{};
     float *d_btr = nullptr, *d_bcon = nullptr;
+    int2 *d_pairoff = nullptr;
+    int *d_ctap = nullptr;           // contrib tap k -> box tap
     unsigned *d_err = nullptr;
     int transform_blocks = 0, contrib_blocks = 0;
     size_t transform_smem = 0, contrib_smem = 0;
@@ -713,10 +717,27 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
     C.np = (T.nph + 15) / 16 * 16;
     // transform K axis: x-neighbouring tap pairs (the second tap of a row's last pair is virtual
     // when nt0 is odd), two pairs per 16-byte unit
+    // taps whose table column is zero for every phase contribute nothing: both GEMMs skip them
+    std::vector<char> nz((size_t)T.ntap, 0);
+    for (int t = 0; t < T.ntap; ++t)
+        for (int p = 0; p < T.nph && !nz[(size_t)t]; ++p) nz[(size_t)t] = tgemm[(size_t)p * T.ntap_pad + t] != 0.f;
+    std::vector<int> ctap;                                   // contrib taps, box order
+    for (int t = 0; t < T.ntap; ++t)
+        if (nz[(size_t)t]) ctap.push_back(t);
+    if (ctap.empty()) return 0;
     C.pairs_x = (T.nt[0] + 1) / 2;
-    C.npairs = C.pairs_x * T.nt[1] * T.nt[2];
+    std::vector<int> pairs;                                  // box index of a pair's first tap
+    for (int tz = 0; tz < T.nt[2]; ++tz)
+        for (int ty = 0; ty < T.nt[1]; ++ty)
+            for (int px = 0; px < C.pairs_x; ++px) {
+                const int t0 = 2 * px + T.nt[0] * (ty + T.nt[1] * tz);
+                const bool second = 2 * px + 1 < T.nt[0];
+                if (nz[(size_t)t0] || (second && nz[(size_t)t0 + 1])) pairs.push_back(t0);
+            }
+    C.npairs = (int)pairs.size();
     C.kp = (4 * ((C.npairs + 1) / 2) + kTcKBlock - 1) / kTcKBlock * kTcKBlock;
-    C.npc = (T.ntap + 15) / 16 * 16;
+    C.nct = (int)ctap.size();
+    C.npc = (C.nct + 15) / 16 * 16;
     C.kpc = (T.nph + kTcKBlock - 1) / kTcKBlock * kTcKBlock;
     if (2 * C.np > 256 || C.npc > 256) return 0;
     const int xpad = 2 * C.pairs_x - T.nt[0];                    // virtual column of odd tap rows
@@ -777,21 +798,28 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
     std::vector<float> bcon((size_t)2 * C.kpc * C.npc, 0.f);
     const size_t lo_off = (size_t)C.kpc * C.npc;
     for (int p = 0; p < T.nph; ++p)
-        for (int t = 0; t < T.ntap; ++t) {
-            const float v = tgemm[(size_t)p * T.ntap_pad + t];
+        for (int k = 0; k < C.nct; ++k) {
+            const float v = tgemm[(size_t)p * T.ntap_pad + ctap[(size_t)k]];
             const float hi = tf32_hi_host(v), lo = v - hi;
-            bcon[kmaj(t, p, C.npc)] = hi;
-            bcon[lo_off + kmaj(t, p, C.npc)] = lo;
+            bcon[kmaj(k, p, C.npc)] = hi;
+            bcon[lo_off + kmaj(k, p, C.npc)] = lo;
         }
-    // transform table in the pair order of the K axis: k = 4 u + j is tap (tx + (j & 1), ty, tz) of
-    // pair 2 u + (j >> 1) = (tx / 2, ty, tz); virtual taps and padding stay zero
+    // transform table in the pair order of the K axis: k = 4 u + j is tap t0 + (j & 1) of pair
+    // 2 u + (j >> 1) (t0 its first box tap); virtual taps and padding stay zero
+    std::vector<int2> pairoff((size_t)C.kp / 4, int2{0, 0});
+    auto region_off = [&](int t) {
+        return t % T.nt[0] + C.rx * ((t / T.nt[0]) % T.nt[1] + C.ry * (t / (T.nt[0] * T.nt[1])));
+    };
+    for (int u = 0; u < C.kp / 4; ++u) {
+        pairoff[(size_t)u].x = 2 * u < C.npairs ? region_off(pairs[(size_t)(2 * u)]) : 0;
+        pairoff[(size_t)u].y = 2 * u + 1 < C.npairs ? region_off(pairs[(size_t)(2 * u + 1)]) : 0;
+    }
     for (int k = 0; k < C.kp; ++k) {
         const int pi = 2 * (k / 4) + ((k & 3) >> 1);
         if (pi >= C.npairs) continue;
-        const int tx = 2 * (pi % C.pairs_x) + (k & 1), ty = (pi / C.pairs_x) % T.nt[1],
-                  tz = pi / (C.pairs_x * T.nt[1]);
-        if (tx >= T.nt[0]) continue;
-        const int t = tx + T.nt[0] * (ty + T.nt[1] * tz);
+        const int t0 = pairs[(size_t)pi];
+        if (t0 % T.nt[0] + (k & 1) >= T.nt[0]) continue;
+        const int t = t0 + (k & 1);
         for (int p = 0; p < T.nph; ++p) {
             const float v = tgemm[(size_t)p * T.ntap_pad + t];
             const float hi = tf32_hi_host(v), lo = v - hi;
@@ -802,6 +830,13 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
     if (cudaMalloc((void **)&tc.d_btr, btr.size() * sizeof(float)) != cudaSuccess) return 2;
     if (cudaMalloc((void **)&tc.d_bcon, bcon.size() * sizeof(float)) != cudaSuccess) return 2;
     if (cudaMalloc((void **)&tc.d_err, sizeof(unsigned)) != cudaSuccess) return 2;
+    if (cudaMalloc((void **)&tc.d_pairoff, pairoff.size() * sizeof(int2)) != cudaSuccess) return 2;
+    if (cudaMalloc((void **)&tc.d_ctap, ctap.size() * sizeof(int)) != cudaSuccess) return 2;
+    if (cudaMemcpyAsync(tc.d_pairoff, pairoff.data(), pairoff.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                        stream) != cudaSuccess ||
+        cudaMemcpyAsync(tc.d_ctap, ctap.data(), ctap.size() * sizeof(int), cudaMemcpyHostToDevice, stream) !=
+            cudaSuccess)
+        return 2;
     if (cudaMemcpyAsync(tc.d_btr, btr.data(), btr.size() * sizeof(float), cudaMemcpyHostToDevice, stream) !=
             cudaSuccess ||
         cudaMemcpyAsync(tc.d_bcon, bcon.data(), bcon.size() * sizeof(float), cudaMemcpyHostToDevice, stream) !=
@@ -811,6 +846,7 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
         return 2;
     C.btr = tc.d_btr;
     C.bcon = tc.d_bcon;
+    C.pairoff = tc.d_pairoff;
     C.err = tc.d_err;
     pl.dev.tc_err = tc.d_err;
 
@@ -888,8 +924,11 @@ inline int table_value(TablePlan &pl, const TcPlan *tc, const EvalParams &P, int
 inline int table_derivative(TablePlan &pl, const TcPlan *tc, const EvalParams &P, const DerivParams &Q, int D,
                             int gather_blocks, cudaStream_t s, cudaEvent_t mid = nullptr)
 {
+    TableDev G = pl.dev;                                     // the gather reads the contrib layout
     if (tc && tc->enabled) {
         if (table_contrib_tc(*tc, pl, Q.stats, s)) return 2;
+        G.gtap = tc->d_ctap;                                 // nonzero taps only
+        G.ngtap = tc->dev.nct;
     } else {
         const size_t smem = table_contrib_smem(pl.dev);
         table_contrib_kernel<<<pl.contrib_blocks, kTabContribThreads, smem, s>>>(pl.dev, Q.stats);
@@ -897,9 +936,9 @@ inline int table_derivative(TablePlan &pl, const TcPlan *tc, const EvalParams &P
     }
     if (mid && cudaEventRecord(mid, s) != cudaSuccess) return 2;
     if (D == 3)
-        table_gather_kernel<3><<<gather_blocks, kGatherThreads, 0, s>>>(P, pl.dev, Q);
+        table_gather_kernel<3><<<gather_blocks, kGatherThreads, 0, s>>>(P, G, Q);
     else
-        table_gather_kernel<2><<<gather_blocks, kGatherThreads, 0, s>>>(P, pl.dev, Q);
+        table_gather_kernel<2><<<gather_blocks, kGatherThreads, 0, s>>>(P, G, Q);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
@@ -918,6 +957,8 @@ inline void table_tc_free(TcPlan &tc)
     if (tc.d_btr) cudaFree(tc.d_btr);
     if (tc.d_bcon) cudaFree(tc.d_bcon);
     if (tc.d_err) cudaFree(tc.d_err);
+    if (tc.d_pairoff) cudaFree(tc.d_pairoff);
+    if (tc.d_ctap) cudaFree(tc.d_ctap);
     tc = TcPlan{};
 }
 
