@@ -202,7 +202,25 @@ __global__ void __launch_bounds__(256, 4) table_warp_kernel(EvalParams P, TableD
     const int nq0 = T.nq[0], nq1 = T.nq[1];
     const FastDiv dq0 = T.div_nq0, dq01 = T.div_nq01;
     const int nphv = T.nph;
+    // u and the fixed value of the next texel are loaded one iteration ahead, so that their
+    // latency overlaps the B-spline gathers of the current texel
+    const int plane = total;
+    float un[3] = {0.f, 0.f, 0.f}, fnx = 0.f;
+    if (i0 < total) {
+        un[0] = T.ucp[i0];
+        un[1] = T.ucp[i0 + plane];
+        if (D > 2) un[2] = T.ucp[i0 + 2 * plane];
+        fnx = T.fixcp[i0];
+    }
     for (int i = i0, cell = i0 / nphv; i < total; i += stride, cell += stride / nphv) {
+        const float u[3] = {un[0], un[1], un[2]};
+        const float f = fnx;
+        if (i + stride < total) {
+            un[0] = T.ucp[i + stride];
+            un[1] = T.ucp[i + stride + plane];
+            if (D > 2) un[2] = T.ucp[i + stride + 2 * plane];
+            fnx = T.fixcp[i + stride];
+        }
         const int cyz = (int)dq0.div((uint32_t)cell), cz = (int)dq01.div((uint32_t)cell);
         const int cc[3] = {cell - cyz * nq0, cyz - cz * nq1, cz};
         int x[3];
@@ -214,8 +232,6 @@ __global__ void __launch_bounds__(256, 4) table_warp_kernel(EvalParams P, TableD
         }
         float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ok) {
-            const int plane = total;
-            const float u[3] = {T.ucp[i], T.ucp[i + plane], D > 2 ? T.ucp[i + 2 * plane] : 0.f};
             double fi[3] = {(double)x[0], (double)x[1], (double)x[2]}, p[3], mp[3], ml[3];
             to_global<D>(P.fixed, fi, p);
 #pragma unroll
@@ -236,7 +252,6 @@ __global__ void __launch_bounds__(256, 4) table_warp_kernel(EvalParams P, TableD
             if (bspline_inside<D>(P.mov, ml)) {
                 float m, g[3] = {0.f, 0.f, 0.f};
                 bspline_derivs4<D>(P.coeffs4, P.mov, ml, m, g);
-                const float f = T.fixcp[i];
                 vf[Q_COUNT] += 1.f;
                 vf[Q_D2] += (m - f) * (m - f);
                 vf[Q_SF] += f;
@@ -338,7 +353,7 @@ constexpr int kGatherGroups = 8;                    // warps per block, each ove
 constexpr int kGatherThreads = 32 * kGatherGroups;
 
 template <int D>
-__global__ void __launch_bounds__(kGatherThreads, 4) table_gather_kernel(EvalParams P, TableDev T, DerivParams Q)
+__global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalParams P, TableDev T, DerivParams Q)
 {
     __shared__ float sacc[kGatherGroups][3][32];
     __shared__ float sreg[kGatherGroups][9][32];
@@ -366,7 +381,7 @@ __global__ void __launch_bounds__(kGatherThreads, 4) table_gather_kernel(EvalPar
     float acc[3] = {0.f, 0.f, 0.f};
     if (active && !Q.values_only) {
         // groups of kU taps: all loads first (independent, predicated), then the sums in tap order
-        constexpr int kU = 8;
+        constexpr int kU = 16;
         const int ntap = T.ngtap, ncell = (int)T.ncell;
         const float *c0p = T.contrib, *c1p = T.contrib + ntap * ncell, *c2p = T.contrib + 2 * ntap * ncell;
         for (int base = grp; base < ntap; base += kGatherGroups * kU) {
