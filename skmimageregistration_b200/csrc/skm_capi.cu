@@ -153,6 +153,14 @@ struct skm_evaluator {
     RngJump jump{};
     bool use_table = true;
 
+    // skm_metric_evaluate replays one CUDA graph (parameter upload, evaluation, result download)
+    // while the metric description, the derivative request, the path and the field stay the same
+    cudaGraphExec_t mgraph = nullptr;
+    skm_metric_desc mg_desc{};
+    bool mg_deriv = false;
+    int mg_path = 0;
+    const double *mg_df = nullptr;
+
     ~skm_evaluator()
     {
         if (device >= 0) cudaSetDevice(device);
@@ -160,6 +168,7 @@ struct skm_evaluator {
                         d_dense_sw_in, d_shifts, d_in, d_counters, d_part, d_stats, d_deriv, d_rpart, d_out};
         for (void *b : bufs)
             if (b) cudaFree(b);
+        if (mgraph) cudaGraphExecDestroy(mgraph);
         table_tc_free(tc);
         table_free(table);
         if (h_in) cudaFreeHost(h_in);
@@ -441,6 +450,8 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
             return fail(SKM_ERR_CUDA, "table kernel attributes: %s", cudaGetErrorString(cudaGetLastError()));
         if (e->table.enabled && table_tc_plan(e->tc, e->table, e->stream))
             return fail(SKM_ERR_CUDA, "tensor-core table plan: %s", cudaGetErrorString(cudaGetLastError()));
+        if (e->table.enabled && e->tc.enabled && warp_tma_plan(e->tc.wt, e->table, e->P, tmp.data(), e->stream))
+            return fail(SKM_ERR_CUDA, "staged warp kernel plan: %s", cudaGetErrorString(cudaGetLastError()));
         return SKM_OK;
     }();
     if (rc) {
@@ -811,6 +822,31 @@ int skm_metric_device(skm_evaluator *e, const skm_metric_desc *m, bool derivativ
     return run_evaluation(e, m->metric, derivative, w, e->d_in);
 }
 
+static bool same_metric(const skm_metric_desc &a, const skm_metric_desc &b)
+{
+    return a.metric == b.metric && a.reg_l1 == b.reg_l1 && a.reg_l21 == b.reg_l21 && a.reg_l2 == b.reg_l2 &&
+           a.reg_rkhs == b.reg_rkhs && a.reg_rd == b.reg_rd && a.reg_rd_scaling == b.reg_rd_scaling &&
+           a.reg_pg == b.reg_pg && a.reg_pg_scaling == b.reg_pg_scaling &&
+           a.use_negative_gradient == b.use_negative_gradient && a.do_resampling == b.do_resampling;
+}
+
+// Enqueues (or captures) the device part of skm_metric_evaluate: parameters from the pinned
+// staging buffer, planar packing, the evaluation and the result download into h_out.
+static int metric_sequence(skm_evaluator *e, const skm_metric_desc *m, bool derivative)
+{
+    const long long C = e->C, n = C * e->D;
+    SKM_CUDA(cudaMemcpyAsync(e->d_in, e->h_in, sizeof(double) * n, cudaMemcpyHostToDevice, e->stream));
+    pack_cp_planar<<<(int)((C + 255) / 256), 256, 0, e->stream>>>(e->d_in, e->d_in + n, C, e->D, e->d_cpd);
+    SKM_CHECK_LAUNCH();
+    int rc = skm_metric_device(e, m, derivative);
+    if (rc) return rc;
+    SKM_CUDA(cudaMemcpyAsync(e->h_out, e->d_out, sizeof(double) * NO, cudaMemcpyDeviceToHost, e->stream));
+    if (derivative)
+        SKM_CUDA(cudaMemcpyAsync(e->h_out + NO, e->d_deriv, sizeof(double) * e->nparams, cudaMemcpyDeviceToHost,
+                                 e->stream));
+    return SKM_OK;
+}
+
 extern "C" int skm_metric_evaluate(skm_evaluator *e, const skm_metric_desc *m, const double *parameters,
                                    const double *cpw, const skm_field *df, double *derivative,
                                    skm_metric_values *out)
@@ -818,12 +854,55 @@ extern "C" int skm_metric_evaluate(skm_evaluator *e, const skm_metric_desc *m, c
     if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
     int rc;
     if ((rc = validate_metric(m))) return rc;
+    if (!parameters || !cpw) return fail(SKM_ERR_INVALID, "control points / weights are NULL");
     SKM_CUDA(cudaSetDevice(e->device));
     if ((rc = upload_field(e, df))) return rc;
-    if ((rc = upload_params(e, parameters, cpw, true))) return rc;
-    if ((rc = draw_shifts(e, m->do_resampling))) return rc;
-    if ((rc = skm_metric_device(e, m, derivative != nullptr))) return rc;
-    if ((rc = fetch(e, derivative))) return rc;
+    const long long C = e->C, n = C * e->D;
+    // (the previous call synchronised the stream, so the staging buffers are free)
+    std::memcpy(e->h_in, parameters, sizeof(double) * n);
+    if (!e->weights_uploaded || std::memcmp(e->h_in + n, cpw, sizeof(double) * C) != 0) {
+        e->weights_uploaded = false;
+        std::memcpy(e->h_in + n, cpw, sizeof(double) * C);
+        SKM_CUDA(cudaMemcpyAsync(e->d_in + n, e->h_in + n, sizeof(double) * C, cudaMemcpyHostToDevice, e->stream));
+        e->weights_uploaded = true;
+    }
+    const bool deriv = derivative != nullptr;
+    if (m->metric == SKM_LCC && (rc = ensure_dense(e))) return rc;   // allocates: not inside a capture
+    if (e->P.sub <= 1) {
+        // no sampling offsets to draw: the whole device part is one graph launch
+        const int path = active_path(e);
+        if (!e->mgraph || !same_metric(e->mg_desc, *m) || e->mg_deriv != deriv || e->mg_path != path ||
+            e->mg_df != e->df_key) {
+            if (e->mgraph) cudaGraphExecDestroy(e->mgraph);
+            e->mgraph = nullptr;
+            SKM_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+            int r = metric_sequence(e, m, deriv);
+            cudaGraph_t g = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+            if (r) {
+                if (g) cudaGraphDestroy(g);
+                return r;
+            }
+            if (ce != cudaSuccess) return fail(SKM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+            cudaError_t ie = cudaGraphInstantiate(&e->mgraph, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) {
+                e->mgraph = nullptr;
+                return fail(SKM_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ie));
+            }
+            e->mg_desc = *m;
+            e->mg_deriv = deriv;
+            e->mg_path = path;
+            e->mg_df = e->df_key;
+        }
+        SKM_CUDA(cudaGraphLaunch(e->mgraph, e->stream));
+    } else {
+        if ((rc = draw_shifts(e, m->do_resampling))) return rc;
+        if ((rc = metric_sequence(e, m, deriv))) return rc;
+    }
+    SKM_CUDA(cudaStreamSynchronize(e->stream));
+    if (e->h_out[O_FAULT] != 0.0) return report_fault(e);
+    if (derivative) std::memcpy(derivative, e->h_out + NO, sizeof(double) * e->nparams);
     if (out) {
         const double *o = e->h_out;
         out->value = o[O_VALUE];

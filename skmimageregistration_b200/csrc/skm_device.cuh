@@ -322,14 +322,11 @@ __device__ __forceinline__ void bspline_derivs(const float *__restrict__ c, cons
     }
 }
 
-// Same as bspline_derivs, reading the coefficients from the row-expanded copy
-// c4[i] = (c[i], c[i+1], c[i+2], c[i+3]): one aligned 16-byte load per stencil row.
+// Cubic B-spline weights (value W and derivative dW) of the four stencil taps per axis at local
+// coordinate l; ii = the stencil's first padded-grid index (VecI(idx): truncation toward zero).
 template <int D>
-__device__ __forceinline__ void bspline_derivs4(const float4 *__restrict__ c4, const Geo &mg, const double *l,
-                                                float &val, float *grad)
+__device__ __forceinline__ void bspline_weights(const double *l, int *ii, float (&W)[4][3], float (&dW)[4][3])
 {
-    int ii[3] = {0, 0, 0};
-    float W[4][3], dW[4][3];
 #pragma unroll
     for (int d = 0; d < D; ++d) {
         ii[d] = (int)l[d];
@@ -343,32 +340,52 @@ __device__ __forceinline__ void bspline_derivs4(const float4 *__restrict__ c4, c
         float d2 = 1.0f + d0 - 2.0f * d3;
         dW[3][d] = d3; dW[0][d] = d0; dW[2][d] = d2; dW[1][d] = -d0 - d2 - d3;
     }
+}
+
+// The 3-D stencil sum shared by the global-memory and the shared-memory versions: row(y, z)
+// returns the four x coefficients of stencil row (y, z).
+template <class Row>
+__device__ __forceinline__ void bspline_sum3(const Row &row, const float (&W)[4][3], const float (&dW)[4][3],
+                                             const Geo &mg, float &val, float *grad)
+{
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+#pragma unroll
+    for (int z = 0; z < 4; ++z) {
+        float z0 = 0.f, z1 = 0.f, z3 = 0.f;
+#pragma unroll
+        for (int y = 0; y < 4; ++y) {
+            const float4 r = row(y, z);
+            float dx = dW[0][0] * r.x + dW[1][0] * r.y + dW[2][0] * r.z + dW[3][0] * r.w;
+            float vx = W[0][0] * r.x + W[1][0] * r.y + W[2][0] * r.z + W[3][0] * r.w;
+            z0 += W[y][1] * dx;
+            z1 += dW[y][1] * vx;
+            z3 += W[y][1] * vx;
+        }
+        c0 += W[z][2] * z0;
+        c1 += W[z][2] * z1;
+        c2 += dW[z][2] * z3;
+        c3 += W[z][2] * z3;
+    }
+    val = c3;
+    grad[0] = c0 * (float)mg.inv[0];
+    grad[1] = c1 * (float)mg.inv[1];
+    grad[2] = c2 * (float)mg.inv[2];
+}
+
+// Same as bspline_derivs, reading the coefficients from the row-expanded copy
+// c4[i] = (c[i], c[i+1], c[i+2], c[i+3]): one aligned 16-byte load per stencil row.
+template <int D>
+__device__ __forceinline__ void bspline_derivs4(const float4 *__restrict__ c4, const Geo &mg, const double *l,
+                                                float &val, float *grad)
+{
+    int ii[3] = {0, 0, 0};
+    float W[4][3], dW[4][3];
+    bspline_weights<D>(l, ii, W, dW);
     if (D == 3) {
-        float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
         // 32-bit offsets: the coefficient volume holds fewer than 2^31 entries (checked at creation)
         const int sy = (int)mg.st[1], sz = (int)mg.st[2];
         const float4 *base = c4 + (ii[0] + ii[1] * sy + ii[2] * sz);
-#pragma unroll
-        for (int z = 0; z < 4; ++z) {
-            float z0 = 0.f, z1 = 0.f, z3 = 0.f;
-#pragma unroll
-            for (int y = 0; y < 4; ++y) {
-                const float4 r = __ldg(base + (y * sy + z * sz));
-                float dx = dW[0][0] * r.x + dW[1][0] * r.y + dW[2][0] * r.z + dW[3][0] * r.w;
-                float vx = W[0][0] * r.x + W[1][0] * r.y + W[2][0] * r.z + W[3][0] * r.w;
-                z0 += W[y][1] * dx;
-                z1 += dW[y][1] * vx;
-                z3 += W[y][1] * vx;
-            }
-            c0 += W[z][2] * z0;
-            c1 += W[z][2] * z1;
-            c2 += dW[z][2] * z3;
-            c3 += W[z][2] * z3;
-        }
-        val = c3;
-        grad[0] = c0 * (float)mg.inv[0];
-        grad[1] = c1 * (float)mg.inv[1];
-        grad[2] = c2 * (float)mg.inv[2];
+        bspline_sum3([&](int y, int z) { return __ldg(base + (y * sy + z * sz)); }, W, dW, mg, val, grad);
     } else {
         float c0 = 0.f, c1 = 0.f, c2 = 0.f;
         const int sy = (int)mg.st[1];

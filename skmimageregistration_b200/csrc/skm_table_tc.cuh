@@ -32,6 +32,7 @@
 
 #include "skm_table.cuh"
 #include "skm_tc.cuh"
+#include "skm_warp_tma.cuh"
 
 namespace skm {
 
@@ -701,6 +702,7 @@ struct TcPlan {
     unsigned *d_err = nullptr;
     int transform_blocks = 0, contrib_blocks = 0;
     size_t transform_smem = 0, contrib_smem = 0;
+    WarpTmaPlan wt;                  // the warp kernel with TMA-staged coefficients (3-D)
 };
 
 // Decides whether the tensor-core kernels apply to a table plan and builds their operand
@@ -914,7 +916,10 @@ inline int table_value(TablePlan &pl, const TcPlan *tc, const EvalParams &P, int
     }
     if (rc) return rc;
     if (mid && cudaEventRecord(mid, s) != cudaSuccess) return 2;
-    if (D == 3)
+    if (D == 3 && tc && tc->enabled && tc->wt.enabled)
+        table_warp_tma_kernel<<<tc->wt.blocks, 256, tc->wt.smem, s>>>(P, pl.dev, tc->wt.dev, tc->wt.map, metric, stats,
+                                                                     counter);
+    else if (D == 3)
         table_warp_kernel<3><<<pl.dev.value_blocks, 256, 0, s>>>(P, pl.dev, metric, stats, counter);
     else
         table_warp_kernel<2><<<pl.dev.value_blocks, 256, 0, s>>>(P, pl.dev, metric, stats, counter);
@@ -958,6 +963,7 @@ inline void table_tc_free(TcPlan &tc)
     if (tc.d_bcon) cudaFree(tc.d_bcon);
     if (tc.d_err) cudaFree(tc.d_err);
     if (tc.d_pairoff) cudaFree(tc.d_pairoff);
+    warp_tma_free(tc.wt);
     if (tc.d_ctap) cudaFree(tc.d_ctap);
     tc = TcPlan{};
 }
