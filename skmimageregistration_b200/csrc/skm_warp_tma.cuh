@@ -30,6 +30,7 @@ struct WarpTma {
     int nb[3];               // bricks per axis
     double a[3], b[3];       // moving-image index of fixed voxel x: a x + b (no displacement)
     int xlo[3];              // lowest voxel offset of a cell's texels: x = h q + xlo .. h q + xlo + h - 1
+    int lanes4x8;            // h = 4 and a 4 x 2 x 2-cell brick: a warp takes 4 x 8 voxels of one z
 };
 
 __device__ __forceinline__ void tma_load_3d(float *dst, const CUtensorMap *map, int x, int y, int z,
@@ -126,8 +127,18 @@ __global__ void __launch_bounds__(256, 3) table_warp_tma_kernel(EvalParams P, Ta
             const int r0[3] = {r0s[buf][0], r0s[buf][1], r0s[buf][2]};
             const int bq[3] = {brick % W.nb[0], (brick / W.nb[0]) % W.nb[1], brick / (W.nb[0] * W.nb[1])};
             for (int t = tid; t < ncb * nph; t += blockDim.x) {
-                const int cl = (int)T.div_nph.div((uint32_t)t);
-                const int p = t - cl * nph;
+                int cl, p;
+                if (W.lanes4x8) {
+                    // lanes = 4 x-neighbours x 8 y-neighbours of one z: with the box's row stride of
+                    // 28 floats (-4 modulo 32 banks) a stencil tap of the warp hits 32 distinct banks
+                    const int lane = t & 31, w = t >> 5;
+                    const int xi = lane & 3, yi = lane >> 2, cx = w & 3, vz = w >> 2;
+                    cl = cx + 4 * ((yi >> 2) + 2 * (vz >> 2));
+                    p = xi + 4 * (yi & 3) + 16 * (vz & 3);
+                } else {
+                    cl = (int)T.div_nph.div((uint32_t)t);
+                    p = t - cl * nph;
+                }
                 const int4 cxyz = cellxyz[cl];
                 const int cc[3] = {bq[0] * W.bc[0] + cxyz.x, bq[1] * W.bc[1] + cxyz.y, bq[2] * W.bc[2] + cxyz.z};
                 if (cc[0] >= T.nq[0] || cc[1] >= T.nq[1] || cc[2] >= T.nq[2]) continue;
@@ -265,6 +276,8 @@ inline int warp_tma_plan(WarpTmaPlan &wt, const TablePlan &pl, const EvalParams 
         else --W.bc[2];
     }
     for (int d = 0; d < 3; ++d) W.nb[d] = (T.nq[d] + W.bc[d] - 1) / W.bc[d];
+    static_assert(kWtBoxX % 32 == 28, "the 4 x 8 lane layout relies on a row stride of -4 banks");
+    W.lanes4x8 = T.h[0] == 4 && T.h[1] == 4 && T.h[2] == 4 && W.bc[0] == 4 && W.bc[1] == 2 && W.bc[2] == 2;
     const long long nbr = (long long)W.nb[0] * W.nb[1] * W.nb[2];
 
     // tensor map over a row-pitched copy (global strides must be multiples of 16 bytes)
