@@ -654,14 +654,22 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
             const int cell = (int)(tile * ct) + c;
             const bool valid = comp < D && cell < ncell;
             const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * C.con_stride);
-            for (int j = half; j < (Np >> 4); j += kConEpiWarps / 4) {
-                float v[16];
-                tc::tmem_ld16(tb + (uint32_t)(16 * j), v);
-                if (valid) {
-                    float *dst = T.contrib + (comp * C.nct + 16 * j) * ncell + cell;
+            // 32-column blocks (one TMEM load and wait each), the two warps of a quarter alternating;
+            // N is a multiple of 16, so the last block may hold 16 columns
+            for (int j = half; 32 * j < Np; j += kConEpiWarps / 4) {
+                float v[32];
+                if (32 * j + 32 <= Np) {
+                    tc::tmem_ld32(tb + (uint32_t)(32 * j), v);
+                } else {
+                    tc::tmem_ld16(tb + (uint32_t)(32 * j), v);
 #pragma unroll
-                    for (int e = 0; e < 16; ++e)
-                        if (16 * j + e < C.nct) dst[e * ncell] = v[e];
+                    for (int e = 16; e < 32; ++e) v[e] = 0.f;
+                }
+                if (valid) {
+                    float *dst = T.contrib + (comp * C.nct + 32 * j) * ncell + cell;
+#pragma unroll
+                    for (int e = 0; e < 32; ++e)
+                        if (32 * j + e < C.nct) dst[e * ncell] = v[e];
                 }
             }
             tc::fence_before_sync();
