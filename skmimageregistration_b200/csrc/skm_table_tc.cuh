@@ -516,7 +516,8 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
     if (warp >= kConEpiWarps + 1) {
         // ---------------- producers: g = (a f + b m + c) grad M, hi/lo stages ----------------
         // Two groups of 4 warps take alternate K chunks, so that one group's global loads are in
-        // flight while the other converts and stores.  Item = (cell c, 4 phases), lanes over cells.
+        // flight while the other converts and stores.  Item = (cell c, 4 phases); 8 consecutive lanes
+        // take the 32 phases of one cell, so a warp's record loads cover 4 contiguous 512-byte runs.
         const int pt = tid - kConProdBase;
         const int grp = pt / kTcGroupThreads, gt = pt - grp * kTcGroupThreads;
         const float cf = (float)stats[S_COEF_F], cm = (float)stats[S_COEF_M], cc = (float)stats[S_COEF_C];
@@ -544,7 +545,7 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
 #pragma unroll
                 for (int u = 0; u < kMaxItems; ++u) {           // all loads first
                     const int i = base + gt + u * kTcGroupThreads;
-                    const int c = i % ct, jg = i / ct;
+                    const int c = i >> 3, jg = i & 7;
                     const long long cell = cell0 + c;
                     const int p0 = k0 + 4 * jg;
                     const bool in = i < nitems && cell < T.ncell;
@@ -564,7 +565,7 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
                 for (int u = 0; u < kMaxItems; ++u) {
                     const int i = base + gt + u * kTcGroupThreads;
                     if (i >= nitems) break;
-                    const int c = i % ct, jg = i / ct;
+                    const int c = i >> 3, jg = i & 7;
                     const float fv[4] = {ff[u].x, ff[u].y, ff[u].z, ff[u].w};
                     float gv[3][4];
 #pragma unroll
