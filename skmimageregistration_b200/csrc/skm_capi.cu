@@ -138,6 +138,7 @@ struct skm_evaluator {
 
     // pinned host staging
     double *h_in = nullptr, *h_out = nullptr;
+    double *dh_in = nullptr, *dh_out = nullptr;   // the same staging buffers as the device addresses them
     bool weights_uploaded = false;       // h_in's weight part is on the device (skip identical weights)
 
     // phase-table fast path (stationary kernel, integral spacing ratio) and its tensor-core GEMMs
@@ -441,8 +442,10 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         if (dalloc(&e->d_rpart, (size_t)NR * std::max<long long>(e->C, std::max(e->deriv_blocks, e->gather_blocks))))
             return SKM_ERR_CUDA;
         if (dalloc(&e->d_out, NO)) return SKM_ERR_CUDA;
-        SKM_CUDA(cudaMallocHost((void **)&e->h_in, sizeof(double) * e->C * (D + 1)));
-        SKM_CUDA(cudaMallocHost((void **)&e->h_out, sizeof(double) * (e->nparams + NO)));
+        SKM_CUDA(cudaHostAlloc((void **)&e->h_in, sizeof(double) * e->C * (D + 1), cudaHostAllocMapped));
+        SKM_CUDA(cudaHostAlloc((void **)&e->h_out, sizeof(double) * (e->nparams + NO), cudaHostAllocMapped));
+        SKM_CUDA(cudaHostGetDevicePointer((void **)&e->dh_in, e->h_in, 0));
+        SKM_CUDA(cudaHostGetDevicePointer((void **)&e->dh_out, e->h_out, 0));
         rng_jump_table(e->jump);
         int trc = table_plan(e->table, e->P, D, e->stream);
         if (trc) return fail(SKM_ERR_CUDA, "table plan failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -631,8 +634,9 @@ struct RegWeights {
 // pass on the generic path), after the warp + statistics kernel, after the statistics kernel, after
 // the contrib GEMM (table path), after the derivative gather and after the result kernel.
 static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const RegWeights &w, const double *params,
-                          cudaEvent_t *ev = nullptr)
+                          cudaEvent_t *ev = nullptr, double *deriv_out = nullptr, double *res_out = nullptr)
 {
+    double *d_deriv = deriv_out ? deriv_out : e->d_deriv, *d_res = res_out ? res_out : e->d_out;
     int rc = SKM_OK;
     const int D = e->D, kind = e->P.K.kind;
     if (metric == SKM_LCC) {
@@ -675,9 +679,9 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     Q.dense_in = e->d_dense_in;
     Q.dense_sw = e->d_dense_sw;
     Q.dense_sw_in = e->d_dense_sw_in;
-    Q.deriv = e->d_deriv;
+    Q.deriv = d_deriv;
     Q.rpart = e->d_rpart;
-    Q.out = e->d_out;
+    Q.out = d_res;
     Q.counter = e->d_counters + 1;
     bool any_reg = w.rkhs > 0 || w.rd > 0 || w.pg > 0 || w.with_metric;
     // few control points (coarse levels): a block per control point keeps every SM busy
@@ -704,7 +708,7 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     if (!((derivative || any_reg) && tab)) {    // the table gather computes the result itself
         result_kernel<<<1, 256, 0, e->stream>>>(e->d_stats, (derivative || any_reg) ? e->d_rpart : nullptr,
                                                split ? (int)e->C : e->deriv_blocks, w.rkhs, w.rd, w.pg, w.l1,
-                                               w.l21, w.l2, e->d_out,
+                                               w.l21, w.l2, d_res,
                                                tab ? e->table.dev.tc_err : nullptr);
         SKM_CHECK_LAUNCH();
     }
@@ -805,8 +809,10 @@ static int validate_metric(const skm_metric_desc *m)
     return SKM_OK;
 }
 
-// Device part of one metric evaluation on already-uploaded planar parameters (e->d_in).
-int skm_metric_device(skm_evaluator *e, const skm_metric_desc *m, bool derivative)
+// Device part of one metric evaluation on already-uploaded planar parameters (e->d_in); the
+// derivative and the result vector go to deriv_out / res_out when given.
+int skm_metric_device(skm_evaluator *e, const skm_metric_desc *m, bool derivative, double *deriv_out = nullptr,
+                      double *res_out = nullptr)
 {
     RegWeights w{};
     w.rkhs = m->reg_rkhs;
@@ -819,7 +825,7 @@ int skm_metric_device(skm_evaluator *e, const skm_metric_desc *m, bool derivativ
     w.l2 = m->reg_l2;
     w.with_metric = 1;
     w.negate = m->use_negative_gradient;
-    return run_evaluation(e, m->metric, derivative, w, e->d_in);
+    return run_evaluation(e, m->metric, derivative, w, e->d_in, nullptr, deriv_out, res_out);
 }
 
 static bool same_metric(const skm_metric_desc &a, const skm_metric_desc &b)
@@ -830,21 +836,17 @@ static bool same_metric(const skm_metric_desc &a, const skm_metric_desc &b)
            a.use_negative_gradient == b.use_negative_gradient && a.do_resampling == b.do_resampling;
 }
 
-// Enqueues (or captures) the device part of skm_metric_evaluate: parameters from the pinned
-// staging buffer, planar packing, the evaluation and the result download into h_out.
+// Enqueues (or captures) the device part of skm_metric_evaluate with no copy operations: the
+// packing kernel reads the parameters from the pinned staging buffer over the bus (and keeps a
+// device copy for the regularizers), and the final kernels write the derivative and the result
+// vector straight into the pinned h_out.
 static int metric_sequence(skm_evaluator *e, const skm_metric_desc *m, bool derivative)
 {
     const long long C = e->C, n = C * e->D;
-    SKM_CUDA(cudaMemcpyAsync(e->d_in, e->h_in, sizeof(double) * n, cudaMemcpyHostToDevice, e->stream));
-    pack_cp_planar<<<(int)((C + 255) / 256), 256, 0, e->stream>>>(e->d_in, e->d_in + n, C, e->D, e->d_cpd);
+    pack_cp_planar_copy<<<(int)((C + 255) / 256), 256, 0, e->stream>>>(e->dh_in, e->d_in + n, C, e->D, e->d_cpd,
+                                                                      e->d_in);
     SKM_CHECK_LAUNCH();
-    int rc = skm_metric_device(e, m, derivative);
-    if (rc) return rc;
-    SKM_CUDA(cudaMemcpyAsync(e->h_out, e->d_out, sizeof(double) * NO, cudaMemcpyDeviceToHost, e->stream));
-    if (derivative)
-        SKM_CUDA(cudaMemcpyAsync(e->h_out + NO, e->d_deriv, sizeof(double) * e->nparams, cudaMemcpyDeviceToHost,
-                                 e->stream));
-    return SKM_OK;
+    return skm_metric_device(e, m, derivative, e->dh_out + NO, e->dh_out);
 }
 
 extern "C" int skm_metric_evaluate(skm_evaluator *e, const skm_metric_desc *m, const double *parameters,

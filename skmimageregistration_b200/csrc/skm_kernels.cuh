@@ -955,6 +955,20 @@ static __global__ void pack_cp_planar(const double *__restrict__ params, const d
     out[i] = r;
 }
 
+// pack_cp_planar reading the parameters from host memory the device maps (the pinned staging
+// buffer), keeping a device copy of them in `copy`.
+static __global__ void pack_cp_planar_copy(const double *__restrict__ params, const double *__restrict__ cpw,
+                                           long long C, int D, float4 *__restrict__ out, double *__restrict__ copy)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) return;
+    const double px = params[i], py = params[i + C], pz = D > 2 ? params[i + 2 * C] : 0.0;
+    copy[i] = px;
+    copy[i + C] = py;
+    if (D > 2) copy[i + 2 * C] = pz;
+    out[i] = make_float4((float)px, (float)py, (float)pz, (float)cpw[i]);
+}
+
 // grid shifts of the PCG32 stream (GpuEvaluator.cu:107-118): texel t takes draws D*t..D*t+D-1
 // counted from `state`; shift = int(nextI/double(UINT_MAX) * subsample).
 static __global__ void shifts_kernel(unsigned long long state, RngJump J, long long Ns, int D, int sub,
