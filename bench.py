@@ -203,9 +203,12 @@ def kernel_work(pb, info, phases):
         tr = {"name": "table_transform_tc_kernel" if tc else "table_transform_kernel",
               "bound": "tensor" if tc else "fp32", "ms": phases["transform"],
               "flops": gemm, "bytes": C * 16 + nph * ntap * 4 + cells * nph * 4 * D}
+        # contributions: one per (cell, tap with a nonzero table column) -- the tensor-core path
+        # skips the all-zero taps, the CUDA-core one stores every tap of the box
+        ctaps = (info.get("tc_contrib_taps") or ntap) if tc else ntap
         co = {"name": "table_contrib_tc_kernel" if tc else "table_contrib_kernel",
               "bound": "tensor" if tc else "fp32", "ms": phases["contrib"], "flops": gemm,
-              "bytes": cells * nph * (16 + 4) + nph * ntap * 4 + D * ntap * cells * 4}
+              "bytes": cells * nph * (16 + 4) + nph * ntap * 4 + D * ctaps * cells * 4}
         if tc:
             tr["tensor_flops"] = (2.0 * 128 * 1.5 * info["tc_transform_n"] * info["tc_transform_k"]
                                   * info["tc_transform_tiles"])
@@ -213,12 +216,13 @@ def kernel_work(pb, info, phases):
                                   * info["tc_contrib_tiles"])
         return {
             "transform": tr,
-            "warp": {"name": "table_warp_kernel", "bound": "hbm", "ms": phases["warp"], "flops": bspline_flops,
+            "warp": {"name": "table_warp_tma_kernel" if info.get("warp_staged") else "table_warp_kernel",
+                     "bound": "hbm", "ms": phases["warp"], "flops": bspline_flops,
                      "bytes": cells * nph * (4 * D + 4 + 16) + ncoef * 4},
             "contrib": co,
             "gather": {"name": "table_gather_kernel", "bound": "hbm", "ms": phases["gather"],
                        "flops": 3.0 * C * ntap + 20.0 * C * info["table_regularizer_offsets"],
-                       "bytes": 3 * ntap * cells * 4 + C * 16 + C * D * 8},
+                       "bytes": 3 * ctaps * cells * 4 + C * 16 + C * D * 8},
         }
     pairs = pair_count(pb)
     return {

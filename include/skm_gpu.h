@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define SKM_ABI_VERSION 2
+#define SKM_ABI_VERSION 3
 
 /* Status codes. */
 #define SKM_OK              0
@@ -159,9 +159,11 @@ typedef struct skm_evaluator_info {
     int64_t tc_transform_tiles;
     int64_t tc_contrib_tiles;
     int32_t tc_transform_n;           /* 2 x phases padded to 16 (tf32 part and remainder of the table) */
-    int32_t tc_transform_k;           /* taps padded to 32 */
-    int32_t tc_contrib_n;             /* taps padded to 16 */
+    int32_t tc_transform_k;           /* tap pairs with a nonzero tap, 4 columns per two pairs, padded to 32 */
+    int32_t tc_contrib_n;             /* taps with a nonzero table column, padded to 16 */
     int32_t tc_contrib_k;             /* phases padded to 32 */
+    int32_t tc_contrib_taps;          /* taps with a nonzero table column (the contributions per cell) */
+    int32_t warp_staged;              /* 1: the warp kernel stages coefficient boxes by TMA */
 } skm_evaluator_info;
 int skm_evaluator_describe(skm_evaluator *ev, skm_evaluator_info *out);
 

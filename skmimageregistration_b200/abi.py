@@ -110,6 +110,8 @@ class EvaluatorInfo(C.Structure):
         ("tc_transform_k", C.c_int32),
         ("tc_contrib_n", C.c_int32),
         ("tc_contrib_k", C.c_int32),
+        ("tc_contrib_taps", C.c_int32),
+        ("warp_staged", C.c_int32),
     ]
 
     def as_dict(self):

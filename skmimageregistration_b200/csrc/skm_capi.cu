@@ -519,6 +519,8 @@ extern "C" int skm_evaluator_describe(skm_evaluator *e, skm_evaluator_info *out)
         r.tc_transform_k = C.kp;
         r.tc_contrib_n = C.npc;
         r.tc_contrib_k = C.kpc;
+        r.tc_contrib_taps = C.nct;
+        r.warp_staged = (e->D == 3 && e->tc.wt.enabled) ? 1 : 0;
     }
     *out = r;
     return SKM_OK;

@@ -56,7 +56,8 @@ def lib():
         L.skm_get_value_and_derivative.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, C.POINTER(Field), _dp, C.c_int32,
                                                    C.POINTER(Result)]
         L.skm_evaluate_displacement_field.argtypes = [C.c_void_p, _dp, _dp, C.POINTER(Field), _dp]
-        L.skm_metric_evaluate.argtypes = [C.c_void_p, C.POINTER(MetricDesc), _dp, _dp, C.POINTER(Field), _dp,
+        L.skm_metric_evaluate.argtypes = [C.c_void_p, C.POINTER(MetricDesc), C.c_void_p, C.c_void_p, C.POINTER(Field),
+                                          C.c_void_p,
                                           C.POINTER(MetricValues)]
         L.skm_optimizer_create.argtypes = [C.c_void_p, C.POINTER(OptimizerDesc), C.POINTER(MetricDesc), _dp, _dp,
                                            C.POINTER(Field), C.POINTER(C.c_void_p)]
@@ -198,7 +199,12 @@ class GpuKernelEvaluator:
         num_parameters) receives the derivative in place of a new array."""
         params = np.ascontiguousarray(params, np.float64)
         cpw = np.ascontiguousarray(cpw, np.float64)
-        f = self._field(df, df_geometry)
+        if df is None and df_geometry is None:           # the common call: no field, one cached struct
+            f = self.__dict__.get("_nofield")
+            if f is None:
+                f = self._nofield = self._field(None, None)
+        else:
+            f = self._field(df, df_geometry)
         out = MetricValues()
         if not derivative:
             der = None
@@ -207,8 +213,8 @@ class GpuKernelEvaluator:
             assert der.dtype == np.float64 and der.flags["C_CONTIGUOUS"] and der.size == self.problem.num_parameters
         else:
             der = np.zeros(self.problem.num_parameters)
-        check(lib().skm_metric_evaluate(self.h, C.byref(mdesc), dptr(params), dptr(cpw), C.byref(f), dptr(der),
-                                        C.byref(out)))
+        check(lib().skm_metric_evaluate(self.h, C.byref(mdesc), params.ctypes.data, cpw.ctypes.data, C.byref(f),
+                                        der.ctypes.data if der is not None else None, C.byref(out)))
         return out.as_dict(), der
 
 
