@@ -507,7 +507,7 @@ def run_ours(args, rank, world, local_rank):
         t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_rate = world * e2e_steps / float(t.item())
-    h2d = (P + pb.C) * 8
+    h2d = P * 8                                     # parameters; identical weights are not sent again
     d2h = P * 8 + 10 * 8
 
     line = None
