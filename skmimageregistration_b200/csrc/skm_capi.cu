@@ -191,6 +191,13 @@ static const TcPlan *tc_of(const skm_evaluator *e)
     return (e->use_tc && e->tc.enabled) ? &e->tc : nullptr;
 }
 
+// the tensor-core transform's weighted control-point planes, written by every packing kernel
+// whenever the plan has them (whichever path the next evaluation takes)
+static RegionPlanes planes_of(const skm_evaluator *e)
+{
+    return e->tc.enabled ? e->tc.rp : RegionPlanes{};
+}
+
 // ------------------------------------------------------------------------------------------------
 // dispatch over dimension and kernel kind
 template <template <int, int> class F, typename... A>
@@ -451,7 +458,7 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         if (trc) return fail(SKM_ERR_CUDA, "table plan failed: %s", cudaGetErrorString(cudaGetLastError()));
         if (e->table.enabled && (table_set_attributes(e->table) || table_size_grids(e->table)))
             return fail(SKM_ERR_CUDA, "table kernel attributes: %s", cudaGetErrorString(cudaGetLastError()));
-        if (e->table.enabled && table_tc_plan(e->tc, e->table, e->stream))
+        if (e->table.enabled && table_tc_plan(e->tc, e->table, e->P.cp.n, e->stream))
             return fail(SKM_ERR_CUDA, "tensor-core table plan: %s", cudaGetErrorString(cudaGetLastError()));
         if (e->table.enabled && e->tc.enabled && warp_tma_plan(e->tc.wt, e->table, e->P, tmp.data(), e->stream))
             return fail(SKM_ERR_CUDA, "staged warp kernel plan: %s", cudaGetErrorString(cudaGetLastError()));
@@ -594,9 +601,9 @@ static int upload_params(skm_evaluator *e, const double *cp, const double *cpw, 
     }
     int blocks = (int)((C + 255) / 256);
     if (planar)
-        pack_cp_planar<<<blocks, 256, 0, e->stream>>>(e->d_in, e->d_in + n, C, e->D, e->d_cpd);
+        pack_cp_planar<<<blocks, 256, 0, e->stream>>>(e->d_in, e->d_in + n, C, e->D, e->d_cpd, planes_of(e));
     else
-        pack_cp_aos<<<blocks, 256, 0, e->stream>>>(e->d_in, e->d_in + n, C, e->D, e->d_cpd);
+        pack_cp_aos<<<blocks, 256, 0, e->stream>>>(e->d_in, e->d_in + n, C, e->D, e->d_cpd, planes_of(e));
     SKM_CHECK_LAUNCH();
     return SKM_OK;
 }
@@ -846,7 +853,7 @@ static int metric_sequence(skm_evaluator *e, const skm_metric_desc *m, bool deri
 {
     const long long C = e->C, n = C * e->D;
     pack_cp_planar_copy<<<(int)((C + 255) / 256), 256, 0, e->stream>>>(e->dh_in, e->d_in + n, C, e->D, e->d_cpd,
-                                                                      e->d_in);
+                                                                      e->d_in, planes_of(e));
     SKM_CHECK_LAUNCH();
     return skm_metric_device(e, m, derivative, e->dh_out + NO, e->dh_out);
 }

@@ -253,7 +253,7 @@ __device__ __forceinline__ bool bspline_inside(const Geo &mg, const double *l)
 {
 #pragma unroll
     for (int d = 0; d < D; ++d)
-        if (l[d] < -0.5 || l[d] + 3.5 >= (double)mg.n[d]) return false;
+        if (!(l[d] >= -0.5 && l[d] + 3.5 < (double)mg.n[d])) return false;   // NaN is outside too
     return true;
 }
 

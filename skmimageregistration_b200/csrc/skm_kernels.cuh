@@ -927,9 +927,35 @@ __global__ void __launch_bounds__(256) displacement_kernel(EvalParams P, double 
 }
 
 // ---- small helpers ----------------------------------------------------------------------------
+// Weighted control points w alpha as planes for the tensor-core transform's tiled loads:
+// [2 D][n2][n1][nxp] floats, planes 0..D-1 the components (E[x] = w alpha(x)), planes D..2D-1 the
+// same stored 3 columns to the right (O[x] = w alpha(x - 3)): loaded from x0 + 4 next to E's load
+// from x0, O's box starts one control point later than E's, so that any two x-neighbours are one
+// aligned 8-byte element pair of E or of O, also for boxes that start left of the grid.  Rows are
+// padded to nxp >= n0 + 3 (a multiple of 4 floats, the tiled loads' stride rule); the padding
+// stays zero.  p == nullptr: not used.
+struct RegionPlanes {
+    float *p;
+    int n0, nxp, D;
+    long long plane;         // floats per plane
+};
+
+__device__ __forceinline__ void write_region_planes(const RegionPlanes &rp, long long i, const float4 &r)
+{
+    if (!rp.p) return;
+    const long long yz = i / rp.n0;
+    const int x = (int)(i - yz * rp.n0);
+    const long long row = yz * rp.nxp;                 // yz = y + n1 z
+    const float v[3] = {r.w * r.x, r.w * r.y, r.w * r.z};
+    for (int k = 0; k < rp.D; ++k) {
+        rp.p[k * rp.plane + row + x] = v[k];
+        rp.p[(rp.D + k) * rp.plane + row + x + 3] = v[k];
+    }
+}
+
 // pack AoS doubles (alpha) + weights into float4 records
 static __global__ void pack_cp_aos(const double *__restrict__ cp, const double *__restrict__ cpw, long long C, int D,
-                            float4 *__restrict__ out)
+                            float4 *__restrict__ out, RegionPlanes rp)
 {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C) return;
@@ -939,11 +965,12 @@ static __global__ void pack_cp_aos(const double *__restrict__ cp, const double *
     r.z = D > 2 ? (float)cp[i * D + 2] : 0.f;
     r.w = (float)cpw[i];
     out[i] = r;
+    write_region_planes(rp, i, r);
 }
 
 // pack planar parameters (metric level, itkTransformAdapter.hxx:202-236) + weights
 static __global__ void pack_cp_planar(const double *__restrict__ params, const double *__restrict__ cpw, long long C, int D,
-                               float4 *__restrict__ out)
+                               float4 *__restrict__ out, RegionPlanes rp)
 {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C) return;
@@ -953,12 +980,14 @@ static __global__ void pack_cp_planar(const double *__restrict__ params, const d
     r.z = D > 2 ? (float)params[i + 2 * C] : 0.f;
     r.w = (float)cpw[i];
     out[i] = r;
+    write_region_planes(rp, i, r);
 }
 
 // pack_cp_planar reading the parameters from host memory the device maps (the pinned staging
 // buffer), keeping a device copy of them in `copy`.
 static __global__ void pack_cp_planar_copy(const double *__restrict__ params, const double *__restrict__ cpw,
-                                           long long C, int D, float4 *__restrict__ out, double *__restrict__ copy)
+                                           long long C, int D, float4 *__restrict__ out, double *__restrict__ copy,
+                                           RegionPlanes rp)
 {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C) return;
@@ -966,7 +995,9 @@ static __global__ void pack_cp_planar_copy(const double *__restrict__ params, co
     copy[i] = px;
     copy[i + C] = py;
     if (D > 2) copy[i + 2 * C] = pz;
-    out[i] = make_float4((float)px, (float)py, (float)pz, (float)cpw[i]);
+    const float4 r = make_float4((float)px, (float)py, (float)pz, (float)cpw[i]);
+    out[i] = r;
+    write_region_planes(rp, i, r);
 }
 
 // grid shifts of the PCG32 stream (GpuEvaluator.cu:107-118): texel t takes draws D*t..D*t+D-1

@@ -118,7 +118,8 @@ static int optimizer_iteration(skm_optimizer *o, cudaEvent_t *ev = nullptr)
     skm_evaluator *e = o->e;
     const long long C = e->C;
     if (ev) SKM_CUDA(cudaEventRecord(ev[0], e->stream));
-    pack_cp_planar<<<(int)((C + 255) / 256), 256, 0, e->stream>>>(o->d_pos, o->d_cpw, C, e->D, e->d_cpd);
+    pack_cp_planar<<<(int)((C + 255) / 256), 256, 0, e->stream>>>(o->d_pos, o->d_cpw, C, e->D, e->d_cpd,
+                                                                  planes_of(e));
     SKM_CHECK_LAUNCH();
     if (ev) SKM_CUDA(cudaEventRecord(ev[1], e->stream));
     if (e->P.sub > 1 && o->md.do_resampling) {

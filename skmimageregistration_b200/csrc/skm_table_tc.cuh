@@ -17,8 +17,8 @@
 // of each K chunk in a ring of shared-memory stages (full/empty mbarriers), one thread issues the
 // MMAs of a chunk as soon as its stage is full and commits them to the stage's empty barrier, and
 // 4 epilogue warps drain the finished accumulator of a tile from TMEM (two accumulators, so the
-// MMAs of the next tile run meanwhile).  The transform's producers stage the control points of
-// the next brick with cp.async while they build the current one.  Operands use the K-major
+// MMAs of the next tile run meanwhile).  The transform's control points of the next brick arrive
+// by one tiled TMA load while the producers build the current one.  Operands use the K-major
 // 128-byte-swizzled canonical layout (32 K elements per 128-byte row, 8-row atoms of 1024 bytes,
 // K blocks of 32 one after the other), which the tensor cores read at full rate.
 // Every mbarrier wait is bounded; a wait that gives up sets *err and a CTA-wide abort flag that
@@ -60,7 +60,7 @@ constexpr int kConProdBase = (kConEpiWarps + 1) * 32;
 constexpr int kConThreads = kConProdBase + kTcProdThreads;     // 544
 static_assert((kTrProdWarps == 8 || kTrProdWarps == 16) && (kTcEpiWarps + 1) % 4 == 1,
               "transform producers: (lane quarter, K slice) pairs");
-constexpr int kTcNumBars = 2 * kTcStages + 6;
+constexpr int kTcNumBars = 2 * kTcStages + 8;
 constexpr int kTcMaxRegion = 4096;                               // staged control points per brick
 constexpr size_t kTcSmemMax = 227 * 1024;
 
@@ -69,8 +69,12 @@ struct TcDev {
     // transform
     int bx, by, bz;          // brick of cells per tile
     int tiles[3];
-    int rx, ry, rz, rv;      // staged control-point region of a brick (rv padded to 4)
-    int rvp;                 // region plane length (rx ry rz + 2, padded to 4)
+    int rx, ry, rz;          // control-point region of a brick
+    int rxp, ryp, rzb;       // its staged box: x covers the origin's rounding down to a multiple of 4,
+                             // y and z padding place the rows on distinct shared-memory banks
+    int rps;                 // floats per staged plane (rxp ryp rzb)
+    int rob;                 // offset of the odd planes in a region buffer (D rps rounded to 32 floats)
+    int rbuf;                // floats per region buffer (2 rob: both halves 128-byte aligned)
     int pairs_x;             // tap pairs per x row: ceil(nt0 / 2)
     int npairs;              // tap pairs (two x-neighbouring taps, the second virtual when nt0 is odd)
                              // with a nonzero table column
@@ -93,12 +97,13 @@ struct TcDev {
 
 // mbarriers of one CTA: full[s] producers -> MMA (kTcProdThreads arrivals), empty[s] MMA ->
 // producers (commit), acc_full[b] MMA -> epilogue (commit), acc_empty[b] epilogue -> MMA
-// (kTcEpiWarps * 32 arrivals), drain (final commit of the MMA thread)
+// (kTcEpiWarps * 32 arrivals), drain (final commit of the MMA thread), table and region[b]
+// (transaction counts of the bulk copies)
 struct TcBars {
-    uint64_t *full, *empty, *acc_full, *acc_empty, *drain, *table;
+    uint64_t *full, *empty, *acc_full, *acc_empty, *drain, *table, *region;
     __device__ explicit TcBars(uint64_t *b)
         : full(b), empty(b + kTcStages), acc_full(b + 2 * kTcStages), acc_empty(b + 2 * kTcStages + 2),
-          drain(b + 2 * kTcStages + 4), table(b + 2 * kTcStages + 5)
+          drain(b + 2 * kTcStages + 4), table(b + 2 * kTcStages + 5), region(b + 2 * kTcStages + 6)
     {
     }
     __device__ void init(int full_count, int epi_threads = kTcEpiWarps * 32) const
@@ -113,6 +118,8 @@ struct TcBars {
         }
         tc::mbar_init(drain, 1);
         tc::mbar_init(table, 1);
+        tc::mbar_init(&region[0], 1);
+        tc::mbar_init(&region[1], 1);
         tc::fence_mbarrier_init();
     }
 };
@@ -164,22 +171,29 @@ __device__ __forceinline__ void tc_teardown(const TcBars &B, uint32_t tmem, uint
 // A stages first (each [hi | lo], 128 rows x 32 K elements = 16 KB per half), then the table.
 constexpr int kTcStageBytes = 2 * kTcRows * kTcKBlock * 4;
 
-// Transform region: w * alpha of the brick's control points, split into tf32 hi and lo parts, each
-// in two copies (even: E[i] = R[i]; odd: O[i] = R[i + 1]) so that any two neighbouring elements
-// R[a], R[a + 1] are one aligned 8-byte load: plane (hilo * 2 + (a & 1)) * 3 + comp at a & ~1.
+// Transform: the table, then two region buffers, each two tiled loads of the weighted control-point
+// planes (RegionPlanes) over the brick's region: [D][rzb][ryp][rxp] floats of even copies
+// (E[i] = R[i]), then at rob the odd ones (O[i] = R[i + 1]), so that any two x-neighbours R[a],
+// R[a + 1] are one aligned 8-byte load: (a & 1) rob + comp rps + (a & ~1).
 struct TcTransformLayout {
-    int b, raw, reg, pairoff, regxyz, bars, total_bytes;
+    int b, reg, pairoff, bars, total_bytes;
     __host__ __device__ explicit TcTransformLayout(const TcDev &C)
     {
         b = 0;                                         // the table (A stages live in TMEM)
-        raw = b + C.kp * 2 * C.np * 4;                 // [rv] float4: staged alpha, w
-        reg = raw + 16 * C.rv;                         // [hi, lo][even, odd][3][rvp] floats
-        pairoff = reg + 4 * 4 * 3 * C.rvp;             // [kp / 4] int2: region offsets of a unit's pairs
-        regxyz = pairoff + 8 * (C.kp / 4);             // [rv] ints: x | y << 10 | z << 20 of a region element
-        bars = (regxyz + 4 * C.rv + 15) / 16 * 16;
+        reg = (b + C.kp * 2 * C.np * 4 + 127) / 128 * 128;   // [2][rbuf] floats, 128-byte aligned
+        pairoff = reg + 2 * 4 * C.rbuf;                // [kp / 4] int2: region offsets of a unit's pairs
+        bars = (pairoff + 8 * (C.kp / 4) + 15) / 16 * 16;
         total_bytes = bars + 8 * kTcNumBars + 8 + 1024;   // + alignment slack of the base
     }
 };
+
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int x, int y, int z, int w,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        :: "r"(tc::smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(tc::smem_addr(bar)) : "memory");
+}
 
 struct TcContribLayout {
     int a, bhi, blo, bars, total_bytes;
@@ -201,31 +215,30 @@ __device__ __forceinline__ unsigned char *tc_aligned_smem(float4 *dyn)
 
 // ------------------------------------------------------------------------------------------------
 // u(q, p) = sum_t T[p][t] (w alpha)[q + t] on the tensor cores; u planar [comp][cell][phase].
-// The A operand (im2col of the split region) goes from registers straight into TMEM stages
-// (tcgen05.st) and the MMAs read it there, so shared memory carries only the region reads and
-// the table reads of the tensor cores.
-__global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalParams P, TableDev T, TcDev C)
+// The region of each brick comes by one tiled TMA load (no multicast) of the weighted
+// control-point planes, double-buffered so that the next brick's load runs during this one; the
+// A operand (im2col of the region, split into tf32 hi / lo in registers) goes from registers
+// straight into TMEM stages (tcgen05.st) and the MMAs read it there, so shared memory carries only
+// the region reads and the table reads of the tensor cores.
+__global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalParams P, TableDev T, TcDev C,
+                                                                           const __grid_constant__ CUtensorMap rmap)
 {
     extern __shared__ float4 tc_smem4[];
     unsigned char *sm = tc_aligned_smem(tc_smem4);
     const TcTransformLayout L(C);
     float *Bs = reinterpret_cast<float *>(sm + L.b);
-    float4 *raw = reinterpret_cast<float4 *>(sm + L.raw);
-    float *Reg = reinterpret_cast<float *>(sm + L.reg);
+    float *Rg = reinterpret_cast<float *>(sm + L.reg);
     int2 *pairoff = reinterpret_cast<int2 *>(sm + L.pairoff);
-    int *regxyz = reinterpret_cast<int *>(sm + L.regxyz);
     uint64_t *barmem = reinterpret_cast<uint64_t *>(sm + L.bars);
     const TcBars B(barmem);
     uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(barmem + kTcNumBars);
     volatile int *abort = reinterpret_cast<volatile int *>(tmem_holder + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int Kp = C.kp, Np = C.np, N2 = 2 * C.np, RVP = C.rvp, NS = C.ns_tr;
-    const int PS = 3 * RVP;                                  // floats per (hilo, parity) plane set
+    const int Kp = C.kp, Np = C.np, N2 = 2 * C.np, NS = C.ns_tr;
     const int D = T.D;
     const int ntiles = C.tiles[0] * C.tiles[1] * C.tiles[2];
     const int nchunk = Kp / kTcKBlock;
     const int brick = C.bx * C.by * C.bz;
-    const int rtotal = C.rx * C.ry * C.rz;
     const uint32_t table_bytes = (uint32_t)(Kp * N2 * 4);
 
     if (tid == 0) {
@@ -235,9 +248,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
     if (warp == kTcMmaWarp) tc::tmem_alloc(tmem_holder, (uint32_t)C.tr_cols);
     // unit u of the K axis = tap pairs 2u and 2u + 1 (pairs: x-neighbouring taps of one x row)
     for (int u = tid; u < Kp / 4; u += kTcThreads) pairoff[u] = C.pairoff[u];
-    for (int i = tid; i < rtotal; i += kTcThreads)
-        regxyz[i] = (i % C.rx) | (((i / C.rx) % C.ry) << 10) | ((i / (C.rx * C.ry)) << 20);
-    for (int i = tid; i < 4 * PS; i += kTcThreads) Reg[i] = 0.f;   // the padding stays zero
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -248,7 +258,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
     }
 
     if (warp >= kTcEpiWarps + 1) {
-        // ---------------- producers: split region -> im2col hi/lo stages in TMEM ----------------
+        // ---------------- producers: region -> split im2col hi/lo stages in TMEM ----------------
         // A warp writes the TMEM lanes of its quarter (warp % 4): thread = row r, and slice h of
         // each 32-column K block (kTrCols / 4 units of 4 columns), hi and lo.
         const int q = warp & 3, h = (warp - (kTcEpiWarps + 1)) >> 2;
@@ -258,56 +268,34 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
         const bool row_exists = comp < D && c < brick;
         const int cx = c % C.bx, cy = (c / C.bx) % C.by, cz = c / (C.bx * C.by);
         // rows without a cell read real region data; the epilogue never stores them
-        const int rowbase = row_exists ? comp * RVP + cx + C.rx * (cy + C.ry * cz) : 0;
+        const int rowbase = row_exists ? cx + C.rxp * (cy + C.ryp * cz) : 0;
+        const int cbase = row_exists ? comp * C.rps : 0;
+        const int obase = C.rob;                             // the odd copies follow the even ones
+        const uint32_t region_bytes = (uint32_t)(2 * D * C.rps * 4);
         const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
-        auto tile_origin = [&](int tile, int *q0) {
+        // control-point index of a tile's region origin
+        auto region_origin = [&](int tile, int *j0) {
             const int t0 = tile % C.tiles[0], t12 = tile / C.tiles[0];
-            q0[0] = t0 * C.bx;
-            q0[1] = (t12 % C.tiles[1]) * C.by;
-            q0[2] = (t12 / C.tiles[1]) * C.bz;
+            j0[0] = T.qmin[0] + t0 * C.bx + T.tlo[0];
+            j0[1] = T.qmin[1] + (t12 % C.tiles[1]) * C.by + T.tlo[1];
+            j0[2] = T.qmin[2] + (t12 / C.tiles[1]) * C.bz + T.tlo[2];
         };
-        // cp.async of the raw control points (alpha, w) of a tile's region
-        auto fetch_region = [&](int tile) {
-            int q0[3];
-            tile_origin(tile, q0);
-            const int j0[3] = {T.qmin[0] + q0[0] + T.tlo[0], T.qmin[1] + q0[1] + T.tlo[1],
-                               T.qmin[2] + q0[2] + T.tlo[2]};
-            for (int i = pt; i < rtotal; i += kTrProdThreads) {
-                const int xyz = regxyz[i];
-                const int jx = j0[0] + (xyz & 1023), jy = j0[1] + ((xyz >> 10) & 1023), jz = j0[2] + (xyz >> 20);
-                const bool in = (unsigned)jx < (unsigned)P.cp.n[0] && (unsigned)jy < (unsigned)P.cp.n[1] &&
-                                (unsigned)jz < (unsigned)P.cp.n[2];
-                const float4 *src = in ? P.cpd + jx + P.cp.st[1] * jy + P.cp.st[2] * jz : P.cpd;
-                cp_async16(raw + i, src, in);
-            }
-            cp_async_commit();
+        // one thread: the two tiled loads (even planes, odd planes) of a tile's region into
+        // buffer buf; x rounds down to a multiple of 4 (the loads' alignment rule), the rows index
+        // from the remainder
+        auto issue_region = [&](int tile, int buf) {
+            int j0[3];
+            region_origin(tile, j0);
+            const int x0 = j0[0] & ~3;
+            tc::mbar_expect_tx(&B.region[buf], region_bytes);
+            tma_load_4d(Rg + buf * C.rbuf, &rmap, x0, j0[1], j0[2], 0, &B.region[buf]);
+            tma_load_4d(Rg + buf * C.rbuf + obase, &rmap, x0 + 4, j0[1], j0[2], D, &B.region[buf]);
         };
-        // raw -> w alpha, split into hi / lo, written to the even and odd copies
-        auto convert_region = [&]() {
-            for (int i = pt; i < rtotal; i += kTrProdThreads) {
-                const float4 cv = raw[i];
-                const float v[3] = {cv.w * cv.x, cv.w * cv.y, cv.w * cv.z};
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    float hi, lo;
-                    tc::split_tf32(v[k], hi, lo);
-                    float *E = Reg + k * RVP;
-                    E[i] = hi;                               // hi, even
-                    E[2 * PS + i] = lo;                      // lo, even
-                    if (i > 0) {
-                        E[PS + i - 1] = hi;                  // hi, odd
-                        E[3 * PS + i - 1] = lo;              // lo, odd
-                    }
-                }
-            }
-        };
-        if ((int)blockIdx.x < ntiles) {
-            fetch_region(blockIdx.x);
-            cp_async_wait_all();
-            tc::bar_sync(kTcProdBar, kTrProdThreads);
-            convert_region();
+        int issued = 0, landed = 0;                          // region loads (thread pt == 0)
+        if (pt == 0 && (int)blockIdx.x < ntiles) {
+            issue_region(blockIdx.x, 0);
+            issued = 1;
         }
-        tc::bar_sync(kTcProdBar, kTrProdThreads);
         int s = 0;
         uint32_t phase = 0;                                  // parity of stage s's current use
         unsigned g = 0;
@@ -316,7 +304,23 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
             const int tile = blockIdx.x + it * gridDim.x;
             if (tile >= ntiles) break;
             const int next = tile + gridDim.x;
-            if (next < ntiles) fetch_region(next);          // raw is free: converted before the last barrier
+            // the other buffer's last reader was the previous tile, which every producer has left
+            if (pt == 0 && next < ntiles) {
+                issue_region(next, (it + 1) & 1);
+                ++issued;
+            }
+            {
+                const bool ok = tc::mbar_wait(&B.region[it & 1], (it >> 1) & 1, abort);
+                if (ok) landed = it + 1;
+                if (__any_sync(0xffffffffu, !ok)) {
+                    if (lane == 0) tc_fail(abort, C.err);
+                    failed = true;
+                }
+            }
+            int j0[3];
+            region_origin(tile, j0);
+            const float *R = Rg + (it & 1) * C.rbuf + cbase;
+            const int rb = rowbase + (j0[0] & 3);
             for (int kc = 0; kc < nchunk; ++kc, ++g) {
                 // a failed wait skips the rest of the tile (warp-uniform: tcgen05.st is warp-wide);
                 // the decision is made uniform across the producers at the tile's end
@@ -334,20 +338,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
 #pragma unroll
                     for (int u = 0; u < kTrCols / 4; ++u) {
                         const int2 o = po[u];
-                        const int a0 = rowbase + o.x, a1 = rowbase + o.y;
-                        const int e0 = (a0 & 1) * PS + (a0 & ~1), e1 = (a1 & 1) * PS + (a1 & ~1);
-                        const float2 h0 = *reinterpret_cast<const float2 *>(Reg + e0);
-                        const float2 h1 = *reinterpret_cast<const float2 *>(Reg + e1);
-                        const float2 l0 = *reinterpret_cast<const float2 *>(Reg + 2 * PS + e0);
-                        const float2 l1 = *reinterpret_cast<const float2 *>(Reg + 2 * PS + e1);
-                        vh[4 * u] = h0.x;
-                        vh[4 * u + 1] = h0.y;
-                        vh[4 * u + 2] = h1.x;
-                        vh[4 * u + 3] = h1.y;
-                        vl[4 * u] = l0.x;
-                        vl[4 * u + 1] = l0.y;
-                        vl[4 * u + 2] = l1.x;
-                        vl[4 * u + 3] = l1.y;
+                        const int a0 = rb + o.x, a1 = rb + o.y;
+                        const float2 v0 = *reinterpret_cast<const float2 *>(R + (a0 & 1) * obase + (a0 & ~1));
+                        const float2 v1 = *reinterpret_cast<const float2 *>(R + (a1 & 1) * obase + (a1 & ~1));
+                        tc::split_tf32(v0.x, vh[4 * u], vl[4 * u]);
+                        tc::split_tf32(v0.y, vh[4 * u + 1], vl[4 * u + 1]);
+                        tc::split_tf32(v1.x, vh[4 * u + 2], vl[4 * u + 2]);
+                        tc::split_tf32(v1.y, vh[4 * u + 3], vl[4 * u + 3]);
                     }
                     const uint32_t col = (uint32_t)(C.tr_abase + 2 * kTcKBlock * s + kTrCols * h);
                     if (kTrCols == 16) {
@@ -366,16 +363,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
                     phase ^= 1u;
                 }
             }
-            // every producer has finished the tile (and read the region for the last time)
+            // every producer has finished the tile (and read its region buffer for the last time)
             if (tc::bar_or(kTcProdBar, kTrProdThreads, failed)) break;
-            if (next < ntiles) {
-                cp_async_wait_all();
-                tc::bar_sync(kTcProdBar, kTrProdThreads);   // every thread's copies have landed
-                convert_region();
-            }
-            tc::bar_sync(kTcProdBar, kTrProdThreads);
         }
-        cp_async_wait_all();
+        // after a failure: region loads still in flight land before the CTA leaves (bounded)
+        for (int k = landed; pt == 0 && k < issued; ++k) tc::mbar_wait(&B.region[k & 1], (k >> 1) & 1);
     } else if (warp == kTcMmaWarp) {
         // ---------------- MMA issue (one thread) ----------------
         if (lane == 0) {
@@ -705,6 +697,8 @@ inline uint32_t pow2_at_least(uint32_t v)
 struct TcPlan {
     bool enabled = false;
     TcDev dev{};
+    RegionPlanes rp{};               // weighted control-point planes (written by the packing kernels)
+    CUtensorMap rmap{};              // tiled loads of a brick's region from rp
     float *d_btr = nullptr, *d_bcon = nullptr;
     int2 *d_pairoff = nullptr;
     int *d_ctap = nullptr;           // contrib tap k -> box tap
@@ -714,9 +708,44 @@ struct TcPlan {
     WarpTmaPlan wt;                  // the warp kernel with TMA-staged coefficients (3-D)
 };
 
+// Shared-memory wavefronts of the producers' region loads (8-byte loads of rows r = 32 q + lane)
+// for a staged box pitch: the sum of two models of the banks (each half warp on its own, and the
+// whole warp), averaged over the four x remainders of the region origin.  Host-side, to choose
+// the box padding.
+inline double region_bank_cost(const TcDev &C, int D, const std::vector<int> &pairs, const int *nt, int rxp, int ryp,
+                               int rzb)
+{
+    const int rps = rxp * ryp * rzb, rob = (D * rps + 31) / 32 * 32, brick = C.bx * C.by * C.bz;
+    long long total = 0;
+    int addr[32];
+    for (int xs = 0; xs < 4; ++xs)
+        for (int q = 0; q < 4; ++q)
+            for (int t0 : pairs) {
+                const int tx = t0 % nt[0], ty = (t0 / nt[0]) % nt[1], tz = t0 / (nt[0] * nt[1]);
+                for (int l = 0; l < 32; ++l) {
+                    const int r = 32 * q + l, comp = r / C.ct, c = r % C.ct;
+                    const bool ex = comp < D && c < brick;
+                    const int cx = ex ? c % C.bx : 0, cy = ex ? (c / C.bx) % C.by : 0, cz = ex ? c / (C.bx * C.by) : 0;
+                    const int a = (cx + xs + tx) + rxp * ((cy + ty) + ryp * (cz + tz));
+                    addr[l] = ((a & 1) * rob + (ex ? comp : 0) * rps + (a & ~1)) / 2;   // 8-byte word
+                }
+                auto conflicts = [&](int lo, int hi) {   // distinct words on the busiest bank
+                    int w[32], cnt[16] = {0};
+                    std::copy(addr + lo, addr + hi, w);
+                    std::sort(w, w + (hi - lo));
+                    for (int i = 0; i < hi - lo; ++i)
+                        if (i == 0 || w[i] != w[i - 1]) ++cnt[w[i] % 16];
+                    return *std::max_element(cnt, cnt + 16);
+                };
+                total += conflicts(0, 16) + conflicts(16, 32) + std::max(2, conflicts(0, 32));
+            }
+    return (double)total / (16.0 * std::max<size_t>(1, pairs.size()));
+}
+
 // Decides whether the tensor-core kernels apply to a table plan and builds their operand
-// tables.  Returns 0 (tc.enabled says whether they apply) or 2 on a CUDA error.
-inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
+// tables.  ncp: control-point grid size per axis.  Returns 0 (tc.enabled says whether they
+// apply) or 2 on a CUDA error.
+inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t stream)
 {
     tc.enabled = false;
     const TableDev &T = pl.dev;
@@ -760,12 +789,13 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
             for (int bx = 1; bx <= std::min(C.ct / (bz * by), T.nq[0]); ++bx) {
                 const long long tiles = (long long)((T.nq[0] + bx - 1) / bx) * ((T.nq[1] + by - 1) / by) *
                                         ((T.nq[2] + bz - 1) / bz);
-                const long long rv =
-                    (long long)(bx + T.nt[0] - 1 + xpad) * (by + T.nt[1] - 1) * (bz + T.nt[2] - 1);
+                const int rx = bx + T.nt[0] - 1 + xpad, ry = by + T.nt[1] - 1, rz = bz + T.nt[2] - 1;
+                const long long rv = (long long)rx * ry * rz;
                 if (rv > kTcMaxRegion) continue;
                 TcDev probe = C;
-                probe.rv = (int)((rv + 3) / 4 * 4);
-                probe.rvp = (int)((rv + 2 + 3) / 4 * 4);
+                probe.rps = (rx + 3 + 3) / 4 * 4 * ry * rz;
+                probe.rob = (T.D * probe.rps + 31) / 32 * 32;
+                probe.rbuf = 2 * probe.rob;
                 if ((size_t)TcTransformLayout(probe).total_bytes > kTcSmemMax) continue;
                 if (best_tiles < 0 || tiles < best_tiles || (tiles == best_tiles && rv < best_rv)) {
                     best_tiles = tiles;
@@ -782,9 +812,34 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
     C.rx = C.bx + T.nt[0] - 1 + xpad;
     C.ry = C.by + T.nt[1] - 1;
     C.rz = C.bz + T.nt[2] - 1;
-    if (C.rx * C.ry * C.rz > kTcMaxRegion || C.rx >= 1024 || C.ry >= 1024) return 0;
-    C.rv = (C.rx * C.ry * C.rz + 3) / 4 * 4;
-    C.rvp = (C.rx * C.ry * C.rz + 2 + 3) / 4 * 4;
+    if (C.rx * C.ry * C.rz > kTcMaxRegion) return 0;
+    // staged box: x covers the region from an origin rounded down to a multiple of 4; among the
+    // paddings that fit, the one with the fewest shared-memory wavefronts (then the smallest)
+    {
+        const int rxp0 = (C.rx + 3 + 3) / 4 * 4;
+        double best = -1.0;
+        for (int rxp = rxp0; rxp <= rxp0 + 8; rxp += 4)
+            for (int ryp = C.ry; ryp <= C.ry + 6; ++ryp)
+                for (int rzb = C.rz; rzb <= C.rz + (T.D == 3 ? 3 : 0); ++rzb) {
+                    if (rxp > 256 || ryp > 256 || rzb > 256) continue;
+                    TcDev probe = C;
+                    probe.rps = rxp * ryp * rzb;
+                    probe.rob = (T.D * probe.rps + 31) / 32 * 32;
+                    probe.rbuf = 2 * probe.rob;
+                    if ((size_t)TcTransformLayout(probe).total_bytes > kTcSmemMax) continue;
+                    const double cost = region_bank_cost(C, T.D, pairs, T.nt, rxp, ryp, rzb);
+                    if (best < 0.0 || cost < best - 1e-9 || (cost < best + 1e-9 && probe.rps < C.rps)) {
+                        best = cost;
+                        C.rxp = rxp;
+                        C.ryp = ryp;
+                        C.rzb = rzb;
+                        C.rps = probe.rps;
+                        C.rob = probe.rob;
+                        C.rbuf = probe.rbuf;
+                    }
+                }
+        if (best < 0.0) return 0;
+    }
     C.tr_stride = (int)pow2_at_least(2 * C.np);
     C.tr_abase = 2 * C.tr_stride;                            // then the A stages: 64 columns each
     C.tr_cols = 512;
@@ -819,7 +874,7 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
     // 2 u + (j >> 1) (t0 its first box tap); virtual taps and padding stay zero
     std::vector<int2> pairoff((size_t)C.kp / 4, int2{0, 0});
     auto region_off = [&](int t) {
-        return t % T.nt[0] + C.rx * ((t / T.nt[0]) % T.nt[1] + C.ry * (t / (T.nt[0] * T.nt[1])));
+        return t % T.nt[0] + C.rxp * ((t / T.nt[0]) % T.nt[1] + C.ryp * (t / (T.nt[0] * T.nt[1])));
     };
     for (int u = 0; u < C.kp / 4; ++u) {
         pairoff[(size_t)u].x = 2 * u < C.npairs ? region_off(pairs[(size_t)(2 * u)]) : 0;
@@ -861,6 +916,38 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
     C.err = tc.d_err;
     pl.dev.tc_err = tc.d_err;
 
+    // weighted control-point planes and the tiled load of a brick's region from them
+    {
+        const int n0 = ncp[0], n1 = ncp[1], n2 = T.D == 3 ? ncp[2] : 1;
+        const int nxp = (n0 + 3 + 3) / 4 * 4;             // the odd planes' columns are shifted by 3
+        const long long plane = (long long)nxp * n1 * n2;
+        if (cudaMalloc((void **)&tc.rp.p, sizeof(float) * 2 * T.D * plane) != cudaSuccess) return 2;
+        if (cudaMemsetAsync(tc.rp.p, 0, sizeof(float) * 2 * T.D * plane, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess)
+            return 2;
+        tc.rp.n0 = n0;
+        tc.rp.nxp = nxp;
+        tc.rp.D = T.D;
+        tc.rp.plane = plane;
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult qr{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr) != cudaSuccess || !fn ||
+            qr != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        const cuuint64_t gdim[4] = {(cuuint64_t)nxp, (cuuint64_t)n1, (cuuint64_t)n2, (cuuint64_t)(2 * T.D)};
+        const cuuint64_t gstride[3] = {(cuuint64_t)nxp * 4, (cuuint64_t)nxp * n1 * 4, (cuuint64_t)plane * 4};
+        // one box = the D even or the D odd planes
+        const cuuint32_t bdim[4] = {(cuuint32_t)C.rxp, (cuuint32_t)C.ryp, (cuuint32_t)C.rzb, (cuuint32_t)T.D};
+        const cuuint32_t estride[4] = {1, 1, 1, 1};
+        if (reinterpret_cast<PfnTensorMapEncodeTiled>(fn)(
+                &tc.rmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, tc.rp.p, gdim, gstride, bdim, estride,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return 0;
+    }
+
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 2;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 2;
@@ -885,7 +972,7 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, cudaStream_t stream)
 
 inline int table_transform_tc(const TcPlan &tc, const TablePlan &pl, const EvalParams &P, cudaStream_t s)
 {
-    table_transform_tc_kernel<<<tc.transform_blocks, kTcThreads, tc.transform_smem, s>>>(P, pl.dev, tc.dev);
+    table_transform_tc_kernel<<<tc.transform_blocks, kTcThreads, tc.transform_smem, s>>>(P, pl.dev, tc.dev, tc.rmap);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
@@ -972,6 +1059,7 @@ inline void table_tc_free(TcPlan &tc)
     if (tc.d_bcon) cudaFree(tc.d_bcon);
     if (tc.d_err) cudaFree(tc.d_err);
     if (tc.d_pairoff) cudaFree(tc.d_pairoff);
+    if (tc.rp.p) cudaFree(tc.rp.p);
     warp_tma_free(tc.wt);
     if (tc.d_ctap) cudaFree(tc.d_ctap);
     tc = TcPlan{};
