@@ -928,12 +928,8 @@ __global__ void __launch_bounds__(256) displacement_kernel(EvalParams P, double 
 
 // ---- small helpers ----------------------------------------------------------------------------
 // Weighted control points w alpha as planes for the tensor-core transform's tiled loads:
-// [2 D][n2][n1][nxp] floats, planes 0..D-1 the components (E[x] = w alpha(x)), planes D..2D-1 the
-// same stored 3 columns to the right (O[x] = w alpha(x - 3)): loaded from x0 + 4 next to E's load
-// from x0, O's box starts one control point later than E's, so that any two x-neighbours are one
-// aligned 8-byte element pair of E or of O, also for boxes that start left of the grid.  Rows are
-// padded to nxp >= n0 + 3 (a multiple of 4 floats, the tiled loads' stride rule); the padding
-// stays zero.  p == nullptr: not used.
+// [D][n2][n1][nxp] floats, one plane per component.  Rows are padded to nxp (a multiple of 4
+// floats, the tiled loads' stride rule); the padding stays zero.  p == nullptr: not used.
 struct RegionPlanes {
     float *p;
     int n0, nxp, D;
@@ -949,7 +945,6 @@ __device__ __forceinline__ void write_region_planes(const RegionPlanes &rp, long
     const float v[3] = {r.w * r.x, r.w * r.y, r.w * r.z};
     for (int k = 0; k < rp.D; ++k) {
         rp.p[k * rp.plane + row + x] = v[k];
-        rp.p[(rp.D + k) * rp.plane + row + x + 3] = v[k];
     }
 }
 

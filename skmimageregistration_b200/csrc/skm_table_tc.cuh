@@ -60,7 +60,8 @@ constexpr int kConProdBase = (kConEpiWarps + 1) * 32;
 constexpr int kConThreads = kConProdBase + kTcProdThreads;     // 544
 static_assert((kTrProdWarps == 8 || kTrProdWarps == 16) && (kTcEpiWarps + 1) % 4 == 1,
               "transform producers: (lane quarter, K slice) pairs");
-constexpr int kTcNumBars = 2 * kTcStages + 8;
+constexpr int kTcRegionBufs = 3;                                 // transform region buffers (at most)
+constexpr int kTcNumBars = 2 * kTcStages + 6 + kTcRegionBufs;
 constexpr int kTcMaxRegion = 4096;                               // staged control points per brick
 constexpr size_t kTcSmemMax = 227 * 1024;
 
@@ -73,8 +74,8 @@ struct TcDev {
     int rxp, ryp, rzb;       // its staged box: x covers the origin's rounding down to a multiple of 4,
                              // y and z padding place the rows on distinct shared-memory banks
     int rps;                 // floats per staged plane (rxp ryp rzb)
-    int rob;                 // offset of the odd planes in a region buffer (D rps rounded to 32 floats)
-    int rbuf;                // floats per region buffer (2 rob: both halves 128-byte aligned)
+    int rbuf;                // floats per region buffer (D planes, 128-byte aligned)
+    int nrb;                 // region buffers (2 or 3: loads run that many tiles ahead, minus one)
     int pairs_x;             // tap pairs per x row: ceil(nt0 / 2)
     int npairs;              // tap pairs (two x-neighbouring taps, the second virtual when nt0 is odd)
                              // with a nonzero table column
@@ -85,7 +86,7 @@ struct TcDev {
     int tr_abase;            // first TMEM column of the A stages
     const float *btr;        // 2 np rows x kp, K-major 128-byte swizzled
     // contrib
-    const int2 *pairoff;     // [kp / 4]: region offsets (tx + rx (ty + ry tz)) of a unit's two pairs
+    const int2 *pairoff;     // [kp / 4]: region offsets (tx + rxp (ty + ryp tz)) of a unit's two pairs
     int kpc;                 // phases padded to 32 (K)
     int nct;                 // contrib taps: the box taps with a nonzero table column
     int npc;                 // nct padded to 16 (N)
@@ -118,8 +119,7 @@ struct TcBars {
         }
         tc::mbar_init(drain, 1);
         tc::mbar_init(table, 1);
-        tc::mbar_init(&region[0], 1);
-        tc::mbar_init(&region[1], 1);
+        for (int b = 0; b < kTcRegionBufs; ++b) tc::mbar_init(&region[b], 1);
         tc::fence_mbarrier_init();
     }
 };
@@ -171,17 +171,15 @@ __device__ __forceinline__ void tc_teardown(const TcBars &B, uint32_t tmem, uint
 // A stages first (each [hi | lo], 128 rows x 32 K elements = 16 KB per half), then the table.
 constexpr int kTcStageBytes = 2 * kTcRows * kTcKBlock * 4;
 
-// Transform: the table, then two region buffers, each two tiled loads of the weighted control-point
-// planes (RegionPlanes) over the brick's region: [D][rzb][ryp][rxp] floats of even copies
-// (E[i] = R[i]), then at rob the odd ones (O[i] = R[i + 1]), so that any two x-neighbours R[a],
-// R[a + 1] are one aligned 8-byte load: (a & 1) rob + comp rps + (a & ~1).
+// Transform: the table, then nrb region buffers, each one tiled load of the weighted control-point
+// planes (RegionPlanes) over a brick's region: [D][rzb][ryp][rxp] floats.
 struct TcTransformLayout {
     int b, reg, pairoff, bars, total_bytes;
     __host__ __device__ explicit TcTransformLayout(const TcDev &C)
     {
         b = 0;                                         // the table (A stages live in TMEM)
-        reg = (b + C.kp * 2 * C.np * 4 + 127) / 128 * 128;   // [2][rbuf] floats, 128-byte aligned
-        pairoff = reg + 2 * 4 * C.rbuf;                // [kp / 4] int2: region offsets of a unit's pairs
+        reg = (b + C.kp * 2 * C.np * 4 + 127) / 128 * 128;   // [nrb][rbuf] floats, 128-byte aligned
+        pairoff = reg + C.nrb * 4 * C.rbuf;            // [kp / 4] int2: region offsets of a unit's pairs
         bars = (pairoff + 8 * (C.kp / 4) + 15) / 16 * 16;
         total_bytes = bars + 8 * kTcNumBars + 8 + 1024;   // + alignment slack of the base
     }
@@ -216,7 +214,7 @@ __device__ __forceinline__ unsigned char *tc_aligned_smem(float4 *dyn)
 // ------------------------------------------------------------------------------------------------
 // u(q, p) = sum_t T[p][t] (w alpha)[q + t] on the tensor cores; u planar [comp][cell][phase].
 // The region of each brick comes by one tiled TMA load (no multicast) of the weighted
-// control-point planes, double-buffered so that the next brick's load runs during this one; the
+// control-point planes, into a ring of nrb buffers so that the loads run ahead of the bricks; the
 // A operand (im2col of the region, split into tf32 hi / lo in registers) goes from registers
 // straight into TMEM stages (tcgen05.st) and the MMAs read it there, so shared memory carries only
 // the region reads and the table reads of the tensor cores.
@@ -270,8 +268,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
         // rows without a cell read real region data; the epilogue never stores them
         const int rowbase = row_exists ? cx + C.rxp * (cy + C.ryp * cz) : 0;
         const int cbase = row_exists ? comp * C.rps : 0;
-        const int obase = C.rob;                             // the odd copies follow the even ones
-        const uint32_t region_bytes = (uint32_t)(2 * D * C.rps * 4);
+        const int NB = C.nrb;
+        const uint32_t region_bytes = (uint32_t)(D * C.rps * 4);
         const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
         // control-point index of a tile's region origin
         auto region_origin = [&](int tile, int *j0) {
@@ -280,22 +278,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
             j0[1] = T.qmin[1] + (t12 % C.tiles[1]) * C.by + T.tlo[1];
             j0[2] = T.qmin[2] + (t12 / C.tiles[1]) * C.bz + T.tlo[2];
         };
-        // one thread: the two tiled loads (even planes, odd planes) of a tile's region into
-        // buffer buf; x rounds down to a multiple of 4 (the loads' alignment rule), the rows index
-        // from the remainder
-        auto issue_region = [&](int tile, int buf) {
+        // one thread: the tiled load of the region of the CTA's k-th tile into buffer k % NB; x
+        // rounds down to a multiple of 4 (the load's alignment rule), the rows index from the
+        // remainder
+        auto issue_region = [&](int k) {
             int j0[3];
-            region_origin(tile, j0);
-            const int x0 = j0[0] & ~3;
-            tc::mbar_expect_tx(&B.region[buf], region_bytes);
-            tma_load_4d(Rg + buf * C.rbuf, &rmap, x0, j0[1], j0[2], 0, &B.region[buf]);
-            tma_load_4d(Rg + buf * C.rbuf + obase, &rmap, x0 + 4, j0[1], j0[2], D, &B.region[buf]);
+            region_origin(blockIdx.x + k * gridDim.x, j0);
+            tc::mbar_expect_tx(&B.region[k % NB], region_bytes);
+            tma_load_4d(Rg + (k % NB) * C.rbuf, &rmap, j0[0] & ~3, j0[1], j0[2], 0, &B.region[k % NB]);
         };
         int issued = 0, landed = 0;                          // region loads (thread pt == 0)
-        if (pt == 0 && (int)blockIdx.x < ntiles) {
-            issue_region(blockIdx.x, 0);
-            issued = 1;
-        }
+        for (; pt == 0 && issued < NB - 1 && (int)blockIdx.x + issued * (int)gridDim.x < ntiles; ++issued)
+            issue_region(issued);
         int s = 0;
         uint32_t phase = 0;                                  // parity of stage s's current use
         unsigned g = 0;
@@ -303,14 +297,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
         for (int it = 0;; ++it) {
             const int tile = blockIdx.x + it * gridDim.x;
             if (tile >= ntiles) break;
-            const int next = tile + gridDim.x;
-            // the other buffer's last reader was the previous tile, which every producer has left
-            if (pt == 0 && next < ntiles) {
-                issue_region(next, (it + 1) & 1);
-                ++issued;
-            }
+            // tile it + NB - 1 goes to the buffer of tile it - 1, which every producer has left
+            if (pt == 0 && (int)blockIdx.x + issued * (int)gridDim.x < ntiles) issue_region(issued++);
             {
-                const bool ok = tc::mbar_wait(&B.region[it & 1], (it >> 1) & 1, abort);
+                const bool ok = tc::mbar_wait(&B.region[it % NB], (it / NB) & 1, abort);
                 if (ok) landed = it + 1;
                 if (__any_sync(0xffffffffu, !ok)) {
                     if (lane == 0) tc_fail(abort, C.err);
@@ -319,8 +309,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
             }
             int j0[3];
             region_origin(tile, j0);
-            const float *R = Rg + (it & 1) * C.rbuf + cbase;
-            const int rb = rowbase + (j0[0] & 3);
+            const float *R = Rg + (it % NB) * C.rbuf + cbase + rowbase + (j0[0] & 3);
             for (int kc = 0; kc < nchunk; ++kc, ++g) {
                 // a failed wait skips the rest of the tile (warp-uniform: tcgen05.st is warp-wide);
                 // the decision is made uniform across the producers at the tile's end
@@ -338,13 +327,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
 #pragma unroll
                     for (int u = 0; u < kTrCols / 4; ++u) {
                         const int2 o = po[u];
-                        const int a0 = rb + o.x, a1 = rb + o.y;
-                        const float2 v0 = *reinterpret_cast<const float2 *>(R + (a0 & 1) * obase + (a0 & ~1));
-                        const float2 v1 = *reinterpret_cast<const float2 *>(R + (a1 & 1) * obase + (a1 & ~1));
-                        tc::split_tf32(v0.x, vh[4 * u], vl[4 * u]);
-                        tc::split_tf32(v0.y, vh[4 * u + 1], vl[4 * u + 1]);
-                        tc::split_tf32(v1.x, vh[4 * u + 2], vl[4 * u + 2]);
-                        tc::split_tf32(v1.y, vh[4 * u + 3], vl[4 * u + 3]);
+                        tc::split_tf32(R[o.x], vh[4 * u], vl[4 * u]);
+                        tc::split_tf32(R[o.x + 1], vh[4 * u + 1], vl[4 * u + 1]);
+                        tc::split_tf32(R[o.y], vh[4 * u + 2], vl[4 * u + 2]);
+                        tc::split_tf32(R[o.y + 1], vh[4 * u + 3], vl[4 * u + 3]);
                     }
                     const uint32_t col = (uint32_t)(C.tr_abase + 2 * kTcKBlock * s + kTrCols * h);
                     if (kTrCols == 16) {
@@ -367,7 +353,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
             if (tc::bar_or(kTcProdBar, kTrProdThreads, failed)) break;
         }
         // after a failure: region loads still in flight land before the CTA leaves (bounded)
-        for (int k = landed; pt == 0 && k < issued; ++k) tc::mbar_wait(&B.region[k & 1], (k >> 1) & 1);
+        for (int k = landed; pt == 0 && k < issued; ++k) tc::mbar_wait(&B.region[k % NB], (k / NB) & 1);
     } else if (warp == kTcMmaWarp) {
         // ---------------- MMA issue (one thread) ----------------
         if (lane == 0) {
@@ -708,37 +694,33 @@ struct TcPlan {
     WarpTmaPlan wt;                  // the warp kernel with TMA-staged coefficients (3-D)
 };
 
-// Shared-memory wavefronts of the producers' region loads (8-byte loads of rows r = 32 q + lane)
-// for a staged box pitch: the sum of two models of the banks (each half warp on its own, and the
-// whole warp), averaged over the four x remainders of the region origin.  Host-side, to choose
-// the box padding.
+// Shared-memory wavefronts of the producers' region loads (4-byte loads of rows r = 32 q + lane,
+// two per tap pair) for a staged box pitch: the distinct words on the busiest bank, averaged over
+// the four x remainders of the region origin.  Host-side, to choose the box padding.
 inline double region_bank_cost(const TcDev &C, int D, const std::vector<int> &pairs, const int *nt, int rxp, int ryp,
                                int rzb)
 {
-    const int rps = rxp * ryp * rzb, rob = (D * rps + 31) / 32 * 32, brick = C.bx * C.by * C.bz;
+    const int rps = rxp * ryp * rzb, brick = C.bx * C.by * C.bz;
+    int rowoff[128];
     long long total = 0;
-    int addr[32];
+    for (int r = 0; r < 128; ++r) {
+        const int comp = r / C.ct, c = r % C.ct;
+        const bool ex = comp < D && c < brick;
+        rowoff[r] = ex ? comp * rps + c % C.bx + rxp * ((c / C.bx) % C.by + ryp * (c / (C.bx * C.by))) : 0;
+    }
     for (int xs = 0; xs < 4; ++xs)
         for (int q = 0; q < 4; ++q)
-            for (int t0 : pairs) {
-                const int tx = t0 % nt[0], ty = (t0 / nt[0]) % nt[1], tz = t0 / (nt[0] * nt[1]);
-                for (int l = 0; l < 32; ++l) {
-                    const int r = 32 * q + l, comp = r / C.ct, c = r % C.ct;
-                    const bool ex = comp < D && c < brick;
-                    const int cx = ex ? c % C.bx : 0, cy = ex ? (c / C.bx) % C.by : 0, cz = ex ? c / (C.bx * C.by) : 0;
-                    const int a = (cx + xs + tx) + rxp * ((cy + ty) + ryp * (cz + tz));
-                    addr[l] = ((a & 1) * rob + (ex ? comp : 0) * rps + (a & ~1)) / 2;   // 8-byte word
+            for (int t0 : pairs)
+                for (int t1 = 0; t1 < 2; ++t1) {
+                    const int tx = t0 % nt[0] + t1, ty = (t0 / nt[0]) % nt[1], tz = t0 / (nt[0] * nt[1]);
+                    const int off = xs + tx + rxp * (ty + ryp * tz);
+                    int w[32], cnt[32] = {0};
+                    for (int l = 0; l < 32; ++l) w[l] = rowoff[32 * q + l] + off;
+                    std::sort(w, w + 32);
+                    for (int i = 0; i < 32; ++i)
+                        if (i == 0 || w[i] != w[i - 1]) ++cnt[w[i] % 32];
+                    total += *std::max_element(cnt, cnt + 32);
                 }
-                auto conflicts = [&](int lo, int hi) {   // distinct words on the busiest bank
-                    int w[32], cnt[16] = {0};
-                    std::copy(addr + lo, addr + hi, w);
-                    std::sort(w, w + (hi - lo));
-                    for (int i = 0; i < hi - lo; ++i)
-                        if (i == 0 || w[i] != w[i - 1]) ++cnt[w[i] % 16];
-                    return *std::max_element(cnt, cnt + 16);
-                };
-                total += conflicts(0, 16) + conflicts(16, 32) + std::max(2, conflicts(0, 32));
-            }
     return (double)total / (16.0 * std::max<size_t>(1, pairs.size()));
 }
 
@@ -794,8 +776,8 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
                 if (rv > kTcMaxRegion) continue;
                 TcDev probe = C;
                 probe.rps = (rx + 3 + 3) / 4 * 4 * ry * rz;
-                probe.rob = (T.D * probe.rps + 31) / 32 * 32;
-                probe.rbuf = 2 * probe.rob;
+                probe.rbuf = (T.D * probe.rps + 31) / 32 * 32;
+                probe.nrb = 2;
                 if ((size_t)TcTransformLayout(probe).total_bytes > kTcSmemMax) continue;
                 if (best_tiles < 0 || tiles < best_tiles || (tiles == best_tiles && rv < best_rv)) {
                     best_tiles = tiles;
@@ -814,18 +796,19 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
     C.rz = C.bz + T.nt[2] - 1;
     if (C.rx * C.ry * C.rz > kTcMaxRegion) return 0;
     // staged box: x covers the region from an origin rounded down to a multiple of 4; among the
-    // paddings that fit, the one with the fewest shared-memory wavefronts (then the smallest)
+    // paddings that fit with two buffers, the one with the fewest shared-memory wavefronts (then
+    // the smallest); a third buffer when it fits too
     {
         const int rxp0 = (C.rx + 3 + 3) / 4 * 4;
         double best = -1.0;
         for (int rxp = rxp0; rxp <= rxp0 + 8; rxp += 4)
-            for (int ryp = C.ry; ryp <= C.ry + 6; ++ryp)
-                for (int rzb = C.rz; rzb <= C.rz + (T.D == 3 ? 3 : 0); ++rzb) {
+            for (int ryp = C.ry; ryp <= C.ry + 4; ++ryp)
+                for (int rzb = C.rz; rzb <= C.rz + (T.D == 3 ? 2 : 0); ++rzb) {
                     if (rxp > 256 || ryp > 256 || rzb > 256) continue;
                     TcDev probe = C;
                     probe.rps = rxp * ryp * rzb;
-                    probe.rob = (T.D * probe.rps + 31) / 32 * 32;
-                    probe.rbuf = 2 * probe.rob;
+                    probe.rbuf = (T.D * probe.rps + 31) / 32 * 32;
+                    probe.nrb = 2;
                     if ((size_t)TcTransformLayout(probe).total_bytes > kTcSmemMax) continue;
                     const double cost = region_bank_cost(C, T.D, pairs, T.nt, rxp, ryp, rzb);
                     if (best < 0.0 || cost < best - 1e-9 || (cost < best + 1e-9 && probe.rps < C.rps)) {
@@ -834,11 +817,12 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
                         C.ryp = ryp;
                         C.rzb = rzb;
                         C.rps = probe.rps;
-                        C.rob = probe.rob;
                         C.rbuf = probe.rbuf;
                     }
                 }
         if (best < 0.0) return 0;
+        C.nrb = kTcRegionBufs;
+        if ((size_t)TcTransformLayout(C).total_bytes > kTcSmemMax) C.nrb = 2;
     }
     C.tr_stride = (int)pow2_at_least(2 * C.np);
     C.tr_abase = 2 * C.tr_stride;                            // then the A stages: 64 columns each
@@ -919,10 +903,10 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
     // weighted control-point planes and the tiled load of a brick's region from them
     {
         const int n0 = ncp[0], n1 = ncp[1], n2 = T.D == 3 ? ncp[2] : 1;
-        const int nxp = (n0 + 3 + 3) / 4 * 4;             // the odd planes' columns are shifted by 3
+        const int nxp = (n0 + 3) / 4 * 4;
         const long long plane = (long long)nxp * n1 * n2;
-        if (cudaMalloc((void **)&tc.rp.p, sizeof(float) * 2 * T.D * plane) != cudaSuccess) return 2;
-        if (cudaMemsetAsync(tc.rp.p, 0, sizeof(float) * 2 * T.D * plane, stream) != cudaSuccess ||
+        if (cudaMalloc((void **)&tc.rp.p, sizeof(float) * T.D * plane) != cudaSuccess) return 2;
+        if (cudaMemsetAsync(tc.rp.p, 0, sizeof(float) * T.D * plane, stream) != cudaSuccess ||
             cudaStreamSynchronize(stream) != cudaSuccess)
             return 2;
         tc.rp.n0 = n0;
@@ -936,9 +920,8 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
             cudaGetLastError();
             return 0;
         }
-        const cuuint64_t gdim[4] = {(cuuint64_t)nxp, (cuuint64_t)n1, (cuuint64_t)n2, (cuuint64_t)(2 * T.D)};
+        const cuuint64_t gdim[4] = {(cuuint64_t)nxp, (cuuint64_t)n1, (cuuint64_t)n2, (cuuint64_t)T.D};
         const cuuint64_t gstride[3] = {(cuuint64_t)nxp * 4, (cuuint64_t)nxp * n1 * 4, (cuuint64_t)plane * 4};
-        // one box = the D even or the D odd planes
         const cuuint32_t bdim[4] = {(cuuint32_t)C.rxp, (cuuint32_t)C.ryp, (cuuint32_t)C.rzb, (cuuint32_t)T.D};
         const cuuint32_t estride[4] = {1, 1, 1, 1};
         if (reinterpret_cast<PfnTensorMapEncodeTiled>(fn)(
