@@ -45,11 +45,13 @@ constexpr int kTrProdWarps = 8;                                  // transform pr
 constexpr int kTrProdThreads = kTrProdWarps * 32;                // K slice of one TMEM lane quarter each
 constexpr int kTrSlices = kTrProdWarps / 4;                      // K slices of a 32-column block
 constexpr int kTrCols = 32 / kTrSlices;                          // columns per producer warp and K block
-constexpr int kTcThreads = kTcProdBase + kTrProdThreads;
+constexpr int kTrTmaWarp = kTcProdBase / 32 + kTrProdWarps;   // transform: issues the region loads
+constexpr int kTcThreads = kTcProdBase + kTrProdThreads + 32;
 constexpr int kTcStages = 4;                                     // mbarrier slots (stages <= 4)
 constexpr int kTcKBlock = 32;                                    // K elements per 128-byte swizzle row
 constexpr int kTcRows = 128;
 constexpr int kTcProdBar = 1;                                    // named barrier of all producers
+constexpr int kTrEpiBar = 2;                                     // transform: named barrier of the epilogue
 constexpr int kTcGroupBar = 2;                                   // + group: named barriers of the groups
 constexpr int kTcGroupThreads = kTcProdThreads / 2;              // contrib: two producer groups
 // contrib: 8 epilogue warps (two per TMEM lane quarter, alternate 16-column chunks), then the
@@ -61,7 +63,7 @@ constexpr int kConThreads = kConProdBase + kTcProdThreads;     // 544
 static_assert((kTrProdWarps == 8 || kTrProdWarps == 16) && (kTcEpiWarps + 1) % 4 == 1,
               "transform producers: (lane quarter, K slice) pairs");
 constexpr int kTcRegionBufs = 3;                                 // transform region buffers (at most)
-constexpr int kTcNumBars = 2 * kTcStages + 6 + kTcRegionBufs;
+constexpr int kTcNumBars = 2 * kTcStages + 6 + 2 * kTcRegionBufs;
 constexpr int kTcMaxRegion = 4096;                               // staged control points per brick
 constexpr size_t kTcSmemMax = 227 * 1024;
 
@@ -76,6 +78,9 @@ struct TcDev {
     int rps;                 // floats per staged plane (rxp ryp rzb)
     int rbuf;                // floats per region buffer (D planes, 128-byte aligned)
     int nrb;                 // region buffers (2 or 3: loads run that many tiles ahead, minus one)
+    int nus;                 // output staging buffers (0: the epilogue stores u directly)
+    int ustr;                // floats per staged output row (np + 4: rows 4 banks apart)
+    int ustage;              // floats per staging buffer (D brick rows, 128-byte aligned)
     int pairs_x;             // tap pairs per x row: ceil(nt0 / 2)
     int npairs;              // tap pairs (two x-neighbouring taps, the second virtual when nt0 is odd)
                              // with a nonzero table column
@@ -99,12 +104,13 @@ struct TcDev {
 // mbarriers of one CTA: full[s] producers -> MMA (kTcProdThreads arrivals), empty[s] MMA ->
 // producers (commit), acc_full[b] MMA -> epilogue (commit), acc_empty[b] epilogue -> MMA
 // (kTcEpiWarps * 32 arrivals), drain (final commit of the MMA thread), table and region[b]
-// (transaction counts of the bulk copies)
+// (transaction counts of the bulk copies), region_empty[b] producers -> region loads (one arrival)
 struct TcBars {
-    uint64_t *full, *empty, *acc_full, *acc_empty, *drain, *table, *region;
+    uint64_t *full, *empty, *acc_full, *acc_empty, *drain, *table, *region, *region_empty;
     __device__ explicit TcBars(uint64_t *b)
         : full(b), empty(b + kTcStages), acc_full(b + 2 * kTcStages), acc_empty(b + 2 * kTcStages + 2),
-          drain(b + 2 * kTcStages + 4), table(b + 2 * kTcStages + 5), region(b + 2 * kTcStages + 6)
+          drain(b + 2 * kTcStages + 4), table(b + 2 * kTcStages + 5), region(b + 2 * kTcStages + 6),
+          region_empty(b + 2 * kTcStages + 6 + kTcRegionBufs)
     {
     }
     __device__ void init(int full_count, int epi_threads = kTcEpiWarps * 32) const
@@ -119,7 +125,10 @@ struct TcBars {
         }
         tc::mbar_init(drain, 1);
         tc::mbar_init(table, 1);
-        for (int b = 0; b < kTcRegionBufs; ++b) tc::mbar_init(&region[b], 1);
+        for (int b = 0; b < kTcRegionBufs; ++b) {
+            tc::mbar_init(&region[b], 1);
+            tc::mbar_init(&region_empty[b], 1);
+        }
         tc::fence_mbarrier_init();
     }
 };
@@ -172,18 +181,28 @@ __device__ __forceinline__ void tc_teardown(const TcBars &B, uint32_t tmem, uint
 constexpr int kTcStageBytes = 2 * kTcRows * kTcKBlock * 4;
 
 // Transform: the table, then nrb region buffers, each one tiled load of the weighted control-point
-// planes (RegionPlanes) over a brick's region: [D][rzb][ryp][rxp] floats.
+// planes (RegionPlanes) over a brick's region: [D][rzb][ryp][rxp] floats; then nus output staging
+// buffers, each the tile's u as [D][bz][by][bx][ustr] floats for one tiled store.
 struct TcTransformLayout {
-    int b, reg, pairoff, bars, total_bytes;
+    int b, reg, pairoff, ust, bars, total_bytes;
     __host__ __device__ explicit TcTransformLayout(const TcDev &C)
     {
         b = 0;                                         // the table (A stages live in TMEM)
         reg = (b + C.kp * 2 * C.np * 4 + 127) / 128 * 128;   // [nrb][rbuf] floats, 128-byte aligned
         pairoff = reg + C.nrb * 4 * C.rbuf;            // [kp / 4] int2: region offsets of a unit's pairs
-        bars = (pairoff + 8 * (C.kp / 4) + 15) / 16 * 16;
+        ust = (pairoff + 8 * (C.kp / 4) + 127) / 128 * 128;  // [nus][ustage] floats
+        bars = (ust + C.nus * 4 * C.ustage + 15) / 16 * 16;
         total_bytes = bars + 8 * kTcNumBars + 8 + 1024;   // + alignment slack of the base
     }
 };
+
+// tiled store of a 5-D box from shared memory (bulk group of the issuing thread; no multicast)
+__device__ __forceinline__ void tma_store_5d(const CUtensorMap *map, const void *src, int c0, int c1, int c2, int c3,
+                                             int c4)
+{
+    asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5, %6}], [%1];"
+                 :: "l"(map), "r"(tc::smem_addr(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4) : "memory");
+}
 
 __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int x, int y, int z, int w,
                                             uint64_t *bar)
@@ -219,7 +238,8 @@ __device__ __forceinline__ unsigned char *tc_aligned_smem(float4 *dyn)
 // straight into TMEM stages (tcgen05.st) and the MMAs read it there, so shared memory carries only
 // the region reads and the table reads of the tensor cores.
 __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalParams P, TableDev T, TcDev C,
-                                                                           const __grid_constant__ CUtensorMap rmap)
+                                                                           const __grid_constant__ CUtensorMap rmap,
+                                                                           const __grid_constant__ CUtensorMap umap)
 {
     extern __shared__ float4 tc_smem4[];
     unsigned char *sm = tc_aligned_smem(tc_smem4);
@@ -238,10 +258,30 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
     const int nchunk = Kp / kTcKBlock;
     const int brick = C.bx * C.by * C.bz;
     const uint32_t table_bytes = (uint32_t)(Kp * N2 * 4);
+    const int NB = C.nrb;
+    const uint32_t region_bytes = (uint32_t)(D * C.rps * 4);
+    const int mine = (int)blockIdx.x < ntiles ? (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+    // the tiled load of the region of the CTA's k-th tile into buffer k % NB (one thread); x
+    // rounds down to a multiple of 4 (the load's alignment rule), the producers index from the
+    // remainder
+    auto issue_region = [&](int k) {
+        const int tile = blockIdx.x + k * gridDim.x;
+        const int t0 = tile % C.tiles[0], t12 = tile / C.tiles[0];
+        const int jx = T.qmin[0] + t0 * C.bx + T.tlo[0];
+        const int jy = T.qmin[1] + (t12 % C.tiles[1]) * C.by + T.tlo[1];
+        const int jz = T.qmin[2] + (t12 / C.tiles[1]) * C.bz + T.tlo[2];
+        tc::mbar_expect_tx(&B.region[k % NB], region_bytes);
+        tma_load_4d(Rg + (k % NB) * C.rbuf, &rmap, jx & ~3, jy, jz, 0, &B.region[k % NB]);
+    };
 
-    if (tid == 0) {
+    // the load-issuing thread sets up the barriers and starts the table and the first regions at
+    // once, while the others allocate TMEM and stage the pair offsets
+    if (warp == kTrTmaWarp && lane == 0) {
         B.init(kTrProdThreads);
         *abort = 0;
+        tc::mbar_expect_tx(B.table, table_bytes);            // the table: one bulk copy
+        tc::bulk_g2s(Bs, C.btr, table_bytes, B.table);
+        for (int k = 0; k < NB && k < mine; ++k) issue_region(k);
     }
     if (warp == kTcMmaWarp) tc::tmem_alloc(tmem_holder, (uint32_t)C.tr_cols);
     // unit u of the K axis = tap pairs 2u and 2u + 1 (pairs: x-neighbouring taps of one x row)
@@ -250,12 +290,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tmem_holder;
-    if (tid == 0) {                                          // the table: one bulk copy
-        tc::mbar_expect_tx(B.table, table_bytes);
-        tc::bulk_g2s(Bs, C.btr, table_bytes, B.table);
-    }
 
-    if (warp >= kTcEpiWarps + 1) {
+    if (warp == kTrTmaWarp) {
+        // ---------------- region loads (one thread), NB tiles ahead ----------------
+        if (lane == 0) {
+            int k = NB;
+            for (; k < mine; ++k) {
+                // buffer k % NB is free once every producer has left tile k - NB
+                if (!tc::mbar_wait(&B.region_empty[k % NB], (k / NB - 1) & 1, abort)) {
+                    tc_fail(abort, C.err);
+                    break;
+                }
+                issue_region(k);
+            }
+            // the last load into each buffer lands before the CTA leaves (bounded): a failed
+            // CTA may leave loads nobody waits for
+            const int issued = k < mine ? k : mine;
+            for (int j = issued > NB ? issued - NB : 0; j < issued; ++j) tc::mbar_wait(&B.region[j % NB], (j / NB) & 1);
+        }
+        __syncwarp();
+    } else if (warp >= kTcEpiWarps + 1) {
         // ---------------- producers: region -> split im2col hi/lo stages in TMEM ----------------
         // A warp writes the TMEM lanes of its quarter (warp % 4): thread = row r, and slice h of
         // each 32-column K block (kTrCols / 4 units of 4 columns), hi and lo.
@@ -268,8 +322,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
         // rows without a cell read real region data; the epilogue never stores them
         const int rowbase = row_exists ? cx + C.rxp * (cy + C.ryp * cz) : 0;
         const int cbase = row_exists ? comp * C.rps : 0;
-        const int NB = C.nrb;
-        const uint32_t region_bytes = (uint32_t)(D * C.rps * 4);
         const uint32_t lane_addr = (uint32_t)(32 * q) << 16;
         // control-point index of a tile's region origin
         auto region_origin = [&](int tile, int *j0) {
@@ -278,18 +330,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
             j0[1] = T.qmin[1] + (t12 % C.tiles[1]) * C.by + T.tlo[1];
             j0[2] = T.qmin[2] + (t12 / C.tiles[1]) * C.bz + T.tlo[2];
         };
-        // one thread: the tiled load of the region of the CTA's k-th tile into buffer k % NB; x
-        // rounds down to a multiple of 4 (the load's alignment rule), the rows index from the
-        // remainder
-        auto issue_region = [&](int k) {
-            int j0[3];
-            region_origin(blockIdx.x + k * gridDim.x, j0);
-            tc::mbar_expect_tx(&B.region[k % NB], region_bytes);
-            tma_load_4d(Rg + (k % NB) * C.rbuf, &rmap, j0[0] & ~3, j0[1], j0[2], 0, &B.region[k % NB]);
-        };
-        int issued = 0, landed = 0;                          // region loads (thread pt == 0)
-        for (; pt == 0 && issued < NB - 1 && (int)blockIdx.x + issued * (int)gridDim.x < ntiles; ++issued)
-            issue_region(issued);
         int s = 0;
         uint32_t phase = 0;                                  // parity of stage s's current use
         unsigned g = 0;
@@ -297,11 +337,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
         for (int it = 0;; ++it) {
             const int tile = blockIdx.x + it * gridDim.x;
             if (tile >= ntiles) break;
-            // tile it + NB - 1 goes to the buffer of tile it - 1, which every producer has left
-            if (pt == 0 && (int)blockIdx.x + issued * (int)gridDim.x < ntiles) issue_region(issued++);
             {
                 const bool ok = tc::mbar_wait(&B.region[it % NB], (it / NB) & 1, abort);
-                if (ok) landed = it + 1;
                 if (__any_sync(0xffffffffu, !ok)) {
                     if (lane == 0) tc_fail(abort, C.err);
                     failed = true;
@@ -351,9 +388,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
             }
             // every producer has finished the tile (and read its region buffer for the last time)
             if (tc::bar_or(kTcProdBar, kTrProdThreads, failed)) break;
+            if (pt == 0) tc::mbar_arrive(&B.region_empty[it % NB]);
         }
-        // after a failure: region loads still in flight land before the CTA leaves (bounded)
-        for (int k = landed; pt == 0 && k < issued; ++k) tc::mbar_wait(&B.region[k % NB], (k / NB) & 1);
     } else if (warp == kTcMmaWarp) {
         // ---------------- MMA issue (one thread) ----------------
         if (lane == 0) {
@@ -403,26 +439,62 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
         __syncwarp();
     } else {
         // ---------------- epilogue: TMEM -> u (lane quarter = warp) ----------------
+        // Staged (nus > 0): the rows go to a shared-memory tile that one tiled store writes to u
+        // (cells past the grid's end fall outside the tensor and are not written), so that the
+        // output leaves as whole lines instead of one 16-byte piece per row and instruction.
         const long long plane = T.ncell * T.nph;
         const int r = warp * 32 + lane;
         const int comp = r / C.ct, c = r - comp * C.ct;
         const int cx = c % C.bx, cy = (c / C.bx) % C.by, cz = c / (C.bx * C.by);
         const bool row_ok = comp < D && c < brick;
+        float *ust = reinterpret_cast<float *>(sm + L.ust);
+        const int NU = C.nus;
         for (int it = 0;; ++it) {
             const int tile = blockIdx.x + it * gridDim.x;
             if (tile >= ntiles) break;
             const int b = it & 1;
-            // warp-uniform decision: tcgen05.ld below is a warp-wide instruction
-            if (!__all_sync(0xffffffffu, tc::mbar_wait(&B.acc_full[b], (it >> 1) & 1, abort))) {
-                if (lane == 0) tc_fail(abort, C.err);
+            const int sb = NU > 0 ? it % NU : 0;
+            // the staging buffer's previous store (NU tiles ago) has read it
+            if (NU > 0 && tid == 0) {
+                if (NU > 1) tc::bulk_wait_read<1>();
+                else tc::bulk_wait_read<0>();
+            }
+            // warp-uniform decision (tcgen05.ld below is a warp-wide instruction), made uniform
+            // across the epilogue warps when they share barriers
+            const bool ok = __all_sync(0xffffffffu, tc::mbar_wait(&B.acc_full[b], (it >> 1) & 1, abort));
+            if (NU > 0 ? tc::bar_or(kTrEpiBar, kTcEpiWarps * 32, !ok) : !ok) {
+                if (lane == 0 && !ok) tc_fail(abort, C.err);
                 break;
             }
             tc::fence_after_sync();
-            const int qx = (tile % C.tiles[0]) * C.bx + cx, qy = ((tile / C.tiles[0]) % C.tiles[1]) * C.by + cy,
-                      qz = (tile / (C.tiles[0] * C.tiles[1])) * C.bz + cz;
+            const int t0 = tile % C.tiles[0], t1 = (tile / C.tiles[0]) % C.tiles[1], t2 = tile / (C.tiles[0] * C.tiles[1]);
+            const uint32_t tb = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * C.tr_stride);
+            if (NU > 0) {
+                float *dst = ust + sb * C.ustage + (comp * brick + c) * C.ustr;
+                for (int j = 0; j < (Np >> 4); ++j) {
+                    float vh[16], vl[16];
+                    tc::tmem_ld16(tb + (uint32_t)(16 * j), vh);
+                    tc::tmem_ld16(tb + (uint32_t)(Np + 16 * j), vl);
+                    if (row_ok)
+#pragma unroll
+                        for (int v = 0; v < 4; ++v)
+                            reinterpret_cast<float4 *>(dst + 16 * j)[v] =
+                                make_float4(vh[4 * v] + vl[4 * v], vh[4 * v + 1] + vl[4 * v + 1],
+                                            vh[4 * v + 2] + vl[4 * v + 2], vh[4 * v + 3] + vl[4 * v + 3]);
+                }
+                tc::fence_before_sync();
+                tc::mbar_arrive(&B.acc_empty[b]);            // the accumulator is free again
+                tc::fence_proxy_async_smem();
+                tc::bar_sync(kTrEpiBar, kTcEpiWarps * 32);
+                if (tid == 0) {
+                    tma_store_5d(&umap, ust + sb * C.ustage, 0, t0 * C.bx, t1 * C.by, t2 * C.bz, 0);
+                    tc::bulk_commit();
+                }
+                continue;
+            }
+            const int qx = t0 * C.bx + cx, qy = t1 * C.by + cy, qz = t2 * C.bz + cz;
             const bool valid = row_ok && qx < T.nq[0] && qy < T.nq[1] && qz < T.nq[2];
             const long long cell = (long long)qx + (long long)T.nq[0] * (qy + (long long)T.nq[1] * qz);
-            const uint32_t tb = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * C.tr_stride);
             for (int j = 0; j < (Np >> 4); ++j) {
                 float vh[16], vl[16];
                 tc::tmem_ld16(tb + (uint32_t)(16 * j), vh);
@@ -444,6 +516,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
             tc::fence_before_sync();
             tc::mbar_arrive(&B.acc_empty[b]);
         }
+        if (NU > 0 && tid == 0) tc::bulk_wait_all();          // the stores complete before the CTA leaves
     }
     // the table copy has completed before the teardown frees nothing in shared memory it writes:
     // the MMA thread waited for it, or (no tile) wait here (bounded)
@@ -685,6 +758,7 @@ struct TcPlan {
     TcDev dev{};
     RegionPlanes rp{};               // weighted control-point planes (written by the packing kernels)
     CUtensorMap rmap{};              // tiled loads of a brick's region from rp
+    CUtensorMap umap{};              // tiled stores of a tile's u (when dev.nus > 0)
     float *d_btr = nullptr, *d_bcon = nullptr;
     int2 *d_pairoff = nullptr;
     int *d_ctap = nullptr;           // contrib tap k -> box tap
@@ -821,6 +895,13 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
                     }
                 }
         if (best < 0.0) return 0;
+        // output staging: two buffers, else one, else none (direct stores); then a third region
+        // buffer when it fits too.  The tiled store needs u's rows (nph floats) 16-byte aligned.
+        C.nrb = 2;
+        C.ustr = C.np + 4;
+        C.ustage = (T.D * C.bx * C.by * C.bz * C.ustr + 31) / 32 * 32;
+        C.nus = (T.nph % 4 == 0 && C.ustr <= 256) ? 2 : 0;
+        while (C.nus > 0 && (size_t)TcTransformLayout(C).total_bytes > kTcSmemMax) --C.nus;
         C.nrb = kTcRegionBufs;
         if ((size_t)TcTransformLayout(C).total_bytes > kTcSmemMax) C.nrb = 2;
     }
@@ -929,6 +1010,22 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return 0;
+        // u as [D][nq2][nq1][nq0][nph]; the box's rows are ustr >= nph floats long, the columns
+        // past nph (and cells past the grid) lie outside the tensor and are not stored
+        if (C.nus > 0) {
+            const cuuint64_t ud[5] = {(cuuint64_t)T.nph, (cuuint64_t)T.nq[0], (cuuint64_t)T.nq[1], (cuuint64_t)T.nq[2],
+                                      (cuuint64_t)T.D};
+            const cuuint64_t us[4] = {(cuuint64_t)T.nph * 4, (cuuint64_t)T.nph * T.nq[0] * 4,
+                                      (cuuint64_t)T.nph * T.nq[0] * T.nq[1] * 4, (cuuint64_t)T.ncell * T.nph * 4};
+            const cuuint32_t ub[5] = {(cuuint32_t)C.ustr, (cuuint32_t)C.bx, (cuuint32_t)C.by, (cuuint32_t)C.bz,
+                                      (cuuint32_t)T.D};
+            const cuuint32_t ue[5] = {1, 1, 1, 1, 1};
+            if (reinterpret_cast<PfnTensorMapEncodeTiled>(fn)(
+                    &tc.umap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, T.ucp, ud, us, ub, ue, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                C.nus = 0;                                   // direct stores
+        }
     }
 
     int dev = 0, sms = 0;
@@ -955,7 +1052,8 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
 
 inline int table_transform_tc(const TcPlan &tc, const TablePlan &pl, const EvalParams &P, cudaStream_t s)
 {
-    table_transform_tc_kernel<<<tc.transform_blocks, kTcThreads, tc.transform_smem, s>>>(P, pl.dev, tc.dev, tc.rmap);
+    table_transform_tc_kernel<<<tc.transform_blocks, kTcThreads, tc.transform_smem, s>>>(P, pl.dev, tc.dev, tc.rmap,
+                                                                                         tc.umap);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 

@@ -234,6 +234,19 @@ __device__ __forceinline__ void bar_sync(int id, int count)
     asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(count) : "memory");
 }
 
+// ---- bulk tensor stores (shared -> global, bulk groups of the issuing thread) ------------------
+// Generic-proxy writes to shared memory become visible to the bulk copies after this fence (each
+// writing thread, before the barrier that precedes the issue).
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// at most N of the thread's bulk groups still read their shared-memory source
+template <int N>
+__device__ __forceinline__ void bulk_wait_read()
+{
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // ---- TMEM -> registers ----------------------------------------------------------------------
 // 32 lanes x 32 bits, 16 consecutive columns: thread t of the warp gets row (lane base + t).
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
