@@ -875,9 +875,9 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
     {
         const int rxp0 = (C.rx + 3 + 3) / 4 * 4;
         double best = -1.0;
-        for (int rxp = rxp0; rxp <= rxp0 + 8; rxp += 4)
-            for (int ryp = C.ry; ryp <= C.ry + 4; ++ryp)
-                for (int rzb = C.rz; rzb <= C.rz + (T.D == 3 ? 2 : 0); ++rzb) {
+        for (int rxp = rxp0; rxp <= rxp0 + 4; rxp += 4)
+            for (int ryp = C.ry; ryp <= C.ry + 2; ++ryp)
+                for (int rzb = C.rz; rzb <= C.rz + (T.D == 3 ? 1 : 0); ++rzb) {
                     if (rxp > 256 || ryp > 256 || rzb > 256) continue;
                     TcDev probe = C;
                     probe.rps = rxp * ryp * rzb;
