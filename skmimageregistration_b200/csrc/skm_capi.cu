@@ -642,9 +642,13 @@ struct RegWeights {
 // ev (optional, 6 events), for per-phase timing: after the transform (table path; the whole value
 // pass on the generic path), after the warp + statistics kernel, after the statistics kernel, after
 // the contrib GEMM (table path), after the derivative gather and after the result kernel.
+// step (optional): the optimizer step, fused into the table gather when that kernel runs (*fused
+// then says so; otherwise the caller applies the step itself)
 static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const RegWeights &w, const double *params,
-                          cudaEvent_t *ev = nullptr, double *deriv_out = nullptr, double *res_out = nullptr)
+                          cudaEvent_t *ev = nullptr, double *deriv_out = nullptr, double *res_out = nullptr,
+                          const OptStep *step = nullptr, bool *fused = nullptr)
 {
+    if (fused) *fused = false;
     double *d_deriv = deriv_out ? deriv_out : e->d_deriv, *d_res = res_out ? res_out : e->d_out;
     int rc = SKM_OK;
     const int D = e->D, kind = e->P.K.kind;
@@ -697,6 +701,11 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     const bool split = derivative && !tab && metric != SKM_LCC && e->deriv_blocks < kSplitBelowBlocks;
     if (derivative) {
         if (tab) {
+            if (step) {
+                Q.step = *step;
+                Q.step.on = 1;
+                if (fused) *fused = true;
+            }
             if (table_derivative(e->table, tc_of(e), e->P, Q, D, e->gather_blocks, e->stream, ev ? ev[3] : nullptr))
                 return fail(SKM_ERR_CUDA, "table derivative: %s", cudaGetErrorString(cudaGetLastError()));
         } else {

@@ -46,6 +46,57 @@ struct EvalParams {
     KernelParams K;
 };
 
+// Device-resident optimizer scalars: adaptive time, best value, learning rate, <g, g_prev>,
+// value, iteration, pixel count, and T_PENDING: the last step was taken from an improving
+// evaluation, so its position (the current one) is the best one -- copied to `best` before the
+// next step overwrites it, or when the best parameters are read.
+enum { T_TIME = 0, T_BEST, T_LR, T_SP, T_VALUE, T_ITER, T_COUNT, T_PENDING, NT };
+
+// The adaptive-step update of the optimizer (see skm_optimizer.cuh), when a derivative kernel
+// applies it to the parameters it owns (on != 0).
+struct OptStep {
+    double *tmp, *base, *pos, *best, *scal;
+    double *sp_part;                    // per-block <g, g_prev> partials
+    int on, orthant;
+    double a, A, alpha, f_max, f_min, omega;
+};
+
+// gamma(t) = a / (A + t + 1)^alpha  (itkAdaptiveStepsizeRegularStepGradientDescent...hxx:86-97)
+__device__ __forceinline__ double opt_learning_rate(const OptStep &S, double t) { return S.a / pow(S.A + t + 1.0, S.alpha); }
+
+// x = x_prev + gamma g with the orthant projection; the previous step's position becomes the best
+// one first when that step came from an improving evaluation (pending).  gprev, b, x: tmp[j],
+// base[j], pos[j] as loaded before the step.
+__device__ __forceinline__ double opt_update(const OptStep &S, long long j, double g, double lr, bool pending,
+                                            double gprev, double b, double x)
+{
+    const double sp = g * gprev;
+    S.tmp[j] = g;
+    if (pending) S.best[j] = x;
+    double nx = b + g * lr;
+    if (S.orthant && nx * b < 0.0) nx = 0.0;
+    S.pos[j] = nx;
+    S.base[j] = nx;
+    return sp;
+}
+
+// the scalars after a step (one thread): t = max(0, t + f(-<g, g_prev>)), best value, counters
+__device__ __forceinline__ void opt_finish(const OptStep &S, double sp, double lr, const double *out)
+{
+    double *scal = S.scal;
+    const double t = scal[T_TIME];
+    const double f = S.f_min + (S.f_max - S.f_min) / (1.0 - (S.f_max / S.f_min) * exp(sp / S.omega));
+    scal[T_TIME] = fmax(0.0, t + f);
+    const bool improving = out[O_VALUE] < scal[T_BEST];
+    if (improving) scal[T_BEST] = out[O_VALUE];
+    scal[T_PENDING] = improving ? 1.0 : 0.0;
+    scal[T_LR] = lr;
+    scal[T_SP] = sp;
+    scal[T_VALUE] = out[O_VALUE];
+    scal[T_ITER] += 1.0;
+    scal[T_COUNT] = out[O_COUNT];
+}
+
 struct DerivParams {
     int metric;                 // 0 MSE, 1 NCC, 2 LCC
     int with_metric;            // 1: metric-level call (host regularizers + sign)
@@ -64,6 +115,7 @@ struct DerivParams {
     double *__restrict__ out;            // result vector (fused finalization)
     unsigned *counter;                   // ticket counter of the fused finalization
     int values_only;                     // table gather: regularizer values only (getValue)
+    OptStep step;                        // table gather: the optimizer step fused (step.on)
 };
 
 // ---- sample positions ------------------------------------------------------------------------

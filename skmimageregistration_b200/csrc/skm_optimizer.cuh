@@ -17,8 +17,6 @@
 
 namespace {
 
-enum { T_TIME = 0, T_BEST, T_LR, T_SP, T_VALUE, T_ITER, T_COUNT, NT };
-
 __global__ void shifts_dev_kernel(const unsigned long long *__restrict__ state, RngJump J, long long Ns, int D,
                                   int sub, uint32_t *__restrict__ shifts)
 {
@@ -41,7 +39,9 @@ __global__ void rng_advance_kernel(unsigned long long *state, RngJump J, unsigne
 }
 
 // One optimizer step over all parameters; the last block (fixed-order sum of the per-block
-// <g, g_prev> partials) then updates the adaptive time, the best value and the counters.
+// <g, g_prev> partials) then updates the adaptive time, the best value and the counters.  Used
+// where the derivative kernel does not apply the step itself (the table gather does, see
+// OptStep): a pending best position left by such a fused step is taken over first.
 __global__ void __launch_bounds__(256) opt_step_kernel(const double *__restrict__ g, double *__restrict__ tmp,
                                                        double *__restrict__ base, double *__restrict__ pos,
                                                        double *__restrict__ best, double *__restrict__ scal,
@@ -53,11 +53,13 @@ __global__ void __launch_bounds__(256) opt_step_kernel(const double *__restrict_
     const double t = scal[T_TIME];
     const double lr = a / pow(A + t + 1.0, alpha);
     const bool improving = out[O_VALUE] < scal[T_BEST];
+    const bool pending = scal[T_PENDING] != 0.0;
     double sp = 0.0;
     for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < P; j += (long long)gridDim.x * blockDim.x) {
         const double gj = g[j];
         sp += gj * tmp[j];
         tmp[j] = gj;
+        if (pending) best[j] = pos[j];
         const double b = base[j];
         double nx = b + gj * lr;
         if (orthant && nx * b < 0.0) nx = 0.0;
@@ -81,8 +83,18 @@ __global__ void __launch_bounds__(256) opt_step_kernel(const double *__restrict_
             scal[T_VALUE] = out[O_VALUE];
             scal[T_ITER] += 1.0;
             scal[T_COUNT] = out[O_COUNT];
+            scal[T_PENDING] = 0.0;
         }
     }
+}
+
+// The best parameters after a fused step from an improving evaluation: the current position.
+__global__ void opt_best_pending_kernel(const double *__restrict__ scal, const double *__restrict__ pos,
+                                        double *__restrict__ best, long long P)
+{
+    if (scal[T_PENDING] == 0.0) return;
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < P; j += (long long)gridDim.x * blockDim.x)
+        best[j] = pos[j];
 }
 
 }  // namespace
@@ -141,13 +153,30 @@ static int optimizer_iteration(skm_optimizer *o, cudaEvent_t *ev = nullptr)
     w.with_metric = 1;
     w.negate = o->md.use_negative_gradient;
     if (ev) SKM_CUDA(cudaEventRecord(ev[2], e->stream));
-    int rc = run_evaluation(e, o->md.metric, true, w, o->d_pos, ev ? ev + 3 : nullptr);
+    OptStep st{};
+    st.tmp = o->d_tmp;
+    st.base = o->d_base;
+    st.pos = o->d_pos;
+    st.best = o->d_best;
+    st.scal = o->d_scal;
+    st.sp_part = o->d_sp;
+    st.orthant = o->od.orthant_projection;
+    st.a = o->od.a;
+    st.A = o->od.A;
+    st.alpha = o->od.alpha;
+    st.f_max = o->od.f_max;
+    st.f_min = o->od.f_min;
+    st.omega = o->od.omega;
+    bool fused = false;
+    int rc = run_evaluation(e, o->md.metric, true, w, o->d_pos, ev ? ev + 3 : nullptr, nullptr, nullptr, &st, &fused);
     if (rc) return rc;
-    opt_step_kernel<<<o->step_blocks, 256, 0, e->stream>>>(e->d_deriv, o->d_tmp, o->d_base, o->d_pos, o->d_best,
-                                                          o->d_scal, e->d_out, o->P, o->od.orthant_projection, o->od.a,
-                                                          o->od.A, o->od.alpha, o->od.f_max, o->od.f_min, o->od.omega,
-                                                          o->d_sp, e->d_counters + 2);
-    SKM_CHECK_LAUNCH();
+    if (!fused) {
+        opt_step_kernel<<<o->step_blocks, 256, 0, e->stream>>>(e->d_deriv, o->d_tmp, o->d_base, o->d_pos, o->d_best,
+                                                              o->d_scal, e->d_out, o->P, o->od.orthant_projection,
+                                                              o->od.a, o->od.A, o->od.alpha, o->od.f_max, o->od.f_min,
+                                                              o->od.omega, o->d_sp, e->d_counters + 2);
+        SKM_CHECK_LAUNCH();
+    }
     if (ev) SKM_CUDA(cudaEventRecord(ev[9], e->stream));
     return SKM_OK;
 }
@@ -175,7 +204,8 @@ extern "C" int skm_optimizer_create(skm_evaluator *e, const skm_optimizer_desc *
     rc = [&]() -> int {
         const long long P = o->P;
         if (dalloc(&o->d_pos, P) || dalloc(&o->d_base, P) || dalloc(&o->d_tmp, P) || dalloc(&o->d_best, P) ||
-            dalloc(&o->d_cpw, e->C) || dalloc(&o->d_scal, NT) || dalloc(&o->d_sp, o->step_blocks) ||
+            dalloc(&o->d_cpw, e->C) || dalloc(&o->d_scal, NT) ||
+            dalloc(&o->d_sp, std::max<long long>(o->step_blocks, e->gather_blocks)) ||
             dalloc(&o->d_rng, 1))
             return SKM_ERR_CUDA;
         SKM_CUDA(cudaMemcpyAsync(o->d_pos, initial, sizeof(double) * P, cudaMemcpyHostToDevice, e->stream));
@@ -183,7 +213,7 @@ extern "C" int skm_optimizer_create(skm_evaluator *e, const skm_optimizer_desc *
         SKM_CUDA(cudaMemsetAsync(o->d_base, 0, sizeof(double) * P, e->stream));
         SKM_CUDA(cudaMemsetAsync(o->d_tmp, 0, sizeof(double) * P, e->stream));
         SKM_CUDA(cudaMemcpyAsync(o->d_cpw, cpw, sizeof(double) * e->C, cudaMemcpyHostToDevice, e->stream));
-        double scal[NT] = {0.0, 1.7976931348623157e308, 0.0, 0.0, 0.0, 0.0, 0.0};
+        double scal[NT] = {0.0, 1.7976931348623157e308, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         SKM_CUDA(cudaMemcpyAsync(o->d_scal, scal, sizeof scal, cudaMemcpyHostToDevice, e->stream));
         SKM_CUDA(cudaMemcpyAsync(o->d_rng, &e->rng_state, sizeof(unsigned long long), cudaMemcpyHostToDevice,
                                  e->stream));
@@ -249,6 +279,10 @@ extern "C" int skm_optimizer_get_parameters(skm_optimizer *o, int32_t best, doub
     if (!params) return fail(SKM_ERR_INVALID, "params is NULL");
     skm_evaluator *e = o->e;
     SKM_CUDA(cudaSetDevice(e->device));
+    if (best) {
+        opt_best_pending_kernel<<<o->step_blocks, 256, 0, e->stream>>>(o->d_scal, o->d_pos, o->d_best, o->P);
+        SKM_CHECK_LAUNCH();
+    }
     SKM_CUDA(cudaMemcpyAsync(params, best ? o->d_best : o->d_pos, sizeof(double) * o->P, cudaMemcpyDeviceToHost,
                              e->stream));
     SKM_CUDA(cudaStreamSynchronize(e->stream));

@@ -378,6 +378,18 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
     int j[3] = {0, 0, 0};
     if (active) cell_of<D>(P.cp.n, j_lin, j);
     const float4 cj = active ? P.cpd[j_lin] : make_float4(0.f, 0.f, 0.f, 0.f);
+    // the fused optimizer step: warp 1 + d applies it to component d; its operands are loaded now
+    // so that their latency overlaps the sums
+    const int sd = grp - 1;
+    const bool stepper = Q.step.on && active && sd >= 0 && sd < D;
+    double st_g = 0.0, st_b = 0.0, st_x = 0.0, st_t = 0.0, st_p = 0.0;
+    if (stepper) {
+        st_g = Q.step.tmp[j_lin + sd * P.C];
+        st_b = Q.step.base[j_lin + sd * P.C];
+        st_x = Q.step.pos[j_lin + sd * P.C];
+        st_t = Q.step.scal[T_TIME];
+        st_p = Q.step.scal[T_PENDING];
+    }
     float acc[3] = {0.f, 0.f, 0.f};
     if (active && !Q.values_only) {
         // groups of kU taps: all loads first (independent, predicated), then the sums in tap order
@@ -484,6 +496,7 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
     double val[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) val[k] = 0.0;
+    __shared__ double sgrad[3][32], ssp[3];
     if (grp == 0 && active) {
         float a[3] = {0.f, 0.f, 0.f}, rk[3] = {0.f, 0.f, 0.f}, rdd[3] = {0.f, 0.f, 0.f}, rp[3] = {0.f, 0.f, 0.f};
         for (int g = 0; g < kGatherGroups; ++g) {           // fixed combination order
@@ -538,6 +551,7 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
                 if (Q.negate) g = -g;
             }
             Q.deriv[j_lin + d * P.C] = g;
+            if (Q.step.on) sgrad[d][lane] = g;
         }
         if (Q.with_metric) {
             double l1 = 0.0;
@@ -555,13 +569,33 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
             if (lane == 0) Q.rpart[(long long)k * gridDim.x + blockIdx.x] = sum;
         }
     }
-    if (last_block_arrived(Q.counter)) {                   // fused result, fixed order
+    if (Q.step.on) {                                       // uniform over the grid
+        __syncthreads();
+        double sp = 0.0;
+        if (stepper)
+            sp = opt_update(Q.step, j_lin + sd * P.C, sgrad[sd][lane], opt_learning_rate(Q.step, st_t), st_p != 0.0,
+                            st_g, st_b, st_x);
+        if (sd >= 0 && sd < D) {
+            sp = warp_sum(sp);
+            if (lane == 0) ssp[sd] = sp;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = 0.0;
+            for (int d = 0; d < D; ++d) b += ssp[d];
+            Q.step.sp_part[blockIdx.x] = b;
+        }
+    }
+    if (last_block_arrived(Q.counter)) {                   // fused result (and step scalars), fixed order
         __shared__ double shr[NR * 32];
-        double w[NR];
+        double w[NR], wsp[1] = {0.0};
         sum_partials<NR>(Q.rpart, gridDim.x, w, shr);
-        if (threadIdx.x == 0)
+        if (Q.step.on) sum_partials<1>(Q.step.sp_part, gridDim.x, wsp, shr);
+        if (threadIdx.x == 0) {
             result_finalize(Q.stats, w, Q.reg_rkhs, Q.reg_rd, Q.reg_pg, Q.reg_l1, Q.reg_l21, Q.reg_l2, Q.out,
                             T.tc_err);
+            if (Q.step.on) opt_finish(Q.step, wsp[0], opt_learning_rate(Q.step, Q.step.scal[T_TIME]), Q.out);
+        }
     }
 }
 
