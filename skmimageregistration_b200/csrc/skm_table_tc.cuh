@@ -59,7 +59,8 @@ constexpr int kTcGroupThreads = kTcProdThreads / 2;              // contrib: two
 constexpr int kConEpiWarps = 8;
 constexpr int kConMmaWarp = kConEpiWarps;
 constexpr int kConProdBase = (kConEpiWarps + 1) * 32;
-constexpr int kConThreads = kConProdBase + kTcProdThreads;     // 544
+constexpr int kConLoadWarp = kConProdBase / 32 + kTcProdWarps;  // contrib: issues the record loads
+constexpr int kConThreads = kConProdBase + kTcProdThreads + 32;     // 576
 static_assert((kTrProdWarps == 8 || kTrProdWarps == 16) && (kTcEpiWarps + 1) % 4 == 1,
               "transform producers: (lane quarter, K slice) pairs");
 constexpr int kTcRegionBufs = 3;                                 // transform region buffers (at most)
@@ -96,6 +97,8 @@ struct TcDev {
     int nct;                 // contrib taps: the box taps with a nonzero table column
     int npc;                 // nct padded to 16 (N)
     int ns_con;              // shared-memory stages (one 32-phase K block each)
+    int nrr;                 // record ring slots (tiled loads of a chunk's records; 0: direct loads)
+    int rslot, rfix;         // bytes per ring slot, offset of the fixed-image values in a slot
     int con_stride, con_cols;
     const float *bcon;       // npc rows x kpc, K-major 128-byte swizzled: hi, then lo
     unsigned *err;           // sticky failure word of the bounded waits (read and reset by the host)
@@ -212,14 +215,18 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
         :: "r"(tc::smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(tc::smem_addr(bar)) : "memory");
 }
 
+// Contrib: A stages, the table (hi, lo), then nrr ring slots, each a chunk's records (cell c, phase
+// p of the chunk: 128-byte rows c * 4 + p / 8, their 16-byte pieces swizzled by the row index, as
+// the tiled load's 128-byte swizzle writes them) and fixed-image values ([cell][32] floats).
 struct TcContribLayout {
-    int a, bhi, blo, bars, total_bytes;
+    int a, bhi, blo, rr, bars, total_bytes;
     __host__ __device__ explicit TcContribLayout(const TcDev &C)
     {
         a = 0;
         bhi = a + C.ns_con * kTcStageBytes;
         blo = bhi + C.kpc * C.npc * 4;
-        bars = blo + C.kpc * C.npc * 4;
+        rr = (blo + C.kpc * C.npc * 4 + 1023) / 1024 * 1024;
+        bars = rr + C.nrr * C.rslot;
         total_bytes = bars + 8 * kTcNumBars + 8 + 1024;
     }
 };
@@ -526,8 +533,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) table_transform_tc_kernel(EvalP
 
 // ------------------------------------------------------------------------------------------------
 // Contrib[comp][t][cell] = sum_p T[p][t] g(cell, p) on the tensor cores
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        :: "r"(tc::smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(tc::smem_addr(bar)) : "memory");
+}
+
 __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableDev T, TcDev C,
-                                                                        const double *__restrict__ stats)
+                                                                        const double *__restrict__ stats,
+                                                                        const __grid_constant__ CUtensorMap recmap,
+                                                                        const __grid_constant__ CUtensorMap fixmap)
 {
     extern __shared__ float4 tc_smem4[];
     unsigned char *sm = tc_aligned_smem(tc_smem4);
@@ -563,8 +579,36 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tmem_holder;
+    unsigned char *Rr = sm + L.rr;
+    const int NR = C.nrr;
 
-    if (warp >= kConEpiWarps + 1) {
+    if (warp == kConLoadWarp) {
+        // ---------------- record loads (one thread), NR chunks ahead ----------------
+        if (lane == 0 && NR > 0) {
+            const long long mine = (long long)blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+            const long long nch = mine * nchunk;
+            const uint32_t bytes = (uint32_t)(ct * 32 * 20);
+            long long g = 0;
+            for (; g < nch; ++g) {
+                const int slot = (int)(g % NR);
+                // slot g % NR is free once its producer group has left chunk g - NR
+                if (g >= NR && !tc::mbar_wait(&B.region_empty[slot], (uint32_t)((g / NR - 1) & 1), abort)) {
+                    tc_fail(abort, C.err);
+                    break;
+                }
+                const long long tile = blockIdx.x + (g / nchunk) * gridDim.x;
+                const int kc = (int)(g % nchunk);
+                unsigned char *dst = Rr + slot * C.rslot;
+                tc::mbar_expect_tx(&B.region[slot], bytes);
+                tma_load_3d(reinterpret_cast<float *>(dst), &recmap, 0, kc * 4, (int)(tile * ct), &B.region[slot]);
+                tma_load_2d(dst + C.rfix, &fixmap, kc * kTcKBlock, (int)(tile * ct), &B.region[slot]);
+            }
+            // the last load into each slot lands before the CTA leaves (bounded)
+            for (long long j = g > NR ? g - NR : 0; j < g; ++j)
+                tc::mbar_wait(&B.region[j % NR], (uint32_t)((j / NR) & 1));
+        }
+        __syncwarp();
+    } else if (warp >= kConEpiWarps + 1) {
         // ---------------- producers: g = (a f + b m + c) grad M, hi/lo stages ----------------
         // Two groups of 4 warps take alternate K chunks, so that one group's global loads are in
         // flight while the other converts and stores.  Item = (cell c, 4 phases); 8 consecutive lanes
@@ -584,6 +628,7 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
             const int s = (int)(g % NS);
             bool ok = true;
             if (g >= (unsigned)NS) ok = tc::mbar_wait(&B.empty[s], ((g / NS) + 1) & 1, abort);
+            if (NR > 0 && ok) ok = tc::mbar_wait(&B.region[g % NR], (g / NR) & 1, abort);   // the records
             if (tc::bar_or(kTcGroupBar + grp, kTcGroupThreads, !ok)) {
                 if (gt == 0) tc_fail(abort, C.err);
                 failed = true;
@@ -591,6 +636,8 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
             }
             unsigned char *Ahi = As + s * kTcStageBytes, *Alo = Ahi + kTcStageBytes / 2;
             const int k0 = kc * kTcKBlock;
+            const unsigned char *slot = Rr + (NR > 0 ? (int)(g % NR) * C.rslot : 0);
+            const float *fsm = reinterpret_cast<const float *>(slot + C.rfix);
             for (int base = 0; base < nitems; base += kMaxItems * kTcGroupThreads) {
                 float4 rr[kMaxItems][4], ff[kMaxItems];
 #pragma unroll
@@ -599,6 +646,18 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
                     const int c = i >> 3, jg = i & 7;
                     const long long cell = cell0 + c;
                     const int p0 = k0 + 4 * jg;
+                    if (NR > 0) {                                // from the ring slot (zeros past the data)
+                        const bool in = i < nitems;
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const int row = 4 * c + ((4 * jg + e) >> 3), piece = ((4 * jg + e) & 7) ^ (row & 7);
+                            rr[u][e] = in ? *reinterpret_cast<const float4 *>(slot + row * 128 + piece * 16)
+                                          : make_float4(0.f, 0.f, 0.f, 0.f);
+                        }
+                        ff[u] = in ? *reinterpret_cast<const float4 *>(fsm + c * kTcKBlock + 4 * jg)
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+                        continue;
+                    }
                     const bool in = i < nitems && cell < T.ncell;
 #pragma unroll
                     for (int e = 0; e < 4; ++e)
@@ -637,6 +696,10 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
                         }
                     }
                 }
+            }
+            if (NR > 0) {                                        // the group has read the slot
+                tc::bar_sync(kTcGroupBar + grp, kTcGroupThreads);
+                if (gt == 0) tc::mbar_arrive(&B.region_empty[g % NR]);
             }
             tc::fence_proxy_async();
             tc::mbar_arrive(&B.full[s]);
@@ -759,6 +822,7 @@ struct TcPlan {
     RegionPlanes rp{};               // weighted control-point planes (written by the packing kernels)
     CUtensorMap rmap{};              // tiled loads of a brick's region from rp
     CUtensorMap umap{};              // tiled stores of a tile's u (when dev.nus > 0)
+    CUtensorMap recmap{}, fixmap{};  // contrib: tiled loads of a chunk's records and fixed values (dev.nrr > 0)
     float *d_btr = nullptr, *d_bcon = nullptr;
     int2 *d_pairoff = nullptr;
     int *d_ctap = nullptr;           // contrib tap k -> box tap
@@ -913,9 +977,21 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
     C.con_stride = (int)pow2_at_least(C.npc);
     C.con_cols = 2 * C.con_stride;
     if (C.tr_cols > 512 || C.con_cols > 512) return 0;
-    // as many stages (up to 3, at least 2) as the shared memory holds
-    for (C.ns_con = 3; C.ns_con > 2 && (size_t)TcContribLayout(C).total_bytes > kTcSmemMax; --C.ns_con) {
+    // contrib: two A stages and a ring of three (else two) record slots when they fit and the
+    // records allow tiled loads (a chunk's 32 phases as four 128-byte rows per cell); else as many
+    // stages (up to 3, at least 2) as the shared memory holds and direct record loads
+    C.nrr = 0;
+    C.rfix = (512 * C.ct + 127) / 128 * 128;
+    C.rslot = (C.rfix + 128 * C.ct + 1023) / 1024 * 1024;
+    if (T.nph % 8 == 0 && C.ct <= 256) {
+        C.ns_con = 2;
+        for (C.nrr = 3; C.nrr >= 2 && (size_t)TcContribLayout(C).total_bytes > kTcSmemMax; --C.nrr) {
+        }
+        if (C.nrr < 2) C.nrr = 0;
     }
+    if (C.nrr == 0)
+        for (C.ns_con = 3; C.ns_con > 2 && (size_t)TcContribLayout(C).total_bytes > kTcSmemMax; --C.ns_con) {
+        }
     tc.transform_smem = (size_t)TcTransformLayout(C).total_bytes;
     tc.contrib_smem = (size_t)TcContribLayout(C).total_bytes;
     // both kernels must hold one CTA per SM alone (their TMEM allocations assume it)
@@ -1026,6 +1102,28 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
                 C.nus = 0;                                   // direct stores
         }
+        // contrib's records as [cell][nph / 8][32 floats] (128-byte rows, swizzled in shared
+        // memory) and fixed values as [cell][nph]; a failed encoding keeps the direct loads
+        if (C.nrr > 0) {
+            const cuuint64_t rd[3] = {32, (cuuint64_t)(T.nph / 8), (cuuint64_t)T.ncell};
+            const cuuint64_t rs[2] = {128, (cuuint64_t)T.nph * 16};
+            const cuuint32_t rb[3] = {32, 4, (cuuint32_t)C.ct};
+            const cuuint64_t fd[2] = {(cuuint64_t)T.nph, (cuuint64_t)T.ncell};
+            const cuuint64_t fs[1] = {(cuuint64_t)T.nph * 4};
+            const cuuint32_t fb[2] = {(cuuint32_t)kTcKBlock, (cuuint32_t)C.ct};
+            const cuuint32_t e1[3] = {1, 1, 1};
+            auto enc = reinterpret_cast<PfnTensorMapEncodeTiled>(fn);
+            if (enc(&tc.recmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)T.rec, rd, rs, rb, e1,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
+                enc(&tc.fixmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)T.fixcp, fd, fs, fb, e1,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+                C.nrr = 0;
+                for (C.ns_con = 3; C.ns_con > 2 && (size_t)TcContribLayout(C).total_bytes > kTcSmemMax; --C.ns_con) {
+                }
+            }
+        }
     }
 
     int dev = 0, sms = 0;
@@ -1059,7 +1157,8 @@ inline int table_transform_tc(const TcPlan &tc, const TablePlan &pl, const EvalP
 
 inline int table_contrib_tc(const TcPlan &tc, const TablePlan &pl, const double *stats, cudaStream_t s)
 {
-    table_contrib_tc_kernel<<<tc.contrib_blocks, kConThreads, tc.contrib_smem, s>>>(pl.dev, tc.dev, stats);
+    table_contrib_tc_kernel<<<tc.contrib_blocks, kConThreads, tc.contrib_smem, s>>>(pl.dev, tc.dev, stats, tc.recmap,
+                                                                                     tc.fixmap);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
