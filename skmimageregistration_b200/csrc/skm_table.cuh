@@ -393,7 +393,8 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
     float acc[3] = {0.f, 0.f, 0.f};
     if (active && !Q.values_only) {
         // groups of kU taps: all loads first (independent, predicated), then the sums in tap order
-        constexpr int kU = 16;
+        // (20: one group covers the 160 taps of a 12-voxel support at 8 warps)
+        constexpr int kU = 20;
         const int ntap = T.ngtap, ncell = (int)T.ncell;
         const float *c0p = T.contrib, *c1p = T.contrib + ntap * ncell, *c2p = T.contrib + 2 * ntap * ncell;
         for (int base = grp; base < ntap; base += kGatherGroups * kU) {
