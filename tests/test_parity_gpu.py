@@ -228,3 +228,35 @@ def test_table_path_metric_level_and_optimizer(case):
     vals = oo.run(4)
     assert rel_err(opt.state()["value"], vals[-1]) <= 1e-4
     assert max_rel(opt.parameters(), oo.position) <= 1e-3
+
+
+@pytest.mark.parametrize("orthant", [False, True])
+@pytest.mark.parametrize("case", [TABLE_CASES[1], TABLE_CASES[2]])
+def test_table_path_fused_step_best_parameters(case, orthant):
+    """The optimizer step fused into the table gather, against the oracle optimizer and against the
+    separate step kernel of the generic path: positions, best parameters read between runs (the
+    pending best position of an improving step is taken over when read), best value, time."""
+    D, h, shape, s4, s0 = case
+    pb, cp, cpw = _table_problem(D, h, shape, s4, s0, seed=57, weights=False)
+    P = pb.num_parameters
+    m = MetricDesc.make("ncc", rd=1e-3, l1=1e-4 if orthant else 0.0)
+    o = OptimizerDesc.make(a=2.0, number_of_iterations=9, orthant_projection=orthant)
+    start = np.ascontiguousarray(cp.T.reshape(-1)) * 0.5
+    ev = GpuKernelEvaluator(pb)
+    assert ev.path() == GpuKernelEvaluator.TABLE_TC
+    opt = Optimizer(ev, o, m, start, cpw)
+    ev_generic = GpuKernelEvaluator(pb)
+    assert ev_generic.path(GpuKernelEvaluator.REQ_GENERIC) == GpuKernelEvaluator.GENERIC
+    opt_generic = Optimizer(ev_generic, o, m, start, cpw)
+    oo = O.OracleOptimizer(O.Oracle(pb), o, m, start, cpw)
+    for chunk in (1, 3, 2, 3):
+        opt.run(chunk)
+        opt_generic.run(chunk)
+        oo.run(chunk)
+        st, sg = opt.state(), opt_generic.state()
+        assert st["iteration"] == sg["iteration"] == oo.state.iteration
+        assert rel_err(st["best_value"], oo.state.best_value) <= 1e-4
+        assert rel_err(st["best_value"], sg["best_value"]) <= 1e-4
+        assert max_rel(opt.parameters(), oo.position) <= 1e-3
+        assert max_rel(opt.parameters(best=True), oo.best) <= 1e-3
+        assert max_rel(opt.parameters(best=True), opt_generic.parameters(best=True)) <= 1e-3
