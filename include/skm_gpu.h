@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define SKM_ABI_VERSION 3
+#define SKM_ABI_VERSION 4
 
 /* Status codes. */
 #define SKM_OK              0
@@ -164,6 +164,9 @@ typedef struct skm_evaluator_info {
     int32_t tc_contrib_k;             /* phases padded to 32 */
     int32_t tc_contrib_taps;          /* taps with a nonzero table column (the contributions per cell) */
     int32_t warp_staged;              /* 1: the warp kernel stages coefficient boxes by TMA */
+    int32_t tc_region_buffers;        /* transform: region buffers of the tiled-load ring */
+    int32_t tc_u_staging;             /* transform: output staging buffers (0: direct stores of u) */
+    int32_t tc_record_slots;          /* contrib: record ring slots (0: direct record loads) */
 } skm_evaluator_info;
 int skm_evaluator_describe(skm_evaluator *ev, skm_evaluator_info *out);
 

@@ -112,6 +112,9 @@ class EvaluatorInfo(C.Structure):
         ("tc_contrib_k", C.c_int32),
         ("tc_contrib_taps", C.c_int32),
         ("warp_staged", C.c_int32),
+        ("tc_region_buffers", C.c_int32),
+        ("tc_u_staging", C.c_int32),
+        ("tc_record_slots", C.c_int32),
     ]
 
     def as_dict(self):

@@ -528,6 +528,9 @@ extern "C" int skm_evaluator_describe(skm_evaluator *e, skm_evaluator_info *out)
         r.tc_contrib_k = C.kpc;
         r.tc_contrib_taps = C.nct;
         r.warp_staged = (e->D == 3 && e->tc.wt.enabled) ? 1 : 0;
+        r.tc_region_buffers = C.nrb;
+        r.tc_u_staging = C.nus;
+        r.tc_record_slots = C.nrr;
     }
     *out = r;
     return SKM_OK;

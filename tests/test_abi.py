@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol(lib):
 
 
 def test_abi_version(lib):
-    assert lib.skm_abi_version() == 3
+    assert lib.skm_abi_version() == 4
 
 
 def _create(pb):

@@ -59,3 +59,35 @@ def test_tensor_core_table_value_only_matches_derivative_call():
     assert r1["num_pixels_counted"] == r2["num_pixels_counted"]
     assert r1["measure"] == r2["measure"]
     assert r1["reg_value_rd"] == r2["reg_value_rd"]
+
+
+# the table path takes spacing ratios 1, 2, 4, 8 per axis, so phase counts below 8 occur for
+# h = 1 (one phase) and, in 2-D, h = 2 (four phases)
+@pytest.mark.parametrize("D,h,shape", [(2, 1, (30, 34)), (2, 2, (40, 46)), (3, 1, (12, 14, 16)), (3, 2, (18, 20, 22))])
+def test_tensor_core_variants_for_small_phase_counts(D, h, shape):
+    """Phase counts that are not multiples of 8 (or of 4) keep the direct record loads (and the
+    direct stores of u) of the tensor-core kernels; the others use the record ring and the staged
+    stores.  Either way the results match the CUDA-core table path and the generic kernels."""
+    from helpers import make_problem
+    pb, cp, cpw = make_problem(D, "stationary", shape=shape, seed=11 + h, sigma_c4=3.0 * h, sigma_c0=6.0 * h,
+                               cp_spacing=float(h), spacing=(1.0,) * D, origin=tuple([0.5, -1.0, 2.0][:D]))
+    ev = GpuKernelEvaluator(pb)
+    assert ev.path(GpuKernelEvaluator.AUTO) == GpuKernelEvaluator.TABLE_TC
+    info = ev.describe()
+    nph = h ** D
+    assert info["table_phases"] == nph
+    assert info["tc_record_slots"] == 0 if nph % 8 else info["tc_record_slots"] >= 2
+    assert info["tc_u_staging"] == 0 if nph % 4 else info["tc_u_staging"] >= 1
+    assert info["tc_region_buffers"] in (2, 3)
+    for metric in (GpuKernelEvaluator.MSE, GpuKernelEvaluator.NCC):
+        r_tc, g_tc = ev.getValueAndDerivative(metric, cp, cpw)
+        assert ev.path(GpuKernelEvaluator.REQ_TABLE_CUDA_CORES) == GpuKernelEvaluator.TABLE
+        r_cc, g_cc = ev.getValueAndDerivative(metric, cp, cpw)
+        assert ev.path(GpuKernelEvaluator.REQ_GENERIC) == GpuKernelEvaluator.GENERIC
+        r_g, g_g = ev.getValueAndDerivative(metric, cp, cpw)
+        ev.path(GpuKernelEvaluator.AUTO)
+        assert r_tc["num_pixels_counted"] == r_cc["num_pixels_counted"] == r_g["num_pixels_counted"] > 0
+        assert rel_err(r_tc["measure"], r_cc["measure"]) <= 1e-5
+        assert rel_err(r_tc["measure"], r_g["measure"]) <= 1e-5
+        assert max_rel(g_tc, g_cc) <= 1e-4
+        assert max_rel(g_tc, g_g) <= 1e-4
