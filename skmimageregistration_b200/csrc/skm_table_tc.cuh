@@ -563,10 +563,11 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
     if (tid == 0) {
         B.init(kTcGroupThreads, kConEpiWarps * 32);
         *abort = 0;
+        // the table (hi, then lo): one bulk copy, waited for by the MMA thread
+        tc::mbar_expect_tx(B.table, (uint32_t)(2 * Kp * Np * 4));
+        tc::bulk_g2s(Bhi, C.bcon, (uint32_t)(2 * Kp * Np * 4), B.table);
     }
     if (warp == kConMmaWarp) tc::tmem_alloc(tmem_holder, (uint32_t)C.con_cols);
-    for (int i = tid; i < 2 * Kp * Np / 4; i += kConThreads)
-        reinterpret_cast<float4 *>(Bhi)[i] = __ldg(reinterpret_cast<const float4 *>(C.bcon) + i);
     // rows past D * ct never receive data: zero their 128-byte rows once in every stage half
     const int pad_rows = kTcRows - D * ct;
     for (int i = tid; i < NS * 2 * pad_rows * 8; i += kConThreads) {
@@ -710,7 +711,9 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
             const uint32_t idesc = tc::idesc_tf32(kTcRows, Np);
             const uint32_t a_base = tc::smem_addr(As), bh_base = tc::smem_addr(Bhi), bl_base = tc::smem_addr(Blo);
             unsigned g = 0;
-            for (int it = 0;; ++it) {
+            const bool table_ok = tc::mbar_wait(B.table, 0, abort);   // the table has landed
+            if (!table_ok) tc_fail(abort, C.err);
+            for (int it = 0; table_ok; ++it) {
                 const long long tile = blockIdx.x + (long long)it * gridDim.x;
                 if (tile >= ntiles) break;
                 const int b = it & 1;
@@ -791,6 +794,8 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
             tc::mbar_arrive(&B.acc_empty[b]);
         }
     }
+    // the table copy lands before the CTA leaves (the MMA thread waited for it, or: no tile)
+    if (tid == 0 && blockIdx.x >= ntiles) tc::mbar_wait(B.table, 0, abort);
     tc_teardown(B, tmem, (uint32_t)C.con_cols, kConMmaWarp);
 }
 
