@@ -437,22 +437,23 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
             const float4 ci4 = __ldg(P.cpd + lin_of<D>(P.cp, ii));
             const float ci[3] = {ci4.x, ci4.y, ci4.z};
             const float kw = k * wj;
+            // per-offset terms in FP32 (relative error ~1e-7), their sums in FP64
             if (rkhs) {                                        // Regularizers.cu:68-73
-                double dot = 0.0;
+                float dot = 0.f;
 #pragma unroll
-                for (int d = 0; d < D; ++d) dot += (double)cjv[d] * (double)ci[d];
-                vr += (double)kw * dot;
+                for (int d = 0; d < D; ++d) dot = fmaf(cjv[d], ci[d], dot);
+                vr += (double)(kw * dot);
 #pragma unroll
                 for (int d = 0; d < D; ++d) drk[d] = fmaf(2.0f * kw, ci[d], drk[d]);
             }
             if (rd) {                                          // Regularizers.cu:141-144
-                double l2 = 0.0;
+                float l2 = 0.f;
 #pragma unroll
                 for (int d = 0; d < D; ++d) {
-                    const double e = (double)cjv[d] - (double)ci[d];
-                    l2 += e * e;
+                    const float e = cjv[d] - ci[d];
+                    l2 = fmaf(e, e, l2);
                 }
-                vd += l2 * (double)kw;
+                vd += (double)(kw * l2);
 #pragma unroll
                 for (int d = 0; d < D; ++d) drd[d] = fmaf(4.0f * kw, cjv[d] - ci[d], drd[d]);
             }
