@@ -419,6 +419,12 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
             }
         }
     }
+    // warp 0's metric-level parameters, loaded now so that their latency overlaps the regularizer
+    // loop (the combine below needs them)
+    double pc[3] = {0.0, 0.0, 0.0};
+    if (Q.with_metric && grp == 0 && active)
+#pragma unroll
+        for (int d = 0; d < D; ++d) pc[d] = Q.params[j_lin + d * P.C];
     // regularizer parts over this group's share of the control-point offsets
     float drk[3] = {0.f, 0.f, 0.f}, drd[3] = {0.f, 0.f, 0.f}, dpg[3] = {0.f, 0.f, 0.f};
     double vr = 0.0, vd = 0.0, vp = 0.0;
@@ -514,13 +520,10 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
             val[R_PG] += sval[g][2][lane];
         }
         const double *st = Q.stats;
-        double pc[3] = {0, 0, 0}, pn2 = 0.0;
+        double pn2 = 0.0;
         if (Q.with_metric) {
 #pragma unroll
-            for (int d = 0; d < D; ++d) {
-                pc[d] = Q.params[j_lin + d * P.C];
-                pn2 += pc[d] * pc[d];
-            }
+            for (int d = 0; d < D; ++d) pn2 += pc[d] * pc[d];
         }
         const double pnorm = sqrt(pn2);
 #pragma unroll
