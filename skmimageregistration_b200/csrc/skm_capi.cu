@@ -521,7 +521,7 @@ extern "C" int skm_evaluator_describe(skm_evaluator *e, skm_evaluator_info *out)
         r.tc_brick[1] = C.by;
         r.tc_brick[2] = C.bz;
         r.tc_transform_tiles = (int64_t)C.tiles[0] * C.tiles[1] * C.tiles[2];
-        r.tc_contrib_tiles = (e->table.dev.ncell + C.ct - 1) / C.ct;
+        r.tc_contrib_tiles = (e->table.dev.ncell + C.ctc - 1) / C.ctc;
         r.tc_transform_n = 2 * C.np;
         r.tc_transform_k = C.kp;
         r.tc_contrib_n = C.npc;

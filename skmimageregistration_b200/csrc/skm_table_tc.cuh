@@ -69,7 +69,9 @@ constexpr int kTcMaxRegion = 4096;                               // staged contr
 constexpr size_t kTcSmemMax = 227 * 1024;
 
 struct TcDev {
-    int ct;                  // cells per tile (rows per component)
+    int ct;                  // transform: cells per tile (rows per component)
+    int ctc;                 // contrib: cells per tile (3-D: 32, so that a lane quarter is one
+                             // component's 32 consecutive cells and its stores are whole lines)
     // transform
     int bx, by, bz;          // brick of cells per tile
     int tiles[3];
@@ -555,7 +557,7 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
     uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(barmem + kTcNumBars);
     volatile int *abort = reinterpret_cast<volatile int *>(tmem_holder + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int Kp = C.kpc, Np = C.npc, ct = C.ct, NS = C.ns_con;
+    const int Kp = C.kpc, Np = C.npc, ct = C.ctc, NS = C.ns_con;
     const int D = T.D, nph = T.nph;
     const long long ntiles = (T.ncell + ct - 1) / ct;
     const int nchunk = Kp / kTcKBlock;
@@ -879,6 +881,7 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
     C = TcDev{};
     if (T.D != 2 && T.D != 3) return 0;
     C.ct = kTcRows / T.D;
+    C.ctc = T.D == 3 ? 32 : kTcRows / T.D;
     C.np = (T.nph + 15) / 16 * 16;
     // transform K axis: x-neighbouring tap pairs (the second tap of a row's last pair is virtual
     // when nt0 is odd), two pairs per 16-byte unit
@@ -986,9 +989,9 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
     // records allow tiled loads (a chunk's 32 phases as four 128-byte rows per cell); else as many
     // stages (up to 3, at least 2) as the shared memory holds and direct record loads
     C.nrr = 0;
-    C.rfix = (512 * C.ct + 127) / 128 * 128;
-    C.rslot = (C.rfix + 128 * C.ct + 1023) / 1024 * 1024;
-    if (T.nph % 8 == 0 && C.ct <= 256) {
+    C.rfix = (512 * C.ctc + 127) / 128 * 128;
+    C.rslot = (C.rfix + 128 * C.ctc + 1023) / 1024 * 1024;
+    if (T.nph % 8 == 0 && C.ctc <= 256) {
         C.ns_con = 2;
         for (C.nrr = 3; C.nrr >= 2 && (size_t)TcContribLayout(C).total_bytes > kTcSmemMax; --C.nrr) {
         }
@@ -1112,10 +1115,10 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
         if (C.nrr > 0) {
             const cuuint64_t rd[3] = {32, (cuuint64_t)(T.nph / 8), (cuuint64_t)T.ncell};
             const cuuint64_t rs[2] = {128, (cuuint64_t)T.nph * 16};
-            const cuuint32_t rb[3] = {32, 4, (cuuint32_t)C.ct};
+            const cuuint32_t rb[3] = {32, 4, (cuuint32_t)C.ctc};
             const cuuint64_t fd[2] = {(cuuint64_t)T.nph, (cuuint64_t)T.ncell};
             const cuuint64_t fs[1] = {(cuuint64_t)T.nph * 4};
-            const cuuint32_t fb[2] = {(cuuint32_t)kTcKBlock, (cuuint32_t)C.ct};
+            const cuuint32_t fb[2] = {(cuuint32_t)kTcKBlock, (cuuint32_t)C.ctc};
             const cuuint32_t e1[3] = {1, 1, 1};
             auto enc = reinterpret_cast<PfnTensorMapEncodeTiled>(fn);
             if (enc(&tc.recmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)T.rec, rd, rs, rb, e1,
@@ -1146,7 +1149,7 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
         return 2;
     if (occ_t < 1 || occ_c < 1) return 0;
     const long long ttiles = (long long)C.tiles[0] * C.tiles[1] * C.tiles[2];
-    const long long ctiles = (T.ncell + C.ct - 1) / C.ct;
+    const long long ctiles = (T.ncell + C.ctc - 1) / C.ctc;
     tc.transform_blocks = (int)std::max<long long>(1, std::min<long long>(ttiles, sms));
     tc.contrib_blocks = (int)std::max<long long>(1, std::min<long long>(ctiles, sms));
     tc.enabled = true;
