@@ -378,10 +378,10 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
     int j[3] = {0, 0, 0};
     if (active) cell_of<D>(P.cp.n, j_lin, j);
     const float4 cj = active ? P.cpd[j_lin] : make_float4(0.f, 0.f, 0.f, 0.f);
-    // the fused optimizer step: warp 1 + d applies it to component d; its operands are loaded now
-    // so that their latency overlaps the sums
-    const int sd = grp - 1;
-    const bool stepper = Q.step.on && active && sd >= 0 && sd < D;
+    // the fused optimizer step: warp d applies it to component d (after combining it, below); its
+    // operands are loaded now so that their latency overlaps the sums
+    const int sd = grp;
+    const bool stepper = Q.step.on && active && sd < D;
     double st_g = 0.0, st_b = 0.0, st_x = 0.0, st_t = 0.0, st_p = 0.0;
     if (stepper) {
         st_g = Q.step.tmp[j_lin + sd * P.C];
@@ -419,10 +419,10 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
             }
         }
     }
-    // warp 0's metric-level parameters, loaded now so that their latency overlaps the regularizer
-    // loop (the combine below needs them)
+    // the metric-level parameters for the combining warps 0..D-1, loaded now so that their latency
+    // overlaps the regularizer loop
     double pc[3] = {0.0, 0.0, 0.0};
-    if (Q.with_metric && grp == 0 && active)
+    if (Q.with_metric && grp < D && active)
 #pragma unroll
         for (int d = 0; d < D; ++d) pc[d] = Q.params[j_lin + d * P.C];
     // regularizer parts over this group's share of the control-point offsets
@@ -504,64 +504,66 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
     double val[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) val[k] = 0.0;
-    __shared__ double sgrad[3][32], ssp[3];
-    if (grp == 0 && active) {
-        float a[3] = {0.f, 0.f, 0.f}, rk[3] = {0.f, 0.f, 0.f}, rdd[3] = {0.f, 0.f, 0.f}, rp[3] = {0.f, 0.f, 0.f};
+    __shared__ double ssp[3];
+    // warp d < D combines component d (the groups' partials in a fixed order), adds the
+    // metric-level terms, writes the derivative and applies the fused step; warp 0 also sums the
+    // regularizer values
+    double sp = 0.0;
+    if (grp < D && active) {
+        const int d = grp;
+        float a = 0.f, rk = 0.f, rdd = 0.f, rp = 0.f;
         for (int g = 0; g < kGatherGroups; ++g) {           // fixed combination order
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                a[d] += sacc[g][d][lane];
-                rk[d] += sreg[g][d][lane];
-                rdd[d] += sreg[g][3 + d][lane];
-                rp[d] += sreg[g][6 + d][lane];
+            a += sacc[g][d][lane];
+            rk += sreg[g][d][lane];
+            rdd += sreg[g][3 + d][lane];
+            rp += sreg[g][6 + d][lane];
+            if (d == 0) {
+                val[R_RKHS] += sval[g][0][lane];
+                val[R_RD] += sval[g][1][lane];
+                val[R_PG] += sval[g][2][lane];
             }
-            val[R_RKHS] += sval[g][0][lane];
-            val[R_RD] += sval[g][1][lane];
-            val[R_PG] += sval[g][2][lane];
         }
         const double *st = Q.stats;
         double pn2 = 0.0;
         if (Q.with_metric) {
 #pragma unroll
-            for (int d = 0; d < D; ++d) pn2 += pc[d] * pc[d];
+            for (int e = 0; e < D; ++e) pn2 += pc[e] * pc[e];
         }
         const double pnorm = sqrt(pn2);
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-            double g;
-            if (Q.metric == 1)
-                g = st[S_DENOM] != 0.0 ? (double)cj.w * (double)a[d] : 0.0;
-            else
-                g = (double)cj.w * (double)a[d];
-            if (rkhs) g += (double)rk[d] * Q.reg_rkhs;
-            if (rd) g += (double)rdd[d] * Q.reg_rd;
-            if (pg) g += (double)rp[d] * Q.reg_pg;
-            if (Q.with_metric) {
-                const double par = pc[d];
-                if (Q.reg_l1 > 0.0) {                          // metric hxx:447-466
-                    const double w = Q.reg_l1;
-                    if (fabs(par) > 0.0) g += w * (par < 0.0 ? -1.0 : 1.0);
-                    else if (g < -w) g += w;
-                    else if (g > w) g -= w;
-                    else g = 0.0;
-                }
-                if (Q.reg_l2 > 0.0) g += Q.reg_l2 * 2.0 * par;  // hxx:482-485
-                if (Q.reg_l21 > 0.0) {                         // hxx:504-521
-                    const double w = Q.reg_l21;
-                    if (pnorm > 0.0) g += w * par / pnorm;
-                    else if (g < -w) g += w;
-                    else if (g > w) g -= w;
-                    else g = 0.0;
-                }
-                if (Q.negate) g = -g;
-            }
-            Q.deriv[j_lin + d * P.C] = g;
-            if (Q.step.on) sgrad[d][lane] = g;
-        }
+        double g;
+        if (Q.metric == 1)
+            g = st[S_DENOM] != 0.0 ? (double)cj.w * (double)a : 0.0;
+        else
+            g = (double)cj.w * (double)a;
+        if (rkhs) g += (double)rk * Q.reg_rkhs;
+        if (rd) g += (double)rdd * Q.reg_rd;
+        if (pg) g += (double)rp * Q.reg_pg;
         if (Q.with_metric) {
+            const double par = pc[d];
+            if (Q.reg_l1 > 0.0) {                              // metric hxx:447-466
+                const double w = Q.reg_l1;
+                if (fabs(par) > 0.0) g += w * (par < 0.0 ? -1.0 : 1.0);
+                else if (g < -w) g += w;
+                else if (g > w) g -= w;
+                else g = 0.0;
+            }
+            if (Q.reg_l2 > 0.0) g += Q.reg_l2 * 2.0 * par;      // hxx:482-485
+            if (Q.reg_l21 > 0.0) {                             // hxx:504-521
+                const double w = Q.reg_l21;
+                if (pnorm > 0.0) g += w * par / pnorm;
+                else if (g < -w) g += w;
+                else if (g > w) g -= w;
+                else g = 0.0;
+            }
+            if (Q.negate) g = -g;
+        }
+        Q.deriv[j_lin + d * P.C] = g;
+        if (stepper)
+            sp = opt_update(Q.step, j_lin + d * P.C, g, opt_learning_rate(Q.step, st_t), st_p != 0.0, st_g, st_b, st_x);
+        if (d == 0 && Q.with_metric) {
             double l1 = 0.0;
 #pragma unroll
-            for (int d = 0; d < D; ++d) l1 += fabs(pc[d]);
+            for (int e = 0; e < D; ++e) l1 += fabs(pc[e]);
             val[R_L1] = Q.reg_l1 > 0.0 ? l1 : 0.0;
             val[R_L2] = Q.reg_l2 > 0.0 ? pn2 : 0.0;
             val[R_L21] = Q.reg_l21 > 0.0 ? pnorm : 0.0;
@@ -575,14 +577,9 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
         }
     }
     if (Q.step.on) {                                       // uniform over the grid
-        __syncthreads();
-        double sp = 0.0;
-        if (stepper)
-            sp = opt_update(Q.step, j_lin + sd * P.C, sgrad[sd][lane], opt_learning_rate(Q.step, st_t), st_p != 0.0,
-                            st_g, st_b, st_x);
-        if (sd >= 0 && sd < D) {
+        if (grp < D) {
             sp = warp_sum(sp);
-            if (lane == 0) ssp[sd] = sp;
+            if (lane == 0) ssp[grp] = sp;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
