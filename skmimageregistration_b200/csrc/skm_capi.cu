@@ -50,7 +50,7 @@ int dalloc(T **p, size_t n)
 {
     *p = nullptr;
     if (n == 0) n = 1;
-    SKM_CUDA(cudaMalloc((void **)p, n * sizeof(T)));
+    SKM_CUDA(pool_malloc((void **)p, n * sizeof(T)));
     return SKM_OK;
 }
 
@@ -168,7 +168,7 @@ struct skm_evaluator {
         void *bufs[] = {d_fixed, d_coeffs, d_coeffs4, d_wimg, d_wten, d_cpd, d_df, d_samp, d_dense, d_dense_sw, d_dense_in,
                         d_dense_sw_in, d_shifts, d_in, d_counters, d_part, d_stats, d_deriv, d_rpart, d_out};
         for (void *b : bufs)
-            if (b) cudaFree(b);
+            if (b) pool_free(b);
         if (mgraph) cudaGraphExecDestroy(mgraph);
         table_tc_free(tc);
         table_free(table);
@@ -571,7 +571,7 @@ static int upload_field(skm_evaluator *e, const skm_field *df)
     if (!geometry_ok(df->geometry, D)) return fail(SKM_ERR_INVALID, "invalid displacement-field geometry");
     long long n = texels(df->geometry, D);
     if (n > e->df_texels) {
-        if (e->d_df) cudaFree(e->d_df);
+        if (e->d_df) pool_free(e->d_df);
         e->d_df = nullptr;
         if (dalloc(&e->d_df, n)) return SKM_ERR_CUDA;
         e->df_texels = n;
@@ -961,7 +961,7 @@ extern "C" int skm_evaluate_displacement_field(skm_evaluator *e, const double *c
             rc = fail(SKM_ERR_CUDA, "displacement field copy failed: %s",
                       cudaGetErrorString(c1 != cudaSuccess ? c1 : c2));
     }
-    cudaFree(d_out);
+    pool_free(d_out);
     return rc;
 }
 
@@ -1002,8 +1002,8 @@ extern "C" int skm_bspline_coefficients(int32_t D, const int32_t *size, const do
         SKM_CUDA(cudaStreamSynchronize(s));
         return SKM_OK;
     }();
-    if (d_img) cudaFree(d_img);
-    if (d_out) cudaFree(d_out);
+    if (d_img) pool_free(d_img);
+    if (d_out) pool_free(d_out);
     if (s) cudaStreamDestroy(s);
     return rc;
 }

@@ -14,6 +14,40 @@
 
 namespace skm {
 
+// Device buffers come from the device's stream-ordered memory pool with a release threshold that
+// keeps freed memory for reuse, so that evaluators created and destroyed level after level (the
+// multi-scale driver) do not map and unmap their buffers every time.  Both calls complete before
+// returning (as cudaMalloc / cudaFree do), so no stream ordering leaks out of them.
+inline cudaError_t pool_malloc(void **p, size_t bytes)
+{
+    static int configured_device = -1;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (configured_device != dev) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+        configured_device = dev;
+    }
+    e = cudaMallocAsync(p, bytes, 0);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(0);
+}
+
+inline cudaError_t pool_free(void *p)
+{
+    if (!p) return cudaSuccess;
+    cudaError_t e = cudaDeviceSynchronize();                 // as cudaFree: no work still uses p
+    if (e != cudaSuccess) return e;
+    e = cudaFreeAsync(p, 0);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(0);
+}
+
 constexpr int kMaxDim = 3;
 
 // Division by a runtime constant d >= 1 for numerators below 2^31: q = (mulhi(n, m) + n) >> s with

@@ -27,7 +27,7 @@ struct DevBuf {
     double *p = nullptr;
     ~DevBuf()
     {
-        if (p) cudaFree(p);
+        if (p) pool_free(p);
     }
 };
 
@@ -44,7 +44,7 @@ int smooth_device(int D, const int *size, const double *spacing, double variance
         if (r > skm::kSmoothMaxRadius) return fail(SKM_ERR_UNSUPPORTED, "smoothing kernel radius %d > %d", r,
                                                   skm::kSmoothMaxRadius);
         DevBuf dc;
-        SKM_CUDA(cudaMalloc((void **)&dc.p, c.size() * sizeof(double)));
+        SKM_CUDA(pool_malloc((void **)&dc.p, c.size() * sizeof(double)));
         SKM_CUDA(cudaMemcpyAsync(dc.p, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
         skm::smooth_axis_kernel<<<blocks, 256, 0, s>>>(src, dst, X, Y, Z, axis, dc.p, r);
@@ -61,8 +61,8 @@ int threshold_rescale_device(long long n, int apply_threshold, double tmin, doub
 {
     const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 4);
     DevBuf part, res;
-    SKM_CUDA(cudaMalloc((void **)&part.p, sizeof(double) * 4 * blocks));
-    SKM_CUDA(cudaMalloc((void **)&res.p, sizeof(double) * 4));
+    SKM_CUDA(pool_malloc((void **)&part.p, sizeof(double) * 4 * blocks));
+    SKM_CUDA(pool_malloc((void **)&res.p, sizeof(double) * 4));
     skm::range_kernel<<<blocks, 256, 0, s>>>(d_img, n, tmin, tmax, part.p);
     SKM_CHECK_LAUNCH();
     skm::range_finish_kernel<<<1, 32, 0, s>>>(part.p, blocks, res.p);
@@ -106,8 +106,8 @@ int device_max(const double *d_v, long long n, double *out, cudaStream_t s)
 {
     const int blocks = grid_blocks(n, 4);
     DevBuf part, res;
-    SKM_CUDA(cudaMalloc((void **)&part.p, sizeof(double) * 4 * blocks));
-    SKM_CUDA(cudaMalloc((void **)&res.p, sizeof(double) * 4));
+    SKM_CUDA(pool_malloc((void **)&part.p, sizeof(double) * 4 * blocks));
+    SKM_CUDA(pool_malloc((void **)&res.p, sizeof(double) * 4));
     skm::range_kernel<<<blocks, 256, 0, s>>>(d_v, n, 0.0, 0.0, part.p);
     SKM_CHECK_LAUNCH();
     skm::range_finish_kernel<<<1, 32, 0, s>>>(part.p, blocks, res.p);
@@ -131,15 +131,15 @@ int anisotropic_tensor_device(int D, const int32_t *size, const double *spacing,
     const int nc = skm::tensor_components(D);
     const int blocks = grid_blocks(n, 16);
     DevBuf f, tmp, comp, tilt;
-    SKM_CUDA(cudaMalloc((void **)&f.p, n * sizeof(double)));
-    SKM_CUDA(cudaMalloc((void **)&tmp.p, n * sizeof(double)));
-    SKM_CUDA(cudaMalloc((void **)&comp.p, nc * n * sizeof(double)));
-    SKM_CUDA(cudaMalloc((void **)&tilt.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&f.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&tmp.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&comp.p, nc * n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&tilt.p, n * sizeof(double)));
     unsigned *d_bad = nullptr;
-    SKM_CUDA(cudaMalloc((void **)&d_bad, sizeof(unsigned)));
+    SKM_CUDA(pool_malloc((void **)&d_bad, sizeof(unsigned)));
     struct FreeBad {
         unsigned *p;
-        ~FreeBad() { cudaFree(p); }
+        ~FreeBad() { pool_free(p); }
     } free_bad{d_bad};
     SKM_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(unsigned), s));
     // weight * image, smoothed with variance sigma (:54-64)
@@ -176,12 +176,12 @@ int max_eigenvalue_tensor(int D, long long n, const double *d_tensor, const doub
                           double *cov_out, cudaStream_t s)
 {
     DevBuf ev;
-    SKM_CUDA(cudaMalloc((void **)&ev.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&ev.p, n * sizeof(double)));
     unsigned *d_bad = nullptr;
-    SKM_CUDA(cudaMalloc((void **)&d_bad, sizeof(unsigned)));
+    SKM_CUDA(pool_malloc((void **)&d_bad, sizeof(unsigned)));
     struct FreeBad {
         unsigned *p;
-        ~FreeBad() { cudaFree(p); }
+        ~FreeBad() { pool_free(p); }
     } free_bad{d_bad};
     SKM_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(unsigned), s));
     const int blocks = grid_blocks(n, 16);
@@ -233,8 +233,8 @@ extern "C" int skm_gaussian_smooth(int32_t dimensions, const skm_geometry *geome
     HostStream hs;
     SKM_CUDA(cudaStreamCreateWithFlags(&hs.s, cudaStreamNonBlocking));
     DevBuf a, b;
-    SKM_CUDA(cudaMalloc((void **)&a.p, n * sizeof(double)));
-    SKM_CUDA(cudaMalloc((void **)&b.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&a.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&b.p, n * sizeof(double)));
     SKM_CUDA(cudaMemcpyAsync(a.p, src, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
     int rc = smooth_device(dimensions, geometry->size, geometry->spacing, variance, use_image_spacing, maximum_error,
                            maximum_kernel_width, a.p, b.p, hs.s);
@@ -256,7 +256,7 @@ extern "C" int skm_threshold_rescale(int32_t dimensions, const int32_t *size, in
     HostStream hs;
     SKM_CUDA(cudaStreamCreateWithFlags(&hs.s, cudaStreamNonBlocking));
     DevBuf a;
-    SKM_CUDA(cudaMalloc((void **)&a.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&a.p, n * sizeof(double)));
     SKM_CUDA(cudaMemcpyAsync(a.p, src, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
     int rc = threshold_rescale_device(n, apply_threshold, threshold_min, threshold_max, out_min, out_max, a.p, hs.s);
     if (rc) return rc;
@@ -281,8 +281,8 @@ extern "C" int skm_anisotropic_tensor(int32_t dimensions, const skm_geometry *ge
     HostStream hs;
     SKM_CUDA(cudaStreamCreateWithFlags(&hs.s, cudaStreamNonBlocking));
     DevBuf img, cov;
-    SKM_CUDA(cudaMalloc((void **)&img.p, n * sizeof(double)));
-    SKM_CUDA(cudaMalloc((void **)&cov.p, nt * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&img.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&cov.p, nt * sizeof(double)));
     SKM_CUDA(cudaMemcpyAsync(img.p, image, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
     double tilt = -DBL_MAX;
     int rc = anisotropic_tensor_device(dimensions, geometry->size, geometry->spacing, img.p, sigma, weight,
@@ -335,9 +335,9 @@ extern "C" int skm_warp_image(int32_t dimensions, const skm_geometry *image_geom
     HostStream hs;
     SKM_CUDA(cudaStreamCreateWithFlags(&hs.s, cudaStreamNonBlocking));
     DevBuf di, df, dout;
-    SKM_CUDA(cudaMalloc((void **)&di.p, ni * sizeof(double)));
-    SKM_CUDA(cudaMalloc((void **)&df.p, nf * D * sizeof(double)));
-    SKM_CUDA(cudaMalloc((void **)&dout.p, nf * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&di.p, ni * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&df.p, nf * D * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&dout.p, nf * sizeof(double)));
     SKM_CUDA(cudaMemcpyAsync(di.p, image, ni * sizeof(double), cudaMemcpyHostToDevice, hs.s));
     SKM_CUDA(cudaMemcpyAsync(df.p, field, nf * D * sizeof(double), cudaMemcpyHostToDevice, hs.s));
     const skm::OutGeo gi = out_geo(D, *image_geometry), gf = out_geo(D, *field_geometry);
@@ -377,8 +377,8 @@ extern "C" int skm_jacobian_determinant(int32_t dimensions, const skm_geometry *
     HostStream hs;
     SKM_CUDA(cudaStreamCreateWithFlags(&hs.s, cudaStreamNonBlocking));
     DevBuf du, dout;
-    SKM_CUDA(cudaMalloc((void **)&du.p, n * D * sizeof(double)));
-    SKM_CUDA(cudaMalloc((void **)&dout.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&du.p, n * D * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&dout.p, n * sizeof(double)));
     SKM_CUDA(cudaMemcpyAsync(du.p, field, n * D * sizeof(double), cudaMemcpyHostToDevice, hs.s));
     const skm::OutGeo g = out_geo(D, *geometry);
     if (D == 2) skm::jacobian_determinant_kernel<2><<<grid_blocks(n, 16), 256, 0, hs.s>>>(du.p, g, dout.p);
@@ -451,9 +451,9 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
 
     // preprocessing of both images (SKMReg.cxx:85-90)
     DevBuf dref, dtar, dtmp;
-    SKM_CUDA(cudaMalloc((void **)&dref.p, n * sizeof(double)));
-    SKM_CUDA(cudaMalloc((void **)&dtar.p, n * sizeof(double)));
-    SKM_CUDA(cudaMalloc((void **)&dtmp.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&dref.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&dtar.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&dtmp.p, n * sizeof(double)));
     SKM_CUDA(cudaMemcpyAsync(dref.p, reference, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
     SKM_CUDA(cudaMemcpyAsync(dtar.p, target, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
     if ((rc = threshold_rescale_device(n, r->apply_threshold, r->threshold_min, r->threshold_max, 0.0, 1.0, dref.p,
@@ -472,7 +472,7 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
     }
     std::vector<double> coeffs((size_t)ncoef);
     DevBuf dsm;
-    SKM_CUDA(cudaMalloc((void **)&dsm.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&dsm.p, n * sizeof(double)));
 
     // kernel weighting (SKMReg.cxx:245-297): a weight image, or per level a covariance tensor built
     // from the guidance image / the smoothed target, or an external tensor where the weight is 0
@@ -485,9 +485,9 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
     std::vector<double> tensor;
     const long long nt = n * D * D;
     if (any_tensor) {
-        SKM_CUDA(cudaMalloc((void **)&dcov.p, nt * sizeof(double)));
+        SKM_CUDA(pool_malloc((void **)&dcov.p, nt * sizeof(double)));
         if (r->guidance_image) {
-            SKM_CUDA(cudaMalloc((void **)&dguide.p, n * sizeof(double)));
+            SKM_CUDA(pool_malloc((void **)&dguide.p, n * sizeof(double)));
             SKM_CUDA(cudaMemcpyAsync(dguide.p, r->guidance_image, n * sizeof(double), cudaMemcpyHostToDevice, hs.s));
         }
         tensor.resize((size_t)nt);
@@ -569,7 +569,7 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
             // case 2 (:259-268): external tensor with tilt -1: the tensor whose largest eigenvalue is
             // largest gives the support covariance and the maximum weight
             if (!ext_ready) {
-                SKM_CUDA(cudaMalloc((void **)&dext.p, nt * sizeof(double)));
+                SKM_CUDA(pool_malloc((void **)&dext.p, nt * sizeof(double)));
                 SKM_CUDA(cudaMemcpyAsync(dext.p, r->weight_tensor, nt * sizeof(double), cudaMemcpyHostToDevice,
                                          hs.s));
                 if ((rc = max_eigenvalue_tensor(D, n, dext.p, r->weight_tensor, &ext_maximum, ext_cov, hs.s)))

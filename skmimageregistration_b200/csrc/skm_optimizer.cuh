@@ -118,7 +118,7 @@ struct skm_optimizer {
         if (graph) cudaGraphDestroy(graph);
         void *bufs[] = {d_pos, d_base, d_tmp, d_best, d_cpw, d_scal, d_sp, d_rng};
         for (void *b : bufs)
-            if (b) cudaFree(b);
+            if (b) pool_free(b);
     }
 };
 

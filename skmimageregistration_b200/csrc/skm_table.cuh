@@ -826,7 +826,7 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
                 fix[cell * T.nph + ph] = fixed_host[x + (size_t)P.fixed.n[0] * (y + (size_t)P.fixed.n[1] * z)];
             }
     auto up = [&](float **dst, const std::vector<float> &src) -> bool {
-        if (cudaMalloc((void **)dst, std::max<size_t>(1, src.size()) * sizeof(float)) != cudaSuccess) return false;
+        if (pool_malloc((void **)dst, std::max<size_t>(1, src.size()) * sizeof(float)) != cudaSuccess) return false;
         return cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(float), cudaMemcpyHostToDevice, stream) ==
                cudaSuccess;
     };
@@ -842,15 +842,15 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
                 kcpo.push_back((T.clo[0] + ox + 512) | ((T.clo[1] + oy + 512) << 10) | ((T.clo[2] + oz + 512) << 20));
             }
     T.nkcp = (int)kcpv.size();
-    if (cudaMalloc((void **)&pl.d_kcpo, std::max<size_t>(1, kcpo.size()) * sizeof(int)) != cudaSuccess ||
+    if (pool_malloc((void **)&pl.d_kcpo, std::max<size_t>(1, kcpo.size()) * sizeof(int)) != cudaSuccess ||
         cudaMemcpyAsync(pl.d_kcpo, kcpo.data(), kcpo.size() * sizeof(int), cudaMemcpyHostToDevice, stream) !=
             cudaSuccess)
         return 2;
     if (!up(&pl.d_tfwd, tfwd) || !up(&pl.d_tgemm, tgemm) || !up(&pl.d_kcp, kcpv) || !up(&pl.d_fixcp, fix)) return 2;
-    if (cudaMalloc((void **)&pl.d_rec, (size_t)T.ncell * T.nph * sizeof(float4)) != cudaSuccess) return 2;
-    if (cudaMalloc((void **)&pl.d_ucp, (size_t)D * T.ncell * T.nph * sizeof(float)) != cudaSuccess) return 2;
-    if (cudaMalloc((void **)&pl.d_contrib, (size_t)3 * T.ntap * T.ncell * sizeof(float)) != cudaSuccess) return 2;
-    if (cudaMalloc((void **)&pl.d_part, (size_t)NQ * T.value_blocks * sizeof(double)) != cudaSuccess) return 2;
+    if (pool_malloc((void **)&pl.d_rec, (size_t)T.ncell * T.nph * sizeof(float4)) != cudaSuccess) return 2;
+    if (pool_malloc((void **)&pl.d_ucp, (size_t)D * T.ncell * T.nph * sizeof(float)) != cudaSuccess) return 2;
+    if (pool_malloc((void **)&pl.d_contrib, (size_t)3 * T.ntap * T.ncell * sizeof(float)) != cudaSuccess) return 2;
+    if (pool_malloc((void **)&pl.d_part, (size_t)NQ * T.value_blocks * sizeof(double)) != cudaSuccess) return 2;
     if (cudaStreamSynchronize(stream) != cudaSuccess) return 2;
     T.tfwd = pl.d_tfwd;
     T.tgemm = pl.d_tgemm;
@@ -931,12 +931,12 @@ inline int table_size_grids(TablePlan &pl)
 inline void table_free(TablePlan &pl)
 {
     float *f[] = {pl.d_tfwd, pl.d_tgemm, pl.d_kcp, pl.d_fixcp, pl.d_contrib};
-    if (pl.d_kcpo) cudaFree(pl.d_kcpo);
+    if (pl.d_kcpo) pool_free(pl.d_kcpo);
     for (float *p : f)
-        if (p) cudaFree(p);
-    if (pl.d_rec) cudaFree(pl.d_rec);
-    if (pl.d_ucp) cudaFree(pl.d_ucp);
-    if (pl.d_part) cudaFree(pl.d_part);
+        if (p) pool_free(p);
+    if (pl.d_rec) pool_free(pl.d_rec);
+    if (pl.d_ucp) pool_free(pl.d_ucp);
+    if (pl.d_part) pool_free(pl.d_part);
     pl = TablePlan{};
 }
 

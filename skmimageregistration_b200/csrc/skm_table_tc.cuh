@@ -1042,11 +1042,11 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
             btr[kmaj(C.np + p, k, 2 * C.np)] = lo;
         }
     }
-    if (cudaMalloc((void **)&tc.d_btr, btr.size() * sizeof(float)) != cudaSuccess) return 2;
-    if (cudaMalloc((void **)&tc.d_bcon, bcon.size() * sizeof(float)) != cudaSuccess) return 2;
-    if (cudaMalloc((void **)&tc.d_err, sizeof(unsigned)) != cudaSuccess) return 2;
-    if (cudaMalloc((void **)&tc.d_pairoff, pairoff.size() * sizeof(int2)) != cudaSuccess) return 2;
-    if (cudaMalloc((void **)&tc.d_ctap, ctap.size() * sizeof(int)) != cudaSuccess) return 2;
+    if (pool_malloc((void **)&tc.d_btr, btr.size() * sizeof(float)) != cudaSuccess) return 2;
+    if (pool_malloc((void **)&tc.d_bcon, bcon.size() * sizeof(float)) != cudaSuccess) return 2;
+    if (pool_malloc((void **)&tc.d_err, sizeof(unsigned)) != cudaSuccess) return 2;
+    if (pool_malloc((void **)&tc.d_pairoff, pairoff.size() * sizeof(int2)) != cudaSuccess) return 2;
+    if (pool_malloc((void **)&tc.d_ctap, ctap.size() * sizeof(int)) != cudaSuccess) return 2;
     if (cudaMemcpyAsync(tc.d_pairoff, pairoff.data(), pairoff.size() * sizeof(int2), cudaMemcpyHostToDevice,
                         stream) != cudaSuccess ||
         cudaMemcpyAsync(tc.d_ctap, ctap.data(), ctap.size() * sizeof(int), cudaMemcpyHostToDevice, stream) !=
@@ -1070,7 +1070,7 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
         const int n0 = ncp[0], n1 = ncp[1], n2 = T.D == 3 ? ncp[2] : 1;
         const int nxp = (n0 + 3) / 4 * 4;
         const long long plane = (long long)nxp * n1 * n2;
-        if (cudaMalloc((void **)&tc.rp.p, sizeof(float) * T.D * plane) != cudaSuccess) return 2;
+        if (pool_malloc((void **)&tc.rp.p, sizeof(float) * T.D * plane) != cudaSuccess) return 2;
         if (cudaMemsetAsync(tc.rp.p, 0, sizeof(float) * T.D * plane, stream) != cudaSuccess ||
             cudaStreamSynchronize(stream) != cudaSuccess)
             return 2;
@@ -1243,13 +1243,13 @@ inline int table_derivative_gather_only(TablePlan &pl, const EvalParams &P, cons
 
 inline void table_tc_free(TcPlan &tc)
 {
-    if (tc.d_btr) cudaFree(tc.d_btr);
-    if (tc.d_bcon) cudaFree(tc.d_bcon);
-    if (tc.d_err) cudaFree(tc.d_err);
-    if (tc.d_pairoff) cudaFree(tc.d_pairoff);
-    if (tc.rp.p) cudaFree(tc.rp.p);
+    if (tc.d_btr) pool_free(tc.d_btr);
+    if (tc.d_bcon) pool_free(tc.d_bcon);
+    if (tc.d_err) pool_free(tc.d_err);
+    if (tc.d_pairoff) pool_free(tc.d_pairoff);
+    if (tc.rp.p) pool_free(tc.rp.p);
     warp_tma_free(tc.wt);
-    if (tc.d_ctap) cudaFree(tc.d_ctap);
+    if (tc.d_ctap) pool_free(tc.d_ctap);
     tc = TcPlan{};
 }
 

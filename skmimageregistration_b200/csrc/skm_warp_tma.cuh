@@ -287,7 +287,7 @@ inline int warp_tma_plan(WarpTmaPlan &wt, const TablePlan &pl, const EvalParams 
     for (long long z = 0; z < PZ; ++z)
         for (long long y = 0; y < PY; ++y)
             std::memcpy(&padded[(size_t)((z * PY + y) * pitch)], h_coeffs + (z * PY + y) * PX, sizeof(float) * PX);
-    if (cudaMalloc((void **)&wt.d_coefp, padded.size() * sizeof(float)) != cudaSuccess) return 2;
+    if (pool_malloc((void **)&wt.d_coefp, padded.size() * sizeof(float)) != cudaSuccess) return 2;
     if (cudaMemcpyAsync(wt.d_coefp, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice,
                         stream) != cudaSuccess ||
         cudaStreamSynchronize(stream) != cudaSuccess)
@@ -328,7 +328,7 @@ inline int warp_tma_plan(WarpTmaPlan &wt, const TablePlan &pl, const EvalParams 
 
 inline void warp_tma_free(WarpTmaPlan &wt)
 {
-    if (wt.d_coefp) cudaFree(wt.d_coefp);
+    if (wt.d_coefp) pool_free(wt.d_coefp);
     wt = WarpTmaPlan{};
 }
 
