@@ -412,15 +412,21 @@ int skm_jacobian_determinant(int32_t dimensions, const skm_geometry *geometry, c
  *
  *   fixed_image          device, float, prod(fixed size) texels
  *   moving_coefficients  device, float, prod(moving size + 3) B-spline coefficients
- *   control_points       device, 4 floats per control point: alpha x, y, z (0 in 2-D), weight
+ *   control_points       device, 4 floats per control point: alpha x, y, z (0 in 2-D), weight;
+ *                        16-byte aligned (read as float4)
  *   result               device, 2 doubles: measure, number of pixels counted
+ *
+ * Misaligned buffers (control_points not 16-byte aligned, images not 4-byte, result not 8-byte
+ * aligned) are rejected with SKM_ERR_INVALID before anything is launched.
  *
  * Same value as skm_get_value for a stationary kernel, subsample 1, no displacement
  * field, MSE or NCC.  Limit: at most 2,097,152 fixed-image texels; larger images are
  * rejected with SKM_ERR_INVALID.  Every call on a device shares the array and leaves its
  * contents behind (each call overwrites what it reads), so calls that overlap on the GPU
  * race.  The first call on each device looks up the array's device address; make that
- * first call before any stream capture.  Errors are reported through skm_last_error(). */
+ * first call before any stream capture.  The address is kept for the life of the process, so
+ * do not call this entry point again after cudaDeviceReset (or after the device's primary
+ * context was released and re-created).  Errors are reported through skm_last_error(). */
 int skm_value_noalloc(int32_t dimensions, int32_t metric,
                       const skm_geometry *fixed_geometry, const float *fixed_image,
                       const skm_geometry *moving_geometry, const float *moving_coefficients,

@@ -165,13 +165,16 @@ struct skm_evaluator {
     ~skm_evaluator()
     {
         if (device >= 0) cudaSetDevice(device);
+        // one device synchronisation for all buffers (no work uses them after it), then the frees
+        cudaDeviceSynchronize();
         void *bufs[] = {d_fixed, d_coeffs, d_coeffs4, d_wimg, d_wten, d_cpd, d_df, d_samp, d_dense, d_dense_sw, d_dense_in,
                         d_dense_sw_in, d_shifts, d_in, d_counters, d_part, d_stats, d_deriv, d_rpart, d_out};
         for (void *b : bufs)
-            if (b) pool_free(b);
+            if (b) pool_release(b);
         if (mgraph) cudaGraphExecDestroy(mgraph);
         table_tc_free(tc);
         table_free(table);
+        cudaStreamSynchronize(0);
         if (h_in) cudaFreeHost(h_in);
         if (h_out) cudaFreeHost(h_out);
         if (stream) cudaStreamDestroy(stream);

@@ -10,32 +10,95 @@
 #pragma once
 
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 
 namespace skm {
 
-// Device buffers come from the device's stream-ordered memory pool with a release threshold that
-// keeps freed memory for reuse, so that evaluators created and destroyed level after level (the
-// multi-scale driver) do not map and unmap their buffers every time.  Both calls complete before
-// returning (as cudaMalloc / cudaFree do), so no stream ordering leaks out of them.
+// Device buffers come from a stream-ordered memory pool private to this library (one per device,
+// created on first use) whose release threshold keeps freed memory for reuse, so that evaluators
+// created and destroyed level after level (the multi-scale driver) do not map and unmap their
+// buffers every time.  The device's default pool, which the host application may use itself, is
+// left untouched.  When the library's last live buffer on a device is freed, the pool is trimmed
+// and its memory goes back to the driver.  pool_malloc and pool_free complete before returning
+// (as cudaMalloc / cudaFree do), so no stream ordering leaks out of them.
+constexpr int kPoolMaxDevices = 64;
+
+struct DevicePool {
+    cudaMemPool_t pool = nullptr;
+    long long live = 0;            // buffers of this library currently allocated from the pool
+};
+
+inline std::mutex &pool_lock()
+{
+    static std::mutex m;
+    return m;
+}
+
+inline DevicePool *pool_table()
+{
+    static DevicePool t[kPoolMaxDevices];
+    return t;
+}
+
 inline cudaError_t pool_malloc(void **p, size_t bytes)
 {
-    static int configured_device = -1;
+    *p = nullptr;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (configured_device != dev) {
-        cudaMemPool_t pool;
-        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    if (dev < 0 || dev >= kPoolMaxDevices) return cudaErrorInvalidDevice;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> g(pool_lock());
+        DevicePool &dp = pool_table()[dev];
+        if (!dp.pool) {
+            cudaMemPoolProps props{};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            e = cudaMemPoolCreate(&dp.pool, &props);
+            if (e != cudaSuccess) {
+                dp.pool = nullptr;
+                return e;
+            }
             uint64_t keep = UINT64_MAX;
-            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            e = cudaMemPoolSetAttribute(dp.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            if (e != cudaSuccess) return e;
         }
-        cudaGetLastError();
-        configured_device = dev;
+        pool = dp.pool;
+        ++dp.live;
     }
-    e = cudaMallocAsync(p, bytes, 0);
+    e = cudaMallocFromPoolAsync(p, bytes, pool, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) {
+        std::lock_guard<std::mutex> g(pool_lock());
+        --pool_table()[dev].live;
+    }
+    return e;
+}
+
+// Frees without synchronising: the caller has made sure (one device synchronisation for many
+// buffers) that no work still uses p.  Trims the pool when its last buffer goes.
+inline cudaError_t pool_release(void *p)
+{
+    if (!p) return cudaSuccess;
+    cudaPointerAttributes at{};
+    cudaError_t e = cudaPointerGetAttributes(&at, p);
     if (e != cudaSuccess) return e;
-    return cudaStreamSynchronize(0);
+    e = cudaFreeAsync(p, 0);
+    if (e != cudaSuccess) return e;
+    const int dev = at.device;
+    if (dev >= 0 && dev < kPoolMaxDevices) {
+        std::lock_guard<std::mutex> g(pool_lock());
+        DevicePool &dp = pool_table()[dev];
+        if (dp.live > 0 && --dp.live == 0 && dp.pool) {
+            e = cudaStreamSynchronize(0);
+            if (e != cudaSuccess) return e;
+            e = cudaMemPoolTrimTo(dp.pool, 0);
+        }
+    }
+    return e;
 }
 
 inline cudaError_t pool_free(void *p)
@@ -43,7 +106,7 @@ inline cudaError_t pool_free(void *p)
     if (!p) return cudaSuccess;
     cudaError_t e = cudaDeviceSynchronize();                 // as cudaFree: no work still uses p
     if (e != cudaSuccess) return e;
-    e = cudaFreeAsync(p, 0);
+    e = pool_release(p);
     if (e != cudaSuccess) return e;
     return cudaStreamSynchronize(0);
 }

@@ -17,7 +17,11 @@
 //     calls that overlap on the GPU (different streams, no ordering) race on it;
 //   * the first call on each device looks up the scratch's device address with
 //     cudaGetSymbolAddress (once per device, under a lock); make that first call before
-//     any stream capture.
+//     any stream capture.  The address is cached for the life of the process: after a
+//     cudaDeviceReset (which unloads the module) the cached address is stale, so the entry
+//     point must not be used across a reset;
+//   * control_points must be 16-byte aligned (float4 loads), the images 4-byte and the
+//     result 8-byte aligned; misaligned buffers are rejected with SKM_ERR_INVALID.
 #include <cstdarg>
 #include <cstdio>
 #include <mutex>
@@ -175,6 +179,15 @@ extern "C" int skm_value_noalloc(int32_t dimensions, int32_t metric, const skm_g
         !control_points || !result)
         return noalloc_fail(SKM_ERR_INVALID, "NULL argument");
     if (!(sigma_c0 > 0.0) || !(sigma_c4 > 0.0)) return noalloc_fail(SKM_ERR_INVALID, "kernel parameters have to be positive");
+    // the kernels read control points as float4 (16-byte loads), images as float, the result as
+    // double: a misaligned buffer would fault on the device, so it is rejected here
+    if (reinterpret_cast<uintptr_t>(control_points) % 16 != 0)
+        return noalloc_fail(SKM_ERR_INVALID, "control_points must be 16-byte aligned (4 floats per control point)");
+    if (reinterpret_cast<uintptr_t>(fixed_image) % alignof(float) != 0 ||
+        reinterpret_cast<uintptr_t>(moving_coefficients) % alignof(float) != 0)
+        return noalloc_fail(SKM_ERR_INVALID, "fixed_image and moving_coefficients must be 4-byte aligned");
+    if (reinterpret_cast<uintptr_t>(result) % alignof(double) != 0)
+        return noalloc_fail(SKM_ERR_INVALID, "result must be 8-byte aligned");
     long long N = 1;
     for (int d = 0; d < D; ++d) {
         if (fixed_geometry->size[d] < 1 || cp_geometry->size[d] < 1 || moving_geometry->size[d] < 2 ||

@@ -931,12 +931,12 @@ inline int table_size_grids(TablePlan &pl)
 inline void table_free(TablePlan &pl)
 {
     float *f[] = {pl.d_tfwd, pl.d_tgemm, pl.d_kcp, pl.d_fixcp, pl.d_contrib};
-    if (pl.d_kcpo) pool_free(pl.d_kcpo);
+    if (pl.d_kcpo) pool_release(pl.d_kcpo);
     for (float *p : f)
-        if (p) pool_free(p);
-    if (pl.d_rec) pool_free(pl.d_rec);
-    if (pl.d_ucp) pool_free(pl.d_ucp);
-    if (pl.d_part) pool_free(pl.d_part);
+        if (p) pool_release(p);
+    if (pl.d_rec) pool_release(pl.d_rec);
+    if (pl.d_ucp) pool_release(pl.d_ucp);
+    if (pl.d_part) pool_release(pl.d_part);
     pl = TablePlan{};
 }
 

@@ -1243,13 +1243,13 @@ inline int table_derivative_gather_only(TablePlan &pl, const EvalParams &P, cons
 
 inline void table_tc_free(TcPlan &tc)
 {
-    if (tc.d_btr) pool_free(tc.d_btr);
-    if (tc.d_bcon) pool_free(tc.d_bcon);
-    if (tc.d_err) pool_free(tc.d_err);
-    if (tc.d_pairoff) pool_free(tc.d_pairoff);
-    if (tc.rp.p) pool_free(tc.rp.p);
+    if (tc.d_btr) pool_release(tc.d_btr);
+    if (tc.d_bcon) pool_release(tc.d_bcon);
+    if (tc.d_err) pool_release(tc.d_err);
+    if (tc.d_pairoff) pool_release(tc.d_pairoff);
+    if (tc.rp.p) pool_release(tc.rp.p);
     warp_tma_free(tc.wt);
-    if (tc.d_ctap) pool_free(tc.d_ctap);
+    if (tc.d_ctap) pool_release(tc.d_ctap);
     tc = TcPlan{};
 }
 

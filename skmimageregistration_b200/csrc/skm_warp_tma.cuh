@@ -328,7 +328,7 @@ inline int warp_tma_plan(WarpTmaPlan &wt, const TablePlan &pl, const EvalParams 
 
 inline void warp_tma_free(WarpTmaPlan &wt)
 {
-    if (wt.d_coefp) pool_free(wt.d_coefp);
+    if (wt.d_coefp) pool_release(wt.d_coefp);
     wt = WarpTmaPlan{};
 }
 

@@ -94,3 +94,25 @@ def test_no_cpu_fallback_without_device(lib):
     rc, msg = _create(pb)
     assert rc == abi.SKM_ERR_CUDA
     assert "no CPU fallback" in msg
+
+
+@pytest.mark.parametrize("which", ["control_points", "fixed_image", "result"])
+def test_noalloc_rejects_misaligned_buffers_before_launching(lib, which):
+    """skm_value_noalloc reads control points as float4: a buffer that is not 16-byte aligned
+    (and images / result not aligned to their element type) is rejected with SKM_ERR_INVALID
+    before any CUDA call, so this runs without a GPU."""
+    fp, dp = C.POINTER(C.c_float), C.POINTER(C.c_double)
+    lib.skm_value_noalloc.argtypes = [C.c_int32, C.c_int32, C.POINTER(abi.Geometry), fp, C.POINTER(abi.Geometry), fp,
+                                      C.POINTER(abi.Geometry), fp, C.c_double, C.c_double, dp, C.c_void_p]
+    lib.skm_value_noalloc.restype = C.c_int
+    buf = (C.c_double * 64)()                       # 8-byte aligned host storage standing in for device buffers
+    base = C.addressof(buf)
+    base += (-base) % 16                            # 16-byte aligned start
+    ptrs = dict(control_points=base, fixed_image=base, result=base)
+    ptrs[which] = base + {"control_points": 4, "fixed_image": 2, "result": 4}[which]
+    g = abi.Geometry.make([4, 4, 4])
+    rc = lib.skm_value_noalloc(3, abi.NCC, C.byref(g), C.cast(ptrs["fixed_image"], fp), C.byref(g),
+                               C.cast(base, fp), C.byref(g), C.cast(ptrs["control_points"], fp), 8.0, 4.0,
+                               C.cast(ptrs["result"], dp), None)
+    assert rc == abi.SKM_ERR_INVALID
+    assert "aligned" in lib.skm_last_error().decode()

@@ -13,7 +13,7 @@ import tempfile
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = "/root/reference"
+from oracle import REFERENCE as REF
 BUILD = os.path.join(ROOT, "tests", "_build")
 
 
