@@ -170,6 +170,18 @@ typedef struct skm_evaluator_info {
 } skm_evaluator_info;
 int skm_evaluator_describe(skm_evaluator *ev, skm_evaluator_info *out);
 
+/* Bounded-wait drill (no counterpart in the reference, whose kernels have no device-side waits).
+ * Every mbarrier wait of the tensor-core kernels gives up after a bounded time, after which the
+ * kernel waits (bounded) for its own copies and MMAs in flight, frees its tensor memory and
+ * returns, and the call reports SKM_ERR_TIMEOUT with its results discarded.  armed != 0 makes the
+ * next skm_get_value_and_derivative on this evaluator exercise that path: in the contrib GEMM,
+ * the first block's first producer group withholds one shared-memory stage that nothing else
+ * depends on, and the waits of that launch give up after 5 ms instead of 2 s.  The call then
+ * returns SKM_ERR_TIMEOUT; the drill disarms itself and the evaluator stays usable.  Only on the
+ * tensor-core table path (SKM_ERR_UNSUPPORTED otherwise); calls through skm_metric_evaluate or
+ * the optimizer replay graphs captured without the drill and are unaffected. */
+int skm_evaluator_wait_drill(skm_evaluator *ev, int32_t armed);
+
 /* GpuKernelEvaluator::SetRegularizerRKHS/RD/PG (GpuEvaluator.h:156-158,
  * GpuEvaluator.cu:786-831).  weight <= 0 switches the term off. */
 int skm_set_regularizer_rkhs(skm_evaluator *ev, double weight);
@@ -397,6 +409,63 @@ int skm_warp_image(int32_t dimensions, const skm_geometry *image_geometry, const
 /* JacobianDeterminant (include/itkUtils.h:153-161): det(I + du/dx) per texel with central
  * differences over 2 spacing, edge texels repeated.  field: N x D doubles (AoS), out: N. */
 int skm_jacobian_determinant(int32_t dimensions, const skm_geometry *geometry, const double *field, double *out);
+
+/* ------------------------------------------------------------------------- */
+/* Batched registration of many image pairs (no counterpart in the reference, which evaluates one
+ * pair per GpuKernelEvaluator, include/cuda/GpuEvaluator.cu:30-91, and one call per optimizer
+ * iteration, GpuEvaluator.cu:361-714, driven by the ITK v4 loop).
+ *
+ * Each pair has its own images, control-point grid, metric (MSE or NCC, with any of the
+ * RKHS / RD / PG / L1 / L2 / L2,1 terms) and adaptive-step optimizer; pairs may differ in size.
+ * One optimizer iteration of ALL pairs is one launch of one persistent kernel (captured in a CUDA
+ * graph): its phases (pack, transform, warp + statistics, statistics, contribution GEMM, gather +
+ * regularizers + step, result) are separated by bounded grid barriers, and the work items of each
+ * phase (bricks of cells, chunks of texels, blocks of control points over all pairs) are handed out
+ * by a device work queue.  The launch shape (transform brick, cells per thread along z, texels per
+ * warp-phase item, blocks per SM) is chosen at creation by timing the candidates on the batch
+ * itself.  Every pair must take the phase-table path (3-D, stationary kernel, control spacing an
+ * integer multiple of the voxel spacing, subsample 1, no displacement field) with the same phase
+ * counts (2 or 4 phases along z); SKM_ERR_UNSUPPORTED otherwise.  Results of each pair equal a
+ * single-pair evaluation within FP32 rounding; sums are taken in a fixed order (deterministic). */
+typedef struct skm_batch_pair {
+    const skm_evaluator_desc *evaluator;  /* images and kernel of the pair (borrowed for the call) */
+    skm_metric_desc    metric;
+    skm_optimizer_desc optimizer;
+    const double      *initial_parameters;  /* planar C*D, or NULL for zeros */
+    const double      *cpw;                 /* C control-point weights, or NULL for ones */
+} skm_batch_pair;
+
+typedef struct skm_batch_info {
+    int32_t pairs;
+    int64_t fixed_texels;             /* sum over the pairs */
+    int64_t control_points;
+    int32_t grid;                     /* persistent CTAs */
+    int32_t ctas_per_sm;
+    int32_t transform_tile[3];        /* cells per transform brick along x, y; cells per thread along z */
+    int32_t warp_chunk;               /* texels per warp-phase item */
+    int32_t items[8];                 /* work items per phase over all pairs */
+    int32_t shared_memory;            /* dynamic shared memory per CTA, bytes */
+    double  tuned_ms;                 /* the chosen shape's time for one evaluation of the batch */
+    int32_t candidates;               /* shapes the autotuner timed */
+} skm_batch_info;
+
+typedef struct skm_batch skm_batch;
+
+int skm_batch_create(int32_t npairs, const skm_batch_pair *pairs, skm_batch **out);
+int skm_batch_destroy(skm_batch *b);
+/* One evaluation of every pair at its current parameters (value and derivative, no step). */
+int skm_batch_evaluate(skm_batch *b);
+/* `iterations` optimizer iterations of every pair (one graph launch each); run waits, enqueue does
+ * not (stream_out, if not NULL, receives the batch's cudaStream_t for event timing). */
+int skm_batch_run(skm_batch *b, int32_t iterations);
+int skm_batch_enqueue(skm_batch *b, int32_t iterations, void *stream_out);
+/* Replace a pair's position (planar C*D) and/or weights (C); NULL leaves either unchanged. */
+int skm_batch_set_parameters(skm_batch *b, int32_t pair, const double *params, const double *cpw);
+/* The pair's last evaluation: metric values and (negated, regularized) derivative, planar C*D. */
+int skm_batch_get_result(skm_batch *b, int32_t pair, skm_metric_values *values, double *derivative);
+int skm_batch_get_parameters(skm_batch *b, int32_t pair, int32_t best, double *params);
+int skm_batch_get_state(skm_batch *b, int32_t pair, skm_optimizer_state *out);
+int skm_batch_describe(skm_batch *b, skm_batch_info *out);
 
 /* ------------------------------------------------------------------------- */
 /* Metric value without any device allocation.  No counterpart in the reference.

@@ -279,3 +279,38 @@ def field(data, geometry):
         f.data = dptr(data)
         f.geometry = geometry
     return f
+
+
+class BatchPair(C.Structure):
+    """skm_batch_pair: one pair of a batched registration."""
+
+    _fields_ = [
+        ("evaluator", C.POINTER(EvaluatorDesc)),
+        ("metric", MetricDesc),
+        ("optimizer", OptimizerDesc),
+        ("initial_parameters", C.POINTER(C.c_double)),
+        ("cpw", C.POINTER(C.c_double)),
+    ]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [
+        ("pairs", C.c_int32),
+        ("fixed_texels", C.c_int64),
+        ("control_points", C.c_int64),
+        ("grid", C.c_int32),
+        ("ctas_per_sm", C.c_int32),
+        ("transform_tile", C.c_int32 * 3),
+        ("warp_chunk", C.c_int32),
+        ("items", C.c_int32 * 8),
+        ("shared_memory", C.c_int32),
+        ("tuned_ms", C.c_double),
+        ("candidates", C.c_int32),
+    ]
+
+    def as_dict(self):
+        out = {}
+        for k, _ in self._fields_:
+            v = getattr(self, k)
+            out[k] = list(v) if hasattr(v, "__len__") else v
+        return out

@@ -6,6 +6,7 @@
 //   [pack] -> [grid shifts] -> value pass -> statistics -> derivative+regularizers -> result
 // on the stream and copies the scalars and the derivative back.  Every reduction is
 // done on the device in a fixed order; no host loops over per-voxel arrays remain.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -112,6 +113,7 @@ unsigned long long rng_advance_host(unsigned long long s, unsigned long long ste
 constexpr int kValueThreads = 256;
 constexpr int kDerivThreads = 256;     // 8 warps = 8 control points per block
 constexpr int kSplitBelowBlocks = 1024; // fewer derivative blocks than this: one block per control point
+constexpr unsigned long long kDrillWaitNs = 5000000ull;   // bounded-wait limit during the wait drill: 5 ms
 
 }  // namespace
 
@@ -161,6 +163,9 @@ struct skm_evaluator {
     bool mg_deriv = false;
     int mg_path = 0;
     const double *mg_df = nullptr;
+
+    // armed by skm_evaluator_wait_drill: the next skm_get_value(_and_derivative) runs the drill
+    bool drill_armed = false;
 
     ~skm_evaluator()
     {
@@ -539,6 +544,16 @@ extern "C" int skm_evaluator_describe(skm_evaluator *e, skm_evaluator_info *out)
     return SKM_OK;
 }
 
+extern "C" int skm_evaluator_wait_drill(skm_evaluator *e, int32_t armed)
+{
+    if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
+    if (armed && active_path(e) != 3)
+        return fail(SKM_ERR_UNSUPPORTED, "the wait drill needs the tensor-core table path (active path %d)",
+                    active_path(e));
+    e->drill_armed = armed != 0;
+    return SKM_OK;
+}
+
 extern "C" int skm_set_regularizer_rkhs(skm_evaluator *e, double w)
 {
     if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
@@ -795,7 +810,18 @@ static int evaluate_common(skm_evaluator *e, int32_t metric, const double *cp, c
     w.rd_scaling = e->rd_scaling;
     w.pg = e->reg_pg > 0 ? e->reg_pg : 0.0;
     w.pg_scaling = e->pg_scaling;
-    if ((rc = run_evaluation(e, metric, derivatives != nullptr, w, nullptr))) return rc;
+    const bool drill = e->drill_armed && derivatives != nullptr && active_path(e) == 3 && metric != SKM_LCC;
+    if (drill) {                      // one launch of the contrib kernel runs the wait drill
+        e->tc.dev.drill = 1;
+        e->tc.dev.wait_ns = kDrillWaitNs;
+    }
+    rc = run_evaluation(e, metric, derivatives != nullptr, w, nullptr);
+    if (drill) {
+        e->tc.dev.drill = 0;
+        e->tc.dev.wait_ns = tc::kTcWaitNs;
+        e->drill_armed = false;
+    }
+    if (rc) return rc;
     if ((rc = fetch(e, derivatives))) return rc;
     if (out) {
         out->measure = e->h_out[O_MEASURE];
@@ -1013,3 +1039,4 @@ extern "C" int skm_bspline_coefficients(int32_t D, const int32_t *size, const do
 
 #include "skm_optimizer.cuh"
 #include "skm_driver.cuh"
+#include "skm_batch.cuh"

@@ -104,6 +104,9 @@ struct TcDev {
     int con_stride, con_cols;
     const float *bcon;       // npc rows x kpc, K-major 128-byte swizzled: hi, then lo
     unsigned *err;           // sticky failure word of the bounded waits (read and reset by the host)
+    unsigned long long wait_ns;  // contrib: limit of one bounded wait (2 s; shortened by the wait drill)
+    int drill;               // contrib: CTA 0's first producer group withholds its first stage from the
+                             // MMA thread, whose wait for it then runs out (skm_evaluator_wait_drill)
 };
 
 // mbarriers of one CTA: full[s] producers -> MMA (kTcProdThreads arrivals), empty[s] MMA ->
@@ -595,7 +598,7 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
             for (; g < nch; ++g) {
                 const int slot = (int)(g % NR);
                 // slot g % NR is free once its producer group has left chunk g - NR
-                if (g >= NR && !tc::mbar_wait(&B.region_empty[slot], (uint32_t)((g / NR - 1) & 1), abort)) {
+                if (g >= NR && !tc::mbar_wait(&B.region_empty[slot], (uint32_t)((g / NR - 1) & 1), abort, C.wait_ns)) {
                     tc_fail(abort, C.err);
                     break;
                 }
@@ -630,8 +633,8 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
             const long long cell0 = tile * ct;
             const int s = (int)(g % NS);
             bool ok = true;
-            if (g >= (unsigned)NS) ok = tc::mbar_wait(&B.empty[s], ((g / NS) + 1) & 1, abort);
-            if (NR > 0 && ok) ok = tc::mbar_wait(&B.region[g % NR], (g / NR) & 1, abort);   // the records
+            if (g >= (unsigned)NS) ok = tc::mbar_wait(&B.empty[s], ((g / NS) + 1) & 1, abort, C.wait_ns);
+            if (NR > 0 && ok) ok = tc::mbar_wait(&B.region[g % NR], (g / NR) & 1, abort, C.wait_ns);   // the records
             if (tc::bar_or(kTcGroupBar + grp, kTcGroupThreads, !ok)) {
                 if (gt == 0) tc_fail(abort, C.err);
                 failed = true;
@@ -705,7 +708,9 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
                 if (gt == 0) tc::mbar_arrive(&B.region_empty[g % NR]);
             }
             tc::fence_proxy_async();
-            tc::mbar_arrive(&B.full[s]);
+            // the wait drill: CTA 0 withholds stage 0 of its first chunk (no MMA, no copy depends on
+            // it), so the MMA thread's first wait runs out and every role leaves through its error path
+            if (!(C.drill && blockIdx.x == 0 && g == 0)) tc::mbar_arrive(&B.full[s]);
         }
     } else if (warp == kConMmaWarp) {
         // ---------------- MMA issue (one thread) ----------------
@@ -719,7 +724,7 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
                 const long long tile = blockIdx.x + (long long)it * gridDim.x;
                 if (tile >= ntiles) break;
                 const int b = it & 1;
-                if (it >= 2 && !tc::mbar_wait(&B.acc_empty[b], ((it >> 1) + 1) & 1, abort)) {
+                if (it >= 2 && !tc::mbar_wait(&B.acc_empty[b], ((it >> 1) + 1) & 1, abort, C.wait_ns)) {
                     tc_fail(abort, C.err);
                     break;
                 }
@@ -727,7 +732,7 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
                 bool failed = false;
                 for (int kc = 0; kc < nchunk; ++kc, ++g) {
                     const int s = (int)(g % NS);
-                    if (!tc::mbar_wait(&B.full[s], (g / NS) & 1, abort)) {
+                    if (!tc::mbar_wait(&B.full[s], (g / NS) & 1, abort, C.wait_ns)) {
                         tc_fail(abort, C.err);
                         failed = true;
                         break;
@@ -766,7 +771,7 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
             if (tile >= ntiles) break;
             const int b = it & 1;
             // warp-uniform decision: tcgen05.ld below is a warp-wide instruction
-            if (!__all_sync(0xffffffffu, tc::mbar_wait(&B.acc_full[b], (it >> 1) & 1, abort))) {
+            if (!__all_sync(0xffffffffu, tc::mbar_wait(&B.acc_full[b], (it >> 1) & 1, abort, C.wait_ns))) {
                 if (lane == 0) tc_fail(abort, C.err);
                 break;
             }
@@ -1063,6 +1068,8 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
     C.bcon = tc.d_bcon;
     C.pairoff = tc.d_pairoff;
     C.err = tc.d_err;
+    C.wait_ns = tc::kTcWaitNs;
+    C.drill = 0;
     pl.dev.tc_err = tc.d_err;
 
     // weighted control-point planes and the tiled load of a brick's region from them

@@ -184,7 +184,8 @@ __device__ __forceinline__ unsigned long long globaltimer()
 // carries a suspend-time hint: a waiting thread sleeps in hardware until the phase completes (or
 // the hint elapses) instead of spinning, so waiting roles leave the issue slots to working ones.
 constexpr uint32_t kTcSuspendNs = 20000;
-__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, const volatile int *abort = nullptr)
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, const volatile int *abort = nullptr,
+                                          unsigned long long limit_ns = kTcWaitNs)
 {
     const uint32_t a = smem_addr(mbar);
     unsigned long long t0 = 0;
@@ -201,7 +202,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, const
         if (abort && *abort) return false;
         const unsigned long long t = globaltimer();
         if (i == 0) t0 = t;
-        else if (t - t0 > kTcWaitNs) return false;
+        else if (t - t0 > limit_ns) return false;
     }
     return false;
 }

@@ -49,6 +49,7 @@ def lib():
         L.skm_evaluator_destroy.argtypes = [C.c_void_p]
         L.skm_evaluator_describe.argtypes = [C.c_void_p, C.POINTER(EvaluatorInfo)]
         L.skm_evaluator_path.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
+        L.skm_evaluator_wait_drill.argtypes = [C.c_void_p, C.c_int32]
         L.skm_set_regularizer_rkhs.argtypes = [C.c_void_p, C.c_double]
         L.skm_set_regularizer_rd.argtypes = [C.c_void_p, C.c_double, C.c_double]
         L.skm_set_regularizer_pg.argtypes = [C.c_void_p, C.c_double, C.c_double]
@@ -80,6 +81,16 @@ def lib():
         L.skm_warp_image.argtypes = [C.c_int32, C.POINTER(abi.Geometry), _dp, C.POINTER(abi.Geometry), _dp, C.c_int32,
                                      C.c_double, _dp]
         L.skm_jacobian_determinant.argtypes = [C.c_int32, C.POINTER(abi.Geometry), _dp, _dp]
+        L.skm_batch_create.argtypes = [C.c_int32, C.POINTER(abi.BatchPair), C.POINTER(C.c_void_p)]
+        L.skm_batch_destroy.argtypes = [C.c_void_p]
+        L.skm_batch_evaluate.argtypes = [C.c_void_p]
+        L.skm_batch_run.argtypes = [C.c_void_p, C.c_int32]
+        L.skm_batch_enqueue.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.skm_batch_set_parameters.argtypes = [C.c_void_p, C.c_int32, _dp, _dp]
+        L.skm_batch_get_result.argtypes = [C.c_void_p, C.c_int32, C.POINTER(MetricValues), _dp]
+        L.skm_batch_get_parameters.argtypes = [C.c_void_p, C.c_int32, C.c_int32, _dp]
+        L.skm_batch_get_state.argtypes = [C.c_void_p, C.c_int32, C.POINTER(OptimizerState)]
+        L.skm_batch_describe.argtypes = [C.c_void_p, C.POINTER(abi.BatchInfo)]
         _lib = L
     return _lib
 
@@ -145,6 +156,11 @@ class GpuKernelEvaluator:
         info = EvaluatorInfo()
         check(lib().skm_evaluator_describe(self.h, C.byref(info)))
         return info.as_dict()
+
+    def wait_drill(self, armed=True):
+        """Arm the bounded-wait drill: the next getValueAndDerivative on the tensor-core table path
+        makes one wait of the contrib GEMM run out and raises SkmError(SKM_ERR_TIMEOUT)."""
+        check(lib().skm_evaluator_wait_drill(self.h, int(bool(armed))))
 
     # --- GpuEvaluator.h:156-158
     def SetRegularizerRKHS(self, weight):
@@ -268,6 +284,85 @@ class Optimizer:
     def close(self):
         if getattr(self, "h", None):
             lib().skm_optimizer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many registration pairs in one persistent kernel per optimizer iteration (skm_batch_*).
+
+    problems: list of Problem; metrics / optimizers: one MetricDesc / OptimizerDesc per pair (or one
+    for all); initial: planar parameters per pair (None: zeros); cpws: weights per pair (None: ones).
+    """
+
+    def __init__(self, problems, metrics, optimizers, initial=None, cpws=None):
+        n = len(problems)
+        metrics = metrics if isinstance(metrics, (list, tuple)) else [metrics] * n
+        optimizers = optimizers if isinstance(optimizers, (list, tuple)) else [optimizers] * n
+        self.problems = list(problems)
+        self._descs = [pb.desc() for pb in self.problems]
+        self._keep = []
+        arr = (abi.BatchPair * n)()
+        for i, pb in enumerate(self.problems):
+            arr[i].evaluator = C.pointer(self._descs[i])
+            arr[i].metric = metrics[i]
+            arr[i].optimizer = optimizers[i]
+            p0 = None if initial is None or initial[i] is None else np.ascontiguousarray(initial[i], np.float64)
+            w0 = None if cpws is None or cpws[i] is None else np.ascontiguousarray(cpws[i], np.float64)
+            self._keep += [p0, w0]
+            arr[i].initial_parameters = dptr(p0)
+            arr[i].cpw = dptr(w0)
+        h = C.c_void_p()
+        check(lib().skm_batch_create(n, arr, C.byref(h)))
+        self.h = h
+
+    def evaluate(self):
+        """One value + derivative evaluation of every pair at its current parameters (no step)."""
+        check(lib().skm_batch_evaluate(self.h))
+
+    def run(self, iterations):
+        check(lib().skm_batch_run(self.h, int(iterations)))
+
+    def enqueue(self, iterations):
+        """Enqueue optimizer iterations without waiting; returns the batch's cudaStream_t."""
+        s = C.c_void_p()
+        check(lib().skm_batch_enqueue(self.h, int(iterations), C.byref(s)))
+        return s.value
+
+    def set_parameters(self, pair, params=None, cpw=None):
+        p = None if params is None else np.ascontiguousarray(params, np.float64)
+        w = None if cpw is None else np.ascontiguousarray(cpw, np.float64)
+        check(lib().skm_batch_set_parameters(self.h, int(pair), dptr(p), dptr(w)))
+
+    def result(self, pair):
+        v = MetricValues()
+        g = np.zeros(self.problems[pair].num_parameters)
+        check(lib().skm_batch_get_result(self.h, int(pair), C.byref(v), dptr(g)))
+        return v.as_dict(), g
+
+    def parameters(self, pair, best=False):
+        out = np.zeros(self.problems[pair].num_parameters)
+        check(lib().skm_batch_get_parameters(self.h, int(pair), int(bool(best)), dptr(out)))
+        return out
+
+    def state(self, pair):
+        s = OptimizerState()
+        check(lib().skm_batch_get_state(self.h, int(pair), C.byref(s)))
+        return s.as_dict()
+
+    def describe(self):
+        i = abi.BatchInfo()
+        check(lib().skm_batch_describe(self.h, C.byref(i)))
+        return i.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().skm_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

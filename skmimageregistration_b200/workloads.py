@@ -49,3 +49,37 @@ def make(name="ncc128", seed=0, coefficients=None):
                 cp_spacing_voxels=w["cp_spacing"], metric=w["metric"], reg_rd=w["rd"], reg_l1=w["l1"],
                 subsample=w["subsample"], seed=seed)
     return pb, m, o, info
+
+
+def make_batch(n=64, seed=0, bases=4, lo=(64, 64, 64), hi=(160, 160, 128), coefficients=None):
+    """Batched workload: `n` config-2-style pairs with sizes uniform in [lo, hi] (X, Y, Z voxels).
+
+    Each pair is a crop (same box in both images, so the registration problem is intact) of one of
+    `bases` seeded 160x160x128 ellipsoid pairs (6 ellipsoids over a smooth background + N(0, 0.02),
+    sliding shear + Wendland displacement), rescaled to [0, 1]; control spacing 4 voxels, support
+    12 voxels; even pairs NCC, odd pairs MSE, both with RD 1e-3.  Returns (problems, metric
+    descriptors, optimizer descriptor, info dict)."""
+    rng = np.random.default_rng(seed)
+    base = [synth.ellipsoids3d(seed=seed * 1000 + k, shape=(hi[2], hi[1], hi[0]))[:2] for k in range(bases)]
+    if coefficients is None:
+        from .evaluator import bspline_coefficients as coefficients
+    problems, metrics, sizes = [], [], []
+    for i in range(n):
+        size = [int(rng.integers(lo[d], hi[d] + 1)) for d in range(3)]        # X, Y, Z
+        off = [int(rng.integers(0, hi[d] - size[d] + 1)) for d in range(3)]
+        fixed, moving = base[int(rng.integers(0, bases))]
+        sl = (slice(off[2], off[2] + size[2]), slice(off[1], off[1] + size[1]), slice(off[0], off[0] + size[0]))
+        f = np.ascontiguousarray(fixed[sl])
+        m = np.ascontiguousarray(moving[sl])
+        pb = Problem(fixed=f, moving_coefficients=coefficients(m), spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0),
+                     sigma_c0=24.0, sigma_c4=12.0, cp_spacing=4.0, subsample=1, subsample_neighborhood=1)
+        problems.append(pb)
+        metrics.append(MetricDesc.make("ncc" if i % 2 == 0 else "mse", rd=1e-3))
+        sizes.append(size)
+    o = OptimizerDesc.make(a=1.0, number_of_iterations=1 << 30)
+    texels = int(sum(np.prod(s) for s in sizes))
+    info = dict(workload="batch%d" % n, pairs=n, sizes="uniform %dx%dx%d .. %dx%dx%d" % (tuple(lo) + tuple(hi)),
+                total_voxels=texels, metrics="NCC (even pairs) / MSE (odd pairs), RD 1e-3",
+                control_points=int(sum(pb.C for pb in problems)), cp_spacing_voxels=4.0, support_voxels=12.0,
+                seed=seed)
+    return problems, metrics, o, info

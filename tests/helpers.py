@@ -58,3 +58,15 @@ def max_rel(a, b):
     """max |a-b| relative to max |b| (norm-wise relative error of a field)."""
     a = np.asarray(a); b = np.asarray(b)
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def componentwise_rel(a, b, floor=1e-3):
+    """Largest componentwise relative error |a_i - b_i| / |b_i| over the components whose
+    reference magnitude |b_i| exceeds `floor` * max |b| (a small component can then not hide
+    behind the largest one, as it can in the norm-wise max_rel)."""
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    sel = np.abs(b) > floor * np.max(np.abs(b))
+    if not np.any(sel):
+        return 0.0
+    return float(np.max(np.abs(a[sel] - b[sel]) / np.abs(b[sel])))

@@ -1,4 +1,5 @@
-"""Pair-parallel scheduling on CPU: assignment properties and a world_size-2 gloo run."""
+"""Pair-parallel scheduling on CPU: assignment properties and a world_size-2 gloo run in which
+each rank registers its pairs for real (FP64 oracle evaluator and optimizer)."""
 import os
 import socket
 
@@ -39,39 +40,68 @@ def _free_port():
     return port
 
 
+# small 2-D pairs of uneven sizes, registered for real on the CPU by the FP64 restatement of the
+# evaluator and of the adaptive-step optimizer (the oracle), so that each rank does actual work
+PAIR_SHAPES = [(22, 24), (30, 26), (24, 34), (28, 28), (20, 36), (34, 30)]
+PAIR_ITERS = 6
+
+
+def _register_pair(i):
+    """One pair: NCC + RD, control spacing 2, PAIR_ITERS optimizer iterations (FP64 oracle)."""
+    from helpers import make_problem
+    from oracle import oracle as O
+    from skmimageregistration_b200.abi import MetricDesc, OptimizerDesc
+    pb, _, _ = make_problem(2, shape=PAIR_SHAPES[i], seed=100 + i, sigma_c4=4.0, sigma_c0=8.0, cp_spacing=2.0,
+                            spacing=(1.0, 1.0), origin=(0.0, 0.0))
+    orc = O.Oracle(pb)
+    m = MetricDesc.make("ncc", rd=1e-3)
+    o = OptimizerDesc.make(a=200.0, number_of_iterations=PAIR_ITERS)
+    opt = O.OracleOptimizer(orc, o, m, np.zeros(pb.num_parameters), np.ones(pb.C))
+    vals = opt.run(PAIR_ITERS)
+    out = {"first_value": float(vals[0]), "best_value": float(opt.state.best_value), "iterations": PAIR_ITERS,
+           "best_checksum": float(np.sum(opt.best * np.arange(1, opt.best.size + 1)))}
+    orc.close()
+    return out
+
+
 def _worker(rank, world, port, costs, q):
     import datetime
+    import sys
     import torch.distributed as dist
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
-        def register(i):
-            # stand-in for a registration: deterministic per pair, independent of the rank
-            return {"value": -1.0 / (1.0 + i), "iterations": 10 + i}
-        out = run_pairs(costs, register, rank, world)
+        out = run_pairs(costs, _register_pair, rank, world)
         q.put((rank, out))
     finally:
         dist.destroy_process_group()
 
 
-def test_gloo_world2_gathers_all_results():
-    costs = [pair_cost(s) for s in _sizes(10, seed=3)]
+def test_gloo_world2_registers_pairs_and_gathers_all_results():
+    costs = [pair_cost(s + (1,), cp_spacing_voxels=2.0, support_voxels=4.0, D=2) for s in PAIR_SHAPES]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
     procs = [ctx.Process(target=_worker, args=(r, 2, port, costs, q)) for r in range(2)]
     for p in procs:
         p.start()
-    res = dict(q.get(timeout=120) for _ in range(2))
+    res = dict(q.get(timeout=300) for _ in range(2))
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
     a = assign_pairs(costs, 2)
+    assert all(a)                                          # both ranks registered pairs
+    # the same registrations run in this process, one after the other
+    single = {i: _register_pair(i) for i in range(len(PAIR_SHAPES))}
     for rank in (0, 1):
         out = res[rank]
-        assert [r["pair"] for r in out] == list(range(len(costs)))
+        assert [r["pair"] for r in out] == list(range(len(PAIR_SHAPES)))
         for r in out:
-            assert r["value"] == pytest.approx(-1.0 / (1.0 + r["pair"]))
             assert r["pair"] in a[r["rank"]]
+            ref = single[r["pair"]]
+            assert r["best_value"] < r["first_value"]      # the optimizer made progress on every pair
+            for k in ("first_value", "best_value", "best_checksum"):
+                assert r[k] == ref[k], (r, ref)          # deterministic: bitwise the single-process run
     assert res[0] == res[1]

@@ -260,3 +260,21 @@ def test_table_path_fused_step_best_parameters(case, orthant):
         assert max_rel(opt.parameters(), oo.position) <= 1e-3
         assert max_rel(opt.parameters(best=True), oo.best) <= 1e-3
         assert max_rel(opt.parameters(best=True), opt_generic.parameters(best=True)) <= 1e-3
+
+
+# LCC with the anisotropic (weight-tensor) kernel: the 3-D derivative keeps the reference's
+# form (neighbour covariance at both ends of k(c_i, n), no control-point weight w_i;
+# GpuEvaluatorLCC.cu:206-530), so the weights are random here and still must match
+@pytest.mark.parametrize("D,shape,cp_spacing", [(2, (48, 52), 1.5), (3, (20, 21, 22), 2.0)])
+@pytest.mark.parametrize("kind", ["weight_tensor", "weight_image"])
+def test_lcc_nonstationary_larger(D, shape, cp_spacing, kind):
+    pb, cp, cpw = make_problem(D, kind, subsample=2, nbh=2, shape=shape, seed=43, sigma_c4=3.0, sigma_c0=6.0,
+                               cp_spacing=cp_spacing)
+    ev = GpuKernelEvaluator(pb)
+    orc = O.Oracle(pb)
+    for call in range(2):                               # the second call redraws the sample shifts
+        r, g = ev.getValueAndDerivative(abi.LCC, cp, cpw)
+        ro, go = orc.evaluate(abi.LCC, cp, cpw)
+        assert r["num_pixels_counted"] == ro["num_pixels_counted"]
+        assert rel_err(r["measure"], ro["measure"]) <= TOL_VALUE
+        assert max_rel(g, go) <= TOL_DERIV

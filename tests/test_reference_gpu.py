@@ -88,3 +88,20 @@ def test_displacement_field_matches_reference_evaluator(D):
     rng = np.random.default_rng(1)
     df = rng.normal(0, 0.5, (pb.n_texels, D))
     assert max_rel(ev.evaluateDisplacementField(cp, cpw, df), ref.displacement_field(cp, cpw, df)) <= 1e-5
+
+
+@pytest.mark.parametrize("D,shape,cp_spacing", [(2, (48, 52), 1.5), (3, (24, 24, 24), 2.0)])
+@pytest.mark.parametrize("kind", ["weight_tensor", "weight_image"])
+def test_lcc_nonstationary_matches_reference_evaluator(D, shape, cp_spacing, kind):
+    """LCC over the anisotropic and the weight-image kernels (config 3's combination is the
+    anisotropic one) at 24^3, subsample 2, neighbourhood stride 2, random control-point weights."""
+    pb, cp, cpw = make_problem(D, kind, subsample=2, nbh=2, shape=shape, seed=109, sigma_c4=3.0, sigma_c0=6.0,
+                               cp_spacing=cp_spacing)
+    ref = _ref(pb)
+    ev = GpuKernelEvaluator(pb)
+    for call in range(2):
+        r, g = ev.getValueAndDerivative(abi.LCC, cp, cpw)
+        rr, gr = ref.evaluate(abi.LCC, cp, cpw)
+        assert r["num_pixels_counted"] == rr["num_pixels_counted"]
+        assert rel_err(r["measure"], rr["measure"]) <= 1e-5
+        assert max_rel(g, gr) <= 1e-4
