@@ -367,6 +367,15 @@ typedef struct skm_register_desc {
      * during the call) -- the df-full-<level> checkpoint SKMReg writes (src/SKMReg.cxx:468). */
     void (*level_done)(int32_t level, const double *displacement, void *user);
     void *level_user;
+    /* learned warm start (no counterpart in the reference): planar C*D kernel weights alpha that the
+     * first level run starts from instead of zeros (count must equal that level's C*D, else
+     * SKM_ERR_INVALID); NULL = zeros.  With num_function_evaluations of that level 0 the weights are
+     * used as they are. */
+    const double *first_level_parameters;
+    int64_t first_level_parameter_count;
+    /* optional: called after every level with its best kernel weights (planar C*D, valid during the
+     * call) -- the labels the warm-start network is trained on. */
+    void (*level_parameters)(int32_t level, const double *parameters, int64_t count, void *user);
 } skm_register_desc;
 
 typedef struct skm_register_report {

@@ -214,6 +214,7 @@ MAX_SCALES = 8
 
 
 LEVEL_CALLBACK = C.CFUNCTYPE(None, C.c_int32, C.POINTER(C.c_double), C.c_void_p)
+PARAMS_CALLBACK = C.CFUNCTYPE(None, C.c_int32, C.POINTER(C.c_double), C.c_int64, C.c_void_p)
 
 
 class RegisterDesc(C.Structure):
@@ -241,6 +242,9 @@ class RegisterDesc(C.Structure):
         ("initial_displacement", C.POINTER(C.c_double)),
         ("level_done", LEVEL_CALLBACK),
         ("level_user", C.c_void_p),
+        ("first_level_parameters", C.POINTER(C.c_double)),
+        ("first_level_parameter_count", C.c_int64),
+        ("level_parameters", PARAMS_CALLBACK),
     ]
 
 

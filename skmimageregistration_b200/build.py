@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libskm_b200.so")
-SOURCES = ["csrc/skm_capi.cu", "csrc/skm_noalloc.cu"]
+SOURCES = ["csrc/skm_capi.cu", "csrc/skm_noalloc.cu", "csrc/skm_conv.cu"]
 
 def deps():
     """Every source the library is compiled from: all of csrc/ and the C headers."""

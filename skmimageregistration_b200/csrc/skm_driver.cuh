@@ -528,6 +528,12 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
         control_grid(D, *geometry, cps, cpg);
         const long long C = texel_count(D, cpg.size);
         std::vector<double> cpw((size_t)C, 1.0), params((size_t)C * D, 0.0), best((size_t)C * D);
+        if (r->first_level_parameters && s == first) {             // learned warm start of the first level run
+            if (r->first_level_parameter_count != C * D)
+                return fail(SKM_ERR_INVALID, "first_level_parameters: %lld values, the level has %lld",
+                            (long long)r->first_level_parameter_count, C * D);
+            std::memcpy(params.data(), r->first_level_parameters, sizeof(double) * C * D);
+        }
 
         skm_evaluator_desc ed{};
         ed.dimensions = D;
@@ -646,6 +652,7 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
             skm_evaluator_destroy(ev);
             return rc;
         }
+        if (r->level_parameters) r->level_parameters(s, best.data(), C * D, r->level_user);
         // summed displacement field on the reference grid (SKMReg.cxx:452-460): planar -> AoS
         std::vector<double> cp_aos((size_t)C * D);
         for (long long i = 0; i < C; ++i)

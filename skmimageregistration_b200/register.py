@@ -87,7 +87,8 @@ def make_desc(config, D) -> RegisterDesc:
 
 
 def register(reference, target, spacing=None, origin=None, config=None, guidance_image=None, weight_tensor=None,
-             weight_image=None, initial_displacement=None, on_level=None):
+             weight_image=None, initial_displacement=None, on_level=None, first_level_parameters=None,
+             on_level_parameters=None):
     """Registers `reference` (moving) onto `target` (fixed); both arrays (Z, Y, X) or (Y, X) with
     the same geometry.  Returns (displacement (..., D) on that grid, report dict).
 
@@ -100,7 +101,11 @@ def register(reference, target, spacing=None, origin=None, config=None, guidance
     Restart (config "restart_at" > 1, src/SKMReg.cxx:96-123): `initial_displacement` (..., D) is
     the summed field after level restart_at - 1; without it every level runs.  `on_level(level,
     displacement)` is called after each level with a copy of the summed field so far (the
-    df-full-<level> checkpoint of the reference)."""
+    df-full-<level> checkpoint of the reference).
+
+    Learned warm start: `first_level_parameters` (planar C*D kernel weights of the first level run's
+    control-point grid) replace the zero start of that level; `on_level_parameters(level, alpha)`
+    receives each level's best kernel weights (the warm-start network's labels)."""
     ref = np.ascontiguousarray(reference, np.float64)
     tar = np.ascontiguousarray(target, np.float64)
     if ref.shape != tar.shape:
@@ -124,6 +129,16 @@ def register(reference, target, spacing=None, origin=None, config=None, guidance
             on_level(int(level), np.ctypeslib.as_array(ptr, shape=ref.shape + (D,)).copy())
         desc.level_done = abi.LEVEL_CALLBACK(_level)
         keep.append(desc.level_done)
+    if first_level_parameters is not None:              # learned warm start of the first level run
+        p0 = np.ascontiguousarray(first_level_parameters, np.float64).reshape(-1)
+        keep.append(p0)
+        desc.first_level_parameters = dptr(p0)
+        desc.first_level_parameter_count = p0.size
+    if on_level_parameters is not None:
+        def _params(level, ptr, count, _user):
+            on_level_parameters(int(level), np.ctypeslib.as_array(ptr, shape=(int(count),)).copy())
+        desc.level_parameters = abi.PARAMS_CALLBACK(_params)
+        keep.append(desc.level_parameters)
     disp = np.zeros(ref.shape + (D,))
     rep = RegisterReport()
     check(lib().skm_register(C.byref(desc), C.byref(geo), dptr(ref), dptr(tar), dptr(disp), C.byref(rep)))

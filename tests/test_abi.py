@@ -15,8 +15,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    txt = open(os.path.join(ROOT, "include", "skm_gpu.h")).read()
-    return sorted(set(re.findall(r"\b(skm_[a-z0-9_]+)\s*\(", txt)))
+    """Every entry point declared by the C headers (include/skm_gpu.h, include/skm_warmstart.h)."""
+    names = set()
+    for h in ("skm_gpu.h", "skm_warmstart.h"):
+        txt = open(os.path.join(ROOT, "include", h)).read()
+        names |= set(re.findall(r"\b(skm_[a-z0-9_]+)\s*\(", txt))
+    return sorted(names)
 
 
 @pytest.fixture(scope="module")
