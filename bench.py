@@ -57,6 +57,7 @@ def parse():
                     help="table-path GEMMs: auto = tensor cores where they fit, cuda = CUDA-core kernels")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps (capped at 300)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-pair batched line (config 4)")
+    ap.add_argument("--no-ct3d", action="store_true", help="skip the CT-like LCC line (config 3)")
     return ap.parse_args()
 
 
@@ -468,6 +469,97 @@ def multiscale_compare(name="ncc128"):
     return out
 
 
+# config 3: CT-like 256x256x160 volume, 1.5 mm voxels, LCC in the reference's form (window = kernel
+# support, radial weight, neighbourhood stride), anisotropic kernels from the structure tensor of each
+# level's smoothed target, RKHS + L1, 4 levels down to a 4-voxel control spacing (64x64x40 points)
+CT3D_CONFIG = dict(num_scales=4, sigma_C4=[144, 72, 36, 18], sigma_C0=[288, 144, 72, 36], cp_spacing_scaler=3.0,
+                   smoothing_variance=[4, 2, 1, 0], sampling_rate=[8], neighborhood_sampling=[16, 16, 12, 12],
+                   num_function_evaluations=[100], metric="lcc", reg_rkhs=[1e-3], reg_l1=[1e-3],
+                   initial_step_size=[100.0], tensor_weights=[400, 200, 100, 50])
+
+
+def ct3d_compare(torch, budget_s=150.0):
+    """Config 3 per level, within a time budget: our device optimizer's iterations/s (one warm-up
+    iteration, then up to 5 timed ones or 2 s), one evaluation of the reference's GpuKernelEvaluator on
+    the same level problem (while the budget lasts) for its iterations/s and for parity (value and
+    derivative at alpha = 0, same PCG32 sample shifts), and s/pair = sum over the levels of 100
+    iterations / iterations per second.  Every level runs without an earlier level's field (the
+    per-iteration cost does not depend on it)."""
+    from oracle import oracle as O
+    from skmimageregistration_b200 import register as R
+    from skmimageregistration_b200 import synth
+    from skmimageregistration_b200.abi import MetricDesc, OptimizerDesc
+    from skmimageregistration_b200.evaluator import GpuKernelEvaluator, Optimizer, bspline_coefficients
+    from skmimageregistration_b200.problem import Problem
+    from skmimageregistration_b200.register import current, full_config
+    t_start = time.perf_counter()
+    fixed, moving, _ = synth.ct3d(seed=0, shape=(160, 256, 256))
+    spacing = (1.5, 1.5, 1.5)
+    c = full_config(CT3D_CONFIG)
+    tar = R.threshold_rescale(fixed, (-1500, 3500))
+    ref_img = R.threshold_rescale(moving, (-1500, 3500))
+    have_ref = os.path.exists(O.ref_gpu_path(3, True))
+    levels, ours_total, ref_total = [], 0.0, 0.0
+    for s in range(int(c["num_scales"])):
+        var = float(current(c, "smoothing_variance", s))
+        tar_s = R.gaussian_smooth(tar, spacing, var) if var > 1e-5 else tar
+        ref_s = R.gaussian_smooth(ref_img, spacing, var) if var > 1e-5 else ref_img
+        s4, s0 = float(current(c, "sigma_C4", s)), float(current(c, "sigma_C0", s))
+        cov, tilt = R.anisotropic_tensor(tar_s, spacing, float(np.float32(s4)), float(current(c, "tensor_weights", s)), 2)
+        cps = float(np.float32(min(s4, s0)) / np.float32(c["cp_spacing_scaler"]))
+        pb = Problem(fixed=tar_s, moving_coefficients=bspline_coefficients(ref_s), spacing=spacing, origin=(0.0,) * 3,
+                     sigma_c0=s0, sigma_c4=s4, cp_spacing=cps, subsample=int(current(c, "sampling_rate", s)),
+                     subsample_neighborhood=int(current(c, "neighborhood_sampling", s)), weight_tensor=cov,
+                     maximum_weight=tilt if tilt >= 0 else 1.0, maximum_eigenvalue_covariance=np.eye(3))
+        m = MetricDesc.make("lcc", rkhs=float(current(c, "reg_rkhs", s)), l1=float(current(c, "reg_l1", s)))
+        zeros, ones = np.zeros(pb.num_parameters), np.ones(pb.C)
+        ev = GpuKernelEvaluator(pb)
+        opt = Optimizer(ev, OptimizerDesc.make(a=float(current(c, "initial_step_size", s)), number_of_iterations=1000),
+                        m, zeros, ones)
+        opt.run(1)
+        torch.cuda.synchronize()
+        k, t0 = 0, time.perf_counter()
+        while k < 5 and (k == 0 or time.perf_counter() - t0 < 2.0):
+            opt.run(1)
+            k += 1
+        ours_it_s = k / (time.perf_counter() - t0)
+        opt.close()
+        ev.close()
+        lv = {"level": s, "control_points": pb.C, "control_spacing_mm": cps, "samples": int(np.prod(
+            [n // pb.subsample for n in pb.size])), "tilt": tilt, "ours_iterations_timed": k,
+            "ours_iterations_per_s": ours_it_s}
+        ours_total += 100.0 / ours_it_s
+        if have_ref and time.perf_counter() - t_start < budget_s:
+            e2 = GpuKernelEvaluator(pb)
+            e2.SetRegularizerRKHS(float(current(c, "reg_rkhs", s)))
+            r, g = e2.getValueAndDerivative(GpuKernelEvaluator.LCC, np.zeros((pb.C, 3)), ones)
+            e2.close()
+            rg = O.RefGpu(pb, double=True)
+            rg.set_regularizers(rkhs=float(current(c, "reg_rkhs", s)))
+            t0 = time.perf_counter()
+            rr, gr = rg.evaluate(2, np.zeros((pb.C, 3)), ones)
+            t_ref = time.perf_counter() - t0
+            rg.close()
+            lv.update(reference_iterations_per_s=1.0 / t_ref,
+                      parity={"measure_rel": abs(r["measure"] - rr["measure"]) / max(abs(rr["measure"]), 1e-300),
+                              "pixels_equal": bool(r["num_pixels_counted"] == rr["num_pixels_counted"]),
+                              "derivative_max_rel": float(np.max(np.abs(g - gr)) / max(np.max(np.abs(gr)), 1e-300))})
+            ref_total += 100.0 * t_ref
+        else:
+            lv["reference_iterations_per_s"] = None
+            ref_total = None if not have_ref else ref_total
+        levels.append(lv)
+    out = {"config": dict(CT3D_CONFIG, volume="256x256x160", spacing_mm=1.5), "levels": levels,
+           "ours_s_per_pair_estimate": ours_total,
+           "reference_s_per_pair_estimate": ref_total if all(l["reference_iterations_per_s"] for l in levels) else None,
+           "budget_s": budget_s, "wall_s": time.perf_counter() - t_start,
+           "protocol": "per level: 100 iterations / measured iterations per s (ours: device optimizer, graph-"
+                       "replayed; reference: one getValueAndDerivative); parity at alpha = 0 on the same level"}
+    if out["reference_s_per_pair_estimate"]:
+        out["speedup_estimate"] = out["reference_s_per_pair_estimate"] / ours_total
+    return out
+
+
 def batch_compare(torch, steps=10, warmup=3):
     """Config 4: 64 config-2-style pairs of uneven sizes (64^3 .. 160x160x128), NCC/MSE mixed, all
     registered together, one persistent kernel per optimizer iteration (graph-replayed); aggregate
@@ -714,6 +806,8 @@ def run_ours(args, rank, world, local_rank):
         line["multiscale_mse2d"] = multiscale_compare("mse2d")
     if rank == 0 and world == 1 and not args.no_batch:
         line["batch64"] = batch_compare(torch)
+    if rank == 0 and world == 1 and not args.no_ct3d:
+        line["ct3d"] = ct3d_compare(torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O  # noqa: F401  (CPU baseline leg only)
         rate, steps, el, threads = cpu_port_rate(pb, mdesc, budget_s=15.0, max_steps=5)

@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define SKM_ABI_VERSION 4
+#define SKM_ABI_VERSION 5
 
 /* Status codes. */
 #define SKM_OK              0
@@ -385,6 +385,7 @@ typedef struct skm_register_report {
     int64_t control_points[SKM_MAX_SCALES];
     double  best_value[SKM_MAX_SCALES];   /* metric value (+ regularizers) at the returned parameters */
     double  seconds[SKM_MAX_SCALES];
+    double  optimize_seconds[SKM_MAX_SCALES];   /* of which the optimizer's iterations (the rest: set-up) */
 } skm_register_report;
 
 /* The scale loop of src/SKMReg.cxx:84-500 (skmreg): threshold + rescale, then per level

@@ -256,13 +256,14 @@ class RegisterReport(C.Structure):
         ("control_points", C.c_int64 * MAX_SCALES),
         ("best_value", C.c_double * MAX_SCALES),
         ("seconds", C.c_double * MAX_SCALES),
+        ("optimize_seconds", C.c_double * MAX_SCALES),
     ]
 
     def as_dict(self):
         n = self.levels_done
         return {"levels_done": n, "first_level": self.first_level, "iterations": list(self.iterations[:n]),
                 "control_points": list(self.control_points[:n]), "best_value": list(self.best_value[:n]),
-                "seconds": list(self.seconds[:n])}
+                "seconds": list(self.seconds[:n]), "optimize_seconds": list(self.optimize_seconds[:n])}
 
 
 def dptr(a):

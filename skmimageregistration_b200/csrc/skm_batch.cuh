@@ -950,6 +950,9 @@ extern "C" int skm_batch_create(int32_t npairs, const skm_batch_pair *pairs, skm
                 return fail(SKM_ERR_UNSUPPORTED, "pair %d: the batch needs the phase-table path (stationary kernel, "
                                                  "control spacing an integer multiple of the voxel spacing, "
                                                  "subsample 1)", i);
+            if (e->table.big)
+                return fail(SKM_ERR_UNSUPPORTED, "pair %d: %d phases per cell; the batch takes at most %d", i,
+                            e->table.dev.nph, kTabSmallPhases);
             const TableDev &T0 = e->table.dev;
             if (i == 0) {
                 b->hl = T0.h[2];

@@ -644,7 +644,9 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
         skm_optimizer *opt = nullptr;
         rc = skm_optimizer_create(ev, &od, &md, params.data(), cpw.data(), &df, &opt);
         skm_optimizer_state st{};
+        const auto t_opt = std::chrono::steady_clock::now();
         if (!rc) rc = skm_optimizer_run(opt, r->num_function_evaluations[s]);
+        rep.optimize_seconds[s] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_opt).count();
         if (!rc) rc = skm_optimizer_get_parameters(opt, 1, best.data());
         if (!rc) rc = skm_optimizer_get_state(opt, &st);
         if (opt) skm_optimizer_destroy(opt);

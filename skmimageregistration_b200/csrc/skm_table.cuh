@@ -31,7 +31,10 @@
 namespace skm {
 
 
-constexpr int kTabMaxPhase = 8;      // phases per axis
+constexpr int kTabMaxPhase = 16;     // phases per axis
+constexpr int kTabSmallPhases = 256; // above this (or when the tables do not fit in shared memory) the
+                                     // transform and the contrib GEMM run their large-phase kernels
+constexpr int kTabBigCells = 8;      // cells per block of the large-phase kernels
 constexpr int kTabMaxTap = 10;       // taps per axis
 constexpr int kTabContribThreads = 288;   // 9 warps
 constexpr int kTabCells = 32;        // cells per contrib block
@@ -47,7 +50,7 @@ struct TableDev {
     long long ncell;
     int qoff[3][kTabMaxPhase];   // cell of texel h*a + p is a + qoff[p]
     int clo[3], nc[3];           // control-point offsets of the regularizer box
-    const float *tfwd;   // [tap][(px,py)][pz]
+    const float *tfwd;   // [tap][(px,py)][pz]; large-phase plans: [tap][phase]
     const float *tgemm;  // [phase][ntap_pad]
     const float *kcp;    // [nkcp]: nonzero kernel values between control points at an offset ...
     const int *kcpo;     // [nkcp]: ... and the offsets, (dx + 512) | (dy + 512) << 10 | (dz + 512) << 20
@@ -75,6 +78,9 @@ struct TablePlan {
     int hl = 1;          // z phases per thread in the transform kernel (template argument)
     int ncz = 1;         // cells per thread along z in the transform kernel
     int transform_blocks = 0, contrib_blocks = 0;
+    bool big = false;    // large-phase plan (coarse levels: control spacing 8 or 16 voxels): the
+                         // tables stay in global memory / L2, table_transform_big_kernel and
+                         // table_contrib_big_kernel replace the shared-memory-table kernels
     std::vector<float> h_tgemm;   // host copy of tgemm (operand tables of the tensor-core kernels)
 };
 
@@ -279,6 +285,133 @@ __global__ void __launch_bounds__(256, 4) table_warp_kernel(EvalParams P, TableD
 }
 
 // ------------------------------------------------------------------------------------------------
+// ------------------------------------------------------------------------------------------------
+// Large-phase plans (coarse scale levels: control spacing 8 or 16 voxels, 512 or 4096 phases): the
+// tables (up to 4096 x 216 floats) stay in global memory, where the L2 keeps them, and a block takes
+// kTabBigCells cells at a time so that every table value it loads serves all of them.
+//   transform: thread = phase, u(q, p) = sum_t T[t][p] (w alpha)[q + t] for the block's cells, the
+//              cells' weighted control points in shared memory (table read [tap][phase]: coalesced)
+//   contrib:   thread = tap, Contrib[t][q] = sum_p T[p][t] g(q, p) for the block's cells, g staged in
+//              shared memory in chunks of kTabBigChunk phases (table read [phase][tap]: coalesced)
+constexpr int kTabBigChunk = 128;
+
+template <int D>
+__global__ void __launch_bounds__(256) table_transform_big_kernel(EvalParams P, TableDev T)
+{
+    constexpr int CB = kTabBigCells;
+    extern __shared__ float4 A[];                            // [CB][ntap] weighted control points
+    const int ntap = T.ntap, nph = T.nph;
+    const long long plane = T.ncell * T.nph;
+    const long long ngroups = (T.ncell + CB - 1) / CB;
+    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+        const long long c0 = grp * CB;
+        __syncthreads();                                     // previous group done with A
+        for (int i = threadIdx.x; i < CB * ntap; i += blockDim.x) {
+            const int c = i / ntap, t = i - c * ntap;
+            const long long cell = c0 + c;
+            float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (cell < T.ncell) {
+                const int cyz = (int)(cell / T.nq[0]), cz = cyz / T.nq[1];
+                const int cc[3] = {(int)(cell - (long long)cyz * T.nq[0]), cyz - cz * T.nq[1], cz};
+                const int tt[3] = {t % T.nt[0], (t / T.nt[0]) % T.nt[1], t / (T.nt[0] * T.nt[1])};
+                int j[3];
+                bool in = true;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    j[d] = T.qmin[d] + cc[d] + T.tlo[d] + tt[d];
+                    if (j[d] < 0 || j[d] >= P.cp.n[d]) in = false;
+                }
+                if (in) {
+                    const float4 cp = __ldg(P.cpd + j[0] + P.cp.st[1] * j[1] + P.cp.st[2] * j[2]);
+                    a = make_float4(cp.w * cp.x, cp.w * cp.y, cp.w * cp.z, 0.f);
+                }
+            }
+            A[c * ntap + t] = a;
+        }
+        __syncthreads();
+        for (int p = threadIdx.x; p < nph; p += blockDim.x) {
+            float acc[CB][3];
+#pragma unroll
+            for (int c = 0; c < CB; ++c) acc[c][0] = acc[c][1] = acc[c][2] = 0.f;
+            const float *tp = T.tfwd + p;
+#pragma unroll 2
+            for (int t = 0; t < ntap; ++t) {
+                const float k = __ldg(tp + (long long)t * nph);
+#pragma unroll
+                for (int c = 0; c < CB; ++c) {
+                    const float4 a = A[c * ntap + t];
+                    acc[c][0] = fmaf(k, a.x, acc[c][0]);
+                    acc[c][1] = fmaf(k, a.y, acc[c][1]);
+                    acc[c][2] = fmaf(k, a.z, acc[c][2]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < CB; ++c) {
+                if (c0 + c >= T.ncell) break;
+                const long long i = (c0 + c) * nph + p;
+                T.ucp[i] = acc[c][0];
+                T.ucp[i + plane] = acc[c][1];
+                if (D > 2) T.ucp[i + 2 * plane] = acc[c][2];
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) table_contrib_big_kernel(TableDev T, const double *__restrict__ stats)
+{
+    constexpr int CB = kTabBigCells;
+    __shared__ float4 G[CB][kTabBigChunk];
+    const int nph = T.nph, ntap = T.ntap, ntp = T.ntap_pad;
+    const float cf = (float)stats[S_COEF_F], cm = (float)stats[S_COEF_M], cc = (float)stats[S_COEF_C];
+    const long long ngroups = (T.ncell + CB - 1) / CB;
+    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+        const long long c0 = grp * CB;
+        float acc[CB][3];
+#pragma unroll
+        for (int c = 0; c < CB; ++c) acc[c][0] = acc[c][1] = acc[c][2] = 0.f;
+        const int t = threadIdx.x;
+        for (int p0 = 0; p0 < nph; p0 += kTabBigChunk) {
+            const int np = min(kTabBigChunk, nph - p0);
+            __syncthreads();                                 // previous chunk done with G
+            for (int i = threadIdx.x; i < CB * kTabBigChunk; i += blockDim.x) {
+                const int c = i / kTabBigChunk, p = i - c * kTabBigChunk;
+                float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (c0 + c < T.ncell && p < np) {
+                    const long long idx = (c0 + c) * nph + p0 + p;
+                    const float4 r = T.rec[idx];
+                    const float coef = fmaf(cf, T.fixcp[idx], fmaf(cm, r.w, cc));
+                    g = make_float4(coef * r.x, coef * r.y, coef * r.z, 0.f);
+                }
+                G[c][p] = g;
+            }
+            __syncthreads();
+            if (t < ntap) {
+                const float *tp = T.tgemm + (long long)p0 * ntp + t;
+#pragma unroll 2
+                for (int p = 0; p < np; ++p) {
+                    const float k = __ldg(tp + (long long)p * ntp);
+#pragma unroll
+                    for (int c = 0; c < CB; ++c) {
+                        const float4 g = G[c][p];
+                        acc[c][0] = fmaf(k, g.x, acc[c][0]);
+                        acc[c][1] = fmaf(k, g.y, acc[c][1]);
+                        acc[c][2] = fmaf(k, g.z, acc[c][2]);
+                    }
+                }
+            }
+        }
+        if (t < ntap) {
+#pragma unroll
+            for (int c = 0; c < CB; ++c) {
+                const long long cell = c0 + c;
+                if (cell >= T.ncell) break;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) T.contrib[((long long)d * ntap + t) * T.ncell + cell] = acc[c][d];
+            }
+        }
+    }
+}
+
 // Contrib[t][cell] = sum_p T[p][t] * g(cell, p),  g = (a f + b m + c) grad M
 __global__ void __launch_bounds__(kTabContribThreads) table_contrib_kernel(TableDev T, const double *__restrict__ stats)
 {
@@ -667,7 +800,7 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
         }
     }
     T.nph = T.h[0] * T.h[1] * T.h[2];
-    if (T.nph * 16 > 4096 || (T.h[0] * T.h[1]) > 256) return 0;
+    if (T.nph > kTabMaxPhase * kTabMaxPhase * kTabMaxPhase) return 0;
     // tap range per axis: every t with |phi - t| * spacing < S for some phase
     for (int d = 0; d < 3; ++d) {
         if (d >= D) {
@@ -735,10 +868,20 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     // transform tiling: threads = (px,py) phases x cells; each thread HL z-phases of NCZ cells
     const int nphxy = T.h[0] * T.h[1];
     const int hl = T.h[2];
-    if (!(hl == 1 || hl == 2 || hl == 4 || hl == 8)) return 0;
-    if (256 % nphxy != 0) return 0;
     const int ncz = D == 3 ? 4 : 1;
-    const int cells = 256 / nphxy;
+    // the shared-memory-table kernels need the tables in shared memory and (px, py) phases that
+    // divide the block; otherwise (coarse levels) the large-phase kernels run
+    {
+        const size_t sv = (size_t)(2 + T.nt[0] - 1) * (2 + T.nt[1] - 1) * (ncz + T.nt[2] - 1) * sizeof(float4) +
+                          (size_t)T.ntap * T.nph * sizeof(float);
+        const size_t sc = (size_t)kTabCells * (T.nph + 1) * sizeof(float4) + (size_t)T.nph * T.ntap_pad * sizeof(float);
+        pl.big = T.nph > kTabSmallPhases || !(hl == 1 || hl == 2 || hl == 4 || hl == 8) || 256 % nphxy != 0 ||
+                 sv > 200 * 1024 || sc > 200 * 1024;
+    }
+    // large-phase kernels: one thread per tap in the contrib GEMM (256 threads), the cells' weighted
+    // control points of the transform in at most 48 KB of shared memory
+    if (pl.big && (T.ntap > 256 || (size_t)kTabBigCells * T.ntap * sizeof(float4) > 48 * 1024)) return 0;
+    const int cells = pl.big ? 1 : 256 / nphxy;
     int tx = 1;
     while (tx * tx < cells) tx *= 2;
     T.tile_x = std::min(tx, cells);
@@ -787,7 +930,10 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
                                 r2 += e * e;
                             }
                             const float k = wendland_host(sqrt(r2), P.K.sc4, P.K.sc0);
-                            tfwd[((size_t)tap * nphxy + px + T.h[0] * py) * hl + pz] = k;
+                            if (pl.big)   // [tap][phase]: the large-phase transform reads it coalesced
+                                tfwd[(size_t)tap * T.nph + px + T.h[0] * (py + T.h[1] * pz)] = k;
+                            else
+                                tfwd[((size_t)tap * nphxy + px + T.h[0] * py) * hl + pz] = k;
                             tgemm[(size_t)(px + T.h[0] * (py + T.h[1] * pz)) * T.ntap_pad + tap] = k;
                         }
             }
@@ -866,10 +1012,12 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
                                   sizeof(float4) + (size_t)T.ntap * nphxy * hl * sizeof(float);
     const size_t smem_contrib =
         (size_t)kTabCells * (T.nph + 1) * sizeof(float4) + (size_t)T.nph * T.ntap_pad * sizeof(float);
-    if (smem_value > 200 * 1024 || smem_contrib > 200 * 1024) return 0;
+    if (!pl.big && (smem_value > 200 * 1024 || smem_contrib > 200 * 1024)) return 0;
     pl.enabled = true;
     return 0;
 }
+
+inline size_t table_big_transform_smem(const TableDev &T) { return (size_t)kTabBigCells * T.ntap * sizeof(float4); }
 
 inline size_t table_value_smem(const TablePlan &pl)
 {
@@ -886,6 +1034,7 @@ inline size_t table_contrib_smem(const TableDev &T)
 // dynamic shared memory limits of the table kernels (set once, outside any stream capture)
 inline int table_set_attributes(const TablePlan &pl)
 {
+    if (pl.big) return 0;                          // large-phase kernels: static / small dynamic shared memory
     const int sv = (int)table_value_smem(pl), sc = (int)table_contrib_smem(pl.dev);
     cudaError_t e = cudaSuccess;
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
@@ -907,6 +1056,12 @@ inline int table_size_grids(TablePlan &pl)
     int dev = 0, sms = 0, bt = 0, bc = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 2;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 2;
+    if (pl.big) {                                  // one group of kTabBigCells cells per block, grid-strided
+        const long long groups = (pl.dev.ncell + kTabBigCells - 1) / kTabBigCells;
+        pl.transform_blocks = (int)std::max<long long>(1, std::min<long long>(groups, 8LL * sms));
+        pl.contrib_blocks = pl.transform_blocks;
+        return 0;
+    }
     cudaError_t e;
     const int sv = (int)table_value_smem(pl);
     if (pl.dev.D == 3) {

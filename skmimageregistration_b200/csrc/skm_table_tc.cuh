@@ -1195,6 +1195,13 @@ inline int table_value(TablePlan &pl, const TcPlan *tc, const EvalParams &P, int
     int rc;
     if (tc && tc->enabled) {
         rc = table_transform_tc(*tc, pl, P, s);
+    } else if (pl.big) {                                     // coarse levels: tables in global memory
+        const size_t smem = table_big_transform_smem(pl.dev);
+        if (D == 3)
+            table_transform_big_kernel<3><<<pl.transform_blocks, 256, smem, s>>>(P, pl.dev);
+        else
+            table_transform_big_kernel<2><<<pl.transform_blocks, 256, smem, s>>>(P, pl.dev);
+        rc = cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
     } else if (D == 3) {
         switch (pl.hl) {
         case 1: rc = table_transform_launch<1, 4>(pl, P, s); break;
@@ -1225,6 +1232,9 @@ inline int table_derivative(TablePlan &pl, const TcPlan *tc, const EvalParams &P
         if (table_contrib_tc(*tc, pl, Q.stats, s)) return 2;
         G.gtap = tc->d_ctap;                                 // nonzero taps only
         G.ngtap = tc->dev.nct;
+    } else if (pl.big) {
+        table_contrib_big_kernel<<<pl.contrib_blocks, 256, 0, s>>>(pl.dev, Q.stats);
+        if (cudaPeekAtLastError() != cudaSuccess) return 2;
     } else {
         const size_t smem = table_contrib_smem(pl.dev);
         table_contrib_kernel<<<pl.contrib_blocks, kTabContribThreads, smem, s>>>(pl.dev, Q.stats);
