@@ -195,6 +195,8 @@ extern "C" int skm_optimizer_create(skm_evaluator *e, const skm_optimizer_desc *
     if (!(od->f_min != 0.0) || !(od->omega != 0.0)) return fail(SKM_ERR_INVALID, "f_min and omega must be nonzero");
     SKM_CUDA(cudaSetDevice(e->device));
     if ((rc = upload_field(e, df))) return rc;
+    // LCC's dense fields are allocated on first use: that must happen before the iteration is captured
+    if (md->metric == SKM_LCC && (rc = ensure_dense(e))) return rc;
     skm_optimizer *o = new skm_optimizer();
     o->e = e;
     o->od = *od;

@@ -278,3 +278,24 @@ def test_lcc_nonstationary_larger(D, shape, cp_spacing, kind):
         assert r["num_pixels_counted"] == ro["num_pixels_counted"]
         assert rel_err(r["measure"], ro["measure"]) <= TOL_VALUE
         assert max_rel(g, go) <= TOL_DERIV
+
+
+@pytest.mark.parametrize("D,kind", [(2, "stationary"), (3, "weight_tensor")])
+def test_optimizer_lcc_matches_oracle(D, kind):
+    """The device optimizer with LCC (its dense fields allocated before the iteration is captured)
+    against the FP64 oracle optimizer, with RKHS + L1 as in the CT-like workload."""
+    shape = (12, 13, 14) if D == 3 else (28, 30)
+    pb, _, cpw = make_problem(D, kind, subsample=2, nbh=2, shape=shape, seed=73, sigma_c4=3.0, sigma_c0=6.0,
+                              cp_spacing=1.5, weights=False)
+    P = pb.num_parameters
+    m = MetricDesc.make("lcc", rkhs=1e-3, l1=1e-4)
+    o = OptimizerDesc.make(a=5.0, number_of_iterations=4)
+    ev = GpuKernelEvaluator(pb)
+    opt = Optimizer(ev, o, m, np.zeros(P), cpw)
+    oo = O.OracleOptimizer(O.Oracle(pb), o, m, np.zeros(P), cpw)
+    opt.run(4)
+    vals = oo.run(4)
+    st = opt.state()
+    assert st["iteration"] == 4
+    assert rel_err(st["value"], vals[-1]) <= 1e-4
+    assert max_rel(opt.parameters(), oo.position) <= 1e-3
