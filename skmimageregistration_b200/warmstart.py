@@ -255,7 +255,7 @@ def _make_pair(seed):
 def make_pairs(seeds, workers=None):
     """Seeded config-2-style pairs at 96x96x64 (a process pool started with spawn)."""
     import multiprocessing as mp
-    workers = workers or min(len(seeds), os.cpu_count() or 1)
+    workers = workers or min(len(seeds), os.cpu_count() or 1, 8)     # a few hundred MB of host memory each
     if workers <= 1:
         return [_make_pair(s) for s in seeds]
     with mp.get_context("spawn").Pool(workers) as pool:
