@@ -430,7 +430,7 @@ def final_mse(fixed, moving, disp, spacing):
     return float(r["measure"])
 
 
-def multiscale_compare(name="ncc128"):
+def multiscale_compare(name="ncc128", override=None):
     """s/pair of the multi-scale registration for both drivers and the final metric each reaches:
     ncc128 (3-D, NCC + RD, the headline) or mse2d (config 1: 2-D 256^2, MSE + L1)."""
     from skmimageregistration_b200 import register as R
@@ -443,7 +443,7 @@ def multiscale_compare(name="ncc128"):
                    dict(MS_CONFIG, num_function_evaluations=[2], sigma_C4=[12], sigma_C0=[24]))   # warm-up
     else:
         fixed, moving, _ = synth.blobs2d(seed=0, shape=(256, 256))
-        spacing, cfg, volume = (1.0, 1.0), MS_CONFIG_2D, "256x256"
+        spacing, cfg, volume = (1.0, 1.0), dict(MS_CONFIG_2D, **(override or {})), "256x256"
         score, key, better = final_mse, "mse", (lambda a, b: a <= b + 1e-3 * abs(b))
         R.register(moving[::4, ::4].copy(), fixed[::4, ::4].copy(), spacing, None,
                    dict(MS_CONFIG_2D, num_function_evaluations=[2], sigma_C4=[16], sigma_C0=[32]))   # warm-up
@@ -804,6 +804,9 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_multiscale:
         line["multiscale"] = multiscale_compare("ncc128")
         line["multiscale_mse2d"] = multiscale_compare("mse2d")
+        # with L1 1e-3 every MSE gradient component stays below the L1 threshold, so the plain method
+        # (ours and the reference alike) keeps alpha = 0; a weaker L1 shows the registration moving
+        line["multiscale_mse2d_l1_1e-6"] = multiscale_compare("mse2d", dict(reg_l1=[1e-6]))
     if rank == 0 and world == 1 and not args.no_batch:
         line["batch64"] = batch_compare(torch)
     if rank == 0 and world == 1 and not args.no_ct3d:

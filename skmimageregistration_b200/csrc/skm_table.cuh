@@ -62,6 +62,8 @@ struct TableDev {
     const int *gtap;     // contrib tap k -> box tap index (NULL: identity, all ntap box taps)
     int ngtap;           // taps in the contrib layout
     double *part;        // [NQ][value blocks]
+    float *bigpart;      // large-phase contrib: [big_splits][3][ntap][ncell] partial sums (big_splits > 1)
+    int big_splits;      // phase splits of a cell group in the large-phase contrib (1: direct)
     unsigned *tc_err;    // failure word of the tensor-core kernels (NULL without them)
     int value_blocks, tile_x, tile_y, tiles_x, tiles_y, tiles_z;
     FastDiv div_nph, div_nq0, div_nq01, div_h0, div_h01;   // index decomposition (ncell * nph < 2^31)
@@ -75,6 +77,7 @@ struct TablePlan {
     float4 *d_rec = nullptr;
     float *d_ucp = nullptr;
     double *d_part = nullptr;
+    float *d_bigpart = nullptr;
     int hl = 1;          // z phases per thread in the transform kernel (template argument)
     int ncz = 1;         // cells per thread along z in the transform kernel
     int transform_blocks = 0, contrib_blocks = 0;
@@ -303,9 +306,12 @@ __global__ void __launch_bounds__(256) table_transform_big_kernel(EvalParams P, 
     const int ntap = T.ntap, nph = T.nph;
     const long long plane = T.ncell * T.nph;
     const long long ngroups = (T.ncell + CB - 1) / CB;
-    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const int npc = (nph + blockDim.x - 1) / blockDim.x;      // phase chunks of one block's threads
+    for (long long item = blockIdx.x; item < ngroups * npc; item += gridDim.x) {
+        const long long grp = item / npc;
+        const int pc = (int)(item - grp * npc);
         const long long c0 = grp * CB;
-        __syncthreads();                                     // previous group done with A
+        __syncthreads();                                     // previous item done with A
         for (int i = threadIdx.x; i < CB * ntap; i += blockDim.x) {
             const int c = i / ntap, t = i - c * ntap;
             const long long cell = c0 + c;
@@ -329,7 +335,8 @@ __global__ void __launch_bounds__(256) table_transform_big_kernel(EvalParams P, 
             A[c * ntap + t] = a;
         }
         __syncthreads();
-        for (int p = threadIdx.x; p < nph; p += blockDim.x) {
+        const int p = pc * blockDim.x + threadIdx.x;
+        if (p < nph) {
             float acc[CB][3];
 #pragma unroll
             for (int c = 0; c < CB; ++c) acc[c][0] = acc[c][1] = acc[c][2] = 0.f;
@@ -364,14 +371,21 @@ __global__ void __launch_bounds__(256) table_contrib_big_kernel(TableDev T, cons
     const int nph = T.nph, ntap = T.ntap, ntp = T.ntap_pad;
     const float cf = (float)stats[S_COEF_F], cm = (float)stats[S_COEF_M], cc = (float)stats[S_COEF_C];
     const long long ngroups = (T.ncell + CB - 1) / CB;
-    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    // the phases of a group may be split over T.big_splits items (few cells, many phases): each
+    // writes partial sums that table_contrib_big_reduce adds in split order
+    const int splits = T.big_splits;
+    const int per = (nph + splits - 1) / splits;
+    for (long long item = blockIdx.x; item < ngroups * splits; item += gridDim.x) {
+        const long long grp = item / splits;
+        const int sp = (int)(item - grp * splits);
         const long long c0 = grp * CB;
         float acc[CB][3];
 #pragma unroll
         for (int c = 0; c < CB; ++c) acc[c][0] = acc[c][1] = acc[c][2] = 0.f;
         const int t = threadIdx.x;
-        for (int p0 = 0; p0 < nph; p0 += kTabBigChunk) {
-            const int np = min(kTabBigChunk, nph - p0);
+        const int pend = min(nph, (sp + 1) * per);
+        for (int p0 = sp * per; p0 < pend; p0 += kTabBigChunk) {
+            const int np = min(kTabBigChunk, pend - p0);
             __syncthreads();                                 // previous chunk done with G
             for (int i = threadIdx.x; i < CB * kTabBigChunk; i += blockDim.x) {
                 const int c = i / kTabBigChunk, p = i - c * kTabBigChunk;
@@ -405,10 +419,22 @@ __global__ void __launch_bounds__(256) table_contrib_big_kernel(TableDev T, cons
             for (int c = 0; c < CB; ++c) {
                 const long long cell = c0 + c;
                 if (cell >= T.ncell) break;
+                float *dst = splits > 1 ? T.bigpart + (long long)sp * 3 * ntap * T.ncell : T.contrib;
 #pragma unroll
-                for (int d = 0; d < 3; ++d) T.contrib[((long long)d * ntap + t) * T.ncell + cell] = acc[c][d];
+                for (int d = 0; d < 3; ++d) dst[((long long)d * ntap + t) * T.ncell + cell] = acc[c][d];
             }
         }
+    }
+}
+
+// Contrib = sum of the big_splits partials, in split order
+__global__ void table_contrib_big_reduce(TableDev T)
+{
+    const long long n = 3LL * T.ntap * T.ncell;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int sp = 0; sp < T.big_splits; ++sp) s += T.bigpart[(long long)sp * n + i];
+        T.contrib[i] = s;
     }
 }
 
@@ -757,6 +783,7 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
     if (P.K.kind != kStationary || P.sub != 1) return 0;
     TableDev &T = pl.dev;
     T = TableDev{};
+    T.big_splits = 1;
     T.D = D;
     const double S = (double)P.K.support_min;
     double phi[3][kTabMaxPhase];
@@ -1056,10 +1083,21 @@ inline int table_size_grids(TablePlan &pl)
     int dev = 0, sms = 0, bt = 0, bc = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 2;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 2;
-    if (pl.big) {                                  // one group of kTabBigCells cells per block, grid-strided
-        const long long groups = (pl.dev.ncell + kTabBigCells - 1) / kTabBigCells;
-        pl.transform_blocks = (int)std::max<long long>(1, std::min<long long>(groups, 8LL * sms));
-        pl.contrib_blocks = pl.transform_blocks;
+    if (pl.big) {                                  // items of kTabBigCells cells, grid-strided
+        TableDev &T = pl.dev;
+        const long long groups = (T.ncell + kTabBigCells - 1) / kTabBigCells;
+        const long long titems = groups * ((T.nph + 255) / 256);
+        pl.transform_blocks = (int)std::max<long long>(1, std::min<long long>(titems, 8LL * sms));
+        // few cell groups (the coarsest levels): split their phases so that every SM gets work
+        const int max_split = (T.nph + kTabBigChunk - 1) / kTabBigChunk;
+        T.big_splits = (int)std::max<long long>(1, std::min<long long>(max_split, (2LL * sms + groups - 1) / groups));
+        if (T.big_splits > 1 && !pl.d_bigpart) {
+            if (pool_malloc((void **)&pl.d_bigpart, sizeof(float) * (size_t)T.big_splits * 3 * T.ntap * T.ncell) !=
+                cudaSuccess)
+                return 2;
+        }
+        T.bigpart = pl.d_bigpart;
+        pl.contrib_blocks = (int)std::max<long long>(1, std::min<long long>(groups * T.big_splits, 8LL * sms));
         return 0;
     }
     cudaError_t e;
@@ -1092,6 +1130,7 @@ inline void table_free(TablePlan &pl)
     if (pl.d_rec) pool_release(pl.d_rec);
     if (pl.d_ucp) pool_release(pl.d_ucp);
     if (pl.d_part) pool_release(pl.d_part);
+    if (pl.d_bigpart) pool_release(pl.d_bigpart);
     pl = TablePlan{};
 }
 

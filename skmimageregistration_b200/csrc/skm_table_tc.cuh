@@ -1234,6 +1234,7 @@ inline int table_derivative(TablePlan &pl, const TcPlan *tc, const EvalParams &P
         G.ngtap = tc->dev.nct;
     } else if (pl.big) {
         table_contrib_big_kernel<<<pl.contrib_blocks, 256, 0, s>>>(pl.dev, Q.stats);
+        if (pl.dev.big_splits > 1) table_contrib_big_reduce<<<592, 256, 0, s>>>(pl.dev);
         if (cudaPeekAtLastError() != cudaSuccess) return 2;
     } else {
         const size_t smem = table_contrib_smem(pl.dev);
