@@ -125,6 +125,13 @@ typedef struct skm_evaluator skm_evaluator;
 const char *skm_last_error(void);
 int32_t     skm_abi_version(void);
 
+/* Device memory (no counterpart in the reference, which calls cudaMalloc/cudaFree per buffer).
+ * The library's buffers come from a stream-ordered pool of its own per device; when its last
+ * buffer on a device is freed the pool keeps 2 GiB for the next evaluator or registration and
+ * returns the rest to the driver.  This call returns everything the pools keep on devices where
+ * none of the library's objects is alive. */
+int         skm_release_memory(void);
+
 /* GpuKernelEvaluator::GpuKernelEvaluator (GpuEvaluator.h:147-154, GpuEvaluator.cu:30-91).
  * Copies the images to device memory; all host pointers in desc are borrowed. */
 int skm_evaluator_create(const skm_evaluator_desc *desc, skm_evaluator **out);

@@ -571,7 +571,8 @@ struct BatchSmem {
 };
 
 template <int HL, int NCZ>
-__global__ void __launch_bounds__(kBatchThreads, 1) batch_iteration_kernel(BatchDev B)
+// 128 registers a thread, so that two CTAs fit on an SM (the autotuner picks 1 or 2 per SM)
+__global__ void __launch_bounds__(kBatchThreads, 2) batch_iteration_kernel(BatchDev B)
 {
     extern __shared__ float4 bsm4[];
     __shared__ __align__(16) unsigned char sp_raw[sizeof(BatchPair)];   // the current pair's descriptor

@@ -288,6 +288,17 @@ extern "C" const char *skm_last_error(void) { return g_last_error.c_str(); }
 void skm_internal_set_error(const char *msg) { g_last_error = msg; }
 extern "C" int32_t skm_abi_version(void) { return SKM_ABI_VERSION; }
 
+extern "C" int skm_release_memory(void)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return SKM_OK;                               // no device: the library holds nothing
+    }
+    SKM_CUDA(pool_release_all());
+    return SKM_OK;
+}
+
 static int validate_desc(const skm_evaluator_desc *d)
 {
     if (!d) return fail(SKM_ERR_INVALID, "descriptor is NULL");

@@ -20,9 +20,13 @@ namespace skm {
 // created and destroyed level after level (the multi-scale driver) do not map and unmap their
 // buffers every time.  The device's default pool, which the host application may use itself, is
 // left untouched.  When the library's last live buffer on a device is freed, the pool is trimmed
-// and its memory goes back to the driver.  pool_malloc and pool_free complete before returning
-// (as cudaMalloc / cudaFree do), so no stream ordering leaks out of them.
+// to kPoolKeepBytes (so that the next registration of a similar size does not map its buffers
+// again) and the rest goes back to the driver; skm_release_memory() trims every pool to zero.
+// pool_malloc and pool_free complete before returning (as cudaMalloc / cudaFree do), so no stream
+// ordering leaks out of them.
 constexpr int kPoolMaxDevices = 64;
+constexpr size_t kPoolKeepBytes = (size_t)2 << 30;      // 2 GiB kept per device between uses
+
 
 struct DevicePool {
     cudaMemPool_t pool = nullptr;
@@ -95,7 +99,7 @@ inline cudaError_t pool_release(void *p)
         if (dp.live > 0 && --dp.live == 0 && dp.pool) {
             e = cudaStreamSynchronize(0);
             if (e != cudaSuccess) return e;
-            e = cudaMemPoolTrimTo(dp.pool, 0);
+            e = cudaMemPoolTrimTo(dp.pool, kPoolKeepBytes);
         }
     }
     return e;
@@ -109,6 +113,23 @@ inline cudaError_t pool_free(void *p)
     e = pool_release(p);
     if (e != cudaSuccess) return e;
     return cudaStreamSynchronize(0);
+}
+
+// Trims the library's pool of every device to zero (nothing of the library may be alive on it).
+inline cudaError_t pool_release_all()
+{
+    std::lock_guard<std::mutex> g(pool_lock());
+    int cur = 0;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return e;
+    for (int d = 0; d < kPoolMaxDevices; ++d) {
+        DevicePool &dp = pool_table()[d];
+        if (!dp.pool || dp.live != 0) continue;
+        if ((e = cudaSetDevice(d)) != cudaSuccess) return e;
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) return e;
+        if ((e = cudaMemPoolTrimTo(dp.pool, 0)) != cudaSuccess) return e;
+    }
+    return cudaSetDevice(cur);
 }
 
 constexpr int kMaxDim = 3;
