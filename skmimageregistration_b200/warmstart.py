@@ -133,6 +133,7 @@ class WarmStartNet:
         self.err = torch.zeros(1, dtype=torch.int32, device="cuda")
         self.loss = torch.zeros(1, dtype=torch.float32, device="cuda")
         self.label_scale = float(label_scale)
+        self.level0_iterations = 0        # first-level iterations after the warm start (validated)
         self.step_count = 0
         self._acts = None
         self.pack()
@@ -222,7 +223,7 @@ class WarmStartNet:
 
     # ---- persistence
     def save(self, path=WEIGHTS_PATH):
-        arrs = {"label_scale": np.array(self.label_scale)}
+        arrs = {"label_scale": np.array(self.label_scale), "level0_iterations": np.array(self.level0_iterations)}
         for i, L in enumerate(self.layers):
             arrs["w%d" % i] = L.w.cpu().numpy()
             arrs["b%d" % i] = L.b.cpu().numpy()
@@ -232,6 +233,7 @@ class WarmStartNet:
     def load(cls, path=WEIGHTS_PATH):
         z = np.load(path)
         net = cls(label_scale=float(z["label_scale"]))
+        net.level0_iterations = int(z["level0_iterations"]) if "level0_iterations" in z else 0
         for i, L in enumerate(net.layers):
             L.load(z["w%d" % i], z["b%d" % i])
         net.pack()
@@ -287,6 +289,8 @@ def train(n_train=256, epochs=40, batch=8, lr=2e-3, seed=0, log=None, pairs=None
     C_ = labels.shape[1] // 3
     # network output (B, z, y, x, 3) with x fastest: [b][j][d] -> labels are planar [b][d][j]
     Y = torch.tensor((labels.reshape(-1, 3, C_).transpose(0, 2, 1) / scale).astype(np.float32), device="cuda")
+    grid = tuple(reversed(out_grid(X.shape)))                                # (z, y, x) of the alpha grid
+    Y = Y.reshape((len(pairs),) + grid + (3,))
     rng = np.random.default_rng(seed)
     hist = []
     t1 = time.perf_counter()
@@ -295,9 +299,16 @@ def train(n_train=256, epochs=40, batch=8, lr=2e-3, seed=0, log=None, pairs=None
         tot = 0.0
         for k in range(0, len(order) - batch + 1, batch):
             idx = torch.tensor(order[k:k + batch], device="cuda")
-            xb = X.index_select(0, idx).contiguous()
-            yb = Y.index_select(0, idx).contiguous()
-            tot += net.train_step(xb, yb.reshape(batch, -1), lr=lr)
+            xb = X.index_select(0, idx)
+            yb = Y.index_select(0, idx)
+            # mirror symmetry: flipping the pair along an axis flips the control-point grid (it is
+            # centred on the image) and negates that component of alpha
+            for axis in range(3):
+                if rng.uniform() < 0.5:
+                    xb = xb.flip(3 - axis)
+                    yb = yb.flip(3 - axis)
+                    yb[..., axis] = -yb[..., axis]
+            tot += net.train_step(xb.contiguous(), yb.reshape(batch, -1).contiguous(), lr=lr)
         hist.append(tot / max(1, len(order) // batch))
         if log:
             log("epoch %d loss %.5f" % (ep, hist[-1]))
@@ -305,7 +316,34 @@ def train(n_train=256, epochs=40, batch=8, lr=2e-3, seed=0, log=None, pairs=None
                  "n_train": len(pairs)}
 
 
-def register_with_warm_start(net, fixed, moving, config=None, level0_iterations=0):
+def out_grid(shape):
+    """(x, y, z) size of the network's output for a (B, Z, Y, X, C) input."""
+    size = (shape[3], shape[2], shape[1])
+    for _, _, s, _ in LAYERS:
+        size = out_size(size, s)
+    return size
+
+
+def choose_level0_iterations(net, seeds, candidates=(0, 10, 25, 50), config=None):
+    """The fewest first-level iterations after the warm start with which every validation pair
+    reaches the plain run's final NCC within 1e-3 (the plain schedule's count if none does)."""
+    from . import register as R
+    cfg = dict(config or MS_CONFIG)
+    pairs = make_pairs(seeds, workers=1)
+    plain = [final_ncc(f, m, R.register(m, f, (1.0, 1.0, 1.0), None, cfg)[0]) for f, m in pairs]
+    for k in candidates:
+        ok = True
+        for (f, m), p in zip(pairs, plain):
+            d, _, used = register_with_warm_start(net, f, m, cfg, level0_iterations=k)
+            if final_ncc(f, m, d) < p - 1e-3:
+                ok = False
+                break
+        if ok:
+            return k
+    return int(cfg["num_function_evaluations"][0])
+
+
+def register_with_warm_start(net, fixed, moving, config=None, level0_iterations=None):
     """Multi-scale registration of `moving` onto `fixed` starting the first level from the network's
     prediction (that level then runs `level0_iterations` iterations, the later levels their plain
     schedule); falls back to the plain zero start when the prediction does not lower the first
@@ -317,7 +355,7 @@ def register_with_warm_start(net, fixed, moving, config=None, level0_iterations=
         disp, rep = R.register(moving, fixed, (1.0, 1.0, 1.0), None, cfg)       # fallback: the plain method
         return disp, rep, False
     its = list(cfg["num_function_evaluations"])
-    its[0] = level0_iterations
+    its[0] = net.level0_iterations if level0_iterations is None else level0_iterations
     disp, rep = R.register(moving, fixed, (1.0, 1.0, 1.0), None, dict(cfg, num_function_evaluations=its),
                            first_level_parameters=alpha)
     return disp, rep, True
@@ -399,9 +437,12 @@ def main(argv=None):
     ap.add_argument("--out", default=WEIGHTS_PATH)
     ap.add_argument("--weights", default=WEIGHTS_PATH)
     ap.add_argument("--held-out", type=int, default=4)
+    ap.add_argument("--validation", type=int, default=6)
     a = ap.parse_args(argv)
     if a.command == "train":
         net, hist = train(n_train=a.n, epochs=a.epochs, batch=a.batch, lr=a.lr, log=print)
+        net.level0_iterations = choose_level0_iterations(net, list(range(800_000, 800_000 + a.validation)))
+        hist["level0_iterations"] = net.level0_iterations
         net.save(a.out)
         print(json.dumps({k: v for k, v in hist.items()}))
     else:
