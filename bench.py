@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0, help="0: same as --steps (capped at 300)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-pair batched line (config 4)")
     ap.add_argument("--no-ct3d", action="store_true", help="skip the CT-like LCC line (config 3)")
+    ap.add_argument("--only", default="all", choices=["all", "batch", "ct3d", "ncc128", "mse2d"],
+                    help="run one secondary measurement alone and print its JSON (batch: --batch-pairs pairs)")
+    ap.add_argument("--batch-pairs", type=int, default=64)
     return ap.parse_args()
 
 
@@ -560,7 +563,7 @@ def ct3d_compare(torch, budget_s=150.0):
     return out
 
 
-def batch_compare(torch, steps=10, warmup=3):
+def batch_compare(torch, steps=10, warmup=3, pairs=64):
     """Config 4: 64 config-2-style pairs of uneven sizes (64^3 .. 160x160x128), NCC/MSE mixed, all
     registered together, one persistent kernel per optimizer iteration (graph-replayed); aggregate
     voxel-evaluations per second = (sum of the pairs' voxels) x iterations / device time.  The
@@ -568,7 +571,7 @@ def batch_compare(torch, steps=10, warmup=3):
     from skmimageregistration_b200 import workloads
     from skmimageregistration_b200.evaluator import Batch
     t0 = time.perf_counter()
-    problems, metrics, odesc, info = workloads.make_batch(64, seed=0)
+    problems, metrics, odesc, info = workloads.make_batch(pairs, seed=0)
     gen_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     b = Batch(problems, metrics, odesc)
@@ -836,6 +839,16 @@ def spawn_ranks(n):
 
 def main():
     args = parse()
+    if args.only != "all":                          # one secondary line alone (profiling, quick checks)
+        import torch
+        if args.only == "batch":
+            out = batch_compare(torch, steps=args.steps, warmup=args.warmup, pairs=args.batch_pairs)
+        elif args.only == "ct3d":
+            out = ct3d_compare(torch)
+        else:
+            out = multiscale_compare(args.only)
+        print(json.dumps(out), flush=True)
+        return 0
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         return spawn_ranks(args.gpus)
     rank = int(os.environ.get("RANK", "0"))

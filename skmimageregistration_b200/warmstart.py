@@ -424,12 +424,39 @@ def final_ncc(fixed, moving, disp):
     return -float(r["measure"])
 
 
+def time_steps(batch=8, steps=20):
+    """Training steps on seeded random 96x96x64 inputs (no data generation): milliseconds per step,
+    the forward + backward + Adam of the whole network on the library's kernels."""
+    import torch
+    rng = np.random.default_rng(0)
+    net = WarmStartNet(seed=0)
+    x = torch.tensor(rng.uniform(size=(batch, INPUT_SIZE[2], INPUT_SIZE[1], INPUT_SIZE[0], 2)).astype(np.float32),
+                     device="cuda").to(torch.bfloat16).contiguous()
+    g = out_grid(x.shape)
+    y = torch.tensor(rng.normal(size=(batch, g[0] * g[1] * g[2] * 3)).astype(np.float32), device="cuda")
+    for _ in range(3):
+        net.train_step(x, y)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        net.train_step(x, y)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) / steps * 1e3
+    flops = 0.0
+    size = (INPUT_SIZE[0], INPUT_SIZE[1], INPUT_SIZE[2])
+    for ci, co, s, _ in LAYERS:
+        o = out_size(size, s)
+        flops += 2.0 * batch * o[0] * o[1] * o[2] * co * 27 * ci * 3          # forward, data and weight grads
+        size = o
+    return {"batch": batch, "ms_per_step": ms, "tflops": flops / (ms * 1e-3) / 1e12, "steps": steps}
+
+
 def main(argv=None):
     """python -m skmimageregistration_b200.warmstart train [--n N] [--epochs E] [--out PATH]"""
     import argparse
     import json
     ap = argparse.ArgumentParser()
-    ap.add_argument("command", choices=["train", "gain"])
+    ap.add_argument("command", choices=["train", "gain", "steps"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--batch", type=int, default=8)
@@ -445,6 +472,8 @@ def main(argv=None):
         hist["level0_iterations"] = net.level0_iterations
         net.save(a.out)
         print(json.dumps({k: v for k, v in hist.items()}))
+    elif a.command == "steps":
+        print(json.dumps(time_steps(batch=a.batch, steps=a.epochs)))
     else:
         net = WarmStartNet.load(a.weights)
         print(json.dumps(evaluate_gain(net, list(range(900_000, 900_000 + a.held_out)))))
