@@ -475,10 +475,14 @@ def multiscale_compare(name="ncc128", override=None):
 # config 3: CT-like 256x256x160 volume, 1.5 mm voxels, LCC in the reference's form (window = kernel
 # support, radial weight, neighbourhood stride), anisotropic kernels from the structure tensor of each
 # level's smoothed target, RKHS + L1, 4 levels down to a 4-voxel control spacing (64x64x40 points)
+# The reference-form LCC costs (control points) x (samples in a point's support box) x (window
+# neighbours), both of the latter growing with the support cubed; the sampling rates and window
+# strides grow with the support (as SKMReg's defaults do, include/ConfigUtils.h) so that every level
+# keeps about 70 samples per box and 50 neighbours per window.
 CT3D_CONFIG = dict(num_scales=4, sigma_C4=[144, 72, 36, 18], sigma_C0=[288, 144, 72, 36], cp_spacing_scaler=3.0,
-                   smoothing_variance=[4, 2, 1, 0], sampling_rate=[8], neighborhood_sampling=[16, 16, 12, 12],
-                   num_function_evaluations=[100], metric="lcc", reg_rkhs=[1e-3], reg_l1=[1e-3],
-                   initial_step_size=[100.0], tensor_weights=[400, 200, 100, 50])
+                   smoothing_variance=[4, 2, 1, 0], sampling_rate=[64, 32, 16, 8],
+                   neighborhood_sampling=[96, 48, 24, 12], num_function_evaluations=[100], metric="lcc",
+                   reg_rkhs=[1e-3], reg_l1=[1e-3], initial_step_size=[100.0], tensor_weights=[400, 200, 100, 50])
 
 
 def ct3d_compare(torch, budget_s=150.0):
@@ -502,7 +506,7 @@ def ct3d_compare(torch, budget_s=150.0):
     tar = R.threshold_rescale(fixed, (-1500, 3500))
     ref_img = R.threshold_rescale(moving, (-1500, 3500))
     have_ref = os.path.exists(O.ref_gpu_path(3, True))
-    levels, ours_total, ref_total = [], 0.0, 0.0
+    levels, ours_total, ref_total, prev = [], 0.0, 0.0, None
     for s in range(int(c["num_scales"])):
         var = float(current(c, "smoothing_variance", s))
         tar_s = R.gaussian_smooth(tar, spacing, var) if var > 1e-5 else tar
@@ -532,7 +536,12 @@ def ct3d_compare(torch, budget_s=150.0):
             [n // pb.subsample for n in pb.size])), "tilt": tilt, "ours_iterations_timed": k,
             "ours_iterations_per_s": ours_it_s}
         ours_total += 100.0 / ours_it_s
-        if have_ref and time.perf_counter() - t_start < budget_s:
+        # the reference's evaluation costs about (ours) x (taps per neighbour, constant over the
+        # levels): its next time is predicted from the last one and run only if it fits the budget
+        pred_ref = None if prev is None else prev[1] * prev[0] / ours_it_s
+        lv["reference_predicted_s"] = pred_ref
+        fits = pred_ref is None or time.perf_counter() - t_start + pred_ref < budget_s
+        if have_ref and fits and time.perf_counter() - t_start < budget_s:
             e2 = GpuKernelEvaluator(pb)
             e2.SetRegularizerRKHS(float(current(c, "reg_rkhs", s)))
             r, g = e2.getValueAndDerivative(GpuKernelEvaluator.LCC, np.zeros((pb.C, 3)), ones)
@@ -548,6 +557,7 @@ def ct3d_compare(torch, budget_s=150.0):
                               "pixels_equal": bool(r["num_pixels_counted"] == rr["num_pixels_counted"]),
                               "derivative_max_rel": float(np.max(np.abs(g - gr)) / max(np.max(np.abs(gr)), 1e-300))})
             ref_total += 100.0 * t_ref
+            prev = (ours_it_s, t_ref)
         else:
             lv["reference_iterations_per_s"] = None
             ref_total = None if not have_ref else ref_total
