@@ -351,7 +351,8 @@ def register_with_warm_start(net, fixed, moving, config=None, level0_iterations=
     from . import register as R
     cfg = dict(config or MS_CONFIG)
     alpha = net.predict_alpha(fixed, moving)
-    if not first_level_value(fixed, moving, alpha) < first_level_value(fixed, moving, np.zeros_like(alpha)):
+    v_warm, v_zero = first_level_values(fixed, moving, [alpha, np.zeros_like(alpha)])
+    if not v_warm < v_zero:
         disp, rep = R.register(moving, fixed, (1.0, 1.0, 1.0), None, cfg)       # fallback: the plain method
         return disp, rep, False
     its = list(cfg["num_function_evaluations"])
@@ -361,8 +362,8 @@ def register_with_warm_start(net, fixed, moving, config=None, level0_iterations=
     return disp, rep, True
 
 
-def first_level_value(fixed, moving, alpha):
-    """Metric value (NCC + RD) of the first level at planar kernel weights `alpha`: the same
+def first_level_values(fixed, moving, alphas):
+    """Metric values (NCC + RD) of the first level at each planar kernel-weight vector: the same
     preprocessing as skm_register's first level (threshold + rescale, smoothing variance 2,
     B-spline prefilter, control spacing float(48) / 3 = 16 voxels)."""
     from . import register as R
@@ -377,9 +378,10 @@ def first_level_value(fixed, moving, alpha):
     pb = Problem(fixed=f, moving_coefficients=bspline_coefficients(m), spacing=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0),
                  sigma_c0=s0, sigma_c4=s4, cp_spacing=cps)
     ev = GpuKernelEvaluator(pb)
-    v, _ = ev.metric(MetricDesc.make("ncc", rd=float(LEVEL0["reg_rd"][0])), alpha, np.ones(pb.C), derivative=False)
+    m = MetricDesc.make("ncc", rd=float(LEVEL0["reg_rd"][0]))
+    out = [ev.metric(m, a, np.ones(pb.C), derivative=False)[0]["value"] for a in alphas]
     ev.close()
-    return v["value"]
+    return out
 
 
 def evaluate_gain(net, seeds, config=None):
