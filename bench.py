@@ -701,9 +701,13 @@ def run_ours(args, rank, world, local_rank):
     e2e_steps = args.e2e_steps or min(args.steps, 300)
     ev2 = GpuKernelEvaluator(pb)
     ev2.path(gemm_request)
-    params = np.zeros(P)
+    # the caller's parameter and derivative arrays in page-locked host memory: the metric call's
+    # kernels read the parameters and write the derivative across the bus, with no staging copies
+    def pinned(n):
+        return torch.zeros(n, dtype=torch.float64, pin_memory=True).numpy()
+    params = pinned(P)
     step = np.zeros(P)
-    grad = [np.zeros(P), np.zeros(P)]               # this and the previous step's derivative
+    grad = [pinned(P), pinned(P)]                    # this and the previous step's derivative
     t_sim = 0.0
     ev2.metric(mdesc, params, cpw)                  # warm-up
     e2e_s = 0.0

@@ -163,6 +163,8 @@ struct skm_evaluator {
     bool mg_deriv = false;
     int mg_path = 0;
     const double *mg_df = nullptr;
+    const double *mg_pdev = nullptr;   // parameter source and derivative destination the graph uses
+    double *mg_gout = nullptr;
 
     // armed by skm_evaluator_wait_drill: the next skm_get_value(_and_derivative) runs the drill
     bool drill_armed = false;
@@ -901,13 +903,28 @@ static bool same_metric(const skm_metric_desc &a, const skm_metric_desc &b)
 // packing kernel reads the parameters from the pinned staging buffer over the bus (and keeps a
 // device copy for the regularizers), and the final kernels write the derivative and the result
 // vector straight into the pinned h_out.
-static int metric_sequence(skm_evaluator *e, const skm_metric_desc *m, bool derivative)
+// params_dev: the parameters as the device reads them (the pinned staging buffer, or the caller's
+// own page-locked buffer); deriv_dev: where the derivative goes (staging, or the caller's buffer).
+static int metric_sequence(skm_evaluator *e, const skm_metric_desc *m, bool derivative, const double *params_dev,
+                           double *deriv_dev)
 {
     const long long C = e->C, n = C * e->D;
-    pack_cp_planar_copy<<<(int)((C + 255) / 256), 256, 0, e->stream>>>(e->dh_in, e->d_in + n, C, e->D, e->d_cpd,
+    pack_cp_planar_copy<<<(int)((C + 255) / 256), 256, 0, e->stream>>>(params_dev, e->d_in + n, C, e->D, e->d_cpd,
                                                                       e->d_in, planes_of(e));
     SKM_CHECK_LAUNCH();
-    return skm_metric_device(e, m, derivative, e->dh_out + NO, e->dh_out);
+    return skm_metric_device(e, m, derivative, deriv_dev, e->dh_out);
+}
+
+// Device address of a page-locked host buffer the GPU can read and write directly, else nullptr.
+static void *mapped_device_ptr(const void *p)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || !a.devicePointer || (reinterpret_cast<uintptr_t>(p) & 7u)) return nullptr;
+    return a.devicePointer;
 }
 
 extern "C" int skm_metric_evaluate(skm_evaluator *e, const skm_metric_desc *m, const double *parameters,
@@ -921,8 +938,15 @@ extern "C" int skm_metric_evaluate(skm_evaluator *e, const skm_metric_desc *m, c
     SKM_CUDA(cudaSetDevice(e->device));
     if ((rc = upload_field(e, df))) return rc;
     const long long C = e->C, n = C * e->D;
-    // (the previous call synchronised the stream, so the staging buffers are free)
-    std::memcpy(e->h_in, parameters, sizeof(double) * n);
+    // page-locked caller buffers are read and written by the kernels directly; others go through the
+    // pinned staging buffers (the previous call synchronised the stream, so those are free)
+    const double *pdev = static_cast<const double *>(mapped_device_ptr(parameters));
+    double *gdev = derivative ? static_cast<double *>(mapped_device_ptr(derivative)) : nullptr;
+    if (!pdev) {
+        std::memcpy(e->h_in, parameters, sizeof(double) * n);
+        pdev = e->dh_in;
+    }
+    double *gout = gdev ? gdev : e->dh_out + NO;
     if (!e->weights_uploaded || std::memcmp(e->h_in + n, cpw, sizeof(double) * C) != 0) {
         e->weights_uploaded = false;
         std::memcpy(e->h_in + n, cpw, sizeof(double) * C);
@@ -935,11 +959,11 @@ extern "C" int skm_metric_evaluate(skm_evaluator *e, const skm_metric_desc *m, c
         // no sampling offsets to draw: the whole device part is one graph launch
         const int path = active_path(e);
         if (!e->mgraph || !same_metric(e->mg_desc, *m) || e->mg_deriv != deriv || e->mg_path != path ||
-            e->mg_df != e->df_key) {
+            e->mg_df != e->df_key || e->mg_pdev != pdev || e->mg_gout != gout) {
             if (e->mgraph) cudaGraphExecDestroy(e->mgraph);
             e->mgraph = nullptr;
             SKM_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-            int r = metric_sequence(e, m, deriv);
+            int r = metric_sequence(e, m, deriv, pdev, gout);
             cudaGraph_t g = nullptr;
             cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
             if (r) {
@@ -957,15 +981,17 @@ extern "C" int skm_metric_evaluate(skm_evaluator *e, const skm_metric_desc *m, c
             e->mg_deriv = deriv;
             e->mg_path = path;
             e->mg_df = e->df_key;
+            e->mg_pdev = pdev;
+            e->mg_gout = gout;
         }
         SKM_CUDA(cudaGraphLaunch(e->mgraph, e->stream));
     } else {
         if ((rc = draw_shifts(e, m->do_resampling))) return rc;
-        if ((rc = metric_sequence(e, m, deriv))) return rc;
+        if ((rc = metric_sequence(e, m, deriv, pdev, gout))) return rc;
     }
     SKM_CUDA(cudaStreamSynchronize(e->stream));
     if (e->h_out[O_FAULT] != 0.0) return report_fault(e);
-    if (derivative) std::memcpy(derivative, e->h_out + NO, sizeof(double) * e->nparams);
+    if (derivative && !gdev) std::memcpy(derivative, e->h_out + NO, sizeof(double) * e->nparams);
     if (out) {
         const double *o = e->h_out;
         out->value = o[O_VALUE];
