@@ -552,10 +552,21 @@ def ct3d_compare(torch, budget_s=150.0):
             rr, gr = rg.evaluate(2, np.zeros((pb.C, 3)), ones)
             t_ref = time.perf_counter() - t0
             rg.close()
-            lv.update(reference_iterations_per_s=1.0 / t_ref,
-                      parity={"measure_rel": abs(r["measure"] - rr["measure"]) / max(abs(rr["measure"]), 1e-300),
-                              "pixels_equal": bool(r["num_pixels_counted"] == rr["num_pixels_counted"]),
-                              "derivative_max_rel": float(np.max(np.abs(g - gr)) / max(np.max(np.abs(gr)), 1e-300))})
+            def parity(rr, gr):
+                return {"measure_rel": abs(r["measure"] - rr["measure"]) / max(abs(rr["measure"]), 1e-300),
+                        "pixels_equal": bool(r["num_pixels_counted"] == rr["num_pixels_counted"]),
+                        "derivative_max_rel": float(np.max(np.abs(g - gr)) / max(np.max(np.abs(gr)), 1e-300))}
+            lv.update(reference_iterations_per_s=1.0 / t_ref, parity=parity(rr, gr))
+            if os.path.exists(O.ref_gpu_path(3, True, ieee=True)):
+                # the same reference sources built with IEEE arithmetic (no fast math, no contraction)
+                ri = O.RefGpu(pb, double=True, ieee=True)
+                ri.set_regularizers(rkhs=float(current(c, "reg_rkhs", s)))
+                rri, gri = ri.evaluate(2, np.zeros((pb.C, 3)), ones)
+                ri.close()
+                lv["parity_ieee_build"] = parity(rri, gri)
+                lv["reference_builds"] = {
+                    "measure_rel": abs(rr["measure"] - rri["measure"]) / max(abs(rri["measure"]), 1e-300),
+                    "derivative_max_rel": float(np.max(np.abs(gr - gri)) / max(np.max(np.abs(gri)), 1e-300))}
             ref_total += 100.0 * t_ref
             prev = (ours_it_s, t_ref)
         else:

@@ -219,15 +219,16 @@ def ref_host(D):
     return L
 
 
-def ref_gpu_path(D, double=True):
-    return os.path.join(REF_DIR, "libskmref_gpu_%s%d.so" % ("d" if double else "f", D))
+def ref_gpu_path(D, double=True, ieee=False):
+    """ieee=True: the double build with IEEE arithmetic (no fast math, no multiply-add contraction)."""
+    return os.path.join(REF_DIR, "libskmref_gpu_%s%d%s.so" % ("d" if double else "f", D, "_ieee" if ieee else ""))
 
 
 class RefGpu:
     """The reference's own GpuKernelEvaluator (needs a GPU and the _ref build)."""
 
-    def __init__(self, problem: Problem, double=True):
-        path = ref_gpu_path(problem.D, double)
+    def __init__(self, problem: Problem, double=True, ieee=False):
+        path = ref_gpu_path(problem.D, double, ieee)
         L = C.CDLL(path)
         L.skmref_create.argtypes = [C.POINTER(EvaluatorDesc), C.POINTER(C.c_void_p)]
         L.skmref_destroy.argtypes = [C.c_void_p]

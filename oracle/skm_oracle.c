@@ -1,8 +1,9 @@
 /*
  * skm_oracle.c -- FP64 CPU restatement of the reference SKM evaluation path.
  *
- * TEST INFRASTRUCTURE ONLY (see skm_oracle.h).  All arithmetic is double; the
- * loops follow the reference's per-thread kernels one for one, including the
+ * TEST INFRASTRUCTURE ONLY (see skm_oracle.h).  Arithmetic is double except where the
+ * reference's own types make a decision in float (the kernel's float members and the weight-tensor
+ * support radius); expressions are evaluated as written (C11, no contraction).  The loops follow the reference's per-thread kernels one for one, including the
  * exact index boxes (truncation toward zero, clamping) because those boxes decide
  * which control points / samples contribute.  Parallelised with OpenMP over the
  * independent outer loop; every reduction is summed per thread and then combined
@@ -113,32 +114,31 @@ static void inv_m(const double *m, int D, double *r)
     for (int i = 0; i < 9; ++i) r[i] = a[i] / dt;
 }
 
-static double max_eig(const double *m, int D)
+/* maxEigenValue (Mat.h:259-281) with Type = float */
+static float max_eig_f(const float *m, int D)
 {
     if (D == 2) {
-        double tr = m[0] + m[3];
-        double dt = det_m(m, 2);
-        double disc = tr * tr - 4.0 * dt;
-        return 0.5 * (tr + sqrt(disc > 0.0 ? disc : 0.0));
+        float trace = m[0] + m[3];
+        float det = m[0] * m[3] - m[2] * m[1];
+        float disc = trace * trace - 4.0f * det;
+        return 0.5f * (trace + sqrtf(disc > 0.0f ? disc : 0.0f));
     }
-    double triSq = m[1] * m[1] + m[2] * m[2] + m[5] * m[5];
-    if (triSq == 0.0) {
-        double r = m[0];
-        if (m[4] > r) r = m[4];
-        if (m[8] > r) r = m[8];
-        return r;
+    float triSq = m[1] * m[1] + m[2] * m[2] + m[5] * m[5];
+    if (triSq == 0.0f) {
+        float r = m[8] > m[4] ? m[8] : m[4];
+        return m[0] > r ? m[0] : r;
     }
-    double q = (1.0 / 3.0) * (m[0] + m[4] + m[8]);
-    double pSq = 2.0 * triSq + (m[0] - q) * (m[0] - q) + (m[4] - q) * (m[4] - q) + (m[8] - q) * (m[8] - q);
-    double p = sqrt(pSq * (1.0 / 6.0));
-    double b[9];
-    memcpy(b, m, sizeof b);
-    b[0] -= q; b[4] -= q; b[8] -= q;          /* Mat - scalar subtracts from the diagonal */
-    double r = det_m(b, 3) * (0.5 / (p * p * p));
-    if (r > 1.0) r = 1.0;
-    if (r < -1.0) r = -1.0;
-    double phi = (1.0 / 3.0) * acos(r);
-    return q + 2.0 * p * cos(phi);
+    float q = (float)(1.0 / 3.0) * (m[0] + m[4] + m[8]);
+    float pSq = 2.0f * triSq + (m[0] - q) * (m[0] - q) + (m[4] - q) * (m[4] - q) + (m[8] - q) * (m[8] - q);
+    float p = sqrtf(pSq * (float)(1.0 / 6.0));
+    float b0 = m[0] - q, b4 = m[4] - q, b8 = m[8] - q;
+    float det = b0 * b4 * b8 + m[3] * m[7] * m[2] + m[6] * m[1] * m[5] - b0 * m[7] * m[5] - m[6] * b4 * m[2] -
+                m[3] * m[1] * b8;
+    float r = det * (0.5f / (p * p * p));
+    if (r > 1.0f) r = 1.0f;
+    if (r < -1.0f) r = -1.0f;
+    float phi = (float)(1.0 / 3.0) * acosf(r);
+    return q + 2.0f * p * cosf(phi);
 }
 
 /* ------------------------------------------------------------------------- */
@@ -152,6 +152,26 @@ typedef struct {
     const double *wi; geo_t gwi;
     const double *wt; geo_t gwt;
 } kern_t;
+
+/* GKernel<float> keeps sigmaC0, sigmaC4, the maximum weight and the maximum-eigenvalue
+ * covariance as float members (Kernel.h:37-41, typedef at :228): the oracle rounds them the same
+ * way, so that support radii (and the window and box bounds truncated from them) are the
+ * reference's to the last bit.  The weight image and tensors stay double (ImageNearest<ScalarType>,
+ * Kernel.h:43-44). */
+static void kern_init(kern_t *K, const skm_evaluator_desc *d)
+{
+    K->D = d->dimensions;
+    K->sc0 = (float)d->sigma_c0;
+    K->sc4 = (float)d->sigma_c4;
+    K->use_wi = d->use_weight_image;
+    K->use_wt = d->use_weight_tensor;
+    K->maxw = (float)d->maximum_weight;
+    for (int i = 0; i < 9; ++i) K->maxcov[i] = (float)d->maximum_eigenvalue_covariance[i];
+    K->wi = d->weight_image;
+    geo_set(&K->gwi, &d->weight_image_geometry, d->dimensions, 0);
+    K->wt = d->weight_tensor;
+    geo_set(&K->gwt, &d->weight_tensor_geometry, d->dimensions, 0);
+}
 
 /* Wendland C4 (Kernel.h:72-77) and C0 (Kernel.h:48-53) radial profiles. */
 static inline double wend_c4(double r)
@@ -202,11 +222,14 @@ static void kern_pinfo(const kern_t *K, const double *p, pinfo_t *pi)
         kern_sigma_at(K, p, &pi->sigma);
         pi->support = smin / sqrt(2.0 / (K->maxw + pi->sigma));           /* Kernel.h:163-166 */
     } else if (K->use_wt) {
-        double s[9];
+        /* Kernel.h:168-171: the float member _maximumEigenvalueCovariance plus the double tensor
+         * goes through Mat<float>::operator+ (Mat.h:108), so the sum, maxEigenValue, the division
+         * and the square root are float */
+        float s[9];
         int D = K->D;
         kern_cov_at(K, p, pi->cov);
-        for (int i = 0; i < D * D; ++i) s[i] = K->maxcov[i] + pi->cov[i];
-        pi->support = smin / sqrt(2.0 / max_eig(s, D));                   /* Kernel.h:168-171 */
+        for (int i = 0; i < D * D; ++i) s[i] = (float)K->maxcov[i] + (float)pi->cov[i];
+        pi->support = (double)((float)smin / sqrtf(2.0f / max_eig_f(s, D)));
     } else {
         pi->support = smin;                                               /* Kernel.h:158-161 */
     }
@@ -443,17 +466,7 @@ ora_ctx *ora_create(const skm_evaluator_desc *d)
     c->sub = d->subsample;
     c->nbh = d->subsample_neighborhood;
     c->nparams = d->num_parameters;
-    c->K.D = D;
-    c->K.sc0 = d->sigma_c0;
-    c->K.sc4 = d->sigma_c4;
-    c->K.use_wi = d->use_weight_image;
-    c->K.use_wt = d->use_weight_tensor;
-    c->K.maxw = d->maximum_weight;
-    memcpy(c->K.maxcov, d->maximum_eigenvalue_covariance, sizeof c->K.maxcov);
-    c->K.wi = d->weight_image;
-    geo_set(&c->K.gwi, &d->weight_image_geometry, D, 0);
-    c->K.wt = d->weight_tensor;
-    geo_set(&c->K.gwt, &d->weight_tensor_geometry, D, 0);
+    kern_init(&c->K, d);
     geo_set(&c->fixed, &d->fixed_geometry, D, 0);
     geo_set(&c->moving_pad, &d->moving_geometry, D, 3);
     geo_set(&c->cp, &d->cp_geometry, D, 0);
@@ -1102,13 +1115,7 @@ void ora_kernel_values(const skm_evaluator_desc *d, int64_t n, const double *p, 
     kern_t K;
     int D = d->dimensions;
     memset(&K, 0, sizeof K);
-    K.D = D;
-    K.sc0 = d->sigma_c0; K.sc4 = d->sigma_c4;
-    K.use_wi = d->use_weight_image; K.use_wt = d->use_weight_tensor;
-    K.maxw = d->maximum_weight;
-    memcpy(K.maxcov, d->maximum_eigenvalue_covariance, sizeof K.maxcov);
-    K.wi = d->weight_image; geo_set(&K.gwi, &d->weight_image_geometry, D, 0);
-    K.wt = d->weight_tensor; geo_set(&K.gwt, &d->weight_tensor_geometry, D, 0);
+    kern_init(&K, d);
     for (int64_t i = 0; i < n; ++i) {
         pinfo_t pi;
         kern_pinfo(&K, p + i * D, &pi);

@@ -7,10 +7,12 @@
 // on the stream and copies the scalars and the derivative back.  Every reduction is
 // done on the device in a fixed order; no host loops over per-voxel arrays remain.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/skm_gpu.h"
@@ -110,6 +112,68 @@ unsigned long long rng_advance_host(unsigned long long s, unsigned long long ste
     return s;
 }
 
+// maxEigenValue (Mat.h:259-281) with Type = float, evaluated as written (no multiply-add
+// contraction on this host).  getRegionSupport(covP) (Kernel.h:168-171) adds the double tensor to
+// the float member _maximumEigenvalueCovariance through Mat<float>::operator+ (Mat.h:108), so the
+// sum, the eigenvalue, the division and the square root are all float.
+float max_eig_f(const float *m, int D)
+{
+    if (D == 2) {
+        float trace = m[0] + m[3];
+        float det = m[0] * m[3] - m[2] * m[1];
+        float disc = trace * trace - 4.0f * det;
+        return 0.5f * (trace + std::sqrt(disc > 0.0f ? disc : 0.0f));
+    }
+    float triSq = m[1] * m[1] + m[2] * m[2] + m[5] * m[5];
+    if (triSq == 0.0f) return std::max(m[0], std::max(m[4], m[8]));
+    float q = (float)(1.0 / 3.0) * (m[0] + m[4] + m[8]);
+    float pSq = 2.0f * triSq + (m[0] - q) * (m[0] - q) + (m[4] - q) * (m[4] - q) + (m[8] - q) * (m[8] - q);
+    float p = std::sqrt(pSq * (float)(1.0 / 6.0));
+    float b0 = m[0] - q, b4 = m[4] - q, b8 = m[8] - q;
+    float det = b0 * b4 * b8 + m[3] * m[7] * m[2] + m[6] * m[1] * m[5] - b0 * m[7] * m[5] - m[6] * b4 * m[2] -
+                m[3] * m[1] * b8;
+    float r = det * (0.5f / (p * p * p));
+    float phi = (float)(1.0 / 3.0) * std::acos(std::min(1.0f, std::max(-1.0f, r)));
+    return q + 2.0f * p * std::cos(phi);
+}
+
+float tensor_support(const KernelParams &K, const double *cov, int D)
+{
+    float s[9];
+    for (int e = 0; e < D * D; ++e) s[e] = K.maxcov[e] + (float)cov[e];
+    return K.support_min / std::sqrt(2.0f / max_eig_f(s, D));
+}
+
+// Support radius per texel of the weight image (double: the float member _maximumWeight plus the
+// double sigma, Kernel.h:163-166) or of the weight tensors (float, above), and the radius where
+// the lookup falls outside the image (sigma 0 / identity covariance).  Radii decide the windows
+// and boxes by truncation; with voxel-commensurate sigmas they sit on integer boundaries, so they
+// are computed once here, exactly as the reference's expressions round them.
+void support_table(const KernelParams &K, int D, const double *src, long long n, double *out, double *dflt)
+{
+    const bool tensor = K.kind == kWeightTensor;
+    if (tensor) {
+        double eye[9] = {0};
+        for (int d = 0; d < D; ++d) eye[d * D + d] = 1.0;
+        *dflt = (double)tensor_support(K, eye, D);
+    } else {
+        *dflt = (double)K.support_min / std::sqrt(2.0 / ((double)K.maxw + 0.0));
+    }
+    auto work = [&](long long b, long long e) {
+        for (long long i = b; i < e; ++i)
+            out[i] = tensor ? (double)tensor_support(K, src + i * D * D, D)
+                            : (double)K.support_min / std::sqrt(2.0 / ((double)K.maxw + src[i]));
+    };
+    unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (n < (1LL << 16)) nt = 1;
+    std::vector<std::thread> th;
+    long long chunk = (n + nt - 1) / nt;
+    for (unsigned t = 1; t < nt; ++t)
+        th.emplace_back(work, std::min(n, t * chunk), std::min(n, (t + 1) * chunk));
+    work(0, std::min(n, chunk));
+    for (auto &x : th) x.join();
+}
+
 constexpr int kValueThreads = 256;
 constexpr int kDerivThreads = 256;     // 8 warps = 8 control points per block
 constexpr int kSplitBelowBlocks = 1024; // fewer derivative blocks than this: one block per control point
@@ -129,6 +193,7 @@ struct skm_evaluator {
 
     // device memory
     float *d_fixed = nullptr, *d_coeffs = nullptr, *d_wimg = nullptr, *d_wten = nullptr;
+    double *d_wsup = nullptr;         // support radius per weight-image / weight-tensor texel
     float4 *d_coeffs4 = nullptr;
     float4 *d_cpd = nullptr, *d_df = nullptr, *d_samp = nullptr, *d_dense = nullptr, *d_dense_sw = nullptr;
     unsigned char *d_dense_in = nullptr, *d_dense_sw_in = nullptr;
@@ -174,7 +239,7 @@ struct skm_evaluator {
         if (device >= 0) cudaSetDevice(device);
         // one device synchronisation for all buffers (no work uses them after it), then the frees
         cudaDeviceSynchronize();
-        void *bufs[] = {d_fixed, d_coeffs, d_coeffs4, d_wimg, d_wten, d_cpd, d_df, d_samp, d_dense, d_dense_sw, d_dense_in,
+        void *bufs[] = {d_fixed, d_coeffs, d_coeffs4, d_wimg, d_wten, d_wsup, d_cpd, d_df, d_samp, d_dense, d_dense_sw, d_dense_in,
                         d_dense_sw_in, d_shifts, d_in, d_counters, d_part, d_stats, d_deriv, d_rpart, d_out};
         for (void *b : bufs)
             if (b) pool_release(b);
@@ -410,6 +475,8 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         for (int i = 0; i < 9; ++i) K.maxcov[i] = (float)d->maximum_eigenvalue_covariance[i];
         K.wimg = nullptr;
         K.wten = nullptr;
+        K.wsup = nullptr;
+        K.sup_default = (double)K.support_min;
         K.gw = make_geo(d->weight_image_geometry, D, 0);
         K.gt = make_geo(d->weight_tensor_geometry, D, 0);
 
@@ -441,6 +508,11 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
             if (dalloc(&e->d_wimg, n)) return SKM_ERR_CUDA;
             SKM_CUDA(cudaMemcpy(e->d_wimg, w.data(), n * sizeof(float), cudaMemcpyHostToDevice));
             K.wimg = e->d_wimg;
+            std::vector<double> sup((size_t)n);
+            support_table(K, D, d->weight_image, n, sup.data(), &K.sup_default);
+            if (dalloc(&e->d_wsup, n)) return SKM_ERR_CUDA;
+            SKM_CUDA(cudaMemcpy(e->d_wsup, sup.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+            K.wsup = e->d_wsup;
         }
         if (d->use_weight_tensor) {
             long long n = texels(d->weight_tensor_geometry, D) * D * D;
@@ -449,6 +521,12 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
             if (dalloc(&e->d_wten, n)) return SKM_ERR_CUDA;
             SKM_CUDA(cudaMemcpy(e->d_wten, w.data(), n * sizeof(float), cudaMemcpyHostToDevice));
             K.wten = e->d_wten;
+            long long nt = texels(d->weight_tensor_geometry, D);
+            std::vector<double> sup((size_t)nt);
+            support_table(K, D, d->weight_tensor, nt, sup.data(), &K.sup_default);
+            if (dalloc(&e->d_wsup, nt)) return SKM_ERR_CUDA;
+            SKM_CUDA(cudaMemcpy(e->d_wsup, sup.data(), nt * sizeof(double), cudaMemcpyHostToDevice));
+            K.wsup = e->d_wsup;
         }
         P.fixed_data = e->d_fixed;
         P.coeffs = e->d_coeffs;

@@ -171,20 +171,28 @@ struct KernelParams {
     Geo gw;
     const float *wten;       // covariance tensors, D*D floats per texel
     Geo gt;
+    const double *wsup;      // support radius per weight-image / weight-tensor texel
+    double sup_default;      // support radius outside that image
 };
 
+// Rounded as written (product, then sum; no contraction): global positions feed the truncated
+// window and box bounds, which must not move by an ulp against the reference's arithmetic.
 template <int D>
 __device__ __forceinline__ void to_global(const Geo &g, const double *idx, double *p)
 {
 #pragma unroll
-    for (int d = 0; d < D; ++d) p[d] = g.o[d] + g.s[d] * idx[d];
+    for (int d = 0; d < D; ++d) p[d] = __dadd_rn(g.o[d], __dmul_rn(g.s[d], idx[d]));
 }
 
+// The product is rounded on its own: callers subtract a support half-width or add 0.5 and
+// truncate, and a multiply-add fused across the inlined call would truncate inv*(p-o) - h + 1
+// from just below an integer where the rounded product lands on it (window and box bounds one
+// cell lower, and with a neighbourhood stride above 1 a different neighbour lattice).
 template <int D>
 __device__ __forceinline__ void to_local(const Geo &g, const double *p, double *l)
 {
 #pragma unroll
-    for (int d = 0; d < D; ++d) l[d] = g.inv[d] * (p[d] - g.o[d]);
+    for (int d = 0; d < D; ++d) l[d] = __dmul_rn(g.inv[d], __dsub_rn(p[d], g.o[d]));
 }
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -262,30 +270,6 @@ __device__ __forceinline__ float quad_inv(const float *m, const float *v)
     return q;
 }
 
-// maxEigenValue (Mat.h:259-281) in double (support radius only).
-template <int D>
-__device__ __forceinline__ double max_eig(const double *m)
-{
-    if (D == 2) {
-        double tr = m[0] + m[3];
-        double dt = m[0] * m[3] - m[2] * m[1];
-        double disc = tr * tr - 4.0 * dt;
-        return 0.5 * (tr + sqrt(disc > 0.0 ? disc : 0.0));
-    }
-    double triSq = m[1] * m[1] + m[2] * m[2] + m[5] * m[5];
-    if (triSq == 0.0) return fmax(m[0], fmax(m[4], m[8]));
-    double q = (1.0 / 3.0) * (m[0] + m[4] + m[8]);
-    double pSq = 2.0 * triSq + (m[0] - q) * (m[0] - q) + (m[4] - q) * (m[4] - q) + (m[8] - q) * (m[8] - q);
-    double p = sqrt(pSq * (1.0 / 6.0));
-    double b0 = m[0] - q, b4 = m[4] - q, b8 = m[8] - q;
-    double dt = b0 * b4 * b8 + m[3] * m[7] * m[2] + m[6] * m[1] * m[5] - b0 * m[7] * m[5] - m[6] * b4 * m[2] -
-                m[3] * m[1] * b8;
-    double r = dt * (0.5 / (p * p * p));
-    r = fmin(1.0, fmax(-1.0, r));
-    double phi = (1.0 / 3.0) * acos(r);
-    return q + 2.0 * p * cos(phi);
-}
-
 // Per-point information of GKernel::evaluate(p, q, [sigmaP | covP]) and its support radius.
 struct PInfo {
     double support;
@@ -313,22 +297,28 @@ __device__ __forceinline__ void cov_at(const KernelParams &K, const double *p, f
     }
 }
 
-// getRegionSupport overloads (Kernel.h:158-171).
+// getRegionSupport overloads (Kernel.h:158-171).  The per-texel radii of the weight image and the
+// weight tensors come from a table the host fills once (support_table in skm_capi.cu); outside the
+// image the lookup default applies (sigma 0, identity covariance) and with it sup_default.
 template <int KIND, int D>
 __device__ __forceinline__ void pinfo_at(const KernelParams &K, const double *p, PInfo &pi)
 {
-    double smin = (double)K.support_min;
     if (KIND == kWeightImage) {
-        pi.sigma = sigma_at<D>(K, p);
-        pi.support = smin / sqrt(2.0 / ((double)K.maxw + (double)pi.sigma));
+        long long i = nearest_index<D>(K.gw, p);
+        pi.sigma = i >= 0 ? K.wimg[i] : 0.0f;          // ImageNearest default 0 (ImageNearest.h:41-45)
+        pi.support = i >= 0 ? K.wsup[i] : K.sup_default;
     } else if (KIND == kWeightTensor) {
-        cov_at<D>(K, p, pi.cov);
-        double s[9];
+        long long i = nearest_index<D>(K.gt, p);
+        if (i >= 0) {
 #pragma unroll
-        for (int e = 0; e < D * D; ++e) s[e] = (double)K.maxcov[e] + (double)pi.cov[e];
-        pi.support = smin / sqrt(2.0 / max_eig<D>(s));
+            for (int e = 0; e < D * D; ++e) pi.cov[e] = K.wten[i * D * D + e];
+        } else {                                       // identity default (ImageNearest.h:47-51)
+#pragma unroll
+            for (int e = 0; e < D * D; ++e) pi.cov[e] = (e % (D + 1) == 0) ? 1.0f : 0.0f;
+        }
+        pi.support = i >= 0 ? K.wsup[i] : K.sup_default;
     } else {
-        pi.support = smin;
+        pi.support = (double)K.support_min;
     }
 }
 
@@ -551,6 +541,66 @@ __device__ __forceinline__ unsigned pcg32_output(unsigned long long old)
 }
 
 // ---------------------------------------------------------------------------------------------
+// LCC window arithmetic (GpuEvaluatorLCC.cu:28-35, 152-191), every operation rounded as written.
+// A window with one neighbour has sff = f*f, msf = f, so sff - 2*msf*sf + n*msf*msf is exactly 0
+// when each product is rounded; a contracted multiply-add leaves the rounding error of f*f
+// instead, which can pass the d1 > 0 && d2 > 0 test and turn into an arbitrary -cc^2/(d1*d2).
+struct LccWindow {
+    double sf = 0, sm = 0, sff = 0, smm = 0, sfm = 0;
+    int n = 0;
+    __device__ __forceinline__ void add(double fv, double mv)
+    {
+        sf = __dadd_rn(sf, fv);
+        sm = __dadd_rn(sm, mv);
+        sff = __dadd_rn(sff, __dmul_rn(fv, fv));
+        smm = __dadd_rn(smm, __dmul_rn(mv, mv));
+        sfm = __dadd_rn(sfm, __dmul_rn(fv, mv));
+        ++n;
+    }
+    __device__ __forceinline__ double msf() const { return __ddiv_rn(sf, (double)n); }
+    __device__ __forceinline__ double msm() const { return __ddiv_rn(sm, (double)n); }
+    // s2 - 2*m*s + n*m*m
+    __device__ __forceinline__ double centred(double s2, double s, double m) const
+    {
+        return __dadd_rn(__dsub_rn(s2, __dmul_rn(__dmul_rn(2.0, m), s)), __dmul_rn(__dmul_rn((double)n, m), m));
+    }
+    __device__ __forceinline__ double d1() const { return centred(sff, sf, msf()); }
+    __device__ __forceinline__ double d2() const { return centred(smm, sm, msm()); }
+    // sfm - msm*sf - msf*sm + n*msf*msm
+    __device__ __forceinline__ double cross() const
+    {
+        double a = msf(), b = msm();
+        return __dadd_rn(__dsub_rn(__dsub_rn(sfm, __dmul_rn(b, sf)), __dmul_rn(a, sm)),
+                         __dmul_rn(__dmul_rn((double)n, a), b));
+    }
+    // the window's value: -cc^2 / (d1*d2) when both centred sums are positive, else 0
+    __device__ __forceinline__ double value() const
+    {
+        if (n <= 0) return 0.0;
+        double a = d1(), b = d2();
+        if (!(a > 0 && b > 0)) return 0.0;
+        double cc = cross();
+        return __ddiv_rn(__dmul_rn(-cc, cc), __dmul_rn(a, b));
+    }
+};
+
+// neighborhoodWeight(p, q, support, 10) (LCC.cu:28-35): (1 - (|p-q|/support)^10)^2, written as
+// (r2/support^2)^5; returns a value <= 0 where the reference's weight is 0.  r2 and support^2
+// are exact for grid positions and a float support, so the sign matches pow(|p-q|/support, 10).
+template <int D>
+__device__ __forceinline__ double lcc_weight_base(const double *p, const double *q, double support)
+{
+    double r2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        double t = __dsub_rn(p[d], q[d]);
+        r2 = __dadd_rn(r2, __dmul_rn(t, t));
+    }
+    double tt = __ddiv_rn(r2, __dmul_rn(support, support));
+    double t2 = __dmul_rn(tt, tt);
+    return __dsub_rn(1.0, __dmul_rn(__dmul_rn(t2, t2), tt));
+}
+
 // deterministic reductions (fixed shuffle tree, fixed block order)
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v)

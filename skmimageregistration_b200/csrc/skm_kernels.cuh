@@ -502,9 +502,8 @@ __device__ __forceinline__ void lcc_sample_derivative(const EvalParams &P, const
     const bool swapped = (D == 3 && KIND != kStationary);
     const float4 *dense = swapped ? Q.dense_sw : Q.dense;
     const unsigned char *dense_in = swapped ? Q.dense_sw_in : Q.dense_in;
-    double sf = 0, sm = 0, sff = 0, smm = 0, sfm = 0;
+    LccWindow W;
     double mkcka[3] = {0, 0, 0}, mkcmkcka[3] = {0, 0, 0}, fkcmka[3] = {0, 0, 0};
-    int n = 0;
     for (int z = flo[2]; z <= fhi[2]; z += P.nbh)
         for (int y = flo[1]; y <= fhi[1]; y += P.nbh)
             for (int x = flo[0]; x <= fhi[0]; x += P.nbh) {
@@ -514,16 +513,9 @@ __device__ __forceinline__ void lcc_sample_derivative(const EvalParams &P, const
                 PInfo pn;
                 pinfo_at<KIND, D>(P.K, q, pn);
                 // neighborhoodWeight with the neighbour's support passed as float (LCC.cu:28-35)
-                double sup = (double)(float)pn.support;
-                double r2 = 0.0;
-#pragma unroll
-                for (int d = 0; d < D; ++d) r2 += (pt[d] - q[d]) * (pt[d] - q[d]);
-                double t = r2 / (sup * sup);
-                double t2 = t * t;
-                double rr = t2 * t2 * t;                       // (r/support)^10
-                double kwf = 1.0 - rr;
+                double kwf = lcc_weight_base<D>(pt, q, (double)(float)pn.support);
                 if (kwf <= 0.0) continue;
-                double kw = kwf * kwf;
+                double kw = __dmul_rn(kwf, kwf);
                 long long nl = lin_of<D>(P.fixed, ni);
                 if (!dense_in[nl]) continue;
                 // ka = k(cp, n) with the neighbour's kernel information (LCC.cu:449-461)
@@ -532,9 +524,9 @@ __device__ __forceinline__ void lcc_sample_derivative(const EvalParams &P, const
                 for (int d = 0; d < D; ++d) v[d] = (float)(gp[d] - q[d]);
                 float ka = k_eval<KIND, D>(P.K, v, q, pn);
                 float4 rec = dense[nl];
-                double mv = (double)rec.w * kw;
-                double fv = kw * (double)P.fixed_data[nl];
-                sf += fv; sm += mv; sff += fv * fv; smm += mv * mv; sfm += fv * mv;
+                double mv = __dmul_rn((double)rec.w, kw);
+                double fv = __dmul_rn(kw, (double)P.fixed_data[nl]);
+                W.add(fv, mv);
                 double g[3] = {rec.x, rec.y, rec.z};
 #pragma unroll
                 for (int d = 0; d < D; ++d) {
@@ -543,13 +535,12 @@ __device__ __forceinline__ void lcc_sample_derivative(const EvalParams &P, const
                     mkcka[d] += gk;
                     fkcmka[d] += fv * gk;
                 }
-                ++n;
             }
-    if (n > 0) {
-        double msf = sf / n, msm = sm / n;
-        double d1 = sff - 2.0 * msf * sf + n * msf * msf;
-        double u = d1 * (smm - 2.0 * msm * sm + n * msm * msm);
-        double vv = sfm - msm * sf - msf * sm + n * msf * msm;
+    if (W.n > 0) {
+        double msf = W.msf(), msm = W.msm();
+        double d1 = W.d1();
+        double u = __dmul_rn(d1, W.d2());
+        double vv = W.cross();
         if (fabs(u) > 1e-16) {
 #pragma unroll
             for (int d = 0; d < D; ++d) {
@@ -903,8 +894,7 @@ __global__ void __launch_bounds__(256) lcc_value_kernel(EvalParams P, const floa
                 lo[d] = clampi((int)(fl[d] - shf + 1.0), 0, P.fixed.n[d] - 1);
                 hi[d] = clampi((int)(fl[d] + shf), 0, P.fixed.n[d] - 1);
             }
-            double sf = 0, sm = 0, sff = 0, smm = 0, sfm = 0;
-            int n = 0;
+            LccWindow W;
             for (int z = lo[2]; z <= hi[2]; z += P.nbh)
                 for (int y = lo[1]; y <= hi[1]; y += P.nbh)
                     for (int x = lo[0]; x <= hi[0]; x += P.nbh) {
@@ -919,30 +909,14 @@ __global__ void __launch_bounds__(256) lcc_value_kernel(EvalParams P, const floa
                             pinfo_at<KIND, D>(P.K, q, pn);
                             sup = (double)(float)pn.support;
                         }
-                        double r2 = 0.0;
-#pragma unroll
-                        for (int d = 0; d < D; ++d) r2 += (p[d] - q[d]) * (p[d] - q[d]);
-                        double tt = r2 / (sup * sup);
-                        double t2 = tt * tt;
-                        double kwf = 1.0 - t2 * t2 * tt;
+                        double kwf = lcc_weight_base<D>(p, q, sup);
                         if (kwf <= 0.0) continue;
-                        double kw = kwf * kwf;
+                        double kw = __dmul_rn(kwf, kwf);
                         long long nl = lin_of<D>(P.fixed, ni);
                         if (!dense_in[nl]) continue;
-                        double mv = (double)dense[nl].w * kw;
-                        double fv = kw * (double)P.fixed_data[nl];
-                        sf += fv; sm += mv; sff += fv * fv; smm += mv * mv; sfm += fv * mv;
-                        ++n;
+                        W.add(__dmul_rn(kw, (double)P.fixed_data[nl]), __dmul_rn((double)dense[nl].w, kw));
                     }
-            if (n > 0) {
-                double msf = sf / n, msm = sm / n;
-                double d1 = sff - 2.0 * msf * sf + n * msf * msf;
-                double d2 = smm - 2.0 * msm * sm + n * msm * msm;
-                if (d1 > 0 && d2 > 0) {
-                    double cc = sfm - msm * sf - msf * sm + n * msf * msm;
-                    v[Q_CC] = -cc * cc / (d1 * d2);
-                }
-            }
+            v[Q_CC] = W.value();
         }
     }
     block_sum<NQ>(v, sh);
