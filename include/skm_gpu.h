@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define SKM_ABI_VERSION 5
+#define SKM_ABI_VERSION 6
 
 /* Status codes. */
 #define SKM_OK              0
@@ -140,7 +140,9 @@ int skm_evaluator_destroy(skm_evaluator *ev);
 /* Kernel path selection (no counterpart in the reference, which has one path).
  * request: -1 query only, 0 automatic (phase-table path where it applies, its two GEMMs on
  * the tensor cores where they fit), 1 generic kernels only, 2 phase-table path with its
- * GEMMs on the CUDA cores.  *active (may be NULL) receives the path MSE/NCC calls take:
+ * GEMMs on the CUDA cores, 3 phase-table path on the tensor cores with the contrib GEMM summing
+ * into per-brick control-point patches instead of the per-tap contribution array (3-D; same
+ * sums in another order; slower on a B200 at 128x128x96, kept selectable).  *active (may be NULL) receives the path MSE/NCC calls take:
  * 1 generic, 2 phase table (stationary kernel, control spacing an integer multiple of
  * the fixed spacing, subsample 1), 3 phase table with tensor-core GEMMs (3xTF32, FP32
  * accuracy).  All paths compute the same sums. */
@@ -174,6 +176,8 @@ typedef struct skm_evaluator_info {
     int32_t tc_region_buffers;        /* transform: region buffers of the tiled-load ring */
     int32_t tc_u_staging;             /* transform: output staging buffers (0: direct stores of u) */
     int32_t tc_record_slots;          /* contrib: record ring slots (0: direct record loads) */
+    int32_t tc_contrib_bricks;        /* 1: the contrib GEMM sums into per-brick control-point
+                                         patches that the gather adds up (no per-tap array) */
 } skm_evaluator_info;
 int skm_evaluator_describe(skm_evaluator *ev, skm_evaluator_info *out);
 

@@ -115,6 +115,7 @@ class EvaluatorInfo(C.Structure):
         ("tc_region_buffers", C.c_int32),
         ("tc_u_staging", C.c_int32),
         ("tc_record_slots", C.c_int32),
+        ("tc_contrib_bricks", C.c_int32),
     ]
 
     def as_dict(self):

@@ -585,11 +585,16 @@ extern "C" int skm_evaluator_path(skm_evaluator *e, int32_t request, int32_t *ac
     } else if (request == 0) {
         e->use_table = true;
         e->use_tc = true;
+        e->tc.fused_on = false;
     } else if (request == 2) {
         e->use_table = true;
         e->use_tc = false;
+    } else if (request == 3) {
+        e->use_table = true;
+        e->use_tc = true;
+        e->tc.fused_on = true;
     } else if (request != -1) {
-        return fail(SKM_ERR_INVALID, "path request must be -1, 0, 1 or 2");
+        return fail(SKM_ERR_INVALID, "path request must be -1, 0, 1, 2 or 3");
     }
     if (active) *active = active_path(e);
     return SKM_OK;
@@ -620,7 +625,8 @@ extern "C" int skm_evaluator_describe(skm_evaluator *e, skm_evaluator_info *out)
         r.tc_brick[1] = C.by;
         r.tc_brick[2] = C.bz;
         r.tc_transform_tiles = (int64_t)C.tiles[0] * C.tiles[1] * C.tiles[2];
-        r.tc_contrib_tiles = (e->table.dev.ncell + C.ctc - 1) / C.ctc;
+        r.tc_contrib_tiles = tc_bricks(e->tc) ? (int64_t)C.nbrick[0] * C.nbrick[1] * C.nbrick[2]
+                                              : (e->table.dev.ncell + C.ctc - 1) / C.ctc;
         r.tc_transform_n = 2 * C.np;
         r.tc_transform_k = C.kp;
         r.tc_contrib_n = C.npc;
@@ -630,6 +636,7 @@ extern "C" int skm_evaluator_describe(skm_evaluator *e, skm_evaluator_info *out)
         r.tc_region_buffers = C.nrb;
         r.tc_u_staging = C.nus;
         r.tc_record_slots = C.nrr;
+        r.tc_contrib_bricks = tc_bricks(e->tc) ? 1 : 0;
     }
     *out = r;
     return SKM_OK;

@@ -40,6 +40,16 @@ constexpr int kTabContribThreads = 288;   // 9 warps
 constexpr int kTabCells = 32;        // cells per contrib block
 constexpr int kTabTapChunk = 12;     // taps per thread in the contrib GEMM
 
+// The contrib GEMM's output summed per brick of cells: every brick (bx x by x bz cells) adds its
+// cells' tap contributions into the patch of control points they reach, (b + nt - 1) per axis,
+// and writes that patch; the gather then sums, for each control point, the patches that hold it.
+struct BrickPartials {
+    const float *partial;   // [brick][comp][pz][py][px]; NULL: the Contrib array and tap gather
+    int b[3];               // cells per brick
+    int nb[3];              // bricks per axis (covering the cell grid)
+    int px, py, pv;         // patch extent along x, y; floats per component patch
+};
+
 struct TableDev {
     int D;
     int h[3];            // phases per axis
@@ -65,6 +75,7 @@ struct TableDev {
     float *bigpart;      // large-phase contrib: [big_splits][3][ntap][ncell] partial sums (big_splits > 1)
     int big_splits;      // phase splits of a cell group in the large-phase contrib (1: direct)
     unsigned *tc_err;    // failure word of the tensor-core kernels (NULL without them)
+    BrickPartials bp;    // set for the gather when the contrib GEMM writes brick partials
     int value_blocks, tile_x, tile_y, tiles_x, tiles_y, tiles_z;
     FastDiv div_nph, div_nq0, div_nq01, div_h0, div_h01;   // index decomposition (ncell * nph < 2^31)
 };
@@ -511,7 +522,13 @@ __global__ void __launch_bounds__(kTabContribThreads) table_contrib_kernel(Table
 constexpr int kGatherGroups = 8;                    // warps per block, each over a share of the taps
 constexpr int kGatherThreads = 32 * kGatherGroups;
 
-template <int D>
+__device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+// BP: the contributions come as brick partials (T.bp): control point j lies in the patch of every
+// brick whose cells q = j - o reach it (o in the tap box), at patch coordinate j - o_min - brick
+// origin; a warp takes every 8th of those bricks (at most 3 x 3 x 4), loads first, then sums in
+// brick order.  Else the Contrib array, tap by tap.
+template <int D, bool BP = false>
 __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalParams P, TableDev T, DerivParams Q)
 {
     __shared__ float sacc[kGatherGroups][3][32];
@@ -550,7 +567,45 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
         st_p = Q.step.scal[T_PENDING];
     }
     float acc[3] = {0.f, 0.f, 0.f};
-    if (active && !Q.values_only) {
+    if (BP && active && !Q.values_only) {
+        const BrickPartials &F = T.bp;
+        int blo[3], nbr[3], pj[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int qhi = j[d] - (T.tlo[d] + T.qmin[d]);      // cell reached through the lowest tap
+            const int lo = max(floor_div(qhi - T.nt[d] + 1, F.b[d]), 0);
+            const int hi = min(floor_div(qhi, F.b[d]), F.nb[d] - 1);
+            blo[d] = lo;
+            nbr[d] = max(hi - lo + 1, 0);
+            pj[d] = qhi;
+        }
+        const int cnt = nbr[0] * nbr[1] * nbr[2];
+        constexpr int kV = 5;                                 // 8 warps x 5 >= 3 x 3 x 4 bricks
+        const long long cstride = F.pv;
+        for (int base = grp; base < cnt; base += kGatherGroups * kV) {
+            float v[kV][3];
+#pragma unroll
+            for (int u = 0; u < kV; ++u) {
+                const int i = base + u * kGatherGroups;
+                const bool in = i < cnt;
+                const int ix = in ? i % nbr[0] : 0, iy = in ? (i / nbr[0]) % nbr[1] : 0,
+                          iz = in ? i / (nbr[0] * nbr[1]) : 0;
+                const int bx = blo[0] + ix, by = blo[1] + iy, bz = blo[2] + iz;
+                const long long brick = ((long long)bz * F.nb[1] + by) * F.nb[0] + bx;
+                const int pidx = (pj[0] - bx * F.b[0]) + F.px * ((pj[1] - by * F.b[1]) + F.py * (pj[2] - bz * F.b[2]));
+                const float *src = F.partial + brick * D * cstride + pidx;
+                v[u][0] = in ? __ldg(src) : 0.f;
+                v[u][1] = in ? __ldg(src + cstride) : 0.f;
+                v[u][2] = (in && D > 2) ? __ldg(src + 2 * cstride) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < kV; ++u) {
+                acc[0] += v[u][0];
+                acc[1] += v[u][1];
+                if (D > 2) acc[2] += v[u][2];
+            }
+        }
+    } else if (active && !Q.values_only) {
         // groups of kU taps: all loads first (independent, predicated), then the sums in tap order
         // (20: one group covers the 160 taps of a 12-voxel support at 8 warps)
         constexpr int kU = 20;
@@ -592,59 +647,74 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
         const float wj = cj.w;
         const float cjv[3] = {cj.x, cj.y, cj.z};
         const float pgs = (float)Q.pg_scaling;
-        for (int o = grp; o < nkcp; o += kGatherGroups) {
-            const float k = kcp_s[o];
-            const int pk = kcpo_s[o];
-            const int ii[3] = {j[0] + (pk & 1023) - 512, j[1] + ((pk >> 10) & 1023) - 512, j[2] + (pk >> 20) - 512};
-            if ((unsigned)ii[0] >= (unsigned)P.cp.n[0] || (unsigned)ii[1] >= (unsigned)P.cp.n[1] ||
-                (unsigned)ii[2] >= (unsigned)P.cp.n[2])
-                continue;
-            const float4 ci4 = __ldg(P.cpd + lin_of<D>(P.cp, ii));
-            const float ci[3] = {ci4.x, ci4.y, ci4.z};
-            const float kw = k * wj;
-            // per-offset terms in FP32 (relative error ~1e-7), their sums in FP64
-            if (rkhs) {                                        // Regularizers.cu:68-73
-                float dot = 0.f;
+        // kR offsets' neighbour loads issued first (independent, predicated), then their terms in
+        // offset order -- the same order and sums as one offset at a time
+        constexpr int kR = 4;
+        for (int o0 = grp; o0 < nkcp; o0 += kGatherGroups * kR) {
+            float4 cn[kR];
+            float kk[kR];
+            bool okk[kR];
 #pragma unroll
-                for (int d = 0; d < D; ++d) dot = fmaf(cjv[d], ci[d], dot);
-                vr += (double)(kw * dot);
-#pragma unroll
-                for (int d = 0; d < D; ++d) drk[d] = fmaf(2.0f * kw, ci[d], drk[d]);
+            for (int u = 0; u < kR; ++u) {
+                const int o = o0 + u * kGatherGroups;
+                const int pk = o < nkcp ? kcpo_s[o] : (512 | (512 << 10) | (512 << 20));
+                kk[u] = o < nkcp ? kcp_s[o] : 0.f;
+                const int ii[3] = {j[0] + (pk & 1023) - 512, j[1] + ((pk >> 10) & 1023) - 512, j[2] + (pk >> 20) - 512};
+                okk[u] = o < nkcp && (unsigned)ii[0] < (unsigned)P.cp.n[0] && (unsigned)ii[1] < (unsigned)P.cp.n[1] &&
+                         (unsigned)ii[2] < (unsigned)P.cp.n[2];
+                cn[u] = okk[u] ? __ldg(P.cpd + lin_of<D>(P.cp, ii)) : make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            if (rd) {                                          // Regularizers.cu:141-144
-                float l2 = 0.f;
 #pragma unroll
-                for (int d = 0; d < D; ++d) {
-                    const float e = cjv[d] - ci[d];
-                    l2 = fmaf(e, e, l2);
+            for (int u = 0; u < kR; ++u) {
+                if (!okk[u]) continue;
+                const float k = kk[u];
+                const float4 ci4 = cn[u];
+                const float ci[3] = {ci4.x, ci4.y, ci4.z};
+                const float kw = k * wj;
+                // per-offset terms in FP32 (relative error ~1e-7), their sums in FP64
+                if (rkhs) {                                        // Regularizers.cu:68-73
+                    float dot = 0.f;
+#pragma unroll
+                    for (int d = 0; d < D; ++d) dot = fmaf(cjv[d], ci[d], dot);
+                    vr += (double)(kw * dot);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) drk[d] = fmaf(2.0f * kw, ci[d], drk[d]);
                 }
-                vd += (double)(kw * l2);
+                if (rd) {                                          // Regularizers.cu:141-144
+                    float l2 = 0.f;
 #pragma unroll
-                for (int d = 0; d < D; ++d) drd[d] = fmaf(4.0f * kw, cjv[d] - ci[d], drd[d]);
-            }
-            if (pg) {
-                if (D == 3) {                                  // Regularizers.cu:218-237
-                    const float cr0 = ci[1] * cjv[2] - ci[2] * cjv[1];
-                    const float cr1 = ci[2] * cjv[0] - ci[0] * cjv[2];
-                    const float cr2 = ci[0] * cjv[1] - ci[1] * cjv[0];
-                    const double n2 = (double)cr0 * cr0 + (double)cr1 * cr1 + (double)cr2 * cr2;
-                    const double sc = (double)pgs;
-                    vp += (double)kw * sc * sc / 2.0 * log(1.0 + n2 / sc);
-                    const float den = 2.0f * ((float)n2 / pgs + 1.0f);
-                    const float dp0 = 2.0f * ci[2] * (ci[2] * cjv[0] - ci[0] * cjv[2]) - 2.0f * ci[1] * (ci[0] * cjv[1] - ci[1] * cjv[0]);
-                    const float dp1 = 2.0f * ci[0] * (ci[0] * cjv[1] - ci[1] * cjv[0]) - 2.0f * ci[2] * (ci[1] * cjv[2] - ci[2] * cjv[1]);
-                    const float dp2 = 2.0f * ci[1] * (ci[1] * cjv[2] - ci[2] * cjv[1]) - 2.0f * ci[0] * (ci[2] * cjv[0] - ci[0] * cjv[2]);
-                    dpg[0] = fmaf(2.0f * kw, pgs * dp0 / den, dpg[0]);
-                    dpg[1] = fmaf(2.0f * kw, pgs * dp1 / den, dpg[1]);
-                    dpg[2] = fmaf(2.0f * kw, pgs * dp2 / den, dpg[2]);
-                } else {                                       // Regularizers.cu:447-459
-                    const float v2d = ci[0] * cjv[1] - ci[1] * cjv[0];
-                    const double v2 = (double)v2d * v2d;
-                    const double sc = (double)pgs;
-                    vp += (double)kw * sc * sc / 2.0 * log(1.0 + v2 / sc);
-                    const float factor = (float)v2 / pgs + 1.0f;
-                    dpg[0] = fmaf(2.0f * kw, -pgs * ci[1] * v2d / factor, dpg[0]);
-                    dpg[1] = fmaf(2.0f * kw, pgs * ci[0] * v2d / factor, dpg[1]);
+                    for (int d = 0; d < D; ++d) {
+                        const float e = cjv[d] - ci[d];
+                        l2 = fmaf(e, e, l2);
+                    }
+                    vd += (double)(kw * l2);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) drd[d] = fmaf(4.0f * kw, cjv[d] - ci[d], drd[d]);
+                }
+                if (pg) {
+                    if (D == 3) {                                  // Regularizers.cu:218-237
+                        const float cr0 = ci[1] * cjv[2] - ci[2] * cjv[1];
+                        const float cr1 = ci[2] * cjv[0] - ci[0] * cjv[2];
+                        const float cr2 = ci[0] * cjv[1] - ci[1] * cjv[0];
+                        const double n2 = (double)cr0 * cr0 + (double)cr1 * cr1 + (double)cr2 * cr2;
+                        const double sc = (double)pgs;
+                        vp += (double)kw * sc * sc / 2.0 * log(1.0 + n2 / sc);
+                        const float den = 2.0f * ((float)n2 / pgs + 1.0f);
+                        const float dp0 = 2.0f * ci[2] * (ci[2] * cjv[0] - ci[0] * cjv[2]) - 2.0f * ci[1] * (ci[0] * cjv[1] - ci[1] * cjv[0]);
+                        const float dp1 = 2.0f * ci[0] * (ci[0] * cjv[1] - ci[1] * cjv[0]) - 2.0f * ci[2] * (ci[1] * cjv[2] - ci[2] * cjv[1]);
+                        const float dp2 = 2.0f * ci[1] * (ci[1] * cjv[2] - ci[2] * cjv[1]) - 2.0f * ci[0] * (ci[2] * cjv[0] - ci[0] * cjv[2]);
+                        dpg[0] = fmaf(2.0f * kw, pgs * dp0 / den, dpg[0]);
+                        dpg[1] = fmaf(2.0f * kw, pgs * dp1 / den, dpg[1]);
+                        dpg[2] = fmaf(2.0f * kw, pgs * dp2 / den, dpg[2]);
+                    } else {                                       // Regularizers.cu:447-459
+                        const float v2d = ci[0] * cjv[1] - ci[1] * cjv[0];
+                        const double v2 = (double)v2d * v2d;
+                        const double sc = (double)pgs;
+                        vp += (double)kw * sc * sc / 2.0 * log(1.0 + v2 / sc);
+                        const float factor = (float)v2 / pgs + 1.0f;
+                        dpg[0] = fmaf(2.0f * kw, -pgs * ci[1] * v2d / factor, dpg[0]);
+                        dpg[1] = fmaf(2.0f * kw, pgs * ci[0] * v2d / factor, dpg[1]);
+                    }
                 }
             }
         }

@@ -107,7 +107,17 @@ struct TcDev {
     unsigned long long wait_ns;  // contrib: limit of one bounded wait (2 s; shortened by the wait drill)
     int drill;               // contrib: CTA 0's first producer group withholds its first stage from the
                              // MMA thread, whose wait for it then runs out (skm_evaluator_wait_drill)
+    // contrib with brick partials (3-D): tiles are bricks of kBrick cells loaded by 5-D / 4-D tiled
+    // loads, the epilogue scatters each cell's tap columns into its brick's control-point patch
+    int fused;               // 1: brick partials (the launch chooses), 0: the Contrib array
+    int nbrick[3];           // bricks per axis
+    int pxp, pyp, pzp, pv;   // patch extent per axis, floats per component patch
+    const int *cpoff;        // [nct]: patch offset (ox + px (oy + py oz)) of contrib tap k
+    float *partial;          // [brick][comp][pv]
 };
+
+constexpr int kBrickX = 4, kBrickY = 4, kBrickZ = 2;   // contrib brick (32 cells: one lane quarter)
+constexpr int kConEpiBar = 4;                          // contrib: named barrier of the epilogue warps
 
 // mbarriers of one CTA: full[s] producers -> MMA (kTcProdThreads arrivals), empty[s] MMA ->
 // producers (commit), acc_full[b] MMA -> epilogue (commit), acc_empty[b] epilogue -> MMA
@@ -224,14 +234,17 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
 // p of the chunk: 128-byte rows c * 4 + p / 8, their 16-byte pieces swizzled by the row index, as
 // the tiled load's 128-byte swizzle writes them) and fixed-image values ([cell][32] floats).
 struct TcContribLayout {
-    int a, bhi, blo, rr, bars, total_bytes;
-    __host__ __device__ explicit TcContribLayout(const TcDev &C)
+    int a, bhi, blo, rr, patch, poff, bars, total_bytes;
+    // fused: patches of the two epilogue halves for every component, and the taps' patch offsets
+    __host__ __device__ TcContribLayout(const TcDev &C, bool fused)
     {
         a = 0;
         bhi = a + C.ns_con * kTcStageBytes;
         blo = bhi + C.kpc * C.npc * 4;
         rr = (blo + C.kpc * C.npc * 4 + 1023) / 1024 * 1024;
-        bars = rr + C.nrr * C.rslot;
+        patch = rr + C.nrr * C.rslot;
+        poff = patch + (fused ? 2 * 3 * C.pv * 4 : 0);
+        bars = (poff + (fused ? C.npc * 4 : 0) + 15) / 16 * 16;
         total_bytes = bars + 8 * kTcNumBars + 8 + 1024;
     }
 };
@@ -545,6 +558,22 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
         :: "r"(tc::smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(tc::smem_addr(bar)) : "memory");
 }
 
+__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+        :: "r"(tc::smem_addr(dst)), "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(tc::smem_addr(bar))
+        : "memory");
+}
+
+// FUSED (3-D, tiled record loads): a tile is a brick of kBrickX x kBrickY x kBrickZ cells (row c =
+// x + 4 y + 16 z of its lane quarter), loaded by 5-D / 4-D tiled loads (cells past the grid read
+// as zeros), and the epilogue scatters each cell's tap columns into the brick's control-point
+// patch in shared memory -- one tap after the other, the lanes of a tap on distinct control
+// points, so every patch entry sums in a fixed order without atomics -- then writes the patch
+// (the two column halves added) as the brick's partial.  Otherwise Contrib[comp][tap][cell].
+template <bool FUSED>
 __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableDev T, TcDev C,
                                                                         const double *__restrict__ stats,
                                                                         const __grid_constant__ CUtensorMap recmap,
@@ -552,7 +581,7 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
 {
     extern __shared__ float4 tc_smem4[];
     unsigned char *sm = tc_aligned_smem(tc_smem4);
-    const TcContribLayout L(C);
+    const TcContribLayout L(C, FUSED);
     unsigned char *As = sm + L.a;
     float *Bhi = reinterpret_cast<float *>(sm + L.bhi), *Blo = reinterpret_cast<float *>(sm + L.blo);
     uint64_t *barmem = reinterpret_cast<uint64_t *>(sm + L.bars);
@@ -562,9 +591,15 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int Kp = C.kpc, Np = C.npc, ct = C.ctc, NS = C.ns_con;
     const int D = T.D, nph = T.nph;
-    const long long ntiles = (T.ncell + ct - 1) / ct;
+    const long long ntiles = FUSED ? (long long)C.nbrick[0] * C.nbrick[1] * C.nbrick[2] : (T.ncell + ct - 1) / ct;
     const int nchunk = Kp / kTcKBlock;
 
+    if (FUSED) {                                            // zeroed patches, the taps' patch offsets
+        float *patch = reinterpret_cast<float *>(sm + L.patch);
+        for (int i = tid; i < 2 * 3 * C.pv; i += kConThreads) patch[i] = 0.f;
+        int *poff = reinterpret_cast<int *>(sm + L.poff);
+        for (int k = tid; k < C.nct; k += kConThreads) poff[k] = C.cpoff[k];
+    }
     if (tid == 0) {
         B.init(kTcGroupThreads, kConEpiWarps * 32);
         *abort = 0;
@@ -606,8 +641,16 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
                 const int kc = (int)(g % nchunk);
                 unsigned char *dst = Rr + slot * C.rslot;
                 tc::mbar_expect_tx(&B.region[slot], bytes);
-                tma_load_3d(reinterpret_cast<float *>(dst), &recmap, 0, kc * 4, (int)(tile * ct), &B.region[slot]);
-                tma_load_2d(dst + C.rfix, &fixmap, kc * kTcKBlock, (int)(tile * ct), &B.region[slot]);
+                if (FUSED) {
+                    const int bx = (int)(tile % C.nbrick[0]) * kBrickX;
+                    const int by = (int)((tile / C.nbrick[0]) % C.nbrick[1]) * kBrickY;
+                    const int bz = (int)(tile / ((long long)C.nbrick[0] * C.nbrick[1])) * kBrickZ;
+                    tma_load_5d(dst, &recmap, 0, kc * 4, bx, by, bz, &B.region[slot]);
+                    tma_load_4d(dst + C.rfix, &fixmap, kc * kTcKBlock, bx, by, bz, &B.region[slot]);
+                } else {
+                    tma_load_3d(reinterpret_cast<float *>(dst), &recmap, 0, kc * 4, (int)(tile * ct), &B.region[slot]);
+                    tma_load_2d(dst + C.rfix, &fixmap, kc * kTcKBlock, (int)(tile * ct), &B.region[slot]);
+                }
             }
             // the last load into each slot lands before the CTA leaves (bounded)
             for (long long j = g > NR ? g - NR : 0; j < g; ++j)
@@ -759,6 +802,60 @@ __global__ void __launch_bounds__(kConThreads, 1) table_contrib_tc_kernel(TableD
             }
         }
         __syncwarp();
+    } else if (FUSED) {
+        // ---------------- epilogue: TMEM -> brick patch -> partial ----------------
+        // warp w reads lane quarter w % 4 (component w % 4, brick cell = lane); warps w and w + 4
+        // take alternate 32-column blocks into their own patch, added when the brick is written
+        const int quarter = warp & 3, half = warp >> 2;
+        const int comp = quarter;
+        const int cbase = (lane & 3) + C.pxp * (((lane >> 2) & 3) + C.pyp * (lane >> 4));
+        float *patch = reinterpret_cast<float *>(sm + L.patch);
+        const int *poff = reinterpret_cast<const int *>(sm + L.poff);
+        float *mine = patch + (half * 3 + (comp < 3 ? comp : 0)) * C.pv + cbase;
+        const int nv = D * C.pv;
+        for (int it = 0;; ++it) {
+            const long long tile = blockIdx.x + (long long)it * gridDim.x;
+            if (tile >= ntiles) break;
+            const int b = it & 1;
+            // every epilogue warp leaves together (the named barriers below need all of them)
+            const bool ok = __all_sync(0xffffffffu, tc::mbar_wait(&B.acc_full[b], (it >> 1) & 1, abort, C.wait_ns));
+            if (tc::bar_or(kConEpiBar, kConEpiWarps * 32, !ok)) {
+                if (!ok && lane == 0) tc_fail(abort, C.err);
+                break;
+            }
+            tc::fence_after_sync();
+            if (comp < D) {                                  // warp-uniform: tcgen05.ld is warp-wide
+                const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * C.con_stride);
+                for (int j = half; 32 * j < Np; j += kConEpiWarps / 4) {
+                    float v[32];
+                    if (32 * j + 32 <= Np) {
+                        tc::tmem_ld32(tb + (uint32_t)(32 * j), v);
+                    } else {
+                        tc::tmem_ld16(tb + (uint32_t)(32 * j), v);
+#pragma unroll
+                        for (int e = 16; e < 32; ++e) v[e] = 0.f;
+                    }
+                    const int ne = C.nct - 32 * j;
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) {
+                        if (e < ne) mine[poff[32 * j + e]] += v[e];
+                        __syncwarp();                        // tap e's adds before tap e + 1's
+                    }
+                }
+            }
+            tc::fence_before_sync();
+            tc::mbar_arrive(&B.acc_empty[b]);                // the accumulator is read
+            tc::bar_sync(kConEpiBar, kConEpiWarps * 32);     // both halves have scattered
+            float *out = C.partial + tile * (long long)nv;
+            for (int i = tid; i < nv; i += kConEpiWarps * 32) {
+                const int cc = i / C.pv, pi = i - cc * C.pv;
+                float *p0 = patch + cc * C.pv + pi, *p1 = patch + (3 + cc) * C.pv + pi;
+                out[i] = *p0 + *p1;
+                *p0 = 0.f;
+                *p1 = 0.f;
+            }
+            tc::bar_sync(kConEpiBar, kConEpiWarps * 32);     // zeroed before the next brick's adds
+        }
     } else {
         // ---------------- epilogue: TMEM -> Contrib ----------------
         // warp w reads TMEM lane quarter w % 4; warps w and w + 4 take alternate 16-column chunks
@@ -842,6 +939,14 @@ struct TcPlan {
     int transform_blocks = 0, contrib_blocks = 0;
     size_t transform_smem = 0, contrib_smem = 0;
     WarpTmaPlan wt;                  // the warp kernel with TMA-staged coefficients (3-D)
+    // contrib with brick partials (3-D): its tiled loads by bricks, the partials, the launch
+    bool fused = false;              // planned
+    bool fused_on = false;           // selected (skm_evaluator_path request 3 turns it on)
+    CUtensorMap recmap5{}, fixmap4{};
+    int *d_cpoff = nullptr;
+    float *d_partial = nullptr;
+    size_t contrib_smem_fused = 0;
+    int contrib_blocks_fused = 0;
 };
 
 // Shared-memory wavefronts of the producers' region loads (4-byte loads of rows r = 32 q + lane,
@@ -998,15 +1103,15 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
     C.rslot = (C.rfix + 128 * C.ctc + 1023) / 1024 * 1024;
     if (T.nph % 8 == 0 && C.ctc <= 256) {
         C.ns_con = 2;
-        for (C.nrr = 3; C.nrr >= 2 && (size_t)TcContribLayout(C).total_bytes > kTcSmemMax; --C.nrr) {
+        for (C.nrr = 3; C.nrr >= 2 && (size_t)TcContribLayout(C, false).total_bytes > kTcSmemMax; --C.nrr) {
         }
         if (C.nrr < 2) C.nrr = 0;
     }
     if (C.nrr == 0)
-        for (C.ns_con = 3; C.ns_con > 2 && (size_t)TcContribLayout(C).total_bytes > kTcSmemMax; --C.ns_con) {
+        for (C.ns_con = 3; C.ns_con > 2 && (size_t)TcContribLayout(C, false).total_bytes > kTcSmemMax; --C.ns_con) {
         }
     tc.transform_smem = (size_t)TcTransformLayout(C).total_bytes;
-    tc.contrib_smem = (size_t)TcContribLayout(C).total_bytes;
+    tc.contrib_smem = (size_t)TcContribLayout(C, false).total_bytes;
     // both kernels must hold one CTA per SM alone (their TMEM allocations assume it)
     if (tc.transform_smem > kTcSmemMax || tc.contrib_smem > kTcSmemMax) return 0;
     if (tc.transform_smem < kTcSmemMax / 2 + 1024) tc.transform_smem = kTcSmemMax / 2 + 1024;
@@ -1135,9 +1240,64 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
                 C.nrr = 0;
-                for (C.ns_con = 3; C.ns_con > 2 && (size_t)TcContribLayout(C).total_bytes > kTcSmemMax; --C.ns_con) {
+                for (C.ns_con = 3; C.ns_con > 2 && (size_t)TcContribLayout(C, false).total_bytes > kTcSmemMax; --C.ns_con) {
                 }
             }
+        }
+    }
+
+    // brick partials (3-D, tiled record loads, a brick of 32 cells = one lane quarter): records as
+    // [cell z][cell y][cell x][nph / 8][32 floats] and fixed values as [z][y][x][nph], boxes of one
+    // brick; the patches of both epilogue halves and the taps' patch offsets in shared memory
+    if (C.nrr > 0 && T.D == 3 && C.ctc == kBrickX * kBrickY * kBrickZ) {
+        const int bdim[3] = {kBrickX, kBrickY, kBrickZ};
+        for (int d = 0; d < 3; ++d) C.nbrick[d] = (T.nq[d] + bdim[d] - 1) / bdim[d];
+        C.pxp = kBrickX + T.nt[0] - 1;
+        C.pyp = kBrickY + T.nt[1] - 1;
+        C.pzp = kBrickZ + T.nt[2] - 1;
+        C.pv = C.pxp * C.pyp * C.pzp;
+        const size_t fsmem = (size_t)TcContribLayout(C, true).total_bytes;
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult qr{};
+        bool ok = fsmem <= kTcSmemMax &&
+                  cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr) == cudaSuccess && fn &&
+                  qr == cudaDriverEntryPointSuccess;
+        if (!ok) cudaGetLastError();
+        if (ok) {
+            const cuuint64_t row = (cuuint64_t)T.nph * 16, frow = (cuuint64_t)T.nph * 4;
+            const cuuint64_t rd[5] = {32, (cuuint64_t)(T.nph / 8), (cuuint64_t)T.nq[0], (cuuint64_t)T.nq[1],
+                                      (cuuint64_t)T.nq[2]};
+            const cuuint64_t rs[4] = {128, row, row * T.nq[0], row * T.nq[0] * T.nq[1]};
+            const cuuint32_t rb[5] = {32, 4, kBrickX, kBrickY, kBrickZ};
+            const cuuint64_t fd[4] = {(cuuint64_t)T.nph, (cuuint64_t)T.nq[0], (cuuint64_t)T.nq[1], (cuuint64_t)T.nq[2]};
+            const cuuint64_t fs[3] = {frow, frow * T.nq[0], frow * T.nq[0] * T.nq[1]};
+            const cuuint32_t fb[4] = {(cuuint32_t)kTcKBlock, kBrickX, kBrickY, kBrickZ};
+            const cuuint32_t e1[5] = {1, 1, 1, 1, 1};
+            auto enc = reinterpret_cast<PfnTensorMapEncodeTiled>(fn);
+            ok = enc(&tc.recmap5, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, (void *)T.rec, rd, rs, rb, e1,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+                 enc(&tc.fixmap4, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)T.fixcp, fd, fs, fb, e1,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        }
+        if (ok) {
+            std::vector<int> cpoff((size_t)C.nct);
+            for (int k = 0; k < C.nct; ++k) {
+                const int i = ctap[(size_t)k];
+                cpoff[(size_t)k] = i % T.nt[0] + C.pxp * ((i / T.nt[0]) % T.nt[1] + C.pyp * (i / (T.nt[0] * T.nt[1])));
+            }
+            const long long nbr = (long long)C.nbrick[0] * C.nbrick[1] * C.nbrick[2];
+            if (pool_malloc((void **)&tc.d_cpoff, cpoff.size() * sizeof(int)) != cudaSuccess ||
+                pool_malloc((void **)&tc.d_partial, (size_t)nbr * T.D * C.pv * sizeof(float)) != cudaSuccess ||
+                cudaMemcpyAsync(tc.d_cpoff, cpoff.data(), cpoff.size() * sizeof(int), cudaMemcpyHostToDevice, stream) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(stream) != cudaSuccess)
+                return 2;
+            C.cpoff = tc.d_cpoff;
+            C.partial = tc.d_partial;
+            tc.contrib_smem_fused = std::max(fsmem, kTcSmemMax / 2 + 1024);
+            tc.fused = true;
         }
     }
 
@@ -1146,12 +1306,22 @@ inline int table_tc_plan(TcPlan &tc, TablePlan &pl, const int *ncp, cudaStream_t
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 2;
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (cudaFuncSetAttribute(table_transform_tc_kernel, a, (int)tc.transform_smem) != cudaSuccess) return 2;
-    if (cudaFuncSetAttribute(table_contrib_tc_kernel, a, (int)tc.contrib_smem) != cudaSuccess) return 2;
+    if (cudaFuncSetAttribute(table_contrib_tc_kernel<false>, a, (int)tc.contrib_smem) != cudaSuccess) return 2;
+    if (tc.fused) {
+        int occ_f = 0;
+        if (cudaFuncSetAttribute(table_contrib_tc_kernel<true>, a, (int)tc.contrib_smem_fused) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, table_contrib_tc_kernel<true>, kConThreads,
+                                                          tc.contrib_smem_fused) != cudaSuccess)
+            return 2;
+        const long long nbr = (long long)C.nbrick[0] * C.nbrick[1] * C.nbrick[2];
+        tc.contrib_blocks_fused = (int)std::max<long long>(1, std::min<long long>(nbr, sms));
+        if (occ_f < 1) tc.fused = false;
+    }
     // both kernels must be launchable with their block sizes and shared memory (else: CUDA cores)
     int occ_t = 0, occ_c = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_t, table_transform_tc_kernel, kTcThreads,
                                                       tc.transform_smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, table_contrib_tc_kernel, kConThreads,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_c, table_contrib_tc_kernel<false>, kConThreads,
                                                       tc.contrib_smem) != cudaSuccess)
         return 2;
     if (occ_t < 1 || occ_c < 1) return 0;
@@ -1170,10 +1340,16 @@ inline int table_transform_tc(const TcPlan &tc, const TablePlan &pl, const EvalP
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
+inline bool tc_bricks(const TcPlan &tc) { return tc.fused && tc.fused_on; }
+
 inline int table_contrib_tc(const TcPlan &tc, const TablePlan &pl, const double *stats, cudaStream_t s)
 {
-    table_contrib_tc_kernel<<<tc.contrib_blocks, kConThreads, tc.contrib_smem, s>>>(pl.dev, tc.dev, stats, tc.recmap,
-                                                                                     tc.fixmap);
+    if (tc_bricks(tc))
+        table_contrib_tc_kernel<true><<<tc.contrib_blocks_fused, kConThreads, tc.contrib_smem_fused, s>>>(
+            pl.dev, tc.dev, stats, tc.recmap5, tc.fixmap4);
+    else
+        table_contrib_tc_kernel<false><<<tc.contrib_blocks, kConThreads, tc.contrib_smem, s>>>(pl.dev, tc.dev, stats,
+                                                                                              tc.recmap, tc.fixmap);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
@@ -1228,10 +1404,22 @@ inline int table_derivative(TablePlan &pl, const TcPlan *tc, const EvalParams &P
                             int gather_blocks, cudaStream_t s, cudaEvent_t mid = nullptr)
 {
     TableDev G = pl.dev;                                     // the gather reads the contrib layout
+    const bool bricks = tc && tc->enabled && tc_bricks(*tc);
     if (tc && tc->enabled) {
         if (table_contrib_tc(*tc, pl, Q.stats, s)) return 2;
         G.gtap = tc->d_ctap;                                 // nonzero taps only
         G.ngtap = tc->dev.nct;
+        if (bricks) {
+            const TcDev &C = tc->dev;
+            G.bp.partial = C.partial;
+            G.bp.b[0] = kBrickX;
+            G.bp.b[1] = kBrickY;
+            G.bp.b[2] = kBrickZ;
+            for (int d = 0; d < 3; ++d) G.bp.nb[d] = C.nbrick[d];
+            G.bp.px = C.pxp;
+            G.bp.py = C.pyp;
+            G.bp.pv = C.pv;
+        }
     } else if (pl.big) {
         table_contrib_big_kernel<<<pl.contrib_blocks, 256, 0, s>>>(pl.dev, Q.stats);
         if (pl.dev.big_splits > 1) table_contrib_big_reduce<<<592, 256, 0, s>>>(pl.dev);
@@ -1242,7 +1430,9 @@ inline int table_derivative(TablePlan &pl, const TcPlan *tc, const EvalParams &P
         if (cudaPeekAtLastError() != cudaSuccess) return 2;
     }
     if (mid && cudaEventRecord(mid, s) != cudaSuccess) return 2;
-    if (D == 3)
+    if (D == 3 && bricks)
+        table_gather_kernel<3, true><<<gather_blocks, kGatherThreads, 0, s>>>(P, G, Q);
+    else if (D == 3)
         table_gather_kernel<3><<<gather_blocks, kGatherThreads, 0, s>>>(P, G, Q);
     else
         table_gather_kernel<2><<<gather_blocks, kGatherThreads, 0, s>>>(P, G, Q);
@@ -1268,6 +1458,8 @@ inline void table_tc_free(TcPlan &tc)
     if (tc.rp.p) pool_release(tc.rp.p);
     warp_tma_free(tc.wt);
     if (tc.d_ctap) pool_release(tc.d_ctap);
+    if (tc.d_cpoff) pool_release(tc.d_cpoff);
+    if (tc.d_partial) pool_release(tc.d_partial);
     tc = TcPlan{};
 }
 

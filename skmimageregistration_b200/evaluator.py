@@ -143,7 +143,7 @@ class GpuKernelEvaluator:
     GENERIC, TABLE, TABLE_TC = 1, 2, 3
     # requests: -1 query, 0 automatic (table path, tensor-core GEMMs where they fit),
     # 1 generic kernels, 2 table path with CUDA-core GEMMs
-    AUTO, REQ_GENERIC, REQ_TABLE_CUDA_CORES = 0, 1, 2
+    AUTO, REQ_GENERIC, REQ_TABLE_CUDA_CORES, REQ_TABLE_TC_BRICKS = 0, 1, 2, 3
 
     def path(self, request=-1):
         """Select and/or query the kernel path: returns 1 generic, 2 table, 3 table on tensor cores."""

@@ -91,3 +91,32 @@ def test_tensor_core_variants_for_small_phase_counts(D, h, shape):
         assert rel_err(r_tc["measure"], r_g["measure"]) <= 1e-5
         assert max_rel(g_tc, g_cc) <= 1e-4
         assert max_rel(g_tc, g_g) <= 1e-4
+
+
+def test_brick_partials_match_tap_gather_and_oracle_at_bench_size():
+    """The contrib GEMM's brick partials (scattered per brick into its control-point patch, summed
+    by the gather; path request 3) against the per-tap Contrib array with the tap gather (the
+    automatic path) and against the FP64 oracle, at ncc128 with RD; repeat calls bitwise identical
+    (no atomics)."""
+    from oracle import oracle as O
+    pb, m, _, _ = workloads.make("ncc128", seed=0)
+    ev = GpuKernelEvaluator(pb)
+    ev.SetRegularizerRD(1e-3)
+    orc = O.Oracle(pb)
+    orc.set_regularizers(rd=1e-3)
+    cp, cpw = _params(pb, 5, 1.0)
+    assert ev.path(GpuKernelEvaluator.AUTO) == GpuKernelEvaluator.TABLE_TC
+    assert ev.describe()["tc_contrib_bricks"] == 0
+    r_t, g_t = ev.getValueAndDerivative(m.metric, cp, cpw)
+    assert ev.path(GpuKernelEvaluator.REQ_TABLE_TC_BRICKS) == GpuKernelEvaluator.TABLE_TC
+    assert ev.describe()["tc_contrib_bricks"] == 1
+    r_b, g_b = ev.getValueAndDerivative(m.metric, cp, cpw)
+    r_b2, g_b2 = ev.getValueAndDerivative(m.metric, cp, cpw)
+    assert np.array_equal(g_b, g_b2) and r_b["measure"] == r_b2["measure"]
+    ro, go = orc.evaluate(m.metric, cp, cpw)
+    assert r_b["measure"] == r_t["measure"]                 # the value pass is the same
+    assert r_b["num_pixels_counted"] == r_t["num_pixels_counted"] == ro["num_pixels_counted"]
+    assert rel_err(r_b["reg_value_rd"], ro["reg_value_rd"]) <= 1e-5
+    assert max_rel(g_b, g_t) <= 1e-5
+    assert max_rel(g_b, go) <= 1e-4
+    assert max_rel(g_t, go) <= 1e-4
