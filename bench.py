@@ -442,14 +442,13 @@ def multiscale_compare(name="ncc128", override=None):
         fixed, moving, _ = synth.ellipsoids3d(seed=0, shape=(96, 128, 128))
         spacing, cfg, volume = (1.0, 1.0, 1.0), MS_CONFIG, "128x128x96"
         score, key, better = final_ncc, "ncc", (lambda a, b: a >= b - 1e-3)
-        R.register(moving[::4, ::4, ::4].copy(), fixed[::4, ::4, ::4].copy(), spacing, None,
-                   dict(MS_CONFIG, num_function_evaluations=[2], sigma_C4=[12], sigma_C0=[24]))   # warm-up
+        R.register(moving, fixed, spacing, None, dict(MS_CONFIG, num_function_evaluations=[2]))   # warm-up
     else:
         fixed, moving, _ = synth.blobs2d(seed=0, shape=(256, 256))
         spacing, cfg, volume = (1.0, 1.0), dict(MS_CONFIG_2D, **(override or {})), "256x256"
         score, key, better = final_mse, "mse", (lambda a, b: a <= b + 1e-3 * abs(b))
-        R.register(moving[::4, ::4].copy(), fixed[::4, ::4].copy(), spacing, None,
-                   dict(MS_CONFIG_2D, num_function_evaluations=[2], sigma_C4=[16], sigma_C0=[32]))   # warm-up
+        R.register(moving, fixed, spacing, None, dict(cfg, num_function_evaluations=[2]))   # warm-up
+    # the warm-up above ran every level of the same volume for 2 iterations (first launches, plans);
     # three timed runs, the median reported
     runs = []
     for _ in range(3):

@@ -57,6 +57,41 @@ int dalloc(T **p, size_t n)
     return SKM_OK;
 }
 
+// a caller's pointer that is device memory (cudaMalloc, a memory pool, managed memory)
+bool device_memory(const void *p)
+{
+    cudaPointerAttributes a{};
+    if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// doubles on the device: the caller's device memory as it is, or a host array copied into a
+// buffer from the pool (released with this object, after the caller synchronised its stream)
+struct StagedDoubles {
+    const double *p = nullptr;
+    double *own = nullptr;
+    int stage(const double *src, long long n, cudaStream_t s)
+    {
+        if (device_memory(src)) {
+            p = src;
+            return SKM_OK;
+        }
+        if (dalloc(&own, n)) return SKM_ERR_CUDA;
+        SKM_CUDA(cudaMemcpyAsync(own, src, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        p = own;
+        return SKM_OK;
+    }
+    ~StagedDoubles()
+    {
+        if (own) pool_release(own);
+    }
+};
+
+int grid_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 16)); }
+
 Geo make_geo(const skm_geometry &g, int D, int pad)
 {
     Geo r;
@@ -480,26 +515,25 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
         K.gw = make_geo(d->weight_image_geometry, D, 0);
         K.gt = make_geo(d->weight_tensor_geometry, D, 0);
 
-        // images: converted to float on the host once, then uploaded
+        // images: the caller's doubles (host arrays, or device memory read in place) become float
+        // copies on the device, the coefficients also as rows of 4 (one aligned 16-byte load per
+        // B-spline stencil row)
         long long ncoef = 1;
         for (int k = 0; k < D; ++k) ncoef *= (d->moving_geometry.size[k] + 3);
-        std::vector<float> tmp((size_t)std::max(e->N, ncoef));
-        for (long long i = 0; i < e->N; ++i) tmp[i] = (float)d->fixed_image[i];
-        if (dalloc(&e->d_fixed, e->N)) return SKM_ERR_CUDA;
-        SKM_CUDA(cudaMemcpy(e->d_fixed, tmp.data(), e->N * sizeof(float), cudaMemcpyHostToDevice));
-
         if (ncoef >= (1LL << 31))
             return fail(SKM_ERR_UNSUPPORTED, "moving image coefficients: %lld entries, at most 2^31 - 1", ncoef);
-        for (long long i = 0; i < ncoef; ++i) tmp[i] = (float)d->moving_coefficients[i];
-        if (dalloc(&e->d_coeffs, ncoef)) return SKM_ERR_CUDA;
-        SKM_CUDA(cudaMemcpy(e->d_coeffs, tmp.data(), ncoef * sizeof(float), cudaMemcpyHostToDevice));
-        {   // row-expanded copy: one aligned 16-byte load per B-spline stencil row
-            std::vector<float4> c4((size_t)ncoef);
-            for (long long i = 0; i < ncoef; ++i)
-                c4[i] = make_float4(tmp[i], i + 1 < ncoef ? tmp[i + 1] : 0.f, i + 2 < ncoef ? tmp[i + 2] : 0.f,
-                                    i + 3 < ncoef ? tmp[i + 3] : 0.f);
-            if (dalloc(&e->d_coeffs4, ncoef)) return SKM_ERR_CUDA;
-            SKM_CUDA(cudaMemcpy(e->d_coeffs4, c4.data(), ncoef * sizeof(float4), cudaMemcpyHostToDevice));
+        {
+            StagedDoubles fix, coef;
+            int src = fix.stage(d->fixed_image, e->N, e->stream);
+            if (!src) src = coef.stage(d->moving_coefficients, ncoef, e->stream);
+            if (src) return src;
+            if (dalloc(&e->d_fixed, e->N) || dalloc(&e->d_coeffs, ncoef) || dalloc(&e->d_coeffs4, ncoef))
+                return SKM_ERR_CUDA;
+            to_float_kernel<<<grid_for(e->N), 256, 0, e->stream>>>(fix.p, e->N, e->d_fixed);
+            to_float_kernel<<<grid_for(ncoef), 256, 0, e->stream>>>(coef.p, ncoef, e->d_coeffs);
+            expand_rows_kernel<<<grid_for(ncoef), 256, 0, e->stream>>>(e->d_coeffs, ncoef, e->d_coeffs4);
+            SKM_CHECK_LAUNCH();
+            SKM_CUDA(cudaStreamSynchronize(e->stream));      // before the staging buffers go back to the pool
         }
         if (d->use_weight_image) {
             long long n = texels(d->weight_image_geometry, D);
@@ -559,7 +593,7 @@ extern "C" int skm_evaluator_create(const skm_evaluator_desc *d, skm_evaluator *
             return fail(SKM_ERR_CUDA, "table kernel attributes: %s", cudaGetErrorString(cudaGetLastError()));
         if (e->table.enabled && table_tc_plan(e->tc, e->table, e->P.cp.n, e->stream))
             return fail(SKM_ERR_CUDA, "tensor-core table plan: %s", cudaGetErrorString(cudaGetLastError()));
-        if (e->table.enabled && e->tc.enabled && warp_tma_plan(e->tc.wt, e->table, e->P, tmp.data(), e->stream))
+        if (e->table.enabled && e->tc.enabled && warp_tma_plan(e->tc.wt, e->table, e->P, e->d_coeffs, e->stream))
             return fail(SKM_ERR_CUDA, "staged warp kernel plan: %s", cudaGetErrorString(cudaGetLastError()));
         return SKM_OK;
     }();
@@ -692,10 +726,15 @@ static int upload_field(skm_evaluator *e, const skm_field *df)
         if (dalloc(&e->d_df, n)) return SKM_ERR_CUDA;
         e->df_texels = n;
     }
-    std::vector<float4> tmp((size_t)n);
-    for (long long i = 0; i < n; ++i)
-        tmp[i] = make_float4((float)key[i * D], (float)key[i * D + 1], D > 2 ? (float)key[i * D + 2] : 0.f, 0.f);
-    SKM_CUDA(cudaMemcpyAsync(e->d_df, tmp.data(), n * sizeof(float4), cudaMemcpyHostToDevice, e->stream));
+    if (device_memory(key)) {                      // a device field: converted in place
+        field_to_float4_kernel<<<grid_for(n), 256, 0, e->stream>>>(key, n, D, e->d_df);
+        SKM_CHECK_LAUNCH();
+    } else {
+        std::vector<float4> tmp((size_t)n);
+        for (long long i = 0; i < n; ++i)
+            tmp[i] = make_float4((float)key[i * D], (float)key[i * D + 1], D > 2 ? (float)key[i * D + 2] : 0.f, 0.f);
+        SKM_CUDA(cudaMemcpyAsync(e->d_df, tmp.data(), n * sizeof(float4), cudaMemcpyHostToDevice, e->stream));
+    }
     SKM_CUDA(cudaStreamSynchronize(e->stream));
     e->P.df = make_geo(df->geometry, D, 0);
     e->P.dfd = e->d_df;
@@ -1102,21 +1141,45 @@ extern "C" int skm_evaluate_displacement_field(skm_evaluator *e, const double *c
     SKM_CUDA(cudaSetDevice(e->device));
     if ((rc = upload_field(e, df))) return rc;
     if ((rc = upload_params(e, cp, cpw, false))) return rc;
-    double *d_out = nullptr;
-    if (dalloc(&d_out, (size_t)e->N * e->D)) return SKM_ERR_CUDA;
+    // a device destination is written in place, a host one through a device buffer
+    const bool on_device = device_memory(dst);
+    double *d_out = on_device ? dst : nullptr;
+    if (!on_device && dalloc(&d_out, (size_t)e->N * e->D)) return SKM_ERR_CUDA;
     rc = dispatch<LaunchDisp>(e->D, e->P.K.kind, e, d_out);
     if (!rc) {
-        cudaError_t c1 = cudaMemcpyAsync(dst, d_out, sizeof(double) * e->N * e->D, cudaMemcpyDeviceToHost, e->stream);
+        cudaError_t c1 = on_device ? cudaSuccess
+                                   : cudaMemcpyAsync(dst, d_out, sizeof(double) * e->N * e->D, cudaMemcpyDeviceToHost,
+                                                     e->stream);
         cudaError_t c2 = cudaStreamSynchronize(e->stream);
         if (c1 != cudaSuccess || c2 != cudaSuccess)
             rc = fail(SKM_ERR_CUDA, "displacement field copy failed: %s",
                       cudaGetErrorString(c1 != cudaSuccess ? c1 : c2));
     }
-    pool_free(d_out);
+    if (!on_device) pool_free(d_out);
     return rc;
 }
 
 // ------------------------------------------------------------------------------------------------
+// B-spline prefilter of a device image in place (BsplineImage.h:174-195), then the mirror-padded
+// coefficient volume (size + 3 per axis) into d_out
+static int bspline_coefficients_device(int D, int X, int Y, int Z, double *d_img, double *d_out, cudaStream_t s)
+{
+    const double pole = sqrt(3.0) - 2.0;
+    if (D == 3) {                                  // z, then y, then x (BsplineImage.h:182-195)
+        bs_prefilter_axis<<<(int)(((long long)X * Y + 127) / 128), 128, 0, s>>>(d_img, X, Y, Z, 2, pole);
+        bs_prefilter_axis<<<(int)(((long long)X * Z + 127) / 128), 128, 0, s>>>(d_img, X, Y, Z, 1, pole);
+        bs_prefilter_axis<<<(int)(((long long)Y * Z + 127) / 128), 128, 0, s>>>(d_img, X, Y, Z, 0, pole);
+    } else {                                       // x, then y (BsplineImage.h:174-180)
+        bs_prefilter_axis<<<(Y + 127) / 128, 128, 0, s>>>(d_img, X, Y, 1, 0, pole);
+        bs_prefilter_axis<<<(X + 127) / 128, 128, 0, s>>>(d_img, X, Y, 1, 1, pole);
+    }
+    SKM_CHECK_LAUNCH();
+    const long long pn = (long long)(X + 3) * (Y + 3) * (D == 3 ? Z + 3 : 1);
+    bs_mirror_pad<<<(int)((pn + 255) / 256), 256, 0, s>>>(d_img, X, Y, Z, D, d_out);
+    SKM_CHECK_LAUNCH();
+    return SKM_OK;
+}
+
 extern "C" int skm_bspline_coefficients(int32_t D, const int32_t *size, const double *image, double *coeffs)
 {
     if (D != 2 && D != 3) return fail(SKM_ERR_INVALID, "dimensions must be 2 or 3");
@@ -1136,20 +1199,11 @@ extern "C" int skm_bspline_coefficients(int32_t D, const int32_t *size, const do
         SKM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         if (dalloc(&d_img, n)) return SKM_ERR_CUDA;
         if (dalloc(&d_out, pn)) return SKM_ERR_CUDA;
-        SKM_CUDA(cudaMemcpyAsync(d_img, image, n * sizeof(double), cudaMemcpyHostToDevice, s));
-        const double pole = sqrt(3.0) - 2.0;
-        if (D == 3) {                                  // z, then y, then x (BsplineImage.h:182-195)
-            bs_prefilter_axis<<<(int)(((long long)X * Y + 127) / 128), 128, 0, s>>>(d_img, X, Y, Z, 2, pole);
-            bs_prefilter_axis<<<(int)(((long long)X * Z + 127) / 128), 128, 0, s>>>(d_img, X, Y, Z, 1, pole);
-            bs_prefilter_axis<<<(int)(((long long)Y * Z + 127) / 128), 128, 0, s>>>(d_img, X, Y, Z, 0, pole);
-        } else {                                       // x, then y (BsplineImage.h:174-180)
-            bs_prefilter_axis<<<(Y + 127) / 128, 128, 0, s>>>(d_img, X, Y, 1, 0, pole);
-            bs_prefilter_axis<<<(X + 127) / 128, 128, 0, s>>>(d_img, X, Y, 1, 1, pole);
-        }
-        SKM_CHECK_LAUNCH();
-        bs_mirror_pad<<<(int)((pn + 255) / 256), 256, 0, s>>>(d_img, X, Y, Z, D, d_out);
-        SKM_CHECK_LAUNCH();
-        SKM_CUDA(cudaMemcpyAsync(coeffs, d_out, pn * sizeof(double), cudaMemcpyDeviceToHost, s));
+        // host or device arrays on either side (the copies infer their direction)
+        SKM_CUDA(cudaMemcpyAsync(d_img, image, n * sizeof(double), cudaMemcpyDefault, s));
+        int rc2 = bspline_coefficients_device(D, X, Y, Z, d_img, d_out, s);
+        if (rc2) return rc2;
+        SKM_CUDA(cudaMemcpyAsync(coeffs, d_out, pn * sizeof(double), cudaMemcpyDefault, s));
         SKM_CUDA(cudaStreamSynchronize(s));
         return SKM_OK;
     }();

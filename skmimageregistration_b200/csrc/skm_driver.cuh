@@ -463,16 +463,21 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
                                        hs.s)))
         return rc;
 
-    std::vector<double> ref_s((size_t)n), tar_s((size_t)n), past((size_t)n * D, 0.0), now((size_t)n * D);
+    // every level's images, coefficients and the summed field stay on the device: the smoothed
+    // copies, the prefiltered reference and the field of the levels so far (past) go to the
+    // evaluator and the optimizer as device pointers, and the next summed field (now) is written
+    // on the device; the host sees the field only for the level callback and at the end
     long long ncoef = 1;
-    int32_t csize[3] = {1, 1, 1};
-    for (int d = 0; d < D; ++d) {
-        csize[d] = geometry->size[d];
-        ncoef *= geometry->size[d] + 3;
-    }
-    std::vector<double> coeffs((size_t)ncoef);
-    DevBuf dsm;
-    SKM_CUDA(pool_malloc((void **)&dsm.p, n * sizeof(double)));
+    for (int d = 0; d < D; ++d) ncoef *= geometry->size[d] + 3;
+    const int GX = geometry->size[0], GY = D > 1 ? geometry->size[1] : 1, GZ = D > 2 ? geometry->size[2] : 1;
+    DevBuf dref_s, dtar_s, dcoef, dpast, dnow;
+    SKM_CUDA(pool_malloc((void **)&dref_s.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&dtar_s.p, n * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&dcoef.p, ncoef * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&dpast.p, n * D * sizeof(double)));
+    SKM_CUDA(pool_malloc((void **)&dnow.p, n * D * sizeof(double)));
+    SKM_CUDA(cudaMemsetAsync(dpast.p, 0, n * D * sizeof(double), hs.s));
+    std::vector<double> past_host;                  // the level callback's copy
 
     // kernel weighting (SKMReg.cxx:245-297): a weight image, or per level a covariance tensor built
     // from the guidance image / the smoothed target, or an external tensor where the weight is 0
@@ -499,25 +504,26 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
     int first = 0;
     if (r->restart_at > 1 && r->restart_at <= r->num_scales && r->initial_displacement) {
         first = r->restart_at - 1;
-        std::memcpy(past.data(), r->initial_displacement, sizeof(double) * n * D);
+        SKM_CUDA(cudaMemcpyAsync(dpast.p, r->initial_displacement, sizeof(double) * n * D, cudaMemcpyDefault, hs.s));
     }
     rep.first_level = first;
 
     for (int s = first; s < r->num_scales; ++s) {
         const auto t0 = std::chrono::steady_clock::now();
-        // smoothed copies of both images (SKMReg.cxx:140-150)
+        // smoothed copies of both images (SKMReg.cxx:140-150), the reference prefiltered into its
+        // B-spline coefficients (in place on a scratch copy)
         for (int which = 0; which < 2; ++which) {
-            double *src = which == 0 ? dref.p : dtar.p;
-            SKM_CUDA(cudaMemcpyAsync(dsm.p, src, n * sizeof(double), cudaMemcpyDeviceToDevice, hs.s));
+            double *dst = which == 0 ? dref_s.p : dtar_s.p;
+            SKM_CUDA(cudaMemcpyAsync(dst, which == 0 ? dref.p : dtar.p, n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                     hs.s));
             if (r->smoothing_variance[s] > 1e-5 &&
                 (rc = smooth_device(D, geometry->size, geometry->spacing, r->smoothing_variance[s], 1, 0.01, 64,
-                                    dsm.p, dtmp.p, hs.s)))
+                                    dst, dtmp.p, hs.s)))
                 return rc;
-            SKM_CUDA(cudaMemcpyAsync(which == 0 ? ref_s.data() : tar_s.data(), dsm.p, n * sizeof(double),
-                                     cudaMemcpyDeviceToHost, hs.s));
         }
+        SKM_CUDA(cudaMemcpyAsync(dtmp.p, dref_s.p, n * sizeof(double), cudaMemcpyDeviceToDevice, hs.s));
+        if ((rc = bspline_coefficients_device(D, GX, GY, GZ, dtmp.p, dcoef.p, hs.s))) return rc;
         SKM_CUDA(cudaStreamSynchronize(hs.s));
-        if ((rc = skm_bspline_coefficients(D, csize, ref_s.data(), coeffs.data()))) return rc;
 
         // control-point grid (SKMReg.cxx:235-247)
         // in float, as the reference computes it
@@ -563,7 +569,7 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
             // the support covariance stays the identity; a negative tilt means no texel passed, every
             // tensor is the identity and so is the one with the largest eigenvalue (weight 1)
             double tilt = -DBL_MAX;
-            if ((rc = anisotropic_tensor_device(D, geometry->size, geometry->spacing, dguide.p ? dguide.p : dsm.p,
+            if ((rc = anisotropic_tensor_device(D, geometry->size, geometry->spacing, dguide.p ? dguide.p : dtar_s.p,
                                                 (double)(float)r->sigma_c4[s], tw, 2, dcov.p, &tilt, hs.s)))
                 return rc;
             SKM_CUDA(cudaMemcpyAsync(tensor.data(), dcov.p, nt * sizeof(double), cudaMemcpyDeviceToHost, hs.s));
@@ -602,9 +608,9 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
             ed.weight_tensor_geometry = *geometry;
             for (int k = 0; k < 9; ++k) ed.maximum_eigenvalue_covariance[k] = tensor_cov[k];
         }
-        ed.moving_coefficients = coeffs.data();
+        ed.moving_coefficients = dcoef.p;                           // device memory, read in place
         ed.moving_geometry = *geometry;
-        ed.fixed_image = tar_s.data();
+        ed.fixed_image = dtar_s.p;
         ed.fixed_geometry = *geometry;
         ed.cp_geometry = cpg;
         ed.cpw_geometry = cpg;
@@ -639,7 +645,7 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
         od.return_best_parameters_and_value = 1;
 
         skm_field df{};
-        df.data = s > 0 ? past.data() : nullptr;
+        df.data = s > 0 ? dpast.p : nullptr;
         df.geometry = *geometry;
         skm_optimizer *opt = nullptr;
         rc = skm_optimizer_create(ev, &od, &md, params.data(), cpw.data(), &df, &opt);
@@ -659,18 +665,22 @@ extern "C" int skm_register(const skm_register_desc *r, const skm_geometry *geom
         std::vector<double> cp_aos((size_t)C * D);
         for (long long i = 0; i < C; ++i)
             for (int d = 0; d < D; ++d) cp_aos[(size_t)(i * D + d)] = best[(size_t)(d * C + i)];
-        rc = skm_evaluate_displacement_field(ev, cp_aos.data(), cpw.data(), &df, now.data());
+        rc = skm_evaluate_displacement_field(ev, cp_aos.data(), cpw.data(), &df, dnow.p);
         skm_evaluator_destroy(ev);
         if (rc) return rc;
-        past.swap(now);
+        std::swap(dpast.p, dnow.p);
         rep.levels_done = s + 1;
         rep.best_value[s] = st.best_value;
         rep.iterations[s] = st.iteration;
         rep.control_points[s] = C;
         rep.seconds[s] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        if (r->level_done) r->level_done(s, past.data(), r->level_user);     // df-full-<s> (SKMReg.cxx:468)
+        if (r->level_done) {                                         // df-full-<s> (SKMReg.cxx:468)
+            past_host.resize((size_t)n * D);
+            SKM_CUDA(cudaMemcpy(past_host.data(), dpast.p, sizeof(double) * n * D, cudaMemcpyDeviceToHost));
+            r->level_done(s, past_host.data(), r->level_user);
+        }
     }
-    std::memcpy(displacement, past.data(), sizeof(double) * n * D);
+    SKM_CUDA(cudaMemcpy(displacement, dpast.p, sizeof(double) * n * D, cudaMemcpyDeviceToHost));
     if (report) *report = rep;
     return SKM_OK;
 }

@@ -1040,4 +1040,25 @@ static __global__ void shifts_kernel(unsigned long long state, RngJump J, long l
     shifts[t] = packed;
 }
 
+// ---- evaluator set-up on the device: the caller's double images become the kernels' float copies
+static __global__ void to_float_kernel(const double *__restrict__ src, long long n, float *__restrict__ dst)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+
+// row-expanded coefficients: c4[i] = (c[i], c[i + 1], c[i + 2], c[i + 3]), zeros past the end
+static __global__ void expand_rows_kernel(const float *__restrict__ c, long long n, float4 *__restrict__ c4)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        c4[i] = make_float4(c[i], i + 1 < n ? c[i + 1] : 0.f, i + 2 < n ? c[i + 2] : 0.f, i + 3 < n ? c[i + 3] : 0.f);
+}
+
+// displacement field (D doubles per texel) as float4 (x, y, z, 0)
+static __global__ void field_to_float4_kernel(const double *__restrict__ src, long long n, int D, float4 *__restrict__ dst)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = make_float4((float)src[i * D], (float)src[i * D + 1], D > 2 ? (float)src[i * D + 2] : 0.f, 0.f);
+}
+
 }  // namespace skm

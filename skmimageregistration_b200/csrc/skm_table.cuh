@@ -847,6 +847,29 @@ inline float wendland_host(double r, double sc4, double sc0)
 
 // Decides whether the table path applies and builds its tables.  Returns 0 (also when the
 // path does not apply; plan.enabled says which) or a CUDA error code.
+// fixed image in cell-phase layout: texel (x, y, z) -> cell q = x / h + qoff[x % h] - qmin per
+// axis, phase p = x % h (x fastest); entries no texel reaches stay 0
+static __global__ void table_fixcp_kernel(const float *__restrict__ fixed, int nx, int ny, int nz, TableDev T,
+                                   float *__restrict__ out)
+{
+    const long long n = (long long)nx * ny * nz;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c[3] = {(int)(i % nx), (int)((i / nx) % ny), (int)(i / ((long long)nx * ny))};
+        long long cell = 0, mul = 1;
+        int ph = 0, phmul = 1;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int p = c[d] % T.h[d];
+            const int q = c[d] / T.h[d] + T.qoff[d][p] - T.qmin[d];
+            cell += mul * q;
+            mul *= T.nq[d];
+            ph += phmul * p;
+            phmul *= T.h[d];
+        }
+        out[cell * T.nph + ph] = fixed[i];
+    }
+}
+
 inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t stream)
 {
     pl.enabled = false;
@@ -1046,28 +1069,6 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
                 }
                 kcp[o] = wendland_host(sqrt(r2), P.K.sc4, P.K.sc0);
             }
-    // fixed image in cell-phase layout
-    std::vector<float> fix((size_t)T.ncell * T.nph, 0.f);
-    std::vector<float> fixed_host((size_t)P.fixed.n[0] * P.fixed.n[1] * P.fixed.n[2]);
-    if (cudaMemcpy(fixed_host.data(), P.fixed_data, fixed_host.size() * sizeof(float), cudaMemcpyDeviceToHost) !=
-        cudaSuccess)
-        return 2;
-    for (int z = 0; z < P.fixed.n[2]; ++z)
-        for (int y = 0; y < P.fixed.n[1]; ++y)
-            for (int x = 0; x < P.fixed.n[0]; ++x) {
-                const int c[3] = {x, y, z};
-                long long cell = 0, mul = 1;
-                int ph = 0, phmul = 1;
-                for (int d = 0; d < 3; ++d) {
-                    const int p = c[d] % T.h[d];
-                    const int q = c[d] / T.h[d] + T.qoff[d][p] - T.qmin[d];
-                    cell += mul * q;
-                    mul *= T.nq[d];
-                    ph += phmul * p;
-                    phmul *= T.h[d];
-                }
-                fix[cell * T.nph + ph] = fixed_host[x + (size_t)P.fixed.n[0] * (y + (size_t)P.fixed.n[1] * z)];
-            }
     auto up = [&](float **dst, const std::vector<float> &src) -> bool {
         if (pool_malloc((void **)dst, std::max<size_t>(1, src.size()) * sizeof(float)) != cudaSuccess) return false;
         return cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(float), cudaMemcpyHostToDevice, stream) ==
@@ -1089,7 +1090,17 @@ inline int table_plan(TablePlan &pl, const EvalParams &P, int D, cudaStream_t st
         cudaMemcpyAsync(pl.d_kcpo, kcpo.data(), kcpo.size() * sizeof(int), cudaMemcpyHostToDevice, stream) !=
             cudaSuccess)
         return 2;
-    if (!up(&pl.d_tfwd, tfwd) || !up(&pl.d_tgemm, tgemm) || !up(&pl.d_kcp, kcpv) || !up(&pl.d_fixcp, fix)) return 2;
+    if (!up(&pl.d_tfwd, tfwd) || !up(&pl.d_tgemm, tgemm) || !up(&pl.d_kcp, kcpv)) return 2;
+    {   // the fixed image in cell-phase layout, from the evaluator's device copy
+        const size_t nfix = (size_t)T.ncell * T.nph;
+        const long long nt = (long long)P.fixed.n[0] * P.fixed.n[1] * P.fixed.n[2];
+        if (pool_malloc((void **)&pl.d_fixcp, std::max<size_t>(1, nfix) * sizeof(float)) != cudaSuccess ||
+            cudaMemsetAsync(pl.d_fixcp, 0, nfix * sizeof(float), stream) != cudaSuccess)
+            return 2;
+        table_fixcp_kernel<<<(int)std::min<long long>((nt + 255) / 256, 4096), 256, 0, stream>>>(
+            P.fixed_data, P.fixed.n[0], P.fixed.n[1], P.fixed.n[2], T, pl.d_fixcp);
+        if (cudaPeekAtLastError() != cudaSuccess) return 2;
+    }
     if (pool_malloc((void **)&pl.d_rec, (size_t)T.ncell * T.nph * sizeof(float4)) != cudaSuccess) return 2;
     if (pool_malloc((void **)&pl.d_ucp, (size_t)D * T.ncell * T.nph * sizeof(float)) != cudaSuccess) return 2;
     if (pool_malloc((void **)&pl.d_contrib, (size_t)3 * T.ntap * T.ncell * sizeof(float)) != cudaSuccess) return 2;

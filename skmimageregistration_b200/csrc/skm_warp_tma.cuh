@@ -238,9 +238,9 @@ typedef CUresult (*PfnTensorMapEncodeTiled)(CUtensorMap *, CUtensorMapDataType, 
                                             CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 // Plans the staged warp kernel for a 3-D table plan whose operands allow it; returns 0
-// (wt.enabled says whether it applies) or 2 on a CUDA error.  h_coeffs: the padded coefficient
-// volume (float, moving size + 3 per axis) on the host.
-inline int warp_tma_plan(WarpTmaPlan &wt, const TablePlan &pl, const EvalParams &P, const float *h_coeffs,
+// (wt.enabled says whether it applies) or 2 on a CUDA error.  d_coeffs: the padded coefficient
+// volume (float, moving size + 3 per axis) on the device.
+inline int warp_tma_plan(WarpTmaPlan &wt, const TablePlan &pl, const EvalParams &P, const float *d_coeffs,
                          cudaStream_t stream)
 {
     wt.enabled = false;
@@ -283,13 +283,11 @@ inline int warp_tma_plan(WarpTmaPlan &wt, const TablePlan &pl, const EvalParams 
     // tensor map over a row-pitched copy (global strides must be multiples of 16 bytes)
     const int PX = P.mov.n[0], PY = P.mov.n[1], PZ = P.mov.n[2];
     const int pitch = (PX + 3) / 4 * 4;
-    std::vector<float> padded((size_t)pitch * PY * PZ, 0.f);
-    for (long long z = 0; z < PZ; ++z)
-        for (long long y = 0; y < PY; ++y)
-            std::memcpy(&padded[(size_t)((z * PY + y) * pitch)], h_coeffs + (z * PY + y) * PX, sizeof(float) * PX);
-    if (pool_malloc((void **)&wt.d_coefp, padded.size() * sizeof(float)) != cudaSuccess) return 2;
-    if (cudaMemcpyAsync(wt.d_coefp, padded.data(), padded.size() * sizeof(float), cudaMemcpyHostToDevice,
-                        stream) != cudaSuccess ||
+    const size_t npad = (size_t)pitch * PY * PZ;
+    if (pool_malloc((void **)&wt.d_coefp, npad * sizeof(float)) != cudaSuccess) return 2;
+    if (cudaMemsetAsync(wt.d_coefp, 0, npad * sizeof(float), stream) != cudaSuccess ||
+        cudaMemcpy2DAsync(wt.d_coefp, (size_t)pitch * 4, d_coeffs, (size_t)PX * 4, (size_t)PX * 4, (size_t)PY * PZ,
+                          cudaMemcpyDeviceToDevice, stream) != cudaSuccess ||
         cudaStreamSynchronize(stream) != cudaSuccess)
         return 2;
     void *fn = nullptr;
