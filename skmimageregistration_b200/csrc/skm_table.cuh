@@ -90,6 +90,7 @@ struct TablePlan {
     double *d_part = nullptr;
     float *d_bigpart = nullptr;
     int hl = 1;          // z phases per thread in the transform kernel (template argument)
+    int big_pb = 1;      // large-phase transform: phases per thread (template argument 1, 2 or 4)
     int ncz = 1;         // cells per thread along z in the transform kernel
     int transform_blocks = 0, contrib_blocks = 0;
     bool big = false;    // large-phase plan (coarse levels: control spacing 8 or 16 voxels): the
@@ -309,7 +310,12 @@ __global__ void __launch_bounds__(256, 4) table_warp_kernel(EvalParams P, TableD
 //              shared memory in chunks of kTabBigChunk phases (table read [phase][tap]: coalesced)
 constexpr int kTabBigChunk = 128;
 
-template <int D>
+constexpr int kTabBigContribCells = 16;           // contrib: two halves of 8 cells, 2 taps per thread
+
+// PB phases per thread (p, p + 256, ..): every staged control point a thread reads serves PB
+// phases, every table value 8 cells, so a tap costs 8 shared loads and PB table loads for
+// 24 PB multiply-adds
+template <int D, int PB>
 __global__ void __launch_bounds__(256) table_transform_big_kernel(EvalParams P, TableDev T)
 {
     constexpr int CB = kTabBigCells;
@@ -317,7 +323,8 @@ __global__ void __launch_bounds__(256) table_transform_big_kernel(EvalParams P, 
     const int ntap = T.ntap, nph = T.nph;
     const long long plane = T.ncell * T.nph;
     const long long ngroups = (T.ncell + CB - 1) / CB;
-    const int npc = (nph + blockDim.x - 1) / blockDim.x;      // phase chunks of one block's threads
+    const int span = blockDim.x * PB;
+    const int npc = (nph + span - 1) / span;                 // phase chunks of one block's threads
     for (long long item = blockIdx.x; item < ngroups * npc; item += gridDim.x) {
         const long long grp = item / npc;
         const int pc = (int)(item - grp * npc);
@@ -346,38 +353,53 @@ __global__ void __launch_bounds__(256) table_transform_big_kernel(EvalParams P, 
             A[c * ntap + t] = a;
         }
         __syncthreads();
-        const int p = pc * blockDim.x + threadIdx.x;
-        if (p < nph) {
-            float acc[CB][3];
+        const int p0 = pc * span + threadIdx.x;
+        if (p0 < nph) {
+            float acc[CB][3][PB];
 #pragma unroll
-            for (int c = 0; c < CB; ++c) acc[c][0] = acc[c][1] = acc[c][2] = 0.f;
-            const float *tp = T.tfwd + p;
+            for (int c = 0; c < CB; ++c)
+#pragma unroll
+                for (int b = 0; b < PB; ++b) acc[c][0][b] = acc[c][1][b] = acc[c][2][b] = 0.f;
+            const float *tp = T.tfwd + p0;
 #pragma unroll 2
             for (int t = 0; t < ntap; ++t) {
-                const float k = __ldg(tp + (long long)t * nph);
+                float k[PB];
+#pragma unroll
+                for (int b = 0; b < PB; ++b)
+                    k[b] = p0 + b * (int)blockDim.x < nph ? __ldg(tp + (long long)t * nph + b * blockDim.x) : 0.f;
 #pragma unroll
                 for (int c = 0; c < CB; ++c) {
                     const float4 a = A[c * ntap + t];
-                    acc[c][0] = fmaf(k, a.x, acc[c][0]);
-                    acc[c][1] = fmaf(k, a.y, acc[c][1]);
-                    acc[c][2] = fmaf(k, a.z, acc[c][2]);
+#pragma unroll
+                    for (int b = 0; b < PB; ++b) {
+                        acc[c][0][b] = fmaf(k[b], a.x, acc[c][0][b]);
+                        acc[c][1][b] = fmaf(k[b], a.y, acc[c][1][b]);
+                        acc[c][2][b] = fmaf(k[b], a.z, acc[c][2][b]);
+                    }
                 }
             }
 #pragma unroll
             for (int c = 0; c < CB; ++c) {
                 if (c0 + c >= T.ncell) break;
-                const long long i = (c0 + c) * nph + p;
-                T.ucp[i] = acc[c][0];
-                T.ucp[i + plane] = acc[c][1];
-                if (D > 2) T.ucp[i + 2 * plane] = acc[c][2];
+#pragma unroll
+                for (int b = 0; b < PB; ++b) {
+                    const int p = p0 + b * blockDim.x;
+                    if (p >= nph) break;
+                    const long long i = (c0 + c) * nph + p;
+                    T.ucp[i] = acc[c][0][b];
+                    T.ucp[i + plane] = acc[c][1][b];
+                    if (D > 2) T.ucp[i + 2 * plane] = acc[c][2][b];
+                }
             }
         }
     }
 }
 
+// Thread = (half, tap pair): half h takes cells 8 h .. 8 h + 7 of the block's 16, taps t and
+// t + 128 (ntap <= 256): every staged g a thread reads serves two taps
 __global__ void __launch_bounds__(256) table_contrib_big_kernel(TableDev T, const double *__restrict__ stats)
 {
-    constexpr int CB = kTabBigCells;
+    constexpr int CB = kTabBigContribCells, CH = CB / 2;
     __shared__ float4 G[CB][kTabBigChunk];
     const int nph = T.nph, ntap = T.ntap, ntp = T.ntap_pad;
     const float cf = (float)stats[S_COEF_F], cm = (float)stats[S_COEF_M], cc = (float)stats[S_COEF_C];
@@ -386,14 +408,16 @@ __global__ void __launch_bounds__(256) table_contrib_big_kernel(TableDev T, cons
     // writes partial sums that table_contrib_big_reduce adds in split order
     const int splits = T.big_splits;
     const int per = (nph + splits - 1) / splits;
+    const int h = threadIdx.x >> 7, t0 = threadIdx.x & 127, t1 = t0 + 128;
     for (long long item = blockIdx.x; item < ngroups * splits; item += gridDim.x) {
         const long long grp = item / splits;
         const int sp = (int)(item - grp * splits);
         const long long c0 = grp * CB;
-        float acc[CB][3];
+        float acc[CH][3][2];
 #pragma unroll
-        for (int c = 0; c < CB; ++c) acc[c][0] = acc[c][1] = acc[c][2] = 0.f;
-        const int t = threadIdx.x;
+        for (int c = 0; c < CH; ++c)
+#pragma unroll
+            for (int u = 0; u < 2; ++u) acc[c][0][u] = acc[c][1][u] = acc[c][2][u] = 0.f;
         const int pend = min(nph, (sp + 1) * per);
         for (int p0 = sp * per; p0 < pend; p0 += kTabBigChunk) {
             const int np = min(kTabBigChunk, pend - p0);
@@ -410,29 +434,37 @@ __global__ void __launch_bounds__(256) table_contrib_big_kernel(TableDev T, cons
                 G[c][p] = g;
             }
             __syncthreads();
-            if (t < ntap) {
-                const float *tp = T.tgemm + (long long)p0 * ntp + t;
+            if (t0 < ntap) {
+                const float *tp = T.tgemm + (long long)p0 * ntp;
+                const bool two = t1 < ntap;
 #pragma unroll 2
                 for (int p = 0; p < np; ++p) {
-                    const float k = __ldg(tp + (long long)p * ntp);
+                    const float k0 = __ldg(tp + (long long)p * ntp + t0);
+                    const float k1 = two ? __ldg(tp + (long long)p * ntp + t1) : 0.f;
 #pragma unroll
-                    for (int c = 0; c < CB; ++c) {
-                        const float4 g = G[c][p];
-                        acc[c][0] = fmaf(k, g.x, acc[c][0]);
-                        acc[c][1] = fmaf(k, g.y, acc[c][1]);
-                        acc[c][2] = fmaf(k, g.z, acc[c][2]);
+                    for (int c = 0; c < CH; ++c) {
+                        const float4 g = G[h * CH + c][p];
+                        acc[c][0][0] = fmaf(k0, g.x, acc[c][0][0]);
+                        acc[c][1][0] = fmaf(k0, g.y, acc[c][1][0]);
+                        acc[c][2][0] = fmaf(k0, g.z, acc[c][2][0]);
+                        acc[c][0][1] = fmaf(k1, g.x, acc[c][0][1]);
+                        acc[c][1][1] = fmaf(k1, g.y, acc[c][1][1]);
+                        acc[c][2][1] = fmaf(k1, g.z, acc[c][2][1]);
                     }
                 }
             }
         }
-        if (t < ntap) {
+        float *dst = splits > 1 ? T.bigpart + (long long)sp * 3 * ntap * T.ncell : T.contrib;
 #pragma unroll
-            for (int c = 0; c < CB; ++c) {
-                const long long cell = c0 + c;
+        for (int u = 0; u < 2; ++u) {
+            const int t = u ? t1 : t0;
+            if (t >= ntap) break;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                const long long cell = c0 + h * CH + c;
                 if (cell >= T.ncell) break;
-                float *dst = splits > 1 ? T.bigpart + (long long)sp * 3 * ntap * T.ncell : T.contrib;
 #pragma unroll
-                for (int d = 0; d < 3; ++d) dst[((long long)d * ntap + t) * T.ncell + cell] = acc[c][d];
+                for (int d = 0; d < 3; ++d) dst[((long long)d * ntap + t) * T.ncell + cell] = acc[c][d][u];
             }
         }
     }
@@ -1167,18 +1199,21 @@ inline int table_size_grids(TablePlan &pl)
     if (pl.big) {                                  // items of kTabBigCells cells, grid-strided
         TableDev &T = pl.dev;
         const long long groups = (T.ncell + kTabBigCells - 1) / kTabBigCells;
-        const long long titems = groups * ((T.nph + 255) / 256);
+        pl.big_pb = T.nph >= 512 ? 2 : 1;          // 2 phases per thread: 98 registers, 2 blocks per SM
+        const long long titems = groups * ((T.nph + 256 * pl.big_pb - 1) / (256 * pl.big_pb));
         pl.transform_blocks = (int)std::max<long long>(1, std::min<long long>(titems, 8LL * sms));
         // few cell groups (the coarsest levels): split their phases so that every SM gets work
+        const long long cgroups = (T.ncell + kTabBigContribCells - 1) / kTabBigContribCells;
         const int max_split = (T.nph + kTabBigChunk - 1) / kTabBigChunk;
-        T.big_splits = (int)std::max<long long>(1, std::min<long long>(max_split, (2LL * sms + groups - 1) / groups));
+        // as many splits as fill two waves of two blocks per SM without starting a third
+        T.big_splits = (int)std::max<long long>(1, std::min<long long>(max_split, (4LL * sms) / cgroups));
         if (T.big_splits > 1 && !pl.d_bigpart) {
             if (pool_malloc((void **)&pl.d_bigpart, sizeof(float) * (size_t)T.big_splits * 3 * T.ntap * T.ncell) !=
                 cudaSuccess)
                 return 2;
         }
         T.bigpart = pl.d_bigpart;
-        pl.contrib_blocks = (int)std::max<long long>(1, std::min<long long>(groups * T.big_splits, 8LL * sms));
+        pl.contrib_blocks = (int)std::max<long long>(1, std::min<long long>(cgroups * T.big_splits, 8LL * sms));
         return 0;
     }
     cudaError_t e;

@@ -1373,10 +1373,16 @@ inline int table_value(TablePlan &pl, const TcPlan *tc, const EvalParams &P, int
         rc = table_transform_tc(*tc, pl, P, s);
     } else if (pl.big) {                                     // coarse levels: tables in global memory
         const size_t smem = table_big_transform_smem(pl.dev);
-        if (D == 3)
-            table_transform_big_kernel<3><<<pl.transform_blocks, 256, smem, s>>>(P, pl.dev);
-        else
-            table_transform_big_kernel<2><<<pl.transform_blocks, 256, smem, s>>>(P, pl.dev);
+        const int nb = pl.transform_blocks;
+        if (D == 3) {
+            if (pl.big_pb == 4) table_transform_big_kernel<3, 4><<<nb, 256, smem, s>>>(P, pl.dev);
+            else if (pl.big_pb == 2) table_transform_big_kernel<3, 2><<<nb, 256, smem, s>>>(P, pl.dev);
+            else table_transform_big_kernel<3, 1><<<nb, 256, smem, s>>>(P, pl.dev);
+        } else {
+            if (pl.big_pb == 4) table_transform_big_kernel<2, 4><<<nb, 256, smem, s>>>(P, pl.dev);
+            else if (pl.big_pb == 2) table_transform_big_kernel<2, 2><<<nb, 256, smem, s>>>(P, pl.dev);
+            else table_transform_big_kernel<2, 1><<<nb, 256, smem, s>>>(P, pl.dev);
+        }
         rc = cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
     } else if (D == 3) {
         switch (pl.hl) {
