@@ -67,9 +67,11 @@ typedef struct skm_geometry {
 /* ImageNearest<VecF,D> used as the displacement field of earlier scale levels
  * (include/cuda/ImageNearest.h, GpuEvaluator.cu:120-126).  data == NULL means
  * "no field".  The device copy is cached by host pointer identity, exactly like
- * the reference (GpuEvaluator.cu:120-126): pass a different pointer to refresh it. */
+ * the reference (GpuEvaluator.cu:120-126): pass a different pointer to refresh it.
+ * data may also be device memory of the evaluator's device (converted there, no copy to the
+ * host). */
 typedef struct skm_field {
-    const double *data;        /* D doubles per texel, AoS */
+    const double *data;        /* D doubles per texel, AoS (host or device memory) */
     skm_geometry  geometry;
 } skm_field;
 
@@ -97,10 +99,10 @@ typedef struct skm_evaluator_desc {
      * BsplineImage::computeCoeffs (BsplineImage.h:209-221): (size+3) texels per
      * axis with a one-texel mirror offset.  moving_geometry.size is the size of
      * the image itself (the BsplineImage constructor adds the 3). */
-    const double *moving_coefficients;
+    const double *moving_coefficients;     /* host or device memory (read in place on the device) */
     skm_geometry  moving_geometry;
 
-    /* fixed image, 1 double per texel */
+    /* fixed image, 1 double per texel (host or device memory) */
     const double *fixed_image;
     skm_geometry  fixed_geometry;
 
@@ -215,7 +217,8 @@ int skm_get_value_and_derivative(skm_evaluator *ev, int32_t metric,
                                  skm_result *out);
 
 /* GpuKernelEvaluator::evaluateDisplacementField (GpuEvaluator.h:175-178,
- * GpuEvaluator.cu:716-784): dst gets D doubles per fixed-image texel. */
+ * GpuEvaluator.cu:716-784): dst gets D doubles per fixed-image texel (dst may be device memory,
+ * written in place). */
 int skm_evaluate_displacement_field(skm_evaluator *ev,
                                     const double *cp, const double *cpw, const skm_field *df,
                                     double *dst);
