@@ -258,13 +258,27 @@ struct skm_evaluator {
 
     // skm_metric_evaluate replays one CUDA graph (parameter upload, evaluation, result download)
     // while the metric description, the derivative request, the path and the field stay the same
-    cudaGraphExec_t mgraph = nullptr;
-    skm_metric_desc mg_desc{};
-    bool mg_deriv = false;
-    int mg_path = 0;
-    const double *mg_df = nullptr;
-    const double *mg_pdev = nullptr;   // parameter source and derivative destination the graph uses
-    double *mg_gout = nullptr;
+    // (a few graphs, least recently used replaced: a caller may alternate derivative buffers)
+    struct MetricGraph {
+        cudaGraphExec_t exec = nullptr;
+        skm_metric_desc desc{};
+        bool deriv = false;
+        int path = 0;
+        const double *df = nullptr;
+        const double *pdev = nullptr;  // parameter source and derivative destination the graph uses
+        double *gout = nullptr;
+        unsigned long long used = 0;
+    };
+    static constexpr int kMetricGraphs = 4;
+    MetricGraph mg[kMetricGraphs];
+    unsigned long long mg_clock = 0;
+    void clear_metric_graphs()
+    {
+        for (MetricGraph &g : mg) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g = MetricGraph{};
+        }
+    }
 
     // armed by skm_evaluator_wait_drill: the next skm_get_value(_and_derivative) runs the drill
     bool drill_armed = false;
@@ -278,7 +292,7 @@ struct skm_evaluator {
                         d_dense_sw_in, d_shifts, d_in, d_counters, d_part, d_stats, d_deriv, d_rpart, d_out};
         for (void *b : bufs)
             if (b) pool_release(b);
-        if (mgraph) cudaGraphExecDestroy(mgraph);
+        clear_metric_graphs();
         table_tc_free(tc);
         table_free(table);
         cudaStreamSynchronize(0);
@@ -721,6 +735,7 @@ static int upload_field(skm_evaluator *e, const skm_field *df)
     if (!geometry_ok(df->geometry, D)) return fail(SKM_ERR_INVALID, "invalid displacement-field geometry");
     long long n = texels(df->geometry, D);
     if (n > e->df_texels) {
+        e->clear_metric_graphs();                  // their kernels read the old buffer
         if (e->d_df) pool_free(e->d_df);
         e->d_df = nullptr;
         if (dalloc(&e->d_df, n)) return SKM_ERR_CUDA;
@@ -1082,10 +1097,18 @@ extern "C" int skm_metric_evaluate(skm_evaluator *e, const skm_metric_desc *m, c
     if (e->P.sub <= 1) {
         // no sampling offsets to draw: the whole device part is one graph launch
         const int path = active_path(e);
-        if (!e->mgraph || !same_metric(e->mg_desc, *m) || e->mg_deriv != deriv || e->mg_path != path ||
-            e->mg_df != e->df_key || e->mg_pdev != pdev || e->mg_gout != gout) {
-            if (e->mgraph) cudaGraphExecDestroy(e->mgraph);
-            e->mgraph = nullptr;
+        skm_evaluator::MetricGraph *hit = nullptr, *victim = nullptr;
+        for (skm_evaluator::MetricGraph &g : e->mg) {
+            if (g.exec && same_metric(g.desc, *m) && g.deriv == deriv && g.path == path && g.df == e->df_key &&
+                g.pdev == pdev && g.gout == gout) {
+                hit = &g;
+                break;
+            }
+            if (!victim || (victim->exec && (!g.exec || g.used < victim->used))) victim = &g;
+        }
+        if (!hit) {
+            if (victim->exec) cudaGraphExecDestroy(victim->exec);
+            *victim = skm_evaluator::MetricGraph{};
             SKM_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
             int r = metric_sequence(e, m, deriv, pdev, gout);
             cudaGraph_t g = nullptr;
@@ -1095,20 +1118,22 @@ extern "C" int skm_metric_evaluate(skm_evaluator *e, const skm_metric_desc *m, c
                 return r;
             }
             if (ce != cudaSuccess) return fail(SKM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
-            cudaError_t ie = cudaGraphInstantiate(&e->mgraph, g, 0);
+            cudaError_t ie = cudaGraphInstantiate(&victim->exec, g, 0);
             cudaGraphDestroy(g);
             if (ie != cudaSuccess) {
-                e->mgraph = nullptr;
+                victim->exec = nullptr;
                 return fail(SKM_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ie));
             }
-            e->mg_desc = *m;
-            e->mg_deriv = deriv;
-            e->mg_path = path;
-            e->mg_df = e->df_key;
-            e->mg_pdev = pdev;
-            e->mg_gout = gout;
+            victim->desc = *m;
+            victim->deriv = deriv;
+            victim->path = path;
+            victim->df = e->df_key;
+            victim->pdev = pdev;
+            victim->gout = gout;
+            hit = victim;
         }
-        SKM_CUDA(cudaGraphLaunch(e->mgraph, e->stream));
+        hit->used = ++e->mg_clock;
+        SKM_CUDA(cudaGraphLaunch(hit->exec, e->stream));
     } else {
         if ((rc = draw_shifts(e, m->do_resampling))) return rc;
         if ((rc = metric_sequence(e, m, deriv, pdev, gout))) return rc;

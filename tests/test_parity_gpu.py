@@ -318,3 +318,10 @@ def test_metric_with_page_locked_caller_buffers_matches_pageable():
         v2, g2 = ev.metric(m, params * scale, cpw)
         assert v1 == v2 and np.array_equal(gp, g2)
     assert v0["value"] == ev.metric(m, params, cpw)[0]["value"]
+    # two derivative buffers used alternately (each keeps its graph in the evaluator's cache)
+    g_alt = [gp, torch.zeros(params.size, dtype=torch.float64, pin_memory=True).numpy()]
+    for i, scale in enumerate((0.9, 0.8, 0.7, 0.6, 0.5)):
+        pp[:] = params * scale
+        ev.metric(m, pp, cpw, out_derivative=g_alt[i & 1])
+        _, g2 = ev.metric(m, params * scale, cpw)
+        assert np.array_equal(g_alt[i & 1], g2)
