@@ -319,15 +319,29 @@ __device__ inline void stats_finalize(const double *v, int metric, double *__res
 }
 
 // Sums the NV per-block partials [k][nblocks] with the whole block in a fixed order (L2 reads,
-// bypassing L1 so that partials written by other blocks of the same launch are seen).
+// bypassing L1 so that partials written by other blocks of the same launch are seen).  A thread
+// issues kB of its partials of every value before adding them (in the order b = tid, tid + blockDim,
+// ...), so the finishing block waits for one L2 latency per kB partials, not one per partial.
 template <int NV>
 __device__ __forceinline__ void sum_partials(const double *part, int nblocks, double *v, double *sh)
 {
+    constexpr int kB = 4;
 #pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double s = 0.0;
-        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += __ldcg(part + (long long)k * nblocks + b);
-        v[k] = s;
+    for (int k = 0; k < NV; ++k) v[k] = 0.0;
+    for (int b0 = threadIdx.x; b0 < nblocks; b0 += kB * blockDim.x) {
+        double x[NV][kB];
+#pragma unroll
+        for (int k = 0; k < NV; ++k)
+#pragma unroll
+            for (int u = 0; u < kB; ++u) {
+                const int b = b0 + u * (int)blockDim.x;
+                x[k][u] = b < nblocks ? __ldcg(part + (long long)k * nblocks + b) : 0.0;
+            }
+#pragma unroll
+        for (int k = 0; k < NV; ++k)
+#pragma unroll
+            for (int u = 0; u < kB; ++u)
+                if (b0 + u * (int)blockDim.x < nblocks) v[k] += x[k][u];
     }
     block_sum<NV>(v, sh);
 }
