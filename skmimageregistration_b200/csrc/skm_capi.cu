@@ -232,6 +232,8 @@ struct skm_evaluator {
     float4 *d_coeffs4 = nullptr;
     float4 *d_cpd = nullptr, *d_df = nullptr, *d_samp = nullptr, *d_dense = nullptr, *d_dense_sw = nullptr;
     unsigned char *d_dense_in = nullptr, *d_dense_sw_in = nullptr;
+    unsigned *d_need = nullptr;       // LCC: bit per texel that a window reads
+    int *d_list = nullptr, *d_nlist = nullptr;   // LCC: those texels, listed once, and their count
     uint32_t *d_shifts = nullptr;
     double *d_in = nullptr;          // uploaded parameters (AoS or planar) followed by weights
     unsigned *d_counters = nullptr;   // ticket counters of the fused last-block finalizations
@@ -288,8 +290,9 @@ struct skm_evaluator {
         if (device >= 0) cudaSetDevice(device);
         // one device synchronisation for all buffers (no work uses them after it), then the frees
         cudaDeviceSynchronize();
-        void *bufs[] = {d_fixed, d_coeffs, d_coeffs4, d_wimg, d_wten, d_wsup, d_cpd, d_df, d_samp, d_dense, d_dense_sw, d_dense_in,
-                        d_dense_sw_in, d_shifts, d_in, d_counters, d_part, d_stats, d_deriv, d_rpart, d_out};
+        void *bufs[] = {d_fixed, d_coeffs, d_coeffs4, d_wimg, d_wten, d_wsup, d_cpd, d_df, d_samp, d_dense, d_dense_sw,
+                        d_dense_in, d_need, d_list, d_nlist, d_dense_sw_in, d_shifts, d_in, d_counters, d_part,
+                        d_stats, d_deriv, d_rpart, d_out};
         for (void *b : bufs)
             if (b) pool_release(b);
         clear_metric_graphs();
@@ -351,10 +354,18 @@ template <int D, int KIND>
 struct LaunchLccValue {
     static int run(skm_evaluator *e)
     {
-        dense_kernel<D, KIND, false><<<e->dense_blocks, 256, 0, e->stream>>>(e->P, e->d_dense, e->d_dense_in);
+        // the texels the windows read (listed once each), then the dense fields there only
+        SKM_CUDA(cudaMemsetAsync(e->d_need, 0, sizeof(unsigned) * ((e->N + 31) / 32), e->stream));
+        SKM_CUDA(cudaMemsetAsync(e->d_nlist, 0, sizeof(int), e->stream));
+        lcc_mark_kernel<D, KIND><<<e->value_blocks, 256, 0, e->stream>>>(e->P, e->d_need, e->d_list, e->d_nlist);
+        SKM_CHECK_LAUNCH();
+        const int lb = grid_for(e->N);
+        dense_list_kernel<D, KIND, false><<<lb, 256, 0, e->stream>>>(e->P, e->d_list, e->d_nlist, e->d_dense,
+                                                                     e->d_dense_in);
         SKM_CHECK_LAUNCH();
         if (D == 3 && KIND != kStationary) {
-            dense_kernel<D, KIND, true><<<e->dense_blocks, 256, 0, e->stream>>>(e->P, e->d_dense_sw, e->d_dense_sw_in);
+            dense_list_kernel<D, KIND, true><<<lb, 256, 0, e->stream>>>(e->P, e->d_list, e->d_nlist, e->d_dense_sw,
+                                                                        e->d_dense_sw_in);
             SKM_CHECK_LAUNCH();
         }
         lcc_value_kernel<D, KIND><<<e->value_blocks, kValueThreads, 0, e->stream>>>(e->P, e->d_dense, e->d_dense_in,
@@ -798,6 +809,9 @@ static int ensure_dense(skm_evaluator *e)
     if (!e->d_dense) {
         if (dalloc(&e->d_dense, e->N)) return SKM_ERR_CUDA;
         if (dalloc(&e->d_dense_in, e->N)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_need, (e->N + 31) / 32)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_list, e->N)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_nlist, 1)) return SKM_ERR_CUDA;
     }
     if (e->D == 3 && e->P.K.kind != kStationary && !e->d_dense_sw) {
         if (dalloc(&e->d_dense_sw, e->N)) return SKM_ERR_CUDA;

@@ -853,15 +853,13 @@ static __global__ void __launch_bounds__(256) result_kernel(const double *__rest
 }
 
 // ---- LCC: dense fields and per-sample values --------------------------------------------------
-// (grad M, m) and the inside flag at every fixed texel: the neighbour transforms of the
-// reference's LCC windows (LCC.cu:112-176) evaluated once per texel instead of per window.
+// (grad M, m) and the inside flag at the fixed texels the LCC windows read: the neighbour
+// transforms of the reference's LCC windows (LCC.cu:112-176) evaluated once per texel instead of
+// once per window.
 template <int D, int KIND, bool SWAP>
-__global__ void __launch_bounds__(256) dense_kernel(EvalParams P, float4 *__restrict__ dense,
-                                                    unsigned char *__restrict__ dense_in)
+__device__ __forceinline__ void dense_texel(const EvalParams &P, long long t, float4 *__restrict__ dense,
+                                            unsigned char *__restrict__ dense_in)
 {
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    long long N = (long long)P.fixed.n[0] * P.fixed.n[1] * P.fixed.n[2];
-    if (t >= N) return;
     int c[3];
     cell_of<D>(P.fixed.n, t, c);
     double fi[3] = {(double)c[0], (double)c[1], (double)c[2]}, p[3], ml[3];
@@ -877,6 +875,83 @@ __global__ void __launch_bounds__(256) dense_kernel(EvalParams P, float4 *__rest
     }
     dense[t] = rec;
     dense_in[t] = in;
+}
+
+__device__ __forceinline__ void lcc_mark(unsigned *__restrict__ bits, int *__restrict__ list, int *__restrict__ count,
+                                         long long i)
+{
+    const unsigned bit = 1u << (i & 31);
+    if (!(atomicOr(bits + (i >> 5), bit) & bit)) list[atomicAdd(count, 1)] = (int)i;
+}
+
+// The texels that the value and derivative kernels read from the dense fields: each sample's own
+// texel and every window point with a nonzero neighbourhood weight -- the same positions, bounds
+// and weight test as lcc_value_kernel and lcc_sample_derivative (the derivative also walks the
+// windows of samples whose shifted position lies past the image) -- listed once each.  With
+// subsampled samples and strided windows this is a small part of the image (at 1.5 mm, sampling
+// 32 and stride 48: ~10^4 of 10^7 texels).  The list's order does not matter: a listed texel
+// writes only its own entry.
+template <int D, int KIND>
+__global__ void __launch_bounds__(256) lcc_mark_kernel(EvalParams P, unsigned *__restrict__ bits,
+                                                       int *__restrict__ list, int *__restrict__ count)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.Ns) return;
+    int c[3], sp[3];
+    cell_of<D>(P.ss, t, c);
+    bool inside = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) sp[d] = c[d];
+    if (P.sub != 1) {
+        const uint32_t s = P.shifts[t];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            sp[d] = c[d] * P.sub + (int)((s >> (8 * d)) & 0xffu);
+            if (sp[d] >= P.fixed.n[d]) inside = false;
+        }
+    }
+    double fi[3] = {(double)sp[0], (double)sp[1], (double)sp[2]}, p[3];
+    to_global<D>(P.fixed, fi, p);
+    if (inside) lcc_mark(bits, list, count, lin_of<D>(P.fixed, sp));
+    PInfo pi;
+    pinfo_at<KIND, D>(P.K, p, pi);
+    double fl[3];
+    to_local<D>(P.fixed, p, fl);
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        double shf = pi.support / P.fixed.s[d];
+        lo[d] = clampi((int)(fl[d] - shf + 1.0), 0, P.fixed.n[d] - 1);
+        hi[d] = clampi((int)(fl[d] + shf), 0, P.fixed.n[d] - 1);
+    }
+    for (int z = lo[2]; z <= hi[2]; z += P.nbh)
+        for (int y = lo[1]; y <= hi[1]; y += P.nbh)
+            for (int x = lo[0]; x <= hi[0]; x += P.nbh) {
+                int ni[3] = {x, y, z};
+                double nf[3] = {(double)x, (double)y, (double)z}, q[3];
+                to_global<D>(P.fixed, nf, q);
+                double sup;
+                if (KIND == kStationary) {
+                    sup = (double)P.K.support_min;
+                } else {
+                    PInfo pn;
+                    pinfo_at<KIND, D>(P.K, q, pn);
+                    sup = (double)(float)pn.support;
+                }
+                if (lcc_weight_base<D>(p, q, sup) <= 0.0) continue;
+                lcc_mark(bits, list, count, lin_of<D>(P.fixed, ni));
+            }
+}
+
+// the dense fields at the listed texels (grid-strided over the count the marking kernel wrote)
+template <int D, int KIND, bool SWAP>
+__global__ void __launch_bounds__(256) dense_list_kernel(EvalParams P, const int *__restrict__ list,
+                                                         const int *__restrict__ count, float4 *__restrict__ dense,
+                                                         unsigned char *__restrict__ dense_in)
+{
+    const int n = *count;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        dense_texel<D, KIND, SWAP>(P, list[i], dense, dense_in);
 }
 
 // LCC value per sample (LCC.cu:38-204) from the dense fields.
