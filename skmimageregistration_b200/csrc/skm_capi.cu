@@ -234,6 +234,7 @@ struct skm_evaluator {
     unsigned char *d_dense_in = nullptr, *d_dense_sw_in = nullptr;
     unsigned *d_need = nullptr;       // LCC: bit per texel that a window reads
     int *d_list = nullptr, *d_nlist = nullptr;   // LCC: those texels, listed once, and their count
+    float4 *d_acache = nullptr;       // LCC 3-D weight tensors: per-texel kernel inverse and factor
     uint32_t *d_shifts = nullptr;
     double *d_in = nullptr;          // uploaded parameters (AoS or planar) followed by weights
     unsigned *d_counters = nullptr;   // ticket counters of the fused last-block finalizations
@@ -291,7 +292,7 @@ struct skm_evaluator {
         // one device synchronisation for all buffers (no work uses them after it), then the frees
         cudaDeviceSynchronize();
         void *bufs[] = {d_fixed, d_coeffs, d_coeffs4, d_wimg, d_wten, d_wsup, d_cpd, d_df, d_samp, d_dense, d_dense_sw,
-                        d_dense_in, d_need, d_list, d_nlist, d_dense_sw_in, d_shifts, d_in, d_counters, d_part,
+                        d_dense_in, d_need, d_list, d_nlist, d_acache, d_dense_sw_in, d_shifts, d_in, d_counters, d_part,
                         d_stats, d_deriv, d_rpart, d_out};
         for (void *b : bufs)
             if (b) pool_release(b);
@@ -365,7 +366,7 @@ struct LaunchLccValue {
         SKM_CHECK_LAUNCH();
         if (D == 3 && KIND != kStationary) {
             dense_list_kernel<D, KIND, true><<<lb, 256, 0, e->stream>>>(e->P, e->d_list, e->d_nlist, e->d_dense_sw,
-                                                                        e->d_dense_sw_in);
+                                                                        e->d_dense_sw_in, e->d_acache);
             SKM_CHECK_LAUNCH();
         }
         lcc_value_kernel<D, KIND><<<e->value_blocks, kValueThreads, 0, e->stream>>>(e->P, e->d_dense, e->d_dense_in,
@@ -817,6 +818,8 @@ static int ensure_dense(skm_evaluator *e)
         if (dalloc(&e->d_dense_sw, e->N)) return SKM_ERR_CUDA;
         if (dalloc(&e->d_dense_sw_in, e->N)) return SKM_ERR_CUDA;
     }
+    if (e->D == 3 && e->P.K.kind == kWeightTensor && !e->d_acache)
+        if (dalloc(&e->d_acache, 3 * e->N)) return SKM_ERR_CUDA;
     return SKM_OK;
 }
 
@@ -879,6 +882,7 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     Q.dense_in = e->d_dense_in;
     Q.dense_sw = e->d_dense_sw;
     Q.dense_sw_in = e->d_dense_sw_in;
+    Q.acache = e->d_acache;
     Q.deriv = d_deriv;
     Q.rpart = e->d_rpart;
     Q.out = d_res;

@@ -322,6 +322,58 @@ __device__ __forceinline__ void pinfo_at(const KernelParams &K, const double *p,
     }
 }
 
+// getRegionSupport alone: pinfo_at's support radius without the sigma / covariance loads
+template <int KIND, int D>
+__device__ __forceinline__ double support_at(const KernelParams &K, const double *p)
+{
+    if (KIND == kWeightImage) {
+        const long long i = nearest_index<D>(K.gw, p);
+        return i >= 0 ? K.wsup[i] : K.sup_default;
+    }
+    if (KIND == kWeightTensor) {
+        const long long i = nearest_index<D>(K.gt, p);
+        return i >= 0 ? K.wsup[i] : K.sup_default;
+    }
+    return (double)K.support_min;
+}
+
+// The 3-D anisotropic kernel with one texel's covariance at both ends (the LCC derivative's
+// k(c_i, n), LCC.cu:449-461): evaluateAnisotropic's factor F and the inverse of (covP + covQ) / 2
+// (adjugate over determinant, as quad_inv forms it) depend on the texel alone, so they are
+// computed once per texel, in the same expressions, and kept as three float4 (inverse row-major,
+// then F).
+__device__ __forceinline__ void aniso_self_cache(const float *c, float4 *out)
+{
+    float ms[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) ms[e] = (c[e] + c[e]) * 0.5f;
+    const float dt = det_m<3>(ms);
+#define M_(i, j) ms[(i) * 3 + (j)]
+    const float a[9] = {M_(1, 1) * M_(2, 2) - M_(1, 2) * M_(2, 1), M_(0, 2) * M_(2, 1) - M_(0, 1) * M_(2, 2),
+                        M_(0, 1) * M_(1, 2) - M_(0, 2) * M_(1, 1), M_(1, 2) * M_(2, 0) - M_(1, 0) * M_(2, 2),
+                        M_(0, 0) * M_(2, 2) - M_(0, 2) * M_(2, 0), M_(0, 2) * M_(1, 0) - M_(0, 0) * M_(1, 2),
+                        M_(1, 0) * M_(2, 1) - M_(1, 1) * M_(2, 0), M_(0, 1) * M_(2, 0) - M_(0, 0) * M_(2, 1),
+                        M_(0, 0) * M_(1, 1) - M_(0, 1) * M_(1, 0)};
+#undef M_
+    const float F = powf(det_m<3>(c), 0.25f) * powf(det_m<3>(c), 0.25f) * powf(det_m<3>(ms), -0.5f);
+    out[0] = make_float4(a[0] / dt, a[1] / dt, a[2] / dt, a[3] / dt);
+    out[1] = make_float4(a[4] / dt, a[5] / dt, a[6] / dt, a[7] / dt);
+    out[2] = make_float4(a[8] / dt, F, 0.f, 0.f);
+}
+
+__device__ __forceinline__ float aniso_self_eval(const KernelParams &K, const float *v, const float4 *c)
+{
+    const float inv[9] = {c[0].x, c[0].y, c[0].z, c[0].w, c[1].x, c[1].y, c[1].z, c[1].w, c[2].x};
+    float q = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float r = v[0] * inv[0 * 3 + i] + v[1] * inv[1 * 3 + i] + v[2] * inv[2 * 3 + i];
+        q += r * v[i];
+    }
+    const float sqrtQ = sqrtf(q), F = c[2].y;
+    return F * wendland_c4(sqrtQ * K.inv_sc4) * F * wendland_c0(sqrtQ * K.inv_sc0);
+}
+
 // GKernel::evaluate(p, q, p-side info) with v = p - q given in float and q's global
 // position (needed for the sigma / covariance lookup at q).
 template <int KIND, int D>

@@ -110,6 +110,7 @@ struct DerivParams {
     const unsigned char *__restrict__ dense_in;
     const float4 *__restrict__ dense_sw; // LCC 3-D swapped-kernel field (non-stationary kinds)
     const unsigned char *__restrict__ dense_sw_in;
+    const float4 *__restrict__ acache;   // LCC 3-D weight tensors: aniso_self_cache per listed texel
     double *__restrict__ deriv;          // planar output
     double *__restrict__ rpart;          // [NR][blocks]
     double *__restrict__ out;            // result vector (fused finalization)
@@ -524,8 +525,14 @@ __device__ __forceinline__ void lcc_sample_derivative(const EvalParams &P, const
                 int ni[3] = {x, y, z};
                 double nf[3] = {(double)x, (double)y, (double)z}, q[3];
                 to_global<D>(P.fixed, nf, q);
+                // the tensor kind's kernel value comes from the texel's cached inverse and factor,
+                // so only the support radius is looked up here
+                constexpr bool cached = (D == 3 && KIND == kWeightTensor);
                 PInfo pn;
-                pinfo_at<KIND, D>(P.K, q, pn);
+                if (cached)
+                    pn.support = support_at<KIND, D>(P.K, q);
+                else
+                    pinfo_at<KIND, D>(P.K, q, pn);
                 // neighborhoodWeight with the neighbour's support passed as float (LCC.cu:28-35)
                 double kwf = lcc_weight_base<D>(pt, q, (double)(float)pn.support);
                 if (kwf <= 0.0) continue;
@@ -536,7 +543,11 @@ __device__ __forceinline__ void lcc_sample_derivative(const EvalParams &P, const
                 float v[3];
 #pragma unroll
                 for (int d = 0; d < D; ++d) v[d] = (float)(gp[d] - q[d]);
-                float ka = k_eval<KIND, D>(P.K, v, q, pn);
+                float ka;
+                if (cached)
+                    ka = aniso_self_eval(P.K, v, Q.acache + 3 * nl);
+                else
+                    ka = k_eval<KIND, D>(P.K, v, q, pn);
                 float4 rec = dense[nl];
                 double mv = __dmul_rn((double)rec.w, kw);
                 double fv = __dmul_rn(kw, (double)P.fixed_data[nl]);
@@ -943,15 +954,29 @@ __global__ void __launch_bounds__(256) lcc_mark_kernel(EvalParams P, unsigned *_
             }
 }
 
-// the dense fields at the listed texels (grid-strided over the count the marking kernel wrote)
+// the dense fields at the listed texels (grid-strided over the count the marking kernel wrote);
+// acache (3-D weight tensors, swapped pass) also takes each listed texel's aniso_self_cache, which
+// the derivative's window walk reads at the same texels
 template <int D, int KIND, bool SWAP>
 __global__ void __launch_bounds__(256) dense_list_kernel(EvalParams P, const int *__restrict__ list,
                                                          const int *__restrict__ count, float4 *__restrict__ dense,
-                                                         unsigned char *__restrict__ dense_in)
+                                                         unsigned char *__restrict__ dense_in,
+                                                         float4 *__restrict__ acache = nullptr)
 {
     const int n = *count;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        dense_texel<D, KIND, SWAP>(P, list[i], dense, dense_in);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int t = list[i];
+        dense_texel<D, KIND, SWAP>(P, t, dense, dense_in);
+        if (D == 3 && KIND == kWeightTensor && acache) {
+            int c[3];
+            cell_of<D>(P.fixed.n, t, c);
+            double nf[3] = {(double)c[0], (double)c[1], (double)c[2]}, q[3];
+            to_global<D>(P.fixed, nf, q);
+            PInfo pn;
+            pinfo_at<KIND, D>(P.K, q, pn);
+            aniso_self_cache(pn.cov, acache + 3 * (long long)t);
+        }
+    }
 }
 
 // LCC value per sample (LCC.cu:38-204) from the dense fields.
