@@ -245,7 +245,7 @@ def kernel_work(pb, info, phases):
                      "bound": "hbm", "ms": phases["warp"], "flops": bspline_flops,
                      "bytes": cells * nph * (4 * D + 4 + 16) + ncoef * 4, "alg_bytes": 8.0 * N},
             "contrib": co,
-            "gather": {"name": "table_gather_kernel", "bound": "hbm", "ms": phases["gather"],
+            "gather": {"name": "table_gather_rows_kernel", "bound": "hbm", "ms": phases["gather"],
                        "flops": 3.0 * C * ntap + 20.0 * C * info["table_regularizer_offsets"],
                        "bytes": 3 * ctaps * cells * 4 + C * 16 + C * D * 8, "alg_bytes": 12.0 * C},
         }

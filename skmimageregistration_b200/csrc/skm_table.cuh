@@ -862,6 +862,322 @@ __global__ void __launch_bounds__(kGatherThreads, 3) table_gather_kernel(EvalPar
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// The same gather (Contrib array, no brick partials) with its index work moved out of the loops:
+// the block's prologue writes, per contrib tap, its cell offset (ox, oy, oz) and the linear offset
+// k ncell - lin(o) of Contrib[k][j - o] relative to the control point's own cell index, and per
+// regularizer offset (dx, dy, dz) its linear control-point offset; both lists are padded to whole
+// rounds of the warps' unrolled loops with entries whose bounds test fails.  A tap then costs one
+// shared-memory read, three index differences and their bounds test, and its three loads; an
+// offset the same plus its terms.  GW warps split the taps and offsets (warp g takes every GW-th),
+// each adds its loads in list order, and the warps' partials are combined in warp order: the sums
+// are fixed for a given GW.  Shared memory is sized at launch (gather_rows_smem).
+constexpr int kRowsTapUnroll = 20;     // taps whose loads a warp has in flight
+constexpr int kRowsRegUnroll = 4;      // regularizer offsets whose loads a warp has in flight
+
+inline size_t gather_rows_smem(int gw, int ntap, int nkcp)
+{
+    const int ntr = (ntap + gw * kRowsTapUnroll - 1) / (gw * kRowsTapUnroll) * (gw * kRowsTapUnroll);
+    const int nkr = (nkcp + gw * kRowsRegUnroll - 1) / (gw * kRowsRegUnroll) * (gw * kRowsRegUnroll);
+    return (size_t)gw * 3 * 32 * sizeof(double) + (size_t)(ntr + nkr) * sizeof(int4) + (size_t)nkr * sizeof(float) +
+           (size_t)gw * 12 * 32 * sizeof(float);
+}
+
+template <int D, int GW>
+__global__ void __launch_bounds__(GW * 32, 24 / GW) table_gather_rows_kernel(EvalParams P, TableDev T, DerivParams Q)
+{
+    constexpr int KU = kRowsTapUnroll, KR = kRowsRegUnroll;
+    static_assert(GW >= 3, "warps 0..D-1 combine one component each");
+    extern __shared__ double gr_smem[];
+    const int ntap = Q.values_only ? 0 : T.ngtap;
+    const int ntr = (ntap + GW * KU - 1) / (GW * KU) * (GW * KU);
+    const int nkcp = T.nkcp;
+    const int nkr = (nkcp + GW * KR - 1) / (GW * KR) * (GW * KR);
+    double *sval = gr_smem;                                        // [GW][3][32]
+    int4 *stap = reinterpret_cast<int4 *>(sval + GW * 3 * 32);     // [ntr] (ox, oy, oz, contrib offset)
+    int4 *soff = stap + ntr;                                       // [nkr] (dx, dy, dz, linear offset)
+    float *skv = reinterpret_cast<float *>(soff + nkr);            // [nkr] kernel values
+    float *sacc = skv + nkr;                                       // [GW][3][32]
+    float *sreg = sacc + GW * 3 * 32;                              // [GW][9][32]
+    const int ncell = (int)T.ncell;
+    for (int k = threadIdx.x; k < ntr; k += blockDim.x) {
+        int4 o = make_int4(1 << 29, 1 << 29, 1 << 29, 0);         // padding: outside every cell range
+        if (k < ntap) {
+            const int i = T.gtap ? T.gtap[k] : k;
+            o.x = T.tlo[0] + T.qmin[0] + i % T.nt[0];
+            o.y = T.tlo[1] + T.qmin[1] + (i / T.nt[0]) % T.nt[1];
+            o.z = T.tlo[2] + T.qmin[2] + i / (T.nt[0] * T.nt[1]);
+            o.w = k * ncell - ((o.z * T.nq[1] + o.y) * T.nq[0] + o.x);
+        }
+        stap[k] = o;
+    }
+    const int st1 = (int)P.cp.st[1], st2 = (int)P.cp.st[2];
+    for (int o = threadIdx.x; o < nkr; o += blockDim.x) {
+        int4 d4 = make_int4(1 << 29, 0, 0, 0);                     // padding: outside the grid
+        float kv = 0.f;
+        if (o < nkcp) {
+            const int pk = T.kcpo[o];
+            d4.x = (pk & 1023) - 512;
+            d4.y = ((pk >> 10) & 1023) - 512;
+            d4.z = (pk >> 20) - 512;
+            d4.w = d4.x + (D > 1 ? st1 * d4.y : 0) + (D > 2 ? st2 * d4.z : 0);
+            kv = T.kcp[o];
+        }
+        soff[o] = d4;
+        skv[o] = kv;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, grp = threadIdx.x >> 5;
+    const int j_lin = blockIdx.x * 32 + lane;                      // C < 2^31 (checked at creation)
+    const bool active = j_lin < P.C;
+    int j[3] = {0, 0, 0};
+    if (active) {
+        j[0] = j_lin % P.cp.n[0];
+        const int r = j_lin / P.cp.n[0];
+        if (D > 1) j[1] = D > 2 ? r % P.cp.n[1] : r;
+        if (D > 2) j[2] = r / P.cp.n[1];
+    }
+    const float4 cj = active ? P.cpd[j_lin] : make_float4(0.f, 0.f, 0.f, 0.f);
+    // the fused optimizer step: warp d applies it to component d (after combining it, below); its
+    // operands are loaded now so that their latency overlaps the sums
+    const int sd = grp;
+    const bool stepper = Q.step.on && active && sd < D;
+    double st_g = 0.0, st_b = 0.0, st_x = 0.0, st_t = 0.0, st_p = 0.0;
+    if (stepper) {
+        st_g = Q.step.tmp[j_lin + sd * P.C];
+        st_b = Q.step.base[j_lin + sd * P.C];
+        st_x = Q.step.pos[j_lin + sd * P.C];
+        st_t = Q.step.scal[T_TIME];
+        st_p = Q.step.scal[T_PENDING];
+    }
+    float acc[3] = {0.f, 0.f, 0.f};
+    if (active && ntap > 0) {
+        const int jcell = (j[2] * T.nq[1] + j[1]) * T.nq[0] + j[0];
+        const unsigned plane = (unsigned)ntap * (unsigned)ncell;  // floats between component planes
+        for (int base = grp; base < ntr; base += GW * KU) {
+            float v[KU][3];
+#pragma unroll
+            for (int u = 0; u < KU; ++u) {
+                const int4 o = stap[base + u * GW];
+                const bool in = (unsigned)(j[0] - o.x) < (unsigned)T.nq[0] && (unsigned)(j[1] - o.y) < (unsigned)T.nq[1] &&
+                                (unsigned)(j[2] - o.z) < (unsigned)T.nq[2];
+                const unsigned c = (unsigned)(o.w + jcell);
+                v[u][0] = in ? __ldg(T.contrib + c) : 0.f;
+                v[u][1] = in ? __ldg(T.contrib + (c + plane)) : 0.f;
+                v[u][2] = (in && D > 2) ? __ldg(T.contrib + (c + 2u * plane)) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < KU; ++u) {
+                acc[0] += v[u][0];
+                acc[1] += v[u][1];
+                if (D > 2) acc[2] += v[u][2];
+            }
+        }
+    }
+    double pc[3] = {0.0, 0.0, 0.0};
+    if (Q.with_metric && grp < D && active)
+#pragma unroll
+        for (int d = 0; d < D; ++d) pc[d] = Q.params[j_lin + d * P.C];
+    float drk[3] = {0.f, 0.f, 0.f}, drd[3] = {0.f, 0.f, 0.f}, dpg[3] = {0.f, 0.f, 0.f};
+    double vr = 0.0, vd = 0.0, vp = 0.0;
+    const bool rkhs = Q.reg_rkhs > 0.0, rd = Q.reg_rd > 0.0, pg = Q.reg_pg > 0.0;
+    if (active && (rkhs || rd || pg)) {
+        const float wj = cj.w;
+        const float cjv[3] = {cj.x, cj.y, cj.z};
+        const float pgs = (float)Q.pg_scaling;
+        for (int o0 = grp; o0 < nkr; o0 += GW * KR) {
+            float4 cn[KR];
+            float kk[KR];
+            bool okk[KR];
+#pragma unroll
+            for (int u = 0; u < KR; ++u) {
+                const int o = o0 + u * GW;
+                const int4 d4 = soff[o];
+                kk[u] = skv[o];
+                okk[u] = (unsigned)(j[0] + d4.x) < (unsigned)P.cp.n[0] && (unsigned)(j[1] + d4.y) < (unsigned)P.cp.n[1] &&
+                         (unsigned)(j[2] + d4.z) < (unsigned)P.cp.n[2];
+                cn[u] = okk[u] ? __ldg(P.cpd + (j_lin + d4.w)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < KR; ++u) {
+                if (!okk[u]) continue;
+                const float k = kk[u];
+                const float4 ci4 = cn[u];
+                const float ci[3] = {ci4.x, ci4.y, ci4.z};
+                const float kw = k * wj;
+                // per-offset terms in FP32 (relative error ~1e-7), their sums in FP64
+                if (rkhs) {                                        // Regularizers.cu:68-73
+                    float dot = 0.f;
+#pragma unroll
+                    for (int d = 0; d < D; ++d) dot = fmaf(cjv[d], ci[d], dot);
+                    vr += (double)(kw * dot);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) drk[d] = fmaf(2.0f * kw, ci[d], drk[d]);
+                }
+                if (rd) {                                          // Regularizers.cu:141-144
+                    float l2 = 0.f;
+#pragma unroll
+                    for (int d = 0; d < D; ++d) {
+                        const float e = cjv[d] - ci[d];
+                        l2 = fmaf(e, e, l2);
+                    }
+                    vd += (double)(kw * l2);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) drd[d] = fmaf(4.0f * kw, cjv[d] - ci[d], drd[d]);
+                }
+                if (pg) {
+                    if (D == 3) {                                  // Regularizers.cu:218-237
+                        const float cr0 = ci[1] * cjv[2] - ci[2] * cjv[1];
+                        const float cr1 = ci[2] * cjv[0] - ci[0] * cjv[2];
+                        const float cr2 = ci[0] * cjv[1] - ci[1] * cjv[0];
+                        const double n2 = (double)cr0 * cr0 + (double)cr1 * cr1 + (double)cr2 * cr2;
+                        const double sc = (double)pgs;
+                        vp += (double)kw * sc * sc / 2.0 * log(1.0 + n2 / sc);
+                        const float den = 2.0f * ((float)n2 / pgs + 1.0f);
+                        const float dp0 = 2.0f * ci[2] * (ci[2] * cjv[0] - ci[0] * cjv[2]) - 2.0f * ci[1] * (ci[0] * cjv[1] - ci[1] * cjv[0]);
+                        const float dp1 = 2.0f * ci[0] * (ci[0] * cjv[1] - ci[1] * cjv[0]) - 2.0f * ci[2] * (ci[1] * cjv[2] - ci[2] * cjv[1]);
+                        const float dp2 = 2.0f * ci[1] * (ci[1] * cjv[2] - ci[2] * cjv[1]) - 2.0f * ci[0] * (ci[2] * cjv[0] - ci[0] * cjv[2]);
+                        dpg[0] = fmaf(2.0f * kw, pgs * dp0 / den, dpg[0]);
+                        dpg[1] = fmaf(2.0f * kw, pgs * dp1 / den, dpg[1]);
+                        dpg[2] = fmaf(2.0f * kw, pgs * dp2 / den, dpg[2]);
+                    } else {                                       // Regularizers.cu:447-459
+                        const float v2d = ci[0] * cjv[1] - ci[1] * cjv[0];
+                        const double v2 = (double)v2d * v2d;
+                        const double sc = (double)pgs;
+                        vp += (double)kw * sc * sc / 2.0 * log(1.0 + v2 / sc);
+                        const float factor = (float)v2 / pgs + 1.0f;
+                        dpg[0] = fmaf(2.0f * kw, -pgs * ci[1] * v2d / factor, dpg[0]);
+                        dpg[1] = fmaf(2.0f * kw, pgs * ci[0] * v2d / factor, dpg[1]);
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        sacc[(grp * 3 + d) * 32 + lane] = acc[d];
+        sreg[(grp * 9 + d) * 32 + lane] = drk[d];
+        sreg[(grp * 9 + 3 + d) * 32 + lane] = drd[d];
+        sreg[(grp * 9 + 6 + d) * 32 + lane] = dpg[d];
+    }
+    sval[(grp * 3 + 0) * 32 + lane] = vr;
+    sval[(grp * 3 + 1) * 32 + lane] = vd;
+    sval[(grp * 3 + 2) * 32 + lane] = vp;
+    __syncthreads();
+    double val[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) val[k] = 0.0;
+    __shared__ double ssp[3];
+    double sp = 0.0;
+    if (grp < D && active) {
+        const int d = grp;
+        float a = 0.f, rk = 0.f, rdd = 0.f, rp = 0.f;
+        for (int g = 0; g < GW; ++g) {                          // fixed combination order
+            a += sacc[(g * 3 + d) * 32 + lane];
+            rk += sreg[(g * 9 + d) * 32 + lane];
+            rdd += sreg[(g * 9 + 3 + d) * 32 + lane];
+            rp += sreg[(g * 9 + 6 + d) * 32 + lane];
+            if (d == 0) {
+                val[R_RKHS] += sval[(g * 3 + 0) * 32 + lane];
+                val[R_RD] += sval[(g * 3 + 1) * 32 + lane];
+                val[R_PG] += sval[(g * 3 + 2) * 32 + lane];
+            }
+        }
+        const double *st = Q.stats;
+        double pn2 = 0.0;
+        if (Q.with_metric) {
+#pragma unroll
+            for (int e = 0; e < D; ++e) pn2 += pc[e] * pc[e];
+        }
+        const double pnorm = sqrt(pn2);
+        double g;
+        if (Q.metric == 1)
+            g = st[S_DENOM] != 0.0 ? (double)cj.w * (double)a : 0.0;
+        else
+            g = (double)cj.w * (double)a;
+        if (rkhs) g += (double)rk * Q.reg_rkhs;
+        if (rd) g += (double)rdd * Q.reg_rd;
+        if (pg) g += (double)rp * Q.reg_pg;
+        if (Q.with_metric) {
+            const double par = pc[d];
+            if (Q.reg_l1 > 0.0) {                              // metric hxx:447-466
+                const double w = Q.reg_l1;
+                if (fabs(par) > 0.0) g += w * (par < 0.0 ? -1.0 : 1.0);
+                else if (g < -w) g += w;
+                else if (g > w) g -= w;
+                else g = 0.0;
+            }
+            if (Q.reg_l2 > 0.0) g += Q.reg_l2 * 2.0 * par;      // hxx:482-485
+            if (Q.reg_l21 > 0.0) {                             // hxx:504-521
+                const double w = Q.reg_l21;
+                if (pnorm > 0.0) g += w * par / pnorm;
+                else if (g < -w) g += w;
+                else if (g > w) g -= w;
+                else g = 0.0;
+            }
+            if (Q.negate) g = -g;
+        }
+        Q.deriv[j_lin + d * P.C] = g;
+        if (stepper)
+            sp = opt_update(Q.step, j_lin + d * P.C, g, opt_learning_rate(Q.step, st_t), st_p != 0.0, st_g, st_b, st_x);
+        if (d == 0 && Q.with_metric) {
+            double l1 = 0.0;
+#pragma unroll
+            for (int e = 0; e < D; ++e) l1 += fabs(pc[e]);
+            val[R_L1] = Q.reg_l1 > 0.0 ? l1 : 0.0;
+            val[R_L2] = Q.reg_l2 > 0.0 ? pn2 : 0.0;
+            val[R_L21] = Q.reg_l21 > 0.0 ? pnorm : 0.0;
+        }
+    }
+    if (grp == 0) {
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+            const double sum = warp_sum(val[k]);
+            if (lane == 0) Q.rpart[(long long)k * gridDim.x + blockIdx.x] = sum;
+        }
+    }
+    if (Q.step.on) {                                       // uniform over the grid
+        if (grp < D) {
+            sp = warp_sum(sp);
+            if (lane == 0) ssp[grp] = sp;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = 0.0;
+            for (int d = 0; d < D; ++d) b += ssp[d];
+            Q.step.sp_part[blockIdx.x] = b;
+        }
+    }
+    if (last_block_arrived(Q.counter)) {                   // fused result (and step scalars), fixed order
+        __shared__ double shr[NR * 32];
+        double w[NR], wsp[1] = {0.0};
+        sum_partials<NR>(Q.rpart, gridDim.x, w, shr);
+        if (Q.step.on) sum_partials<1>(Q.step.sp_part, gridDim.x, wsp, shr);
+        if (threadIdx.x == 0) {
+            result_finalize(Q.stats, w, Q.reg_rkhs, Q.reg_rd, Q.reg_pg, Q.reg_l1, Q.reg_l21, Q.reg_l2, Q.out,
+                            T.tc_err);
+            if (Q.step.on) opt_finish(Q.step, wsp[0], opt_learning_rate(Q.step, Q.step.scal[T_TIME]), Q.out);
+        }
+    }
+}
+
+// Warps per 32 control points: 4 puts every block of the 128x128x96, 24,576-point grid on the GPU at
+// once (768 blocks, 6 per SM); 8 was 4 us slower per launch on a B200 (two waves).
+constexpr int kRowsWarps = 4;
+
+// The gather over the Contrib array: the hoisted-index kernel when its tables fit in 48 KB of
+// shared memory (no opt-in needed), else the kernel that indexes in its loops.
+template <int D>
+inline void table_gather_launch(const EvalParams &P, const TableDev &G, const DerivParams &Q, int blocks,
+                                cudaStream_t s)
+{
+    const size_t smem = gather_rows_smem(kRowsWarps, Q.values_only ? 0 : G.ngtap, G.nkcp);
+    if (smem <= 48 * 1024)
+        table_gather_rows_kernel<D, kRowsWarps><<<blocks, kRowsWarps * 32, smem, s>>>(P, G, Q);
+    else
+        table_gather_kernel<D><<<blocks, kGatherThreads, 0, s>>>(P, G, Q);
+}
+
 
 
 // ------------------------------------------------------------------------------------------------

@@ -1439,9 +1439,9 @@ inline int table_derivative(TablePlan &pl, const TcPlan *tc, const EvalParams &P
     if (D == 3 && bricks)
         table_gather_kernel<3, true><<<gather_blocks, kGatherThreads, 0, s>>>(P, G, Q);
     else if (D == 3)
-        table_gather_kernel<3><<<gather_blocks, kGatherThreads, 0, s>>>(P, G, Q);
+        table_gather_launch<3>(P, G, Q, gather_blocks, s);
     else
-        table_gather_kernel<2><<<gather_blocks, kGatherThreads, 0, s>>>(P, G, Q);
+        table_gather_launch<2>(P, G, Q, gather_blocks, s);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
@@ -1449,9 +1449,9 @@ inline int table_derivative_gather_only(TablePlan &pl, const EvalParams &P, cons
                                         int gather_blocks, cudaStream_t s)
 {
     if (D == 3)
-        table_gather_kernel<3><<<gather_blocks, kGatherThreads, 0, s>>>(P, pl.dev, Q);
+        table_gather_launch<3>(P, pl.dev, Q, gather_blocks, s);
     else
-        table_gather_kernel<2><<<gather_blocks, kGatherThreads, 0, s>>>(P, pl.dev, Q);
+        table_gather_launch<2>(P, pl.dev, Q, gather_blocks, s);
     return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
 }
 
