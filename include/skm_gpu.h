@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define SKM_ABI_VERSION 6
+#define SKM_ABI_VERSION 7
 
 /* Status codes. */
 #define SKM_OK              0
@@ -55,6 +55,12 @@ extern "C" {
 #define SKM_MSE 0
 #define SKM_NCC 1
 #define SKM_LCC 2
+/* Box-window local correlation: every texel a window centre, 5^D box window, separable window
+ * sums.  No counterpart in the reference (its LCC windows are the kernel support weighted by
+ * (1 - (r/s)^10)^2, include/cuda/GpuEvaluatorLCC.cu:28-35); requires subsample 1, any kernel kind,
+ * runs on the generic kernels.  Value -(1/count) sum cov^2/(vf vm) over the centres whose window
+ * variances exceed 1e-12 of their raw second moments; count = num_pixels_counted. */
+#define SKM_LCC_BOX 3
 
 /* ImageBase geometry (include/cuda/ImageBase.h:40-49): physical point of index i is
  * origin + spacing*i, no direction matrix.  For 2-D images entries [2] are ignored. */
@@ -229,7 +235,7 @@ int skm_evaluate_displacement_field(skm_evaluator *ev,
  * L1, L2,1 and L2 terms (hxx:431-526), the sign flip (hxx:528-529) and the
  * weighted sum of all terms (hxx:531-538) on the device. */
 typedef struct skm_metric_desc {
-    int32_t metric;            /* SKM_MSE / SKM_NCC / SKM_LCC */
+    int32_t metric;            /* SKM_MSE / SKM_NCC / SKM_LCC / SKM_LCC_BOX */
     double  reg_l1;
     double  reg_l21;
     double  reg_l2;
@@ -347,7 +353,7 @@ int skm_threshold_rescale(int32_t dimensions, const int32_t *size, int32_t apply
 typedef struct skm_register_desc {
     int32_t dimensions;
     int32_t num_scales;
-    int32_t metric;                   /* SKM_MSE / SKM_NCC / SKM_LCC */
+    int32_t metric;                   /* SKM_MSE / SKM_NCC / SKM_LCC / SKM_LCC_BOX */
     double  cp_spacing_scaler;        /* control spacing = min(sigma_C4, sigma_C0) / scaler (1 below 1) */
     int32_t apply_threshold;          /* intensity_thresholds given (2 entries) */
     double  threshold_min, threshold_max;

@@ -19,8 +19,8 @@ SKM_ERR_STATE = 5
 SKM_ERR_TIMEOUT = 6
 
 # GpuKernelEvaluator::MEASURE (include/cuda/GpuEvaluator.h:160)
-MSE, NCC, LCC = 0, 1, 2
-METRICS = {"mse": MSE, "ncc": NCC, "lcc": LCC}
+MSE, NCC, LCC, LCC_BOX = 0, 1, 2, 3
+METRICS = {"mse": MSE, "ncc": NCC, "lcc": LCC, "lcc_box": LCC_BOX}
 
 _dp = C.POINTER(C.c_double)
 

@@ -928,7 +928,8 @@ extern "C" int skm_batch_create(int32_t npairs, const skm_batch_pair *pairs, skm
         if (!q.evaluator) return fail(SKM_ERR_INVALID, "pair %d: evaluator descriptor is NULL", i);
         int rc = validate_metric(&q.metric);
         if (rc) return rc;
-        if (q.metric.metric == SKM_LCC) return fail(SKM_ERR_UNSUPPORTED, "pair %d: the batch runs MSE and NCC", i);
+        if (q.metric.metric != SKM_MSE && q.metric.metric != SKM_NCC)
+            return fail(SKM_ERR_UNSUPPORTED, "pair %d: the batch runs MSE and NCC", i);
         if (q.evaluator->dimensions != 3) return fail(SKM_ERR_UNSUPPORTED, "pair %d: the batch runs 3-D pairs", i);
         if (!(q.optimizer.f_min != 0.0) || !(q.optimizer.omega != 0.0))
             return fail(SKM_ERR_INVALID, "pair %d: f_min and omega must be nonzero", i);

@@ -18,6 +18,7 @@
 #include "../../include/skm_gpu.h"
 #include "skm_device.cuh"
 #include "skm_kernels.cuh"
+#include "skm_lccbox.cuh"
 #include "skm_prefilter.cuh"
 #include "skm_table.cuh"
 #include "skm_table_tc.cuh"
@@ -235,6 +236,9 @@ struct skm_evaluator {
     unsigned *d_need = nullptr;       // LCC: bit per texel that a window reads
     int *d_list = nullptr, *d_nlist = nullptr;   // LCC: those texels, listed once, and their count
     float4 *d_acache = nullptr;       // LCC 3-D weight tensors: per-texel kernel inverse and factor
+    unsigned char *d_box_in = nullptr;   // box-window LCC: texel warped inside the moving image
+    double *d_box_a = nullptr, *d_box_b = nullptr;   // box-window LCC: 6 planar FP64 fields each
+    float *d_box_coef = nullptr;         // box-window LCC: derivative coefficient per texel
     uint32_t *d_shifts = nullptr;
     double *d_in = nullptr;          // uploaded parameters (AoS or planar) followed by weights
     unsigned *d_counters = nullptr;   // ticket counters of the fused last-block finalizations
@@ -293,7 +297,7 @@ struct skm_evaluator {
         cudaDeviceSynchronize();
         void *bufs[] = {d_fixed, d_coeffs, d_coeffs4, d_wimg, d_wten, d_wsup, d_cpd, d_df, d_samp, d_dense, d_dense_sw,
                         d_dense_in, d_need, d_list, d_nlist, d_acache, d_dense_sw_in, d_shifts, d_in, d_counters, d_part,
-                        d_stats, d_deriv, d_rpart, d_out};
+                        d_stats, d_deriv, d_rpart, d_out, d_box_in, d_box_a, d_box_b, d_box_coef};
         for (void *b : bufs)
             if (b) pool_release(b);
         clear_metric_graphs();
@@ -371,6 +375,39 @@ struct LaunchLccValue {
         }
         lcc_value_kernel<D, KIND><<<e->value_blocks, kValueThreads, 0, e->stream>>>(e->P, e->d_dense, e->d_dense_in,
                                                                                       e->d_part);
+        SKM_CHECK_LAUNCH();
+        return SKM_OK;
+    }
+};
+
+// box-window LCC value pass: per-texel samples, window moments (x, y[, z] passes), centres (value
+// partials and A, B, E), their box sums (x, y[, z]) and the texel coefficients.  Buffers alternate:
+// a pass reads one of d_box_a / d_box_b and writes the other.
+template <int D, int KIND>
+struct LaunchBoxValue {
+    static int run(skm_evaluator *e)
+    {
+        const long long N = e->N;
+        const int nx = e->P.fixed.n[0], ny = e->P.fixed.n[1], nz = D > 2 ? e->P.fixed.n[2] : 1;
+        const int lb = grid_for(N);
+        cudaStream_t s = e->stream;
+        double *a = e->d_box_a, *b = e->d_box_b;
+        box_texel_kernel<D, KIND><<<lb, 256, 0, s>>>(e->P, e->d_samp, e->d_box_in);
+        box_moments_x_kernel<<<lb, 256, 0, s>>>(e->d_fixed, e->d_samp, e->d_box_in, N, nx, a);
+        box_axis_kernel<kBoxMoments><<<lb, 256, 0, s>>>(a, b, N, nx, ny);
+        if (D > 2) {
+            box_axis_kernel<kBoxMoments><<<lb, 256, 0, s>>>(b, a, N, (long long)nx * ny, nz);
+            std::swap(a, b);
+        }
+        // final moments in b; the centres' A, B, E into a
+        box_centers_kernel<<<e->value_blocks, kValueThreads, 0, s>>>(b, e->d_box_in, N, a, e->d_part);
+        box_axis_kernel<3><<<lb, 256, 0, s>>>(a, b, N, 1, nx);
+        box_axis_kernel<3><<<lb, 256, 0, s>>>(b, a, N, nx, ny);
+        if (D > 2) {
+            box_axis_kernel<3><<<lb, 256, 0, s>>>(a, b, N, (long long)nx * ny, nz);
+            std::swap(a, b);
+        }
+        box_coef_kernel<<<lb, 256, 0, s>>>(a, e->d_fixed, e->d_samp, e->d_box_in, N, e->d_box_coef);
         SKM_CHECK_LAUNCH();
         return SKM_OK;
     }
@@ -823,6 +860,20 @@ static int ensure_dense(skm_evaluator *e)
     return SKM_OK;
 }
 
+static int check_metric_for(const skm_evaluator *e, int metric);
+
+// box-window LCC buffers (allocated on its first use, outside any stream capture)
+static int ensure_box(skm_evaluator *e)
+{
+    if (!e->d_box_in) {
+        if (dalloc(&e->d_box_in, e->N)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_box_a, (size_t)kBoxMoments * e->N)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_box_b, (size_t)kBoxMoments * e->N)) return SKM_ERR_CUDA;
+        if (dalloc(&e->d_box_coef, e->N)) return SKM_ERR_CUDA;
+    }
+    return SKM_OK;
+}
+
 struct RegWeights {
     double rkhs, rd, rd_scaling, pg, pg_scaling, l1, l21, l2;
     int with_metric, negate;
@@ -842,12 +893,17 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     double *d_deriv = deriv_out ? deriv_out : e->d_deriv, *d_res = res_out ? res_out : e->d_out;
     int rc = SKM_OK;
     const int D = e->D, kind = e->P.K.kind;
+    const bool local = metric == SKM_LCC || metric == SKM_LCC_BOX;   // generic kernels only
     if (metric == SKM_LCC) {
         if ((rc = ensure_dense(e))) return rc;
         if ((rc = dispatch<LaunchLccValue>(D, kind, e))) return rc;
+    } else if (metric == SKM_LCC_BOX) {
+        if ((rc = check_metric_for(e, metric))) return rc;        // every texel a sample
+        if ((rc = ensure_box(e))) return rc;
+        if ((rc = dispatch<LaunchBoxValue>(D, kind, e))) return rc;
     }
-    const bool tab = e->use_table && e->table.enabled && metric != SKM_LCC;
-    if (metric != SKM_LCC) {
+    const bool tab = e->use_table && e->table.enabled && !local;
+    if (!local) {
         if (tab) {
             if (table_value(e->table, tc_of(e), e->P, D, metric, e->d_stats, e->d_counters, e->stream,
                             ev ? ev[0] : nullptr))
@@ -883,6 +939,7 @@ static int run_evaluation(skm_evaluator *e, int metric, bool derivative, const R
     Q.dense_sw = e->d_dense_sw;
     Q.dense_sw_in = e->d_dense_sw_in;
     Q.acache = e->d_acache;
+    Q.boxcoef = metric == SKM_LCC_BOX ? e->d_box_coef : nullptr;
     Q.deriv = d_deriv;
     Q.rpart = e->d_rpart;
     Q.out = d_res;
@@ -959,8 +1016,18 @@ static int fetch(skm_evaluator *e, double *derivative)
 
 static int check_metric(int metric)
 {
-    if (metric != SKM_MSE && metric != SKM_NCC && metric != SKM_LCC)
+    if (metric != SKM_MSE && metric != SKM_NCC && metric != SKM_LCC && metric != SKM_LCC_BOX)
         return fail(SKM_ERR_INVALID, "unknown metric %d", metric);
+    return SKM_OK;
+}
+
+// the metric against the evaluator: the box-window LCC takes every texel as a window centre
+static int check_metric_for(const skm_evaluator *e, int metric)
+{
+    int rc = check_metric(metric);
+    if (rc) return rc;
+    if (metric == SKM_LCC_BOX && e->P.sub != 1)
+        return fail(SKM_ERR_INVALID, "the box-window LCC needs subsample 1 (every texel a window centre)");
     return SKM_OK;
 }
 
@@ -969,7 +1036,7 @@ static int evaluate_common(skm_evaluator *e, int32_t metric, const double *cp, c
 {
     if (!e) return fail(SKM_ERR_STATE, "evaluator is NULL");
     int rc;
-    if ((rc = check_metric(metric))) return rc;
+    if ((rc = check_metric_for(e, metric))) return rc;
     SKM_CUDA(cudaSetDevice(e->device));
     if ((rc = upload_field(e, df))) return rc;
     if ((rc = upload_params(e, cp, cpw, false))) return rc;
@@ -980,7 +1047,8 @@ static int evaluate_common(skm_evaluator *e, int32_t metric, const double *cp, c
     w.rd_scaling = e->rd_scaling;
     w.pg = e->reg_pg > 0 ? e->reg_pg : 0.0;
     w.pg_scaling = e->pg_scaling;
-    const bool drill = e->drill_armed && derivatives != nullptr && active_path(e) == 3 && metric != SKM_LCC;
+    const bool drill = e->drill_armed && derivatives != nullptr && active_path(e) == 3 && metric != SKM_LCC &&
+                       metric != SKM_LCC_BOX;
     if (drill) {                      // one launch of the contrib kernel runs the wait drill
         e->tc.dev.drill = 1;
         e->tc.dev.wait_ns = kDrillWaitNs;
@@ -1112,6 +1180,7 @@ extern "C" int skm_metric_evaluate(skm_evaluator *e, const skm_metric_desc *m, c
     }
     const bool deriv = derivative != nullptr;
     if (m->metric == SKM_LCC && (rc = ensure_dense(e))) return rc;   // allocates: not inside a capture
+    if (m->metric == SKM_LCC_BOX && ((rc = check_metric_for(e, m->metric)) || (rc = ensure_box(e)))) return rc;
     if (e->P.sub <= 1) {
         // no sampling offsets to draw: the whole device part is one graph launch
         const int path = active_path(e);

@@ -418,7 +418,7 @@ int check_register_desc(const skm_register_desc *r)
     if (r->dimensions != 2 && r->dimensions != 3) return fail(SKM_ERR_INVALID, "dimensions must be 2 or 3");
     if (r->num_scales < 1 || r->num_scales > SKM_MAX_SCALES)
         return fail(SKM_ERR_INVALID, "num_scales must be in [1, %d]", SKM_MAX_SCALES);
-    if (r->metric != SKM_MSE && r->metric != SKM_NCC && r->metric != SKM_LCC)
+    if (r->metric != SKM_MSE && r->metric != SKM_NCC && r->metric != SKM_LCC && r->metric != SKM_LCC_BOX)
         return fail(SKM_ERR_INVALID, "unknown metric %d", r->metric);
     for (int s = 0; s < r->num_scales; ++s) {
         if (!(r->sigma_c4[s] > 0.0) || !(r->sigma_c0[s] > 0.0))

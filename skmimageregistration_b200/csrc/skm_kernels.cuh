@@ -111,6 +111,7 @@ struct DerivParams {
     const float4 *__restrict__ dense_sw; // LCC 3-D swapped-kernel field (non-stationary kinds)
     const unsigned char *__restrict__ dense_sw_in;
     const float4 *__restrict__ acache;   // LCC 3-D weight tensors: aniso_self_cache per listed texel
+    const float *__restrict__ boxcoef;   // box-window LCC: coefficient per fixed texel (else null)
     double *__restrict__ deriv;          // planar output
     double *__restrict__ rpart;          // [NR][blocks]
     double *__restrict__ out;            // result vector (fused finalization)
@@ -647,8 +648,14 @@ __global__ void __launch_bounds__(256) derivative_kernel(EvalParams P, DerivPara
                             k = k_eval<KIND, D>(P.K, v, q, pj);
                         }
                         if (k != 0.0f) {
-                            float f = __ldg(P.fixed_data + lin_of<D>(P.fixed, pos));
-                            float coef = fmaf(cf, f, fmaf(cm, rec.w, cc)) * k;
+                            // box-window LCC: the texel's coefficient from its windows (times 1/count)
+                            float coef;
+                            if (Q.boxcoef) {
+                                coef = cc * __ldg(Q.boxcoef + idx) * k;
+                            } else {
+                                const float f = __ldg(P.fixed_data + lin_of<D>(P.fixed, pos));
+                                coef = fmaf(cf, f, fmaf(cm, rec.w, cc)) * k;
+                            }
                             acc[0] = fmaf(coef, rec.x, acc[0]);
                             acc[1] = fmaf(coef, rec.y, acc[1]);
                             if (D > 2) acc[2] = fmaf(coef, rec.z, acc[2]);
@@ -722,7 +729,7 @@ __global__ void __launch_bounds__(256) derivative_kernel(EvalParams P, DerivPara
                 double g;
                 if (Q.metric == 1)
                     g = st[S_DENOM] != 0.0 ? (double)cj.w * (double)acc[d] : 0.0;
-                else if (Q.metric == 0)
+                else if (Q.metric == 0 || Q.metric == 3)
                     g = (double)cj.w * (double)acc[d];
                 else
                     g = (double)acc[d] / n;                    // LCC derivative omits w_i (LCC.cu:518)

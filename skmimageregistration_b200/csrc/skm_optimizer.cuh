@@ -197,6 +197,7 @@ extern "C" int skm_optimizer_create(skm_evaluator *e, const skm_optimizer_desc *
     if ((rc = upload_field(e, df))) return rc;
     // LCC's dense fields are allocated on first use: that must happen before the iteration is captured
     if (md->metric == SKM_LCC && (rc = ensure_dense(e))) return rc;
+    if (md->metric == SKM_LCC_BOX && ((rc = check_metric_for(e, md->metric)) || (rc = ensure_box(e)))) return rc;
     skm_optimizer *o = new skm_optimizer();
     o->e = e;
     o->od = *od;

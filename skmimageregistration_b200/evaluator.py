@@ -117,7 +117,7 @@ class GpuKernelEvaluator:
     derivative is planar (D*C,) like the reference's parameter layout.
     """
 
-    MSE, NCC, LCC = abi.MSE, abi.NCC, abi.LCC
+    MSE, NCC, LCC, LCC_BOX = abi.MSE, abi.NCC, abi.LCC, abi.LCC_BOX
 
     def __init__(self, problem: Problem):
         self.problem = problem

@@ -37,7 +37,7 @@ def test_library_exports_every_declared_symbol(lib):
 
 
 def test_abi_version(lib):
-    assert lib.skm_abi_version() == 6
+    assert lib.skm_abi_version() == 7
 
 
 def _create(pb):
