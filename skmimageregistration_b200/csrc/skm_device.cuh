@@ -532,6 +532,57 @@ __device__ __forceinline__ void bspline_sum3(const Row &row, const float (&W)[4]
     grad[2] = c2 * (float)mg.inv[2];
 }
 
+// The same stencil sum on packed FP32 pairs (sm_100 `fma.rn.f32x2`: one instruction, two
+// round-to-nearest fused multiply-adds).  Rows y and y + 1 of a z slice travel together, so the
+// x contractions of two rows, the y accumulations (even and odd y apart) and the z accumulations
+// are all pair operations; the two halves are added at the end.  About 110 arithmetic
+// instructions per stencil instead of 195; the sums group the rows differently from
+// bspline_sum3, so results agree to FP32 rounding, not bitwise.
+template <class Row>
+__device__ __forceinline__ void bspline_sum3_x2(const Row &row, const float (&W)[4][3], const float (&dW)[4][3],
+                                                const Geo &mg, float &val, float *grad)
+{
+    float2 bw[4], bd[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        bw[k] = make_float2(W[k][0], W[k][0]);
+        bd[k] = make_float2(dW[k][0], dW[k][0]);
+    }
+    const float2 wy[2] = {make_float2(W[0][1], W[1][1]), make_float2(W[2][1], W[3][1])};
+    const float2 dy[2] = {make_float2(dW[0][1], dW[1][1]), make_float2(dW[2][1], dW[3][1])};
+    float2 c0 = make_float2(0.f, 0.f), c1 = c0, c2 = c0, c3 = c0;
+#pragma unroll
+    for (int z = 0; z < 4; ++z) {
+        float2 z0 = make_float2(0.f, 0.f), z1 = z0, z3 = z0;
+#pragma unroll
+        for (int yp = 0; yp < 2; ++yp) {
+            const float4 ra = row(2 * yp, z), rb = row(2 * yp + 1, z);
+            const float2 px = make_float2(ra.x, rb.x), py = make_float2(ra.y, rb.y);
+            const float2 pz = make_float2(ra.z, rb.z), pw = make_float2(ra.w, rb.w);
+            float2 dx = __fmul2_rn(bd[0], px);
+            dx = __ffma2_rn(bd[1], py, dx);
+            dx = __ffma2_rn(bd[2], pz, dx);
+            dx = __ffma2_rn(bd[3], pw, dx);
+            float2 vx = __fmul2_rn(bw[0], px);
+            vx = __ffma2_rn(bw[1], py, vx);
+            vx = __ffma2_rn(bw[2], pz, vx);
+            vx = __ffma2_rn(bw[3], pw, vx);
+            z0 = __ffma2_rn(wy[yp], dx, z0);
+            z1 = __ffma2_rn(dy[yp], vx, z1);
+            z3 = __ffma2_rn(wy[yp], vx, z3);
+        }
+        const float2 wz = make_float2(W[z][2], W[z][2]), dz = make_float2(dW[z][2], dW[z][2]);
+        c0 = __ffma2_rn(wz, z0, c0);
+        c1 = __ffma2_rn(wz, z1, c1);
+        c2 = __ffma2_rn(dz, z3, c2);
+        c3 = __ffma2_rn(wz, z3, c3);
+    }
+    val = c3.x + c3.y;
+    grad[0] = (c0.x + c0.y) * (float)mg.inv[0];
+    grad[1] = (c1.x + c1.y) * (float)mg.inv[1];
+    grad[2] = (c2.x + c2.y) * (float)mg.inv[2];
+}
+
 // Same as bspline_derivs, reading the coefficients from the row-expanded copy
 // c4[i] = (c[i], c[i+1], c[i+2], c[i+3]): one aligned 16-byte load per stencil row.
 template <int D>

@@ -7,10 +7,13 @@
 // first loads the coefficient box that the brick's stencils can reach -- the brick's extent in
 // moving-image index space plus kWtMargin voxels of displacement on every side -- with one
 // cp.async.bulk.tensor.3d load (no multicast) into one of two buffers, so the next brick's load
-// runs while this one is evaluated.  A texel whose stencil leaves the box (displacement beyond
-// the margin) reads the global row-expanded copy instead, so results do not depend on the
-// margin.  Each wait on the load's mbarrier is bounded; a wait that gives up sets the evaluator's
-// sticky fault word (the result then reports SKM_ERR_TIMEOUT) and the CTA skips its texels.
+// runs while this one is evaluated.  The two buffers form a full/empty mbarrier pipeline with no
+// block-wide barrier per brick: a warp starts its next brick once that brick's box has landed, and
+// the next load into a buffer is issued once every warp has released it.  A texel whose stencil
+// leaves the box (displacement beyond the margin) reads the global row-expanded copy instead, so
+// results do not depend on the margin.  The stencil sums run on packed FP32 pairs
+// (bspline_sum3_x2).  Each mbarrier wait is bounded; a wait that gives up sets the evaluator's
+// sticky fault word (the result then reports SKM_ERR_TIMEOUT) and the warp skips its later bricks.
 #pragma once
 
 #include <cuda.h>
@@ -54,19 +57,21 @@ __global__ void __launch_bounds__(256, 3) table_warp_tma_kernel(EvalParams P, Ta
     float *wbuf = reinterpret_cast<float *>(wsm);
     int4 *phx = reinterpret_cast<int4 *>(wbuf + 2 * kWtBufFloats);
     int4 *cellxyz = phx + T.nph;
-    __shared__ __align__(8) uint64_t bar[2];
+    // full[b]: the box of buffer b has landed (TMA transaction count); empty[b]: every warp is done
+    // reading buffer b (one arrival per warp), so the next load may overwrite it
+    __shared__ __align__(8) uint64_t full[2], empty[2];
     __shared__ int r0s[2][3];                                       // box origin of each buffer
     __shared__ double sh[NQ * 32];
-    __shared__ int wt_fail;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     const int nph = T.nph;
     const int ncb = W.bc[0] * W.bc[1] * W.bc[2];
     const int nbr = W.nb[0] * W.nb[1] * W.nb[2];
     if (tid == 0) {
-        tc::mbar_init(&bar[0], 1);
-        tc::mbar_init(&bar[1], 1);
+        tc::mbar_init(&full[0], 1);
+        tc::mbar_init(&full[1], 1);
+        tc::mbar_init(&empty[0], blockDim.x / 32);
+        tc::mbar_init(&empty[1], blockDim.x / 32);
         tc::fence_mbarrier_init();
-        wt_fail = 0;
     }
     for (int c = tid; c < ncb; c += blockDim.x)
         cellxyz[c] = make_int4(c % W.bc[0], (c / W.bc[0]) % W.bc[1], c / (W.bc[0] * W.bc[1]), 0);
@@ -94,8 +99,8 @@ __global__ void __launch_bounds__(256, 3) table_warp_tma_kernel(EvalParams P, Ta
         r0s[buf][0] = r0[0];
         r0s[buf][1] = r0[1];
         r0s[buf][2] = r0[2];
-        tc::mbar_expect_tx(&bar[buf], kWtBoxBytes);
-        tma_load_3d(wbuf + buf * kWtBufFloats, &map, r0[0], r0[1], r0[2], &bar[buf]);
+        tc::mbar_expect_tx(&full[buf], kWtBoxBytes);               // arrival (release): r0s visible
+        tma_load_3d(wbuf + buf * kWtBufFloats, &map, r0[0], r0[1], r0[2], &full[buf]);
     };
 
     float vf[NQ];
@@ -103,26 +108,39 @@ __global__ void __launch_bounds__(256, 3) table_warp_tma_kernel(EvalParams P, Ta
     for (int k = 0; k < NQ; ++k) vf[k] = 0.f;
     const int fn[3] = {P.fixed.n[0], P.fixed.n[1], P.fixed.n[2]};
     const int plane = (int)(T.ncell * T.nph);
-    unsigned issued = 0, waited = 0;                                // loads per buffer, as bit counts
-    if (tid == 0 && (int)blockIdx.x < nbr) issue(blockIdx.x, 0);
-    if (tid == 0 && (int)blockIdx.x < nbr) issued = 1;
+    // Thread 0 issues the loads: brick it + 1 into buffer (it + 1) & 1 once every warp has released
+    // that buffer (brick it - 1).  No block-wide barrier inside the loop: a warp moves on to its next
+    // brick as soon as that brick's box has landed, whatever the other warps are doing.  Every wait
+    // is bounded; a thread whose wait gives up records the fault and stops working (its warp's later
+    // bricks are skipped, the result reports SKM_ERR_TIMEOUT).
+    int issued = 0, waited0 = 0;                                    // thread 0's load bookkeeping
+    if (tid == 0 && (int)blockIdx.x < nbr) {
+        issue(blockIdx.x, 0);
+        issued = 1;
+    }
     int it = 0;
     for (int brick = blockIdx.x; brick < nbr; brick += gridDim.x, ++it) {
         const int buf = it & 1;
         const int next = brick + gridDim.x;
-        if (tid == 0 && next < nbr) {                               // buffer buf^1 was released below
-            issue(next, buf ^ 1);
-            ++issued;
+        bool ok = true;
+        if (tid == 0 && next < nbr) {
+            // buffer buf ^ 1 held brick it - 1 (use (it - 1) >> 1 of that buffer); warp 0's own
+            // arrival for it came at the end of the previous iteration
+            if (it == 0 || tc::mbar_wait(&empty[buf ^ 1], (uint32_t)(((it - 1) >> 1) & 1))) {
+                issue(next, buf ^ 1);
+                ++issued;
+            } else {
+                ok = false;
+            }
         }
-        // every thread waits on the load (bounded); a failure is recorded and the brick skipped
-        const bool ok = tc::mbar_wait(&bar[buf], (uint32_t)((it >> 1) & 1));
-        if (tid == 0) ++waited;
-        if (!ok) {
-            if (T.tc_err) atomicOr(T.tc_err, 2u);
-            wt_fail = 1;
+        if (ok) ok = tc::mbar_wait(&full[buf], (uint32_t)((it >> 1) & 1));
+        if (tid == 0 && ok) ++waited0;
+        // the decision to stop is the warp's (its lanes then leave the loop together)
+        if (__any_sync(0xffffffffu, !ok)) {
+            if (lane == 0 && T.tc_err) atomicOr(T.tc_err, 2u);
+            break;
         }
-        __syncthreads();
-        if (!wt_fail) {
+        {
             const float *box = wbuf + buf * kWtBufFloats;
             const int r0[3] = {r0s[buf][0], r0s[buf][1], r0s[buf][2]};
             const int bq[3] = {brick % W.nb[0], (brick / W.nb[0]) % W.nb[1], brick / (W.nb[0] * W.nb[1])};
@@ -131,7 +149,7 @@ __global__ void __launch_bounds__(256, 3) table_warp_tma_kernel(EvalParams P, Ta
                 if (W.lanes4x8) {
                     // lanes = 4 x-neighbours x 8 y-neighbours of one z: with the box's row stride of
                     // 28 floats (-4 modulo 32 banks) a stencil tap of the warp hits 32 distinct banks
-                    const int lane = t & 31, w = t >> 5;
+                    const int w = t >> 5;
                     const int xi = lane & 3, yi = lane >> 2, cx = w & 3, vz = w >> 2;
                     cl = cx + 4 * ((yi >> 2) + 2 * (vz >> 2));
                     p = xi + 4 * (yi & 3) + 16 * (vz & 3);
@@ -176,7 +194,7 @@ __global__ void __launch_bounds__(256, 3) table_warp_tma_kernel(EvalParams P, Ta
                         if (j0 >= 0 && j0 + 4 <= kWtBoxX && j1 >= 0 && j1 + 4 <= kWtBoxY && j2 >= 0 &&
                             j2 + 4 <= kWtBoxZ) {
                             const float *bb = box + j0 + kWtBoxX * (j1 + kWtBoxY * j2);
-                            bspline_sum3(
+                            bspline_sum3_x2(
                                 [&](int y, int z) {
                                     const float *rr = bb + kWtBoxX * (y + kWtBoxY * z);
                                     return make_float4(rr[0], rr[1], rr[2], rr[3]);
@@ -185,8 +203,8 @@ __global__ void __launch_bounds__(256, 3) table_warp_tma_kernel(EvalParams P, Ta
                         } else {                                    // beyond the margin: global rows
                             const int sy = (int)P.mov.st[1], sz = (int)P.mov.st[2];
                             const float4 *base = P.coeffs4 + (ii[0] + ii[1] * sy + ii[2] * sz);
-                            bspline_sum3([&](int y, int z) { return __ldg(base + (y * sy + z * sz)); }, Wt, dW,
-                                         P.mov, m, g);
+                            bspline_sum3_x2([&](int y, int z) { return __ldg(base + (y * sy + z * sz)); }, Wt,
+                                            dW, P.mov, m, g);
                         }
                         vf[Q_COUNT] += 1.f;
                         vf[Q_D2] += (m - f) * (m - f);
@@ -201,11 +219,15 @@ __global__ void __launch_bounds__(256, 3) table_warp_tma_kernel(EvalParams P, Ta
                 T.rec[i] = rec;
             }
         }
-        __syncthreads();                                            // buffer buf is free again
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[buf]);                // this warp is done with buffer buf
     }
-    // a load that was issued but never waited for (after a failure) must land before the CTA
-    // leaves: wait for it, bounded
-    if (tid == 0 && issued > waited) tc::mbar_wait(&bar[it & 1], (uint32_t)((it >> 1) & 1));
+    // every issued load must land before the CTA leaves (after a failure some were never waited
+    // for): thread 0 waits for the rest, bounded
+    if (tid == 0)
+        for (; waited0 < issued; ++waited0)
+            if (!tc::mbar_wait(&full[waited0 & 1], (uint32_t)((waited0 >> 1) & 1))) break;
+    __syncthreads();
     double v[NQ];
 #pragma unroll
     for (int k = 0; k < NQ; ++k) v[k] = (double)vf[k];
