@@ -449,16 +449,18 @@ def multiscale_compare(name="ncc128", override=None):
         score, key, better = final_mse, "mse", (lambda a, b: a <= b + 1e-3 * abs(b))
         R.register(moving, fixed, spacing, None, cfg)                        # warm-up: one untimed run
     # the warm-up above ran the same registration once, untimed (first launches, the memory pool);
-    # three timed runs, the median reported
-    runs, run_levels = [], []
-    for _ in range(3):
+    # five timed runs, the median reported, every run's level times (whole level, and the optimizer
+    # iterations alone) kept beside it
+    runs, run_levels, run_opt = [], [], []
+    for _ in range(5):
         t0 = time.perf_counter()
         disp, rep = R.register(moving, fixed, spacing, None, cfg)
         runs.append(time.perf_counter() - t0)
         run_levels.append([round(x, 4) for x in rep["seconds"][:rep["levels_done"]]])
-    ours_s = sorted(runs)[1]
+        run_opt.append([round(x, 4) for x in rep["optimize_seconds"][:rep["levels_done"]]])
+    ours_s = sorted(runs)[len(runs) // 2]
     out = {"config": dict(cfg, volume=volume), "ours_s_per_pair": ours_s, "ours_runs_s": runs,
-           "ours_runs_level_seconds": run_levels,
+           "ours_runs_level_seconds": run_levels, "ours_runs_level_optimize_seconds": run_opt,
            "ours_final_" + key: score(fixed, moving, disp, spacing),
            key + "_before": score(fixed, moving, 0 * disp, spacing), "ours_levels": rep}
     from oracle import oracle as O  # noqa: F401  (reference arm: needs the reference build)
